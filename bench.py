@@ -1,0 +1,323 @@
+"""Benchmark: FP64 ENO-Roe RK3 cell-updates/s on the 4096^2 Orszag-Tang vortex.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one TimeIntegrationRK3 step (3 spatial operators with boundary
+fills, CFL control with the reference's power-of-two dt and retry logic,
+stage updates) of the whole 4096^2 grid; one cell-update is one interior cell
+advanced by one step.  Inputs (8 x 4100^2 doubles = 1.08 GB per state) are
+larger than the 126 MB L2, so no flush is needed between steps.
+
+`value` is device-resident throughput (state in HBM, CUDA events on the
+library's stream, max over ranks); `e2e` runs the same steps through the
+host-buffer C ABI call (mhd_step_host: pinned host state -> device, step,
+device -> host every step).  With --gpus N each rank advances its own
+independent 4096^2 run (replicas; the single-run halo-exchange sharding is
+not built), so scaling is weak.
+
+--impl reference times the reference's own CPU code (the unmodified
+reference sources compiled by oracle/Makefile into oracle/_ref/ref_bench),
+one process per host core - the reference's own parallelisation - each
+advancing a 512^2 Orszag-Tang sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mhd2d-solver_b200"))
+
+METRIC = "FP64 ENO-Roe cell-updates/s at 4096^2 (Orszag-Tang, RK3-TVD, CFL 0.4)"
+UNIT = "cell-updates/s"
+N_GRID = 4096
+REF_SAMPLE = 512
+
+# Floating-point operations per interior cell (+, -, *, /, sqrt = 1), counted
+# by oracle/opcount.cpp on a random state with structural zeros excluded,
+# extrapolated to 4096^2 (tests/test_flop_constants.py re-derives them).
+FLOPS_PER_CELL_INTEGRATE = {2: 3011.9, 3: 3514.0}
+FLOPS_PER_CELL_STEP = {2: 9147.6, 3: 10653.9}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_GRID)
+    ap.add_argument("--scheme", default="roe", choices=["roe", "lf"])
+    ap.add_argument("--fast-math", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=None)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline_sample(scheme_code, steps=8):
+    """The reference (oracle/_ref) on one core, bounded sample: 512^2 OT."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    if not os.path.exists(exe):
+        return None
+    out = subprocess.run([exe, str(REF_SAMPLE), str(steps), str(scheme_code)], capture_output=True,
+                         text=True, timeout=600)
+    times = [float(ln.split()[2]) for ln in out.stdout.splitlines() if ln.startswith("step")]
+    if len(times) < 2:
+        return None
+    t = sum(times[1:])
+    return {"value": REF_SAMPLE * REF_SAMPLE * (len(times) - 1) / t, "unit": UNIT, "cores": 1,
+            "kind": "reference",
+            "sample": f"reference RK3+ENO on Orszag-Tang {REF_SAMPLE}^2, {len(times) - 1} timed "
+                      f"steps after 1 warm-up, 1 thread ({t:.1f} s)"}
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    scheme = 3 if args.scheme == "lf" else 2
+    config = {"workload": f"orszag-tang {args.n}x{args.n}, eno-{args.scheme}, rk3, cfl 0.4, fp64",
+              "grid": [args.n, args.n], "scheme": f"eno-{args.scheme}", "parallelism": "cpu",
+              "l2": "inputs larger than L2"}
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_bench not built (the reference checkout was absent "
+                          "when the oracle was compiled)"}))
+        return 0
+    cores = os.cpu_count() or 1
+    nsteps = args.warmup + args.steps
+    procs = [subprocess.Popen([exe, str(REF_SAMPLE), str(nsteps), str(scheme)],
+                              stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+             for _ in range(cores)]
+    t0 = time.time()
+    outs = [p.communicate()[0] for p in procs]
+    wall = time.time() - t0
+    rates, per_step = [], []
+    for o in outs:
+        ts = [float(ln.split()[2]) for ln in o.splitlines() if ln.startswith("step")]
+        if len(ts) == nsteps:
+            timed = ts[args.warmup:]
+            rates.append(REF_SAMPLE * REF_SAMPLE * len(timed) / sum(timed))
+            per_step.append(sum(timed) / len(timed))
+    if not rates:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU run failed"}))
+        return 0
+    value = sum(rates)  # each copy's main-loop rate, summed (one copy per core)
+    ms = 1000.0 * max(per_step)
+    sample = (f"{len(rates)} concurrent copies of the reference RK3+ENO-{args.scheme} on "
+              f"Orszag-Tang {REF_SAMPLE}^2 (one per host thread), {args.steps} timed steps after "
+              f"{args.warmup} warm-up; aggregate = sum of per-copy rates; wall {wall:.1f} s")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (Orszag-Tang initial state, seeded by its formula)",
+            "config": config, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(rates),
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import mhd2d_b200 as M
+    from mhd2d_b200 import problems as P
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    scheme = M.ENO_LF if args.scheme == "lf" else M.ENO_ROE
+    flags = M.FLAG_FAST_MATH if args.fast_math else 0
+    n = args.n
+    p = P.ot_vortex(n)
+    ctx = M.Context(n, n, p.dx, p.dy, p.gamma, p.bc, scheme=scheme, time_method=M.RK3,
+                    dt_min=1e-9, dt_max=0.03125, cfl=0.4, flags=flags, device=dev)
+    ctx.upload(p.U)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    dt = 0.03125
+    for _ in range(max(args.warmup, 0)):
+        st, dt = ctx.step(dt)
+        if st.isError:
+            raise RuntimeError(st.message)
+    launches0 = ctx.counters()["launches"]
+    sampler = ClockSampler(dev) if rank == 0 else None
+    barrier(world)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st, dt = ctx.step(dt)
+        if st.isError:
+            raise RuntimeError(st.message)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    barrier(world)
+    ms_local = ev0.elapsed_time(ev1)
+    launches = ctx.counters()["launches"] - launches0
+    ms = allreduce_max(world, ms_local)
+    cells = float(n) * n
+    value = world * cells * args.steps / (ms / 1000.0)
+
+    # end to end through the host-buffer ABI call (pinned host state)
+    host = torch.empty((8, n + 4, n + 4), dtype=torch.float64, pin_memory=True).numpy()
+    host[...] = ctx.download()
+    e2e_steps = max(1, args.e2e_steps)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        st, dt = ctx.step_host(host, dt)
+        if st.isError:
+            raise RuntimeError(st.message)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = allreduce_max(world, e0.elapsed_time(e1))
+    e2e_value = world * cells * e2e_steps / (e2e_ms / 1000.0)
+    state_bytes = 8 * (n + 4) * (n + 4) * 8
+
+    # roofline of the dominant kernel (the fused flux kernel; one spatial
+    # operator = boundary fill + flux kernel, timed back to back on the
+    # library stream)
+    t_int = ctx.time_integrate(5)
+    peak = M.fp64_peak_tflops(dev)
+    flops = FLOPS_PER_CELL_INTEGRATE[scheme] * cells
+    achieved = flops / (t_int * 1e-3) / 1e12
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (Orszag-Tang initial state from its formula, no dataset)",
+            "config": {"workload": f"orszag-tang {n}x{n}, eno-{args.scheme}, rk3, cfl 0.4, fp64"
+                                   + (", fast-math" if args.fast_math else ", bit-exact build"),
+                       "grid": [n, n], "scheme": f"eno-{args.scheme}",
+                       "parallelism": "replicas" if world > 1 else "single-gpu",
+                       "l2": "inputs larger than L2 (1.08 GB state), no flush"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
+                    "call": "mhd_step_host (pinned host state)"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_flux (fused spatial operator) + boundary fill",
+                         "flops_per_launch": flops, "launch_ms": t_int,
+                         "peak_source": "measured live: FP64 FMA-chain probe (mhd_fp64_peak); "
+                                        "MEASURED_PEAKS.json has no FP64 figure"},
+            "clocks": clocks,
+        }
+        if world == 1:
+            line["cpu_baseline"] = cpu_baseline_sample(scheme)
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,159 @@
+/*
+ * mhd2d_b200 — C ABI of the B200 (sm_100a) implementation of the mhd2d-solver
+ * time-step hot path: ENO-Roe / ENO-LF characteristic fluxes, RK3-TVD and
+ * Euler stages with boundary fills, the CFL wave-speed reduction and the
+ * div-B diagnostics / SOR correction.  Arithmetic is IEEE binary64.
+ *
+ * Data model (shared with the reference, vector_utilities.cpp:81-98): a
+ * state is ONE contiguous block of 8 x NX x NY doubles, NX = nx+4,
+ * NY = ny+4, element (k, i, j) at (k*NX + i)*NY + j, k = rho, mx, my, mz,
+ * Bx, By, Bz, E; two ghost cells per side; j (y) fastest.  The host pointer
+ * a caller passes is exactly the reference's U[0][0].
+ *
+ * Boundary codes (enums.hpp: BoundaryCondition): 1 periodic, 2 Dirichlet,
+ * 3 Neumann, 4 open; bc[] is ordered left, right, bottom, top.
+ * Scheme codes (IntegrationMethod): 2 ENO-Roe, 3 ENO-LF.
+ * Time codes (TimeStepMethod): 1 Euler, 2 RK3-TVD.
+ * Every entry point returns an int holding the reference's ReturnStatus
+ * value (enums.hpp); the t_status::isError half comes from
+ * mhd_last_error().  No exception crosses this boundary.
+ *
+ * Threading: a context is single-threaded, like the reference objects it
+ * replaces.  All device work of a context runs on the context's own CUDA
+ * stream; calls return after that work completed.
+ */
+#ifndef MHD2D_B200_H
+#define MHD2D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ReturnStatus (enums.hpp) plus one code for CUDA runtime failures. */
+enum {
+   MHD_OK = 0, MHD_NO_CHANGE = 1, MHD_UPDATED = 2,
+   MHD_ERR_NOT_IMPLEMENTED = 3, MHD_ERR_TIME_UNDERFLOW = 4, MHD_ERR_NOT_CONVERGED = 5,
+   MHD_ERR_NEGATIVE_DENSITY = 6, MHD_ERR_NEGATIVE_PRESSURE = 7,
+   MHD_ERR_FILE_NOT_FOUND = 8, MHD_ERR_FAILED_TO_PARSE = 9, MHD_ERR_WRONG_PARAMETER = 10,
+   MHD_ERR_CUDA = 100
+};
+
+/* mhd_ctx_create flags */
+#define MHD_FLAG_CHARACTERISTICS 0x1  /* keep cx, cy, LUx, LUy of the last integrate */
+#define MHD_FLAG_FAST_MATH       0x2  /* FMA-contracted kernels (not bit-identical) */
+
+typedef struct mhd_ctx mhd_ctx;
+
+/* [divb corrector] parameters (file_access.cpp:273-299). */
+typedef struct {
+   int    divb_skip_steps;   /* stepping rate */
+   int    sor_steps;         /* outer cleaning passes; <= 0 disables */
+   double sor_rsteps;        /* maximum sweeps per solve */
+   double sor_rmax;          /* sweep tolerance on max|update| / max|phi| */
+   double sor_divbmax;       /* target max|div B| */
+   int    omega_use_static;
+   double omega;
+} mhd_sor_params;
+
+/* Context = the reference's method + stepper pair on one GPU.
+   Replaces: SpatialMethodEnoRoe / SpatialMethodEnoLF constructors
+   (spatialmethodenoroe.cpp:5-20, spatialmethodenolf.cpp:5-20) and
+   TimeIntegrationRK3 / TimeIntegrationEuler constructors
+   (timeintegrationrk3.cpp:4-27, timeintegrationeuler.cpp:4-15).
+   halo must be 2 (bufferWidth = NXFIRST, main.cpp:117); a smaller halo is
+   the reference's std::domain_error (spatialmethodeno.cpp:17-20) and
+   returns MHD_ERR_WRONG_PARAMETER. */
+int mhd_ctx_create( int nx, int ny, int halo, double dx, double dy, double gamma,
+                    const int bc[4], int scheme, int time_method,
+                    double dt_min, double dt_max, double cfl, int flags, int device,
+                    mhd_ctx** out );
+int mhd_ctx_destroy( mhd_ctx* ctx );
+
+/* Re-binds the stepper half of a context (time method, dt_min, dt_max,
+   CFL number; cfl = 0 is the constant time mode), as constructing a
+   TimeIntegrationRK3 / TimeIntegrationEuler around an existing method does
+   (main.cpp:141-151).  Stage buffers are allocated on first use. */
+int mhd_set_stepper( mhd_ctx* ctx, int time_method, double dt_min, double dt_max, double cfl );
+
+/* Last status message and t_status::isError of this context. */
+int mhd_last_error( const mhd_ctx* ctx, char* msg, size_t len, int* is_error );
+
+/* Host <-> device copies of the state block U[0][0] (8*NX*NY doubles). */
+int mhd_upload( mhd_ctx* ctx, const double* U );
+int mhd_download( mhd_ctx* ctx, double* U );
+/* UL (dU/dt) of the last integrate: same block shape, interior valid. */
+int mhd_download_ul( mhd_ctx* ctx, double* UL );
+
+/* Replaces SpatialIntegrationMethod::initializeDirichletBoundaries
+   (spatialintegrationmethod.cpp:39-59): snapshot of the edge cells of the
+   state currently on the device. */
+int mhd_init_dirichlet( mhd_ctx* ctx );
+
+/* Replaces SpatialMethodEnoRoe::integrate (spatialmethodenoroe.cpp:33-179)
+   and SpatialMethodEnoLF::integrate (spatialmethodenolf.cpp:33-230) on the
+   device state: boundary fill (in place), fluxes, dtIdeal, UL. */
+int mhd_integrate( mhd_ctx* ctx, double* dtIdeal );
+
+/* Host-buffer form of the same call, as the plugin subclass uses it:
+   U is uploaded, boundaries filled, UL computed; U (with its ghost cells)
+   and UL are copied back. */
+int mhd_integrate_host( mhd_ctx* ctx, double* U, double* UL, double* dtIdeal );
+
+/* Replaces TimeIntegrationRK3::step (timeintegrationrk3.cpp:48-156) /
+   TimeIntegrationEuler::step (timeintegrationeuler.cpp:26-64) on the device
+   state; *dt_inout is the reference's dtCurrent. */
+int mhd_step( mhd_ctx* ctx, double* dt_inout );
+
+/* Host-buffer form: upload U, one step, download U. */
+int mhd_step_host( mhd_ctx* ctx, double* U, double* dt_inout );
+
+/* Several steps without host round trips in between (fixed count);
+   dts (optional, length nsteps) receives each step's dt. */
+int mhd_steps( mhd_ctx* ctx, int nsteps, double* dt_inout, double* dts );
+
+/* Replaces SpatialMethodEno::getCharacteristicsX/Y (spatialmethodeno.cpp:55-86)
+   as called at timeintegrationrk3.cpp:151-152; requires
+   MHD_FLAG_CHARACTERISTICS.  Any pointer may be NULL. */
+int mhd_get_characteristics( mhd_ctx* ctx, double* cx, double* cy, double* LUx, double* LUy );
+
+/* Replaces divBCalculation (div_b_fix.cpp:4-126) on the device state. */
+int mhd_divb_calc( mhd_ctx* ctx, double* maxdivb, double* totdivb );
+
+/* Replaces divBCorrectionSOR (div_b_fix.cpp:129-403): one solve with the
+   sublattice red-black ordering, warm-started from the context's
+   potential, followed by the B correction.  *sweeps gets the sweep count. */
+int mhd_divb_sor( mhd_ctx* ctx, const mhd_sor_params* p, int* sweeps );
+
+/* The cleaning loop of main.cpp:207-242 (up to sor_steps solves until
+   max|div B| < sor_divbmax), final max|div B| in *maxdivb. */
+int mhd_divb_clean( mhd_ctx* ctx, const mhd_sor_params* p, double* maxdivb, int* total_sweeps );
+
+/* Counters of the last integrate / step: clamped midpoint pressures
+   (the reference's "negative pressure" warning count) and kernel launches. */
+int mhd_get_counters( mhd_ctx* ctx, long long* neg_pressure, long long* launches );
+
+/* Device row layout of a state block: element (k, i, j) of the device copy
+   sits at k*NX*pitch + i*pitch + row_offset + j doubles from its base. */
+int mhd_layout( const mhd_ctx* ctx, int* pitch, int* row_offset );
+
+/* The context's CUDA stream (a cudaStream_t), for callers that record
+   events or order their own work against the context's kernels. */
+int mhd_stream( const mhd_ctx* ctx, void** stream );
+
+/* Launches `n` back-to-back spatial operators (boundary fill + fused flux
+   kernel, no host synchronisation in between) on the device state and
+   returns their average device time in ms, measured with CUDA events on the
+   context's stream.  For profiling and roofline accounting. */
+int mhd_time_integrate( mhd_ctx* ctx, int n, double* avg_ms );
+
+/* Measured FP64 FMA throughput of `device` (TFLOP/s, 2 flops per FMA):
+   a grid of independent fused multiply-add chains timed with CUDA events.
+   The denominator of the FP64 roofline of the flux kernels. */
+int mhd_fp64_peak( int device, double* tflops );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

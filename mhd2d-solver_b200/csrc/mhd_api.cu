@@ -1,0 +1,589 @@
+// C ABI of the device hot path (include/mhd2d_b200.h): context, memory,
+// and the host-side orchestration of one integrate / step / SOR solve.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+
+#include "../../include/mhd2d_b200.h"
+#include "mhd_launch.h"
+
+using namespace mhd;
+
+namespace {
+// FP64 FMA throughput probe: 8 independent chains per thread.
+__global__ void __launch_bounds__(256) k_fma_peak(double* out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) x[q] = threadIdx.x * 1e-3 + q;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) x[q] = __fma_rn(x[q], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) s += x[q];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live; never true in practice
+}
+}  // namespace
+
+struct mhd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Grid g{};
+  int scheme = 2, time_method = 2, flags = 0;
+  double dt_min = 0, dt_max = 0, cfl = 0;
+  bool dirichlet_needed = false, dirichlet_ready = false;
+  const KernelSet* ks = &kExact;
+  size_t block_elems = 0;  // doubles per state block
+  double *U = nullptr, *U1 = nullptr, *U2 = nullptr, *UL = nullptr;
+  double *ch[4] = {nullptr, nullptr, nullptr, nullptr};  // cx, cy, LUx, LUy
+  double *aF = nullptr, *aG = nullptr;
+  double *snap[4] = {nullptr, nullptr, nullptr, nullptr};  // left, right, bottom, top
+  double *phi = nullptr, *partial = nullptr, *ratio = nullptr;
+  int npartial = 0;
+  Ctl* ctl = nullptr;
+  Ctl* hctl = nullptr;  // pinned mirror
+  std::string msg;
+  bool is_error = false;
+  long long launches = 0, neg_pressure = 0;
+};
+
+namespace {
+
+int set_status(mhd_ctx* c, int st, bool err, const std::string& m) {
+  c->is_error = err;
+  c->msg = m;
+  return st;
+}
+
+int cuda_fail(mhd_ctx* c, cudaError_t e, const char* where) {
+  std::string m = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+  if (c) return set_status(c, MHD_ERR_CUDA, true, m);
+  std::fprintf(stderr, "mhd2d_b200: %s\n", m.c_str());
+  return MHD_ERR_CUDA;
+}
+
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);   \
+  } while (0)
+
+int pitch_for(int NY) { return ((NY + ROW_OFF + 15) / 16) * 16; }
+
+cudaError_t alloc_block(mhd_ctx* c, double** p) {
+  cudaError_t e = cudaMalloc(p, c->block_elems * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, c->block_elems * sizeof(double), c->stream);
+  return e;
+}
+
+// copy a host [8][NX][NY] block into / out of the pitched device block
+cudaError_t h2d(mhd_ctx* c, double* dst, const double* src) {
+  const Grid& g = c->g;
+  return cudaMemcpy2DAsync(dst + g.off, g.pitch * sizeof(double), src, g.NY * sizeof(double),
+                           g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyHostToDevice,
+                           c->stream);
+}
+cudaError_t d2h(mhd_ctx* c, double* dst, const double* src) {
+  const Grid& g = c->g;
+  return cudaMemcpy2DAsync(dst, g.NY * sizeof(double), src + g.off, g.pitch * sizeof(double),
+                           g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyDeviceToHost,
+                           c->stream);
+}
+
+int read_ctl(mhd_ctx* c) {
+  CK(cudaMemcpyAsync(c->hctl, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  return MHD_OK;
+}
+
+int check_bc_ready(mhd_ctx* c) {
+  if (c->dirichlet_needed && !c->dirichlet_ready)
+    return set_status(c, MHD_ERR_WRONG_PARAMETER, true,
+                      "SpatialIntegrationMethod::applyBoundaryConditions: boundary not initialized.");
+  return MHD_OK;
+}
+
+// Enqueue one spatial integration of state X into UL.
+void enqueue_integrate(mhd_ctx* c, double* X, bool chars) {
+  const Grid& g = c->g;
+  c->ks->bc(g, X, c->snap, c->ctl, c->stream);
+  if (c->scheme == 3) c->ks->lf_alpha(g, X, c->aF, c->aG, c->ctl, c->stream);
+  c->ks->flux(c->scheme, g, X, c->UL, c->aF, c->aG, c->ctl, chars ? c->ch : nullptr, c->stream);
+  c->launches += c->ks->launches_per_integrate(c->scheme);
+}
+
+void enqueue_control(mhd_ctx* c, int phase, double arg = 0.0) {
+  c->ks->control(c->ctl, c->g.dx, c->g.dy, c->dt_min, c->dt_max, c->cfl, phase, arg, c->stream);
+  c->launches += 1;
+}
+
+void enqueue_combine(mhd_ctx* c, int mode) {
+  c->ks->combine(c->g, mode, c->U, c->U1, c->U2, c->UL, c->ctl, c->stream);
+  c->launches += 1;
+}
+
+// The stage loop of TimeIntegrationRK3::step from U1 = U + dt*UL onwards.
+void enqueue_rk3_tail(mhd_ctx* c, bool chars) {
+  enqueue_combine(c, 1);
+  enqueue_integrate(c, c->U1, false);
+  enqueue_control(c, PH_RK_SECOND);
+  enqueue_combine(c, 2);
+  enqueue_integrate(c, c->U2, chars);
+  enqueue_control(c, PH_RK_FINAL);
+  enqueue_combine(c, 3);
+  enqueue_control(c, PH_DONE);
+}
+
+int step_status(mhd_ctx* c) {
+  const Ctl& h = *c->hctl;
+  c->neg_pressure += (long long)h.neg_count;
+  if (h.error == 6)
+    return set_status(c, MHD_ERR_NEGATIVE_DENSITY, true,
+                      "negative density encountered\n! getEigens_F\n! mhd_step: spatial integration");
+  if (h.error == 4) {
+    char buf[256];
+    std::snprintf(buf, sizeof buf,
+                  "CFL condition violated!\nMinimum time step = %f\n! updateDt\n! mhd_step: update time step",
+                  c->dt_min);
+    return set_status(c, MHD_ERR_TIME_UNDERFLOW, true, buf);
+  }
+  if (h.error == 10)
+    return set_status(c, MHD_ERR_WRONG_PARAMETER, true,
+                      "updateDt: no power-of-two time step satisfies the CFL window\n! mhd_step");
+  return MHD_OK;
+}
+
+// One full time step on the device state; dt in/out.
+int do_step(mhd_ctx* c, double* dt_inout) {
+  int st = check_bc_ready(c);
+  if (st) return st;
+  const bool chars = (c->flags & MHD_FLAG_CHARACTERISTICS) != 0;
+  enqueue_control(c, PH_RESET_STEP, *dt_inout);
+  enqueue_integrate(c, c->U, c->time_method == 1 && chars);
+  if (c->time_method == 1) {
+    enqueue_control(c, PH_EULER);
+    enqueue_combine(c, 0);
+    enqueue_control(c, PH_DONE);
+    if ((st = read_ctl(c))) return st;
+  } else {
+    enqueue_control(c, PH_RK_FIRST);
+    enqueue_rk3_tail(c, chars);
+    if ((st = read_ctl(c))) return st;
+    int guard = 0;
+    while (c->hctl->retry && !c->hctl->error) {
+      if (++guard > 64)
+        return set_status(c, MHD_ERR_WRONG_PARAMETER, true, "RK3 retry loop did not settle");
+      enqueue_control(c, PH_RK_RETRY);
+      enqueue_rk3_tail(c, chars);
+      if ((st = read_ctl(c))) return st;
+    }
+  }
+  if ((st = step_status(c))) return st;
+  *dt_inout = c->hctl->dt;
+  return set_status(c, MHD_OK, false, "");
+}
+
+void divb_range(const mhd_ctx* c, int r[4]) {
+  const Grid& g = c->g;
+  r[0] = g.bc[LEFT] == PERIODIC ? 2 : 3;
+  r[1] = g.bc[RIGHT] == PERIODIC ? g.nx + 2 : g.nx + 1;
+  r[2] = g.bc[BOTTOM] == PERIODIC ? 2 : 3;
+  r[3] = g.bc[TOP] == PERIODIC ? g.ny + 2 : g.ny + 1;
+}
+
+int do_divb_calc(mhd_ctx* c, double* mx, double* tot) {
+  int r[4];
+  divb_range(c, r);
+  c->ks->divb(c->g, c->U, r, c->partial, c->npartial, c->ctl, c->stream);
+  c->launches += 3;
+  int st = read_ctl(c);
+  if (st) return st;
+  const unsigned long long b = c->hctl->divb_max;
+  double m;
+  std::memcpy(&m, &b, sizeof m);
+  *mx = m;
+  *tot = c->hctl->divb_sum;
+  return MHD_OK;
+}
+
+int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
+  int r[4];
+  divb_range(c, r);
+  const Grid& g = c->g;
+  // periodic wrap of the B ghosts, as divBCorrectionSOR starts with (div_b_fix.cpp:161-245)
+  c->ks->divb(g, c->U, r, c->partial, c->npartial, c->ctl, c->stream);
+  const double pxf = 1.0 / (g.dx * g.dx), pyf = 1.0 / (g.dy * g.dy);
+  double omega;
+  if (p->omega_use_static) {
+    omega = p->omega;
+  } else {
+    const double t = std::cos(g.dx) + std::cos(g.dy);
+    omega = (8.0 - std::sqrt(64.0 - 16.0 * t * t)) / (t * t);
+  }
+  const double coef[6] = {pxf, pyf, 4.0 / (2.0 * g.dx), 4.0 / (2.0 * g.dy),
+                          1.0 / (2 * (pxf + pyf)), omega};
+  double nan_ratio = std::numeric_limits<double>::quiet_NaN();  // no sweep: 0/0, "converged"
+  CK(cudaMemsetAsync(&c->ctl->rmax, 0, 2 * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(&c->ctl->sor_done, 0, 2 * sizeof(int), c->stream));
+  CK(cudaMemcpyAsync(c->ratio, &nan_ratio, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  long long issued = 0;
+  const int chunk = 16;
+  if (p->sor_rsteps > 0) {
+    for (;;) {
+      for (int s = 0; s < chunk; s++) {
+        c->ks->sor_sweep(g, c->phi, c->U, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio, c->ctl,
+                         c->stream);
+        c->launches += 5;
+      }
+      issued += chunk;
+      int st = read_ctl(c);
+      if (st) return st;
+      if (c->hctl->sor_done) break;
+    }
+  }
+  double last = 0.0;
+  CK(cudaMemcpyAsync(&last, c->ratio, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *sweeps = c->hctl->sor_sweeps;
+  if (last > p->sor_rmax)  // div_b_fix.cpp:387: NaN counts as converged
+    return set_status(c, MHD_ERR_NOT_CONVERGED, true, "SOR divergence cleaning failed to converge");
+  c->ks->sor_correct(g, c->U, c->phi, r, 1.0 / (2.0 * g.dx), 1.0 / (2.0 * g.dy), c->stream);
+  c->launches += 1;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  (void)issued;
+  return set_status(c, MHD_OK, false, "");
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhd_ctx_create(int nx, int ny, int halo, double dx, double dy, double gamma, const int bc[4],
+                   int scheme, int time_method, double dt_min, double dt_max, double cfl, int flags,
+                   int device, mhd_ctx** out) {
+  if (!out) return MHD_ERR_WRONG_PARAMETER;
+  *out = nullptr;
+  if (halo != 2 || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0) || (scheme != 2 && scheme != 3) ||
+      (time_method != 1 && time_method != 2) || !bc)
+    return MHD_ERR_WRONG_PARAMETER;
+  for (int s = 0; s < 4; s++)
+    if (bc[s] < PERIODIC || bc[s] > OPEN) return MHD_ERR_WRONG_PARAMETER;
+  mhd_ctx* c = new (std::nothrow) mhd_ctx();
+  if (!c) return MHD_ERR_CUDA;
+  c->device = device;
+  c->scheme = scheme;
+  c->time_method = time_method;
+  c->flags = flags;
+  c->dt_min = dt_min;
+  c->dt_max = dt_max;
+  c->cfl = cfl;
+  c->ks = (flags & MHD_FLAG_FAST_MATH) ? &kFast : &kExact;
+  Grid& g = c->g;
+  g.nx = nx; g.ny = ny; g.NX = nx + 4; g.NY = ny + 4;
+  g.pitch = pitch_for(g.NY);
+  g.off = ROW_OFF;
+  g.fstride = (long long)g.NX * g.pitch;
+  g.dx = dx; g.dy = dy; g.gamma = gamma;
+  for (int s = 0; s < 4; s++) g.bc[s] = bc[s];
+  c->dirichlet_needed = bc[0] == DIRICHLET || bc[1] == DIRICHLET || bc[2] == DIRICHLET ||
+                        bc[3] == DIRICHLET;
+  c->block_elems = size_t(NF) * g.fstride;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = alloc_block(c, &c->U);
+  if (e == cudaSuccess) e = alloc_block(c, &c->UL);
+  if (e == cudaSuccess && time_method == 2) e = alloc_block(c, &c->U1);
+  if (e == cudaSuccess && time_method == 2) e = alloc_block(c, &c->U2);
+  if (e == cudaSuccess && (flags & MHD_FLAG_CHARACTERISTICS))
+    for (int q = 0; q < 4 && e == cudaSuccess; q++) e = alloc_block(c, &c->ch[q]);
+  const size_t edge = size_t(NF) * std::max(g.NX, g.NY);
+  for (int q = 0; q < 4 && e == cudaSuccess; q++) {
+    e = cudaMalloc(&c->snap[q], edge * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->snap[q], 0, edge * sizeof(double), c->stream);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&c->aF, sizeof(double) * NF * g.NY);
+  if (e == cudaSuccess) e = cudaMalloc(&c->aG, sizeof(double) * NF * g.NX);
+  if (e == cudaSuccess) e = cudaMalloc(&c->phi, sizeof(double) * g.fstride);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->phi, 0, sizeof(double) * g.fstride, c->stream);
+  c->npartial = 148 * 16;
+  if (e == cudaSuccess) e = cudaMalloc(&c->partial, sizeof(double) * c->npartial);
+  if (e == cudaSuccess) e = cudaMalloc(&c->ratio, sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->ctl, sizeof(Ctl));
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->ctl, 0, sizeof(Ctl), c->stream);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hctl, sizeof(Ctl));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    cuda_fail(nullptr, e, "mhd_ctx_create");
+    mhd_ctx_destroy(c);
+    return MHD_ERR_CUDA;
+  }
+  std::memset(c->hctl, 0, sizeof(Ctl));
+  *out = c;
+  return MHD_OK;
+}
+
+int mhd_ctx_destroy(mhd_ctx* c) {
+  if (!c) return MHD_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  double* bufs[] = {c->U, c->U1, c->U2, c->UL, c->ch[0], c->ch[1], c->ch[2], c->ch[3], c->aF,
+                    c->aG, c->snap[0], c->snap[1], c->snap[2], c->snap[3], c->phi, c->partial,
+                    c->ratio};
+  for (double* b : bufs)
+    if (b) cudaFree(b);
+  if (c->ctl) cudaFree(c->ctl);
+  if (c->hctl) cudaFreeHost(c->hctl);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return MHD_OK;
+}
+
+int mhd_set_stepper(mhd_ctx* c, int time_method, double dt_min, double dt_max, double cfl) {
+  if (!c || (time_method != 1 && time_method != 2)) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  if (time_method == 2) {
+    if (!c->U1) CK(alloc_block(c, &c->U1));
+    if (!c->U2) CK(alloc_block(c, &c->U2));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  c->time_method = time_method;
+  c->dt_min = dt_min;
+  c->dt_max = dt_max;
+  c->cfl = cfl;
+  return set_status(c, MHD_OK, false, "");
+}
+
+int mhd_last_error(const mhd_ctx* c, char* msg, size_t len, int* is_error) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  if (msg && len) {
+    std::strncpy(msg, c->msg.c_str(), len - 1);
+    msg[len - 1] = '\0';
+  }
+  if (is_error) *is_error = c->is_error ? 1 : 0;
+  return MHD_OK;
+}
+
+int mhd_upload(mhd_ctx* c, const double* U) {
+  if (!c || !U) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  CK(h2d(c, c->U, U));
+  CK(cudaStreamSynchronize(c->stream));
+  return set_status(c, MHD_OK, false, "");
+}
+
+int mhd_download(mhd_ctx* c, double* U) {
+  if (!c || !U) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  CK(d2h(c, U, c->U));
+  CK(cudaStreamSynchronize(c->stream));
+  return MHD_OK;
+}
+
+int mhd_download_ul(mhd_ctx* c, double* UL) {
+  if (!c || !UL) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  CK(d2h(c, UL, c->UL));
+  CK(cudaStreamSynchronize(c->stream));
+  return MHD_OK;
+}
+
+int mhd_init_dirichlet(mhd_ctx* c) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  c->ks->snapshot(c->g, c->U, c->snap, c->stream);
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  c->dirichlet_ready = true;
+  return set_status(c, MHD_OK, false, "");
+}
+
+int mhd_integrate(mhd_ctx* c, double* dtIdeal) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  int st = check_bc_ready(c);
+  if (st) return st;
+  enqueue_control(c, PH_RESET_INTEGRATE);
+  enqueue_integrate(c, c->U, (c->flags & MHD_FLAG_CHARACTERISTICS) != 0);
+  enqueue_control(c, PH_IDEAL);
+  if ((st = read_ctl(c))) return st;
+  const Ctl& h = *c->hctl;
+  c->neg_pressure += (long long)h.neg_count;
+  if (h.error == 6)
+    return set_status(c, MHD_ERR_NEGATIVE_DENSITY, true,
+                      "negative density encountered\n! getEigens_F\n! mhd_integrate");
+  if (dtIdeal) *dtIdeal = h.dtIdeal;
+  if (h.neg_last)  // status of the last interface, as the reference reports it
+    return set_status(c, MHD_ERR_NEGATIVE_PRESSURE, false,
+                      "negative pressure encountered\n! getEigens_F\n! mhd_integrate");
+  return set_status(c, MHD_OK, false, "");
+}
+
+int mhd_integrate_host(mhd_ctx* c, double* U, double* UL, double* dtIdeal) {
+  if (!c || !U) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  CK(h2d(c, c->U, U));
+  int st = mhd_integrate(c, dtIdeal);
+  if (c->is_error) return st;
+  CK(d2h(c, U, c->U));
+  if (UL) CK(d2h(c, UL, c->UL));
+  CK(cudaStreamSynchronize(c->stream));
+  return st;
+}
+
+int mhd_step(mhd_ctx* c, double* dt_inout) {
+  if (!c || !dt_inout) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  return do_step(c, dt_inout);
+}
+
+int mhd_step_host(mhd_ctx* c, double* U, double* dt_inout) {
+  if (!c || !U || !dt_inout) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  CK(h2d(c, c->U, U));
+  int st = do_step(c, dt_inout);
+  CK(d2h(c, U, c->U));
+  CK(cudaStreamSynchronize(c->stream));
+  return st;
+}
+
+int mhd_steps(mhd_ctx* c, int nsteps, double* dt_inout, double* dts) {
+  if (!c || !dt_inout || nsteps < 0) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  for (int n = 0; n < nsteps; n++) {
+    int st = do_step(c, dt_inout);
+    if (st) return st;
+    if (dts) dts[n] = *dt_inout;
+  }
+  return MHD_OK;
+}
+
+int mhd_get_characteristics(mhd_ctx* c, double* cx, double* cy, double* LUx, double* LUy) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  if (!(c->flags & MHD_FLAG_CHARACTERISTICS))
+    return set_status(c, MHD_ERR_WRONG_PARAMETER, true,
+                      "characteristics were not requested at context creation");
+  CK(cudaSetDevice(c->device));
+  double* dst[4] = {cx, cy, LUx, LUy};
+  for (int q = 0; q < 4; q++)
+    if (dst[q]) CK(d2h(c, dst[q], c->ch[q]));
+  CK(cudaStreamSynchronize(c->stream));
+  return MHD_OK;
+}
+
+int mhd_divb_calc(mhd_ctx* c, double* maxdivb, double* totdivb) {
+  if (!c || !maxdivb || !totdivb) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  return do_divb_calc(c, maxdivb, totdivb);
+}
+
+int mhd_divb_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
+  if (!c || !p) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  int sw = 0;
+  int st = do_sor(c, p, &sw);
+  if (sweeps) *sweeps = sw;
+  return st;
+}
+
+int mhd_divb_clean(mhd_ctx* c, const mhd_sor_params* p, double* maxdivb, int* total_sweeps) {
+  if (!c || !p) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  double mx = -1.0, tot = 0.0;
+  int total = 0, st = MHD_OK;
+  if (p->sor_steps > 0) {
+    for (int it = 0; it < p->sor_steps; it++) {
+      if ((st = do_divb_calc(c, &mx, &tot))) return st;
+      if (mx < p->sor_divbmax) break;
+      int sw = 0;
+      st = do_sor(c, p, &sw);
+      total += sw;
+      if (st == MHD_ERR_NOT_CONVERGED) break;
+      if (st) return st;
+    }
+    int st2 = do_divb_calc(c, &mx, &tot);
+    if (st2) return st2;
+  }
+  if (maxdivb) *maxdivb = mx;
+  if (total_sweeps) *total_sweeps = total;
+  return st;
+}
+
+int mhd_get_counters(mhd_ctx* c, long long* neg_pressure, long long* launches) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  if (neg_pressure) *neg_pressure = c->neg_pressure;
+  if (launches) *launches = c->launches;
+  return MHD_OK;
+}
+
+int mhd_layout(const mhd_ctx* c, int* pitch, int* row_offset) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  if (pitch) *pitch = c->g.pitch;
+  if (row_offset) *row_offset = c->g.off;
+  return MHD_OK;
+}
+
+int mhd_fp64_peak(int device, double* tflops) {
+  mhd_ctx* c = nullptr;
+  if (!tflops) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  double* out = nullptr;
+  CK(cudaMalloc(&out, sizeof(double)));
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  const int blocks = sms * 8, threads = 256, iters = 8192;
+  k_fma_peak<<<blocks, threads>>>(out, 64, 0.999999, 1e-9);  // warm-up
+  CK(cudaEventRecord(a));
+  k_fma_peak<<<blocks, threads>>>(out, iters, 0.999999, 1e-9);
+  CK(cudaEventRecord(b));
+  CK(cudaEventSynchronize(b));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  CK(cudaGetLastError());
+  *tflops = 2.0 * 8.0 * double(iters) * blocks * threads / (double(ms) * 1e-3) / 1e12;
+  return MHD_OK;
+}
+
+int mhd_stream(const mhd_ctx* c, void** stream) {
+  if (!c || !stream) return MHD_ERR_WRONG_PARAMETER;
+  *stream = (void*)c->stream;
+  return MHD_OK;
+}
+
+int mhd_time_integrate(mhd_ctx* c, int n, double* avg_ms) {
+  if (!c || n < 1 || !avg_ms) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  int st = check_bc_ready(c);
+  if (st) return st;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  enqueue_control(c, PH_RESET_INTEGRATE);
+  CK(cudaEventRecord(a, c->stream));
+  for (int q = 0; q < n; q++) enqueue_integrate(c, c->U, false);
+  CK(cudaEventRecord(b, c->stream));
+  CK(cudaEventSynchronize(b));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  CK(cudaGetLastError());
+  *avg_ms = double(ms) / n;
+  return MHD_OK;
+}
+
+}  // extern "C"

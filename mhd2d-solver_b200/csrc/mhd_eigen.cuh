@@ -1,0 +1,320 @@
+// Midpoint eigen-system of ideal MHD for the x-direction flux, evaluated one
+// characteristic at a time.
+//
+// Follows SpatialMethodEno::getEigensF (spatialmethodeno.cpp:288-571):
+// arithmetic-mean midpoint state (not a sqrt(rho)-weighted Roe average),
+// pressure from the mean total pressure clamped at zero, the 8-wave
+// right/left eigenvectors with the alpha_f / alpha_s / beta normalisation
+// and the sign flips that keep the fast and slow vectors continuous across
+// By = 0.  Row 7 (the dummy wave) and column 4 (Bx) are structurally zero
+// and never formed; the other rows are produced on demand, so a thread holds
+// ~30 midpoint scalars plus one row instead of two dense 8x8 matrices.
+//
+// Every expression keeps the reference's association order; the parity
+// build compiles this with -fmad=false, which makes each entry bit-identical
+// to the reference's x86-64 double arithmetic (IEEE division and sqrt on
+// both sides).  The y direction uses the same code on x/y-swapped inputs,
+// as getEigensG / getNumericalFluxG do (spatialmethodeno.cpp:574-598).
+#pragma once
+
+#include "mhd_common.cuh"
+
+#ifndef MHD_KNS
+#define MHD_KNS exact
+#endif
+
+namespace mhd {
+namespace MHD_KNS {
+
+struct Mid {
+  double u, v, w, uu;
+  double a2, a, ca2, ca, cs2, cs, cf2, cf;
+  double rr, sbx, af2, af, as2, as, bty, btz, th1, th2, g1, g21, vb;
+  double fcf, fcs;  // sign factors of the fast / slow rows
+  int negp;         // midpoint pressure was negative and clamped
+};
+
+// Returns false on non-positive midpoint density (the reference's
+// ErrorNegativeDensity, spatialmethodeno.cpp:307-310).
+__device__ __forceinline__ bool midpoint(double gm, const double* U1, const double* U2, Mid& e) {
+  const double r = 0.5 * (U1[0] + U2[0]);
+  e.u = 0.5 * (U1[1] / U1[0] + U2[1] / U2[0]);
+  e.v = 0.5 * (U1[2] / U1[0] + U2[2] / U2[0]);
+  e.w = 0.5 * (U1[3] / U1[0] + U2[3] / U2[0]);
+  const double bx = 0.5 * (U1[4] + U2[4]);
+  const double by = 0.5 * (U1[5] + U2[5]);
+  const double bz = 0.5 * (U1[6] + U2[6]);
+  if (r <= 0.0) return false;
+  const double u = e.u, v = e.v, w = e.w;
+  e.uu = u * u + v * v + w * w;
+  const double bb = bx * bx + by * by + bz * bz;
+  const double mml = U1[1] * U1[1] + U1[2] * U1[2] + U1[3] * U1[3];
+  const double bbl = U1[4] * U1[4] + U1[5] * U1[5] + U1[6] * U1[6];
+  const double mmr = U2[1] * U2[1] + U2[2] * U2[2] + U2[3] * U2[3];
+  const double bbr = U2[4] * U2[4] + U2[5] * U2[5] + U2[6] * U2[6];
+  const double ptl = (gm - 1.0) * (U1[7] - 0.5 * mml / U1[0] - 0.5 * bbl) + 0.5 * bbl;
+  const double ptr = (gm - 1.0) * (U2[7] - 0.5 * mmr / U2[0] - 0.5 * bbr) + 0.5 * bbr;
+  const double pt = 0.5 * (ptl + ptr);
+  double p = pt - 0.5 * bb;
+  e.negp = 0;
+  if (p < 0.0) { p = 0.0; e.negp = 1; }
+
+  double a2 = gm * p / r;
+  if (a2 < 0.0) a2 = 0.0;
+  e.a2 = a2;
+  e.a = sqrt(a2);
+  e.ca2 = bx * bx / r;
+  e.ca = sqrt(e.ca2);
+  const double c2 = 0.5 * (bb / r + a2);
+  double ct = c2 * c2 - a2 * e.ca2;
+  if (ct < 0.0) ct = 0.0;
+  const double sct = sqrt(ct);
+  double cs2 = c2 - sct;
+  if (cs2 < 0.0) cs2 = SMALL;
+  double cf2 = c2 + sct;
+  if (cf2 < 0.0) cf2 = SMALL;
+  e.cs2 = cs2; e.cs = sqrt(cs2);
+  e.cf2 = cf2; e.cf = sqrt(cf2);
+
+  e.rr = sqrt(r);
+  const double bp2 = by * by + bz * bz;
+  e.sbx = (bx < 0.0) ? -1.0 : 1.0;
+  const bool deg = (bp2 < SMALL) && (fabs(e.ca2 - a2) < SMALL);
+  double af2 = deg ? 1.0 : (cf2 - e.ca2) / (cf2 - cs2);
+  if (af2 < 0.0) af2 = 0.0;
+  double as2 = deg ? 1.0 : (cf2 - a2) / (cf2 - cs2);
+  if (as2 < 0.0) as2 = 0.0;
+  e.af2 = af2; e.af = sqrt(af2);
+  e.as2 = as2; e.as = sqrt(as2);
+  if (bp2 > SMALL) {
+    const double sb = sqrt(bp2);
+    e.bty = by / sb;
+    e.btz = bz / sb;
+  } else {
+    e.bty = 1.0 / sqrt(2.0);
+    e.btz = 1.0 / sqrt(2.0);
+  }
+  e.g1 = gm - 1.0;
+  e.g21 = (gm - 2.0) / (gm - 1.0);
+  e.th1 = 1.0 / (af2 * a2 * (cf2 - e.g21 * a2) + as2 * cf2 * (cs2 - e.g21 * a2));
+  e.th2 = 1.0 / (af2 * e.cf * e.a * e.sbx + as2 * e.cs * e.ca * e.sbx);
+  e.vb = e.bty * v + e.btz * w;
+
+  const double sgnbt = ((by > 0.0) || (fabs(by) < SMALL && (bz > 0.0))) ? 1.0 : -1.0;
+  e.fcs = a2 > e.ca2 ? sgnbt : 1.0;
+  e.fcf = a2 < e.ca2 ? sgnbt : 1.0;
+  return true;
+}
+
+__device__ __forceinline__ double eigenvalue(const Mid& e, int k) {
+  switch (k) {
+    case 0: return e.u - e.cf;
+    case 1: return e.u - e.ca;
+    case 2: return e.u - e.cs;
+    case 3: return e.u;
+    case 4: return e.u + e.cs;
+    case 5: return e.u + e.ca;
+    case 6: return e.u + e.cf;
+    default: return 0.0;
+  }
+}
+
+// Structurally non-zero columns of each left / right row (bit m = column m).
+__host__ __device__ constexpr unsigned lv_mask(int k) {
+  return (k == 1 || k == 5) ? 0x6Du /* 0,2,3,5,6 */ : (k == 7 ? 0u : 0xEFu /* all but 4 */);
+}
+__host__ __device__ constexpr unsigned rv_mask(int k) {
+  return (k == 1 || k == 5) ? 0xECu /* 2,3,5,6,7 */
+       : (k == 3 ? 0x8Fu /* 0,1,2,3,7 */ : (k == 7 ? 0u : 0xEFu));
+}
+
+// Left eigenvector row k (spatialmethodeno.cpp:473-552, sign flips 554-568).
+__device__ __forceinline__ void lv_row(const Mid& e, int k, double* l) {
+  const double u = e.u, v = e.v, w = e.w, uu = e.uu, a2 = e.a2, a = e.a, ca = e.ca;
+  const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr, sbx = e.sbx;
+  const double af = e.af, as = e.as, af2 = e.af2, as2 = e.as2, bty = e.bty, btz = e.btz;
+  const double th1 = e.th1, th2 = e.th2, g21 = e.g21, vb = e.vb;
+  switch (k) {
+    case 0:
+    case 6: {
+      const double f = e.fcf;
+      if (k == 0) {
+        l[0] = 0.25 * th1 * af * a2 * uu + 0.5 * th2 * (af * a * u * sbx - as * cs * vb);
+        l[1] = -0.5 * th1 * af * a2 * u - 0.5 * th2 * af * a * sbx;
+        l[2] = -0.5 * th1 * af * a2 * v + 0.5 * th2 * as * bty * cs;
+        l[3] = -0.5 * th1 * af * a2 * w + 0.5 * th2 * as * btz * cs;
+      } else {
+        l[0] = 0.25 * th1 * af * a2 * uu - 0.5 * th2 * (af * a * u * sbx - as * cs * vb);
+        l[1] = -0.5 * th1 * af * a2 * u + 0.5 * th2 * af * a * sbx;
+        l[2] = -0.5 * th1 * af * a2 * v - 0.5 * th2 * as * bty * cs;
+        l[3] = -0.5 * th1 * af * a2 * w - 0.5 * th2 * as * btz * cs;
+      }
+      l[5] = 0.5 * th1 * as * bty * cf * rr * (cs2 - g21 * a2);
+      l[6] = 0.5 * th1 * as * btz * cf * rr * (cs2 - g21 * a2);
+      l[7] = 0.5 * th1 * af * a2;
+      l[0] *= f; l[1] *= f; l[2] *= f; l[3] *= f; l[5] *= f; l[6] *= f; l[7] *= f;
+      break;
+    }
+    case 1:
+      l[0] = -0.5 * (btz * v - bty * w) * sbx;
+      l[2] = 0.5 * btz * sbx;
+      l[3] = -0.5 * bty * sbx;
+      l[5] = 0.5 * btz * rr;
+      l[6] = -0.5 * bty * rr;
+      break;
+    case 2:
+    case 4: {
+      const double f = e.fcs;
+      if (k == 2) {
+        l[0] = 0.25 * th1 * as * cf2 * uu + 0.5 * th2 * (as * ca * u * sbx + af * cf * vb);
+        l[1] = -0.5 * th1 * as * cf2 * u - 0.5 * th2 * as * ca * sbx;
+        l[2] = -0.5 * th1 * as * cf2 * v - 0.5 * th2 * af * bty * cf;
+        l[3] = -0.5 * th1 * as * cf2 * w - 0.5 * th2 * af * btz * cf;
+      } else {
+        l[0] = 0.25 * th1 * as * cf2 * uu - 0.5 * th2 * (as * ca * u * sbx + af * cf * vb);
+        l[1] = -0.5 * th1 * as * cf2 * u + 0.5 * th2 * as * ca * sbx;
+        l[2] = -0.5 * th1 * as * cf2 * v + 0.5 * th2 * af * bty * cf;
+        l[3] = -0.5 * th1 * as * cf2 * w + 0.5 * th2 * af * btz * cf;
+      }
+      l[5] = -0.5 * th1 * af * bty * cf * rr * (cf2 - g21 * a2);
+      l[6] = -0.5 * th1 * af * btz * cf * rr * (cf2 - g21 * a2);
+      l[7] = 0.5 * th1 * as * cf2;
+      l[0] *= f; l[1] *= f; l[2] *= f; l[3] *= f; l[5] *= f; l[6] *= f; l[7] *= f;
+      break;
+    }
+    case 3: {
+      l[0] = 1.0 - 0.5 * th1 * uu * (af2 * a2 + as2 * cf2);
+      l[1] = th1 * (af2 * a2 + as2 * cf2) * u;
+      l[2] = th1 * (af2 * a2 + as2 * cf2) * v;
+      l[3] = th1 * (af2 * a2 + as2 * cf2) * w;
+      l[5] = th1 * af * as * bty * cf * rr * (cf2 - cs2);
+      l[6] = th1 * af * as * btz * cf * rr * (cf2 - cs2);
+      l[7] = -th1 * (af2 * a2 + as2 * cf2);
+      break;
+    }
+    case 5:
+      l[0] = +0.5 * (btz * v - bty * w) * sbx;
+      l[2] = -0.5 * btz * sbx;
+      l[3] = 0.5 * bty * sbx;
+      l[5] = 0.5 * btz * rr;
+      l[6] = -0.5 * bty * rr;
+      break;
+    default:
+      break;
+  }
+}
+
+// Right eigenvector row k (spatialmethodeno.cpp:392-471, sign flips 554-568).
+__device__ __forceinline__ void rv_row(const Mid& e, int k, double* q) {
+  const double u = e.u, v = e.v, w = e.w, uu = e.uu, a2 = e.a2, a = e.a, ca = e.ca;
+  const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr, sbx = e.sbx;
+  const double af = e.af, as = e.as, bty = e.bty, btz = e.btz, g1 = e.g1, g21 = e.g21;
+  const double vb = e.vb;
+  switch (k) {
+    case 0: {
+      const double f = e.fcf;
+      q[0] = af;
+      q[1] = af * (u - cf);
+      q[2] = af * v + as * bty * ca * sbx;
+      q[3] = af * w + as * btz * ca * sbx;
+      q[5] = as * bty * cf / rr;
+      q[6] = as * btz * cf / rr;
+      q[7] = 0.5 * af * uu + af * cf2 / g1 - af * cf * u + as * ca * sbx * vb + g21 * af * (cf2 - a2);
+      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
+      break;
+    }
+    case 1:
+      q[2] = btz * sbx;
+      q[3] = -bty * sbx;
+      q[5] = btz / rr;
+      q[6] = -bty / rr;
+      q[7] = (btz * v - bty * w) * sbx;
+      break;
+    case 2: {
+      const double f = e.fcs;
+      q[0] = as;
+      q[1] = as * (u - cs);
+      q[2] = as * v - af * bty * a * sbx;
+      q[3] = as * w - af * btz * a * sbx;
+      q[5] = -af * bty * a2 / (cf * rr);
+      q[6] = -af * btz * a2 / (cf * rr);
+      q[7] = 0.5 * as * uu + as * cs2 / g1 - as * cs * u - af * a * sbx * vb + g21 * as * (cs2 - a2);
+      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
+      break;
+    }
+    case 3:
+      q[0] = 1.0;
+      q[1] = u;
+      q[2] = v;
+      q[3] = w;
+      q[7] = 0.5 * uu;
+      break;
+    case 4: {
+      const double f = e.fcs;
+      q[0] = as;
+      q[1] = as * (u + cs);
+      q[2] = as * v + af * bty * a * sbx;
+      q[3] = as * w + af * btz * a * sbx;
+      q[5] = -af * bty * a2 / (cf * rr);
+      q[6] = -af * btz * a2 / (cf * rr);
+      q[7] = 0.5 * as * uu + as * cs2 / g1 + as * cs * u + af * a * sbx * vb + g21 * as * (cs2 - a2);
+      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
+      break;
+    }
+    case 5:
+      q[2] = -btz * sbx;
+      q[3] = +bty * sbx;
+      q[5] = btz / rr;
+      q[6] = -bty / rr;
+      q[7] = -(btz * v - bty * w) * sbx;
+      break;
+    case 6: {
+      const double f = e.fcf;
+      q[0] = af;
+      q[1] = af * (u + cf);
+      q[2] = af * v - as * bty * ca * sbx;
+      q[3] = af * w - as * btz * ca * sbx;
+      q[5] = as * bty * cf / rr;
+      q[6] = as * btz * cf / rr;
+      q[7] = 0.5 * af * uu + af * cf2 / g1 + af * cf * u - as * ca * sbx * vb + g21 * af * (cf2 - a2);
+      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// Cell-centred eigenvalues (SpatialMethodEno::getEigenvaluesAt,
+// spatialmethodeno.cpp:130-206), used for the ENO-LF dissipation.
+// Returns false on non-positive density.
+__device__ __forceinline__ bool eigenvalues_at(double gm, const double* U, double* lam, int& negp) {
+  const double r = U[0], mx = U[1], u = U[1] / U[0], my = U[2], mz = U[3];
+  const double bx = U[4], by = U[5], bz = U[6], en = U[7];
+  negp = 0;
+  if (r <= 0.0) return false;
+  const double mm = mx * mx + my * my + mz * mz;
+  const double bb = bx * bx + by * by + bz * bz;
+  double p = (gm - 1.0) * (en - 0.5 * mm / r - 0.5 * bb);
+  if (p < 0.0) { p = 0.0; negp = 1; }
+  double a2 = gm * p / r;
+  if (a2 < 0.0) a2 = 0.0;
+  const double ca2 = bx * bx / r;
+  const double ca = sqrt(ca2);
+  const double c2 = 0.5 * (bb / r + a2);
+  double ct = c2 * c2 - a2 * ca2;
+  if (ct < 0.0) ct = 0.0;
+  const double sct = sqrt(ct);
+  double cs2 = c2 - sct;
+  if (cs2 < 0.0) cs2 = SMALL;
+  const double cs = sqrt(cs2);
+  double cf2 = c2 + sct;
+  if (cf2 < 0.0) cf2 = SMALL;
+  const double cf = sqrt(cf2);
+  lam[0] = u - cf; lam[1] = u - ca; lam[2] = u - cs; lam[3] = u;
+  lam[4] = u + cs; lam[5] = u + ca; lam[6] = u + cf; lam[7] = 0.0;
+  return true;
+}
+
+}  // namespace MHD_KNS
+}  // namespace mhd

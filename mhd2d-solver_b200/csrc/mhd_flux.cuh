@@ -1,0 +1,429 @@
+// Fused spatial operator L(U) for the ENO-Roe and ENO-LF schemes.
+//
+// One CTA owns a TI x TJ tile of interior cells (i rows, j columns; j is the
+// contiguous direction).  It
+//   0. stages the (TI+4) x (TJ+4) box of the 8 fields into shared memory,
+//   1. computes the physical fluxes F (x) and G (y) once per cell
+//      (SpatialMethodEno::updateFluxes, spatialmethodeno.cpp:89-127),
+//   2. evaluates the (TI+1) x TJ x-interfaces and TI x (TJ+1) y-interfaces
+//      the tile needs (getNumericalFluxF/G of the Roe and LF schemes), one
+//      interface per lane, warp-uniform direction, and keeps the numerical
+//      fluxes in shared memory,
+//   3. forms UL = -(F_i - F_{i-1})/dx - (G_j - G_{j-1})/dy
+//      (spatialmethodenoroe.cpp:169-176) and writes it to HBM,
+// and folds max|lambda| of its interfaces into the context's CFL maxima.
+// The reference runs these steps as separate full-grid passes with F, G,
+// VUF, VUG, F_, G_ arrays in memory; here nothing but U and UL crosses HBM.
+//
+// Interface work per tile: x rows ii = -1..TI-1 (TI+1 warp tasks of TJ
+// lanes), y rows of TJ lanes (TI tasks) plus the TI left-edge y interfaces
+// (1 task).  With TI = 8, TJ = 32 that is 18 warp tasks, 3 per warp for 6
+// warps.
+#pragma once
+
+#include "mhd_eigen.cuh"
+
+#ifndef MHD_MINB
+#define MHD_MINB 2
+#endif
+
+#ifndef MHD_KNS
+#define MHD_KNS exact
+#endif
+
+namespace mhd {
+namespace MHD_KNS {
+
+// Component -> slot of a 7-wide flux vector (column 4 is structurally 0).
+__host__ __device__ constexpr int slot_of(int m) { return m < 4 ? m : m - 1; }
+// x <-> y role swap of a state / flux component.
+__host__ __device__ constexpr int swap_xy(int m) {
+  return m == 1 ? 2 : m == 2 ? 1 : m == 4 ? 5 : m == 5 ? 4 : m;
+}
+
+struct CharOut {
+  double *cx, *cy, *LUx, *LUy;  // pitched like U; null when not requested
+};
+
+template <int TI_, int TJ_>
+struct TileGeom {
+  static constexpr int TI = TI_, TJ = TJ_;
+  static constexpr int RU = TI + 4, CU = TJ + 4;
+  static constexpr int OFF_U = 0;
+  static constexpr int OFF_F = OFF_U + NF * RU * CU;       // sF[7][RU][TJ]
+  static constexpr int OFF_G = OFF_F + 7 * RU * TJ;        // sG[7][TI][CU], slots in y frame order
+  static constexpr int OFF_FX = OFF_G + 7 * TI * CU;       // sFx[7][TI+1][TJ]
+  static constexpr int OFF_GY = OFF_FX + 7 * (TI + 1) * TJ;  // sGy[7][TI][TJ+1], y frame order
+  static constexpr int TOTAL = OFF_GY + 7 * TI * (TJ + 1);
+  static constexpr size_t BYTES = size_t(TOTAL) * sizeof(double);
+};
+
+// Physical x / y fluxes of one cell, same arithmetic as updateFluxes.
+__device__ __forceinline__ void phys_flux(double gm, const double* q, double* F, double* G) {
+  const double r = q[0], mx = q[1], my = q[2], mz = q[3];
+  const double bx = q[4], by = q[5], bz = q[6], en = q[7];
+  const double u = mx / r, v = my / r, w = mz / r;
+  const double uu = u * u + v * v + w * w;
+  const double ub = u * bx + v * by + w * bz;
+  const double bb = bx * bx + by * by + bz * bz;
+  const double p = (gm - 1.0) * (en - 0.5 * r * uu - 0.5 * bb);
+  const double pt = p + 0.5 * bb;
+  F[0] = mx;
+  F[1] = mx * u - bx * bx + pt;
+  F[2] = my * u - bx * by;
+  F[3] = mz * u - bx * bz;
+  F[5] = by * u - bx * v;
+  F[6] = bz * u - bx * w;
+  F[7] = (en + pt) * u - bx * ub;
+  G[0] = my;
+  G[1] = mx * v - by * bx;
+  G[2] = my * v - by * by + pt;
+  G[3] = mz * v - by * bz;
+  G[4] = bx * v - by * u;
+  G[6] = bz * v - by * w;
+  G[7] = (en + pt) * v - by * ub;
+}
+
+// ENO-2 stencil choice on one characteristic (spatialmethodenoroe.cpp:240-254).
+__device__ __forceinline__ double eno_minus(double w0, double w1, double w2, double v0, double v1) {
+  return (fabs(v0) < fabs(v1)) ? (-(1.0 / 2.0) * w0 + (3.0 / 2.0) * w1)
+                               : ((1.0 / 2.0) * w1 + (1.0 / 2.0) * w2);
+}
+__device__ __forceinline__ double eno_plus(double w1, double w2, double w3, double v1, double v2) {
+  return (fabs(v1) < fabs(v2)) ? ((1.0 / 2.0) * w1 + (1.0 / 2.0) * w2)
+                               : ((3.0 / 2.0) * w2 - (1.0 / 2.0) * w3);
+}
+
+// One lane's view of its interface stencil inside the shared tile.
+struct Lane {
+  const double* f;   // flux stencil point l of slot s at f[s*fplane + l*fstep]
+  int fplane, fstep;
+  const double* q;   // state stencil point l of field k at q[k*qplane + l*qstep]
+  int qplane, qstep;
+  bool swp;          // y interface: x/y roles swapped
+  int l1, l2;        // stencil points of U1 / U2 (1 / 2, or open-boundary substitutes)
+  __device__ __forceinline__ double F(int m, int l) const { return f[slot_of(m) * fplane + l * fstep]; }
+  __device__ __forceinline__ double Q(int k, int l) const {
+    return q[(swp ? swap_xy(k) : k) * qplane + l * qstep];
+  }
+};
+
+// Numerical flux of one interface in the lane's frame.  Fn gets the 7
+// non-zero components (slot order), lam / LU the characteristic outputs.
+template <int SCHEME, bool CHARS>
+__device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const double* alpha,
+                                               double* Fn, double& smax, int& negp,
+                                               double* lam, double* LU) {
+  double U1[NF], U2[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    U1[k] = L.Q(k, L.l1);
+    U2[k] = L.Q(k, L.l2);
+  }
+  Mid e;
+  if (!midpoint(gm, U1, U2, e)) return false;
+  negp = e.negp;
+  smax = 0.0;
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    const double lk = eigenvalue(e, k);
+    if (CHARS) lam[k] = lk;
+    smax = take_max(smax, fabs(lk));
+  }
+#pragma unroll
+  for (int s = 0; s < 7; s++) Fn[s] = 0.0;
+
+#pragma unroll 1
+  for (int k = 0; k < 7; k++) {
+    double l[NF];
+    lv_row(e, k, l);
+    const unsigned lm = lv_mask(k);
+    double fw;
+    if (SCHEME == 2) {  // ENO-Roe: project F and its undivided differences
+      double w[4], vw[3];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int m = 0; m < NF; m++)
+          if (lm & (1u << m)) acc += l[m] * L.F(m, p);
+        w[p] = acc;
+      }
+#pragma unroll
+      for (int p = 0; p < 3; p++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int m = 0; m < NF; m++)
+          if (lm & (1u << m)) acc += l[m] * (L.F(m, p + 1) - L.F(m, p));
+        vw[p] = acc;
+      }
+      const double wm = eno_minus(w[0], w[1], w[2], vw[0], vw[1]);
+      const double wp = eno_plus(w[1], w[2], w[3], vw[1], vw[2]);
+      const double ak = eigenvalue(e, k);
+      fw = (ak >= 0 && wm < 1.0e10) ? wm : ((ak <= 0 && wp < 1.0e10) ? wp : 0.0);
+    } else {  // ENO-LF: split w = (RF +- alpha RU)/2, ENO on each half
+      double ru[4], rf[4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        double a = 0.0, b = 0.0;
+#pragma unroll
+        for (int m = 0; m < NF; m++)
+          if (lm & (1u << m)) {
+            a += l[m] * L.Q(m, p);
+            b += l[m] * L.F(m, p);
+          }
+        ru[p] = a;
+        rf[p] = b;
+      }
+      const double al = alpha[k];
+      double w[4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) w[p] = 0.5 * (rf[p] + al * ru[p]);
+      const double wm = eno_minus(w[0], w[1], w[2], w[1] - w[0], w[2] - w[1]);
+#pragma unroll
+      for (int p = 0; p < 4; p++) w[p] = 0.5 * (rf[p] - al * ru[p]);
+      const double wp = eno_plus(w[1], w[2], w[3], w[2] - w[1], w[3] - w[2]);
+      fw = wm + wp;
+      if (CHARS) LU[k] = ru[1];
+    }
+    if (CHARS && SCHEME == 2) {
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (lm & (1u << m)) acc += l[m] * U1[m];
+      LU[k] = acc;
+    }
+    double q[NF];
+    rv_row(e, k, q);
+    const unsigned rm = rv_mask(k);
+#pragma unroll
+    for (int m = 0; m < NF; m++)
+      if (rm & (1u << m)) Fn[slot_of(m)] += q[m] * fw;
+  }
+  // The dummy wave 7 contributes +0 * +0 last in the reference's sums.
+#pragma unroll
+  for (int s = 0; s < 7; s++) Fn[s] = Fn[s] + 0.0;
+  if (CHARS) LU[7] = 0.0;
+  return true;
+}
+
+template <int SCHEME, bool CHARS, int TI, int TJ, int NW>
+__global__ void __launch_bounds__(NW * 32, MHD_MINB)
+k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
+       const double* __restrict__ alphaF, const double* __restrict__ alphaG,
+       double inv_dx, double inv_dy, Ctl* ctl, CharOut co) {
+  using T = TileGeom<TI, TJ>;
+  constexpr int RU = T::RU, CU = T::CU;
+  if (ctl->skip) return;
+  extern __shared__ double sm[];
+  double* sU = sm + T::OFF_U;
+  double* sF = sm + T::OFF_F;
+  double* sG = sm + T::OFF_G;
+  double* sFx = sm + T::OFF_FX;
+  double* sGy = sm + T::OFF_GY;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i0 = 2 + blockIdx.y * TI, j0 = 2 + blockIdx.x * TJ;
+  const double gm = g.gamma;
+
+  // 0. stage the state box
+  for (int e = tid; e < NF * RU * CU; e += NW * 32) {
+    const int k = e / (RU * CU), rem = e - k * (RU * CU);
+    const int r = rem / CU, c = rem - r * CU;
+    const int i = i0 - 2 + r, j = j0 - 2 + c;
+    sU[e] = (i < g.NX && j < g.NY) ? U[g.at(k, i, j)] : 0.0;
+  }
+  __syncthreads();
+
+  // 1. physical fluxes: F on rows [0,RU) x cols [2,TJ+2), G on rows [2,TI+2) x cols [0,CU)
+  for (int e = tid; e < RU * CU; e += NW * 32) {
+    const int r = e / CU, c = e - r * CU;
+    const bool needF = (c >= 2 && c < TJ + 2), needG = (r >= 2 && r < TI + 2);
+    if (!needF && !needG) continue;
+    const int i = i0 - 2 + r, j = j0 - 2 + c;
+    double q[NF], F[NF], G[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) q[k] = sU[(k * RU + r) * CU + c];
+    if (i < g.NX && j < g.NY) {
+      phys_flux(gm, q, F, G);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NF; k++) { F[k] = 0.0; G[k] = 0.0; }
+    }
+    if (needF) {
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (m != 4) sF[(slot_of(m) * RU + r) * TJ + (c - 2)] = F[m];
+    }
+    if (needG) {
+#pragma unroll
+      for (int m = 0; m < NF; m++)  // y frame: slot s holds G[swap_xy(frame m)]
+        if (m != 4) sG[(slot_of(m) * TI + (r - 2)) * CU + c] = G[swap_xy(m)];
+    }
+  }
+  __syncthreads();
+
+  // 2. interfaces
+  double smaxX = 0.0, smaxY = 0.0;
+  int negc = 0;
+  constexpr int NTASK = 2 * TI + 2;
+  for (int t = warp; t < NTASK; t += NW) {
+    Lane L;
+    int ii, jj, gi, gj;
+    bool valid, isx;
+    double al[NF];
+    if (t <= TI) {  // x interfaces between rows i0+ii and i0+ii+1
+      isx = true;
+      ii = t - 1; jj = lane;
+      gi = i0 + ii; gj = j0 + jj;
+      valid = (gi <= g.nx + 1) && (gj < g.ny + 2);
+      L.f = sF + (ii + 1) * TJ + jj; L.fplane = RU * TJ; L.fstep = TJ;
+      L.q = sU + (ii + 1) * CU + (jj + 2); L.qplane = RU * CU; L.qstep = CU;
+      L.swp = false;
+      L.l1 = (g.bc[LEFT] == OPEN && gi < 2) ? 2 : 1;
+      L.l2 = (g.bc[RIGHT] == OPEN && gi > g.nx) ? 1 : 2;
+      if (SCHEME == 3 && valid) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) al[k] = alphaF[k * g.NY + gj];
+      }
+    } else {  // y interfaces between columns j and j+1
+      isx = false;
+      int rr;
+      if (t < NTASK - 1) { rr = t - (TI + 1); jj = lane; }
+      else { rr = lane; jj = -1; }
+      ii = rr;
+      gi = i0 + rr; gj = j0 + jj;
+      valid = (rr < TI) && (gi < g.nx + 2) && (gj < g.ny + 2);
+      L.f = sG + rr * CU + (jj + 1); L.fplane = TI * CU; L.fstep = 1;
+      L.q = sU + (rr + 2) * CU + (jj + 1); L.qplane = RU * CU; L.qstep = 1;
+      L.swp = true;
+      L.l1 = (g.bc[BOTTOM] == OPEN && gj < 2) ? 2 : 1;
+      L.l2 = (g.bc[TOP] == OPEN && gj > g.ny) ? 1 : 2;
+      if (SCHEME == 3 && valid) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) al[k] = alphaG[k * g.NX + gi];
+      }
+    }
+    if (!valid) continue;
+    double Fn[7], lam[NF], LU[NF], smax;
+    int negp = 0;
+    if (!interface_flux<SCHEME, CHARS>(gm, L, al, Fn, smax, negp, lam, LU)) {
+      atomicExch(&ctl->error, 6);  // ErrorNegativeDensity
+      atomicAdd(&ctl->negd_count, 1ull);
+      continue;
+    }
+    negc += negp;
+    if (isx) {
+      smaxX = take_max(smaxX, smax);
+#pragma unroll
+      for (int s = 0; s < 7; s++) sFx[(s * (TI + 1) + (ii + 1)) * TJ + jj] = Fn[s];
+    } else {
+      smaxY = take_max(smaxY, smax);
+#pragma unroll
+      for (int s = 0; s < 7; s++) sGy[(s * TI + ii) * (TJ + 1) + (jj + 1)] = Fn[s];
+      if (gi == g.nx + 1 && gj == g.ny + 1) ctl->neg_last = negp;  // last interface of the sweep
+    }
+    if (CHARS) {
+      double* cdst = isx ? co.cx : co.cy;
+      double* ldst = isx ? co.LUx : co.LUy;
+#pragma unroll
+      for (int k = 0; k < NF; k++) {
+        cdst[g.at(k, gi, gj)] = lam[k];
+        ldst[g.at(k, gi, gj)] = LU[k];
+      }
+    }
+  }
+  __syncthreads();
+
+  // 3. UL of the tile's cells
+  for (int e = tid; e < TI * TJ; e += NW * 32) {
+    const int r = e / TJ, c = e - r * TJ;
+    const int i = i0 + r, j = j0 + c;
+    if (i >= g.nx + 2 || j >= g.ny + 2) continue;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      double fr = 0.0, fl = 0.0, gr = 0.0, gl = 0.0;
+      if (k != 4) {
+        fr = sFx[(slot_of(k) * (TI + 1) + (r + 1)) * TJ + c];
+        fl = sFx[(slot_of(k) * (TI + 1) + r) * TJ + c];
+      }
+      const int fk = swap_xy(k);
+      if (fk != 4) {
+        gr = sGy[(slot_of(fk) * TI + r) * (TJ + 1) + (c + 1)];
+        gl = sGy[(slot_of(fk) * TI + r) * (TJ + 1) + c];
+      }
+      UL[g.at(k, i, j)] = -(inv_dx) * (fr - fl) - (inv_dy) * (gr - gl);
+    }
+  }
+
+  // CFL maxima and counters
+  smaxX = warp_max(smaxX);
+  smaxY = warp_max(smaxY);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) negc += __shfl_xor_sync(0xffffffffu, negc, o);
+  if (lane == 0) {
+    atomic_max_pos(&ctl->maxX, smaxX);
+    atomic_max_pos(&ctl->maxY, smaxY);
+    if (negc) atomicAdd(&ctl->neg_count, (unsigned long long)negc);
+  }
+}
+
+// ENO-LF dissipation coefficients (spatialmethodenolf.cpp:66-125):
+// alphaF[k][j] = max_i |lambda_k(U_ij)|, alphaG[k][i] = max_j |lambda_k(swap U_ij)|
+// over i in [1, nx+2), j in [1, ny+2) without the (i < 2 && j < 2) corner.
+// The arrays must be zero on entry.  Block = 32 (j) x 8 (i) cells.
+__global__ void __launch_bounds__(256)
+k_lf_alpha(Grid g, const double* __restrict__ U, double* alphaF, double* alphaG, Ctl* ctl) {
+  if (ctl->skip) return;
+  __shared__ double col[8][NF][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int j = 1 + blockIdx.x * 32 + tx, i = 1 + blockIdx.y * 8 + ty;
+  double lx[NF], ly[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) { lx[k] = 0.0; ly[k] = 0.0; }
+  const bool valid = (i < g.nx + 2) && (j < g.ny + 2) && !(i < 2 && j < 2);
+  int negp = 0;
+  if (valid) {
+    double q[NF], lam[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) q[k] = U[g.at(k, i, j)];
+    int np;
+    if (!eigenvalues_at(g.gamma, q, lam, np)) {
+      atomicExch(&ctl->error, 6);
+      atomicAdd(&ctl->negd_count, 1ull);
+    } else {
+      negp += np;
+#pragma unroll
+      for (int k = 0; k < NF; k++) lx[k] = fabs(lam[k]);
+      double s[NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++) s[k] = q[swap_xy(k)];
+      eigenvalues_at(g.gamma, s, lam, np);
+      negp += np;
+#pragma unroll
+      for (int k = 0; k < NF; k++) ly[k] = fabs(lam[k]);
+    }
+  }
+  // per-row (alphaG, over j = lanes) maxima
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    const double m = warp_max(ly[k]);
+    if (tx == 0 && i < g.nx + 2) atomic_max_pos(reinterpret_cast<unsigned long long*>(&alphaG[k * g.NX + i]), m);
+  }
+  // per-column (alphaF, over i = warps) maxima
+#pragma unroll
+  for (int k = 0; k < NF; k++) col[ty][k][tx] = lx[k];
+  __syncthreads();
+  if (ty == 0 && j < g.ny + 2) {
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      double m = 0.0;
+#pragma unroll
+      for (int r = 0; r < 8; r++) m = take_max(m, col[r][k][tx]);
+      atomic_max_pos(reinterpret_cast<unsigned long long*>(&alphaF[k * g.NY + j]), m);
+    }
+  }
+  (void)negp;
+}
+
+}  // namespace MHD_KNS
+}  // namespace mhd

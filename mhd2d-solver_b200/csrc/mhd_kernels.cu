@@ -1,0 +1,130 @@
+// Kernel instantiations and launchers.  Built twice from this one source:
+//   MHD_KSET = kExact  with -fmad=false  (bit-identical to the reference)
+//   MHD_KSET = kFast   with -fmad=true   (FMA contraction)
+#include "mhd_flux.cuh"
+#include "mhd_launch.h"
+#include "mhd_misc.cuh"
+
+#ifndef MHD_KSET
+#define MHD_KSET kExact
+#define MHD_KSET_NAME "exact"
+#endif
+
+namespace mhd {
+namespace MHD_KNS {
+
+constexpr int TI = 8, TJ = 32, NW = 6;
+using Geom = TileGeom<TI, TJ>;
+
+int grid1d(long long n, int block) {
+  long long b = (n + block - 1) / block;
+  if (b < 1) b = 1;
+  if (b > 148LL * 16) b = 148LL * 16;
+  return int(b);
+}
+
+void l_bc(const Grid& g, double* U, const double* const snap[4], const Ctl* ctl, cudaStream_t s) {
+  Snap d{snap[0], snap[1], snap[2], snap[3]};
+  const long long n = 4LL * NF * g.ny + 4LL * NF * g.nx;
+  k_bc<<<grid1d(n, 256), 256, 0, s>>>(g, U, d, ctl);
+}
+
+void l_snapshot(const Grid& g, const double* U, double* const snap[4], cudaStream_t s) {
+  const int m = g.nx > g.ny ? g.nx : g.ny;
+  k_snapshot<<<grid1d(NF * m, 256), 256, 0, s>>>(g, U, snap[0], snap[1], snap[2], snap[3]);
+}
+
+void l_lf_alpha(const Grid& g, const double* U, double* aF, double* aG, Ctl* ctl, cudaStream_t s) {
+  cudaMemsetAsync(aF, 0, sizeof(double) * NF * g.NY, s);
+  cudaMemsetAsync(aG, 0, sizeof(double) * NF * g.NX, s);
+  dim3 grid((g.ny + 1 + 31) / 32, (g.nx + 1 + 7) / 8);
+  k_lf_alpha<<<grid, 256, 0, s>>>(g, U, aF, aG, ctl);
+}
+
+template <int SCHEME, bool CHARS>
+void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const double* aG,
+            Ctl* ctl, double* const ch[4], cudaStream_t s) {
+  auto kern = k_flux<SCHEME, CHARS, TI, TJ, NW>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Geom::BYTES));
+    attr = true;
+  }
+  dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + TI - 1) / TI);
+  CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
+             ch ? ch[3] : nullptr};
+  kern<<<grid, NW * 32, Geom::BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, ctl, co);
+}
+
+void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
+            const double* aG, Ctl* ctl, double* const ch[4], cudaStream_t s) {
+  const bool chars = ch && ch[0];
+  if (scheme == 3) {
+    if (chars) flux_t<3, true>(g, U, UL, aF, aG, ctl, ch, s);
+    else flux_t<3, false>(g, U, UL, aF, aG, ctl, ch, s);
+  } else {
+    if (chars) flux_t<2, true>(g, U, UL, aF, aG, ctl, ch, s);
+    else flux_t<2, false>(g, U, UL, aF, aG, ctl, ch, s);
+  }
+}
+
+void l_combine(const Grid& g, int mode, double* U, double* U1, double* U2, const double* UL,
+               const Ctl* ctl, cudaStream_t s) {
+  dim3 grid((g.ny + 255) / 256, g.nx, NF);
+  k_combine<<<grid, 256, 0, s>>>(g, mode, U, U1, U2, UL, ctl);
+}
+
+void l_control(Ctl* ctl, double dx, double dy, double dt_min, double dt_max, double cfl,
+               int phase, double arg, cudaStream_t s) {
+  StepParams p{dx, dy, dt_min, dt_max, cfl};
+  k_control<<<1, 32, 0, s>>>(ctl, p, phase, arg);
+}
+
+void l_divb(const Grid& g, double* U, const int range[4], double* partial, int npartial,
+            Ctl* ctl, cudaStream_t s) {
+  const int m = g.nx > g.ny ? g.nx : g.ny;
+  k_divb_wrap<<<grid1d(4LL * m, 256), 256, 0, s>>>(g, U);
+  DivRange R{range[0], range[1], range[2], range[3]};
+  cudaMemsetAsync(&ctl->divb_max, 0, sizeof(unsigned long long), s);
+  const long long n = (long long)(R.x1 - R.x0) * (R.y1 - R.y0);
+  int nb = grid1d(n, 256);
+  if (nb > npartial) nb = npartial;
+  k_divb_reduce<<<nb, 256, 0, s>>>(g, U, R, partial, ctl);
+  k_divb_finish<<<1, 32, 0, s>>>(partial, nb, g.dx * g.dy, ctl);
+}
+
+void l_sor_sweep(const Grid& g, double* phi, const double* U, const int range[4],
+                 const double coef[6], double rtol, double max_sweeps, double* last_ratio,
+                 Ctl* ctl, cudaStream_t s) {
+  DivRange R{range[0], range[1], range[2], range[3]};
+  SorCoef c{coef[0], coef[1], coef[2], coef[3], coef[4], coef[5]};
+  const int q = (R.y1 + 3) / 4 + 1;
+  dim3 grid((q + 127) / 128, R.x1 - R.x0);
+  const int m = g.nx > g.ny ? g.nx : g.ny;
+  // ghosts are refreshed after each colour: with periodic sides they mirror
+  // points of the other colour (see k_sor_half)
+  k_sor_half<<<grid, 128, 0, s>>>(g, phi, U, R, c, 0, ctl);
+  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl);
+  k_sor_half<<<grid, 128, 0, s>>>(g, phi, U, R, c, 1, ctl);
+  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl);
+  k_sor_check<<<1, 32, 0, s>>>(ctl, rtol, max_sweeps, last_ratio);
+}
+
+void l_sor_correct(const Grid& g, double* U, const double* phi, const int range[4], double bxf,
+                   double byf, cudaStream_t s) {
+  DivRange R{range[0], range[1], range[2], range[3]};
+  const long long n = (long long)(R.x1 - R.x0 + 2) * (R.y1 - R.y0 + 2);
+  k_sor_correct<<<grid1d(n, 256), 256, 0, s>>>(g, U, phi, R, bxf, byf);
+}
+
+int l_smem() { return int(Geom::BYTES); }
+int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
+
+}  // namespace MHD_KNS
+
+using namespace MHD_KNS;
+extern const KernelSet MHD_KSET = {MHD_KSET_NAME, l_bc, l_snapshot, l_lf_alpha, l_flux,
+                                   l_combine, l_control, l_divb, l_sor_sweep, l_sor_correct,
+                                   l_smem, l_launches};
+
+}  // namespace mhd

@@ -1,0 +1,51 @@
+// Host-side launchers of the device kernels.  The kernel translation unit
+// is compiled twice: once with -fmad=false (bit-identical to the reference,
+// the default) and once with FMA contraction (MHD_FLAG_FAST_MATH); each
+// build exports one KernelSet.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mhd_common.cuh"
+
+namespace mhd {
+
+struct CharOut;
+struct Snap;
+struct StepParams;
+struct DivRange;
+struct SorCoef;
+
+struct KernelSet {
+  const char* name;
+  // boundary fill of U in place
+  void (*bc)(const Grid& g, double* U, const double* const snap[4], const Ctl* ctl,
+             cudaStream_t s);
+  void (*snapshot)(const Grid& g, const double* U, double* const snap[4], cudaStream_t s);
+  // ENO-LF dissipation (arrays zeroed here)
+  void (*lf_alpha)(const Grid& g, const double* U, double* aF, double* aG, Ctl* ctl,
+                   cudaStream_t s);
+  // fused spatial operator; chars: cx, cy, LUx, LUy or nulls
+  void (*flux)(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
+               const double* aG, Ctl* ctl, double* const chars[4], cudaStream_t s);
+  void (*combine)(const Grid& g, int mode, double* U, double* U1, double* U2, const double* UL,
+                  const Ctl* ctl, cudaStream_t s);
+  void (*control)(Ctl* ctl, double dx, double dy, double dt_min, double dt_max, double cfl,
+                  int phase, double arg, cudaStream_t s);
+  // div B: wrap periodic B ghosts, reduce max / sum over [x0,x1) x [y0,y1)
+  void (*divb)(const Grid& g, double* U, const int range[4], double* partial, int npartial,
+               Ctl* ctl, cudaStream_t s);
+  // one SOR sweep (both colours, potential ghosts, convergence check)
+  void (*sor_sweep)(const Grid& g, double* phi, const double* U, const int range[4],
+                    const double coef[6], double rtol, double max_sweeps, double* last_ratio,
+                    Ctl* ctl, cudaStream_t s);
+  void (*sor_correct)(const Grid& g, double* U, const double* phi, const int range[4],
+                      double bxf, double byf, cudaStream_t s);
+  int (*flux_smem_bytes)();
+  int (*launches_per_integrate)(int scheme);
+};
+
+extern const KernelSet kExact;
+extern const KernelSet kFast;
+
+}  // namespace mhd

@@ -1,0 +1,411 @@
+// Boundary fill, RK3 / Euler stage updates, the time-step controller and
+// the div-B kernels.  All arithmetic keeps the reference's association
+// order (the parity build uses -fmad=false).
+#pragma once
+
+#include "mhd_common.cuh"
+
+#ifndef MHD_KNS
+#define MHD_KNS exact
+#endif
+
+namespace mhd {
+namespace MHD_KNS {
+
+// ---------------------------------------------------------------------------
+// Ghost-cell fill, SpatialIntegrationMethod::applyBoundaryConditions
+// (spatialintegrationmethod.cpp:85-300).  The reference fills the sides in
+// the order left, right, bottom, top, each reading only interior cells or
+// its own freshly mirrored ghosts; every ghost value is therefore a function
+// of interior cells alone and all four sides are filled in one pass here.
+// Neumann adds the div B = 0 extrapolation of the normal field component
+// (lines 122-130, 174-182, 226-234, 278-286), written below in terms of the
+// interior cells its mirrored operands came from.  Corners are not touched.
+struct Snap {
+  const double *l, *r, *b, *t;  // Dirichlet edge snapshots [8][NY], [8][NX]
+};
+
+__global__ void k_bc(Grid g, double* __restrict__ U, Snap d, const Ctl* ctl) {
+  if (ctl->skip) return;
+  const int nx = g.nx, ny = g.ny;
+  const long long nlr = 2LL * 2 * NF * ny, nbt = 2LL * 2 * NF * nx;
+  const double rxy = g.dx / g.dy, ryx = g.dy / g.dx;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nlr + nbt;
+       e += (long long)gridDim.x * blockDim.x) {
+    if (e < nlr) {  // left / right: side, layer, field, row j (fastest)
+      const int j = 2 + int(e % ny);
+      long long q = e / ny;
+      const int k = int(q % NF); q /= NF;
+      const int gl = 1 + int(q % 2);
+      const int side = int(q / 2);  // 0 left, 1 right
+      const int b = g.bc[side];
+      if (side == 0) {
+        const int it = 2 - gl;
+        double v;
+        if (b == PERIODIC) v = U[g.at(k, nx + 2 - gl, j)];
+        else if (b == DIRICHLET) v = d.l[k * g.NY + j];
+        else v = U[g.at(k, 2 + gl, j)];
+        if (b == NEUMANN && k == 4 && j >= 3 && j < ny + 1) {
+          // it = 1: U4[1] = U4[3] - rxy*(U5[2][j-1] - U5[2][j+1])
+          // it = 0: U4[0] = U4[2] - rxy*(U5[1][j-1] - U5[1][j+1]), U5[1] mirrors U5[3]
+          const int s5 = (it == 1) ? 2 : 3;
+          v = U[g.at(4, it + 2, j)] - rxy * (U[g.at(5, s5, j - 1)] - U[g.at(5, s5, j + 1)]);
+        }
+        U[g.at(k, it, j)] = v;
+      } else {
+        const int it = nx + 1 + gl;
+        double v;
+        if (b == PERIODIC) v = U[g.at(k, 1 + gl, j)];
+        else if (b == DIRICHLET) v = d.r[k * g.NY + j];
+        else v = U[g.at(k, nx + 1 - gl, j)];
+        if (b == NEUMANN && k == 4 && j >= 3 && j < ny + 1) {
+          // it = nx+2: U4[nx]   - rxy*(U5[nx+1][j+1] - U5[nx+1][j-1])
+          // it = nx+3: U4[nx+1] - rxy*(U5[nx+2][j+1] - U5[nx+2][j-1]), U5[nx+2] mirrors U5[nx]
+          const int s5 = (it == nx + 2) ? nx + 1 : nx;
+          v = U[g.at(4, it - 2, j)] - rxy * (U[g.at(5, s5, j + 1)] - U[g.at(5, s5, j - 1)]);
+        }
+        U[g.at(k, it, j)] = v;
+      }
+    } else {  // bottom / top: side, field, column i, layer (fastest)
+      long long q = e - nlr;
+      const int gl = 1 + int(q % 2); q /= 2;
+      const int i = 2 + int(q % nx); q /= nx;
+      const int k = int(q % NF);
+      const int side = int(q / NF);  // 0 bottom, 1 top
+      const int b = g.bc[2 + side];
+      if (side == 0) {
+        const int jt = 2 - gl;
+        double v;
+        if (b == PERIODIC) v = U[g.at(k, i, ny + 2 - gl)];
+        else if (b == DIRICHLET) v = d.b[k * g.NX + i];
+        else v = U[g.at(k, i, 2 + gl)];
+        if (b == NEUMANN && k == 5 && i >= 3 && i < nx + 1) {
+          // jt = 1: U5[i][3] - ryx*(U4[i-1][2] - U4[i+1][2])
+          // jt = 0: U5[i][2] - ryx*(U4[i-1][1] - U4[i+1][1]), U4[.][1] mirrors U4[.][3]
+          const int s4 = (jt == 1) ? 2 : 3;
+          v = U[g.at(5, i, jt + 2)] - ryx * (U[g.at(4, i - 1, s4)] - U[g.at(4, i + 1, s4)]);
+        }
+        U[g.at(k, i, jt)] = v;
+      } else {
+        const int jt = ny + 1 + gl;
+        double v;
+        if (b == PERIODIC) v = U[g.at(k, i, 1 + gl)];
+        else if (b == DIRICHLET) v = d.t[k * g.NX + i];
+        else v = U[g.at(k, i, ny + 1 - gl)];
+        if (b == NEUMANN && k == 5 && i >= 3 && i < nx + 1) {
+          // jt = ny+2: U5[i][ny]   - ryx*(U4[i+1][ny+1] - U4[i-1][ny+1])
+          // jt = ny+3: U5[i][ny+1] - ryx*(U4[i+1][ny+2] - U4[i-1][ny+2]), U4[.][ny+2] mirrors U4[.][ny]
+          const int s4 = (jt == ny + 2) ? ny + 1 : ny;
+          v = U[g.at(5, i, jt - 2)] - ryx * (U[g.at(4, i + 1, s4)] - U[g.at(4, i - 1, s4)]);
+        }
+        U[g.at(k, i, jt)] = v;
+      }
+    }
+  }
+}
+
+// Dirichlet edge snapshot (spatialintegrationmethod.cpp:39-59).
+__global__ void k_snapshot(Grid g, const double* __restrict__ U, double* l, double* r, double* b,
+                           double* t) {
+  const int n = NF * (g.nx > g.ny ? g.nx : g.ny);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int m = g.nx > g.ny ? g.nx : g.ny;
+    const int k = e / m, p = 2 + e % m;
+    if (p < g.nx + 2) {
+      b[k * g.NX + p] = U[g.at(k, p, 2)];
+      t[k * g.NX + p] = U[g.at(k, p, g.ny + 1)];
+    }
+    if (p < g.ny + 2) {
+      l[k * g.NY + p] = U[g.at(k, 2, p)];
+      r[k * g.NY + p] = U[g.at(k, g.nx + 1, p)];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage updates on the interior (timeintegrationrk3.cpp:85-88, 108-111,
+// 131-134; timeintegrationeuler.cpp:55-58).  dt comes from the control block.
+//   mode 0: U  = U + dt*UL                           (Euler)
+//   mode 1: U1 = U + dt*UL
+//   mode 2: U2 = (3/4)U + (1/4)U1 + (1/4)dt*UL
+//   mode 3: U  = (1/3)U + (2/3)U2 + (2/3)dt*UL
+__global__ void k_combine(Grid g, int mode, double* __restrict__ U, double* __restrict__ U1,
+                          double* __restrict__ U2, const double* __restrict__ UL, const Ctl* ctl) {
+  if (ctl->skip) return;
+  const double dt = ctl->dt;
+  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = 2 + blockIdx.y;
+  const int k = blockIdx.z;
+  if (j >= g.ny + 2) return;
+  const long long a = g.at(k, i, j);
+  switch (mode) {
+    case 0: U[a] = U[a] + dt * UL[a]; break;
+    case 1: U1[a] = U[a] + dt * UL[a]; break;
+    case 2: U2[a] = (3.0 / 4.0) * U[a] + (1.0 / 4.0) * U1[a] + (1.0 / 4.0) * dt * UL[a]; break;
+    default: U[a] = (1.0 / 3.0) * U[a] + (2.0 / 3.0) * U2[a] + (2.0 / 3.0) * dt * UL[a]; break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Time-step control (timeintegrationmethod.cpp:35-90 and the retry logic of
+// timeintegrationrk3.cpp:48-156), one thread.
+struct StepParams {
+  double dx, dy, dt_min, dt_max, cfl;
+};
+
+// updateDt: returns the ReturnStatus value; 10 (WrongParameter) stands for
+// the inputs on which the reference's doubling / halving loops never end
+// (dt = 0 with a positive target, or a negative target).
+__device__ __forceinline__ int update_dt(const StepParams& p, double& cur, double ideal) {
+  if (p.cfl == 0.0) return 1;  // NoChange: constant time mode
+  double dt = cur;
+  int n = 0;
+  while (dt < 0.5 * p.cfl * ideal) {
+    dt *= 2.0;
+    if (++n > 4200) return 10;
+  }
+  n = 0;
+  while (dt > p.cfl * ideal) {
+    dt /= 2.0;
+    if (++n > 4200) return 10;
+  }
+  if (dt > p.dt_max) dt = p.dt_max;
+  if (dt < p.dt_min) return 4;  // ErrorTimeUnderflow
+  if (dt == cur) return 1;
+  cur = dt;
+  return 2;
+}
+
+__device__ __forceinline__ double min3(double a, double b, double c) {
+  double m = a;          // std::min({a, b, c}): the first smallest
+  if (b < m) m = b;
+  if (c < m) m = c;
+  return m;
+}
+
+
+__global__ void k_control(Ctl* c, StepParams p, int phase, double arg) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (phase == PH_RESET_STEP || phase == PH_RESET_INTEGRATE) {
+    c->skip = 0; c->retry = 0; c->error = 0; c->neg_last = 0; c->step_done = 0;
+    c->maxX = 0ull; c->maxY = 0ull;
+    c->neg_count = 0ull; c->negd_count = 0ull;
+    if (phase == PH_RESET_STEP) {
+      c->dt1 = arg; c->dt = arg; c->dt2 = p.dt_max; c->dt3 = p.dt_max;
+    }
+    return;
+  }
+  if (phase == PH_RK_RETRY) {
+    if (!c->retry || c->error) return;
+    c->skip = 0; c->retry = 0;
+    c->dt = min3(c->dt1, c->dt2, c->dt3);
+    return;
+  }
+  if (phase == PH_DONE) {
+    if (!c->skip && !c->error) c->step_done = 1;
+    return;
+  }
+  if (c->skip) return;
+  if (c->error) { c->skip = 1; return; }
+  const double ax = p.dx / bits_to_double(c->maxX), ay = p.dy / bits_to_double(c->maxY);
+  const double ideal = (ay < ax) ? ay : ax;  // std::min(a, b)
+  c->dtIdeal = ideal;
+  c->maxX = 0ull; c->maxY = 0ull;
+  int st = 1;
+  switch (phase) {
+    case PH_RK_FIRST:
+      st = update_dt(p, c->dt1, ideal);
+      if (st == 4 || st == 10) break;
+      c->dt = min3(c->dt1, c->dt2, c->dt3);
+      break;
+    case PH_RK_SECOND:
+      st = update_dt(p, c->dt2, ideal);
+      if (st == 4 || st == 10) break;
+      if (c->dt2 < c->dt) { c->retry = 1; c->skip = 1; }
+      break;
+    case PH_RK_FINAL:
+      st = update_dt(p, c->dt3, ideal);
+      if (st == 4 || st == 10) break;
+      if (c->dt3 < c->dt) { c->retry = 1; c->skip = 1; }
+      break;
+    case PH_EULER:
+      st = update_dt(p, c->dt, ideal);
+      break;
+    default:
+      break;
+  }
+  c->upd_status = st;
+  if (st == 4 || st == 10) { c->error = st; c->skip = 1; }
+}
+
+// ---------------------------------------------------------------------------
+// div B (div_b_fix.cpp).  Range [x0,x1) x [y0,y1): one cell in from every
+// non-periodic side; periodic sides first wrap the Bx, By ghost layers.
+struct DivRange {
+  int x0, x1, y0, y1;
+};
+
+__global__ void k_divb_wrap(Grid g, double* __restrict__ U) {
+  const int nx = g.nx, ny = g.ny;
+  const int n = 2 * 2 * (nx > ny ? nx : ny);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int m = nx > ny ? nx : ny;
+    const int k = 4 + (e / m) % 2, which = e / (2 * m), p = 2 + e % m;
+    if (which == 0 && p < ny + 2) {
+      if (g.bc[LEFT] == PERIODIC) {
+        U[g.at(k, 0, p)] = U[g.at(k, nx, p)];
+        U[g.at(k, 1, p)] = U[g.at(k, nx + 1, p)];
+      }
+      if (g.bc[RIGHT] == PERIODIC) {
+        U[g.at(k, nx + 2, p)] = U[g.at(k, 2, p)];
+        U[g.at(k, nx + 3, p)] = U[g.at(k, 3, p)];
+      }
+    }
+    if (which == 1 && p < nx + 2) {
+      if (g.bc[BOTTOM] == PERIODIC) {
+        U[g.at(k, p, 0)] = U[g.at(k, p, ny)];
+        U[g.at(k, p, 1)] = U[g.at(k, p, ny + 1)];
+      }
+      if (g.bc[TOP] == PERIODIC) {
+        U[g.at(k, p, ny + 2)] = U[g.at(k, p, 2)];
+        U[g.at(k, p, ny + 3)] = U[g.at(k, p, 3)];
+      }
+    }
+  }
+}
+
+// max and sum of |central div B|; sums go to per-block partials, reduced in
+// a fixed order by k_divb_finish so repeated runs give identical totals.
+__global__ void __launch_bounds__(256) k_divb_reduce(Grid g, const double* __restrict__ U,
+                                                     DivRange R, double* partial, Ctl* c) {
+  const int w = R.y1 - R.y0, h = R.x1 - R.x0;
+  const long long n = (long long)w * h;
+  double mx = 0.0, sum = 0.0;
+  const double d2x = 2.0 * g.dx, d2y = 2.0 * g.dy;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = R.x0 + int(e / w), j = R.y0 + int(e % w);
+    const double d = fabs((U[g.at(4, i + 1, j)] - U[g.at(4, i - 1, j)]) / d2x +
+                          (U[g.at(5, i, j + 1)] - U[g.at(5, i, j - 1)]) / d2y);
+    mx = take_max(mx, d);
+    sum += d;
+  }
+  __shared__ double sm[2][8];
+  mx = warp_max(mx);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sm[0][wid] = mx; sm[1][wid] = sum; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0, s = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) { m = take_max(m, sm[0][q]); s += sm[1][q]; }
+    partial[blockIdx.x] = s;
+    atomic_max_pos(&c->divb_max, m);
+  }
+}
+
+__global__ void k_divb_finish(double* partial, int nb, double dxdy, Ctl* c) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; b++) s += partial[b];
+  c->divb_sum = s * dxdy;
+}
+
+// One colour of a red-black sweep of the reference's SOR update
+// (div_b_fix.cpp:262-280).  The stride-2 Laplacian couples (i, j) only to
+// (i+-2, j) and (i, j+-2), so colour ((i>>1) + (j>>1)) & 1 makes every
+// point's neighbours the other colour: a half sweep updates its points in
+// any order with the same result.  Each thread owns one same-colour pair
+// j, j+1 (j even) of one row.
+struct SorCoef {
+  double pxf, pyf, bxf, byf, coef, omega;
+};
+
+__global__ void __launch_bounds__(256) k_sor_half(Grid g, double* __restrict__ phi,
+                                                  const double* __restrict__ U, DivRange R,
+                                                  SorCoef s, int color, Ctl* c) {
+  if (c->sor_done) return;
+  const int i = R.x0 + blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  // even column blocks jb = 2*(2q + b) with b chosen so the block has this colour
+  const int b = (color + (i >> 1)) & 1;
+  const int jb = 2 * (2 * q + b);
+  double rmax = 0.0, pmax = 0.0;
+  const long long P = g.pitch;
+  double* prow = phi + (long long)i * P + g.off;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int j = jb + t;
+    if (i < R.x1 && j >= R.y0 && j < R.y1) {
+      double r = s.pxf * (prow[j + 2 * P] + prow[j - 2 * P]);
+      r += s.pyf * (prow[j + 2] + prow[j - 2]);
+      r += s.bxf * (U[g.at(4, i + 1, j)] - U[g.at(4, i - 1, j)]);
+      r += s.byf * (U[g.at(5, i, j + 1)] - U[g.at(5, i, j - 1)]);
+      r *= s.coef;
+      r -= prow[j];
+      prow[j] += s.omega * r;
+      rmax = take_max(rmax, fabs(r));
+      pmax = take_max(pmax, fabs(prow[j]));
+    }
+  }
+  rmax = warp_max(rmax);
+  pmax = warp_max(pmax);
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_pos(&c->rmax, rmax);
+    atomic_max_pos(&c->pmax, pmax);
+  }
+}
+
+// Potential ghosts after each sweep (div_b_fix.cpp:282-364).
+__global__ void k_phi_bc(Grid g, double* __restrict__ phi, const Ctl* c) {
+  if (c->sor_done) return;
+  const int nx = g.nx, ny = g.ny, m = nx > ny ? nx : ny;
+  const long long P = g.pitch;
+  auto PH = [&](int i, int j) -> double& { return phi[(long long)i * P + g.off + j]; };
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 2 * m; e += gridDim.x * blockDim.x) {
+    const int which = e / m, p = 2 + e % m;
+    if (which == 0 && p < ny + 2) {
+      if (g.bc[LEFT] == PERIODIC) { PH(0, p) = PH(nx, p); PH(1, p) = PH(nx + 1, p); }
+      else if (g.bc[LEFT] == OPEN) PH(1, p) = PH(2, p);
+      if (g.bc[RIGHT] == PERIODIC) { PH(nx + 2, p) = PH(2, p); PH(nx + 3, p) = PH(3, p); }
+      else if (g.bc[RIGHT] == OPEN) PH(nx + 2, p) = PH(nx + 1, p);
+    }
+    if (which == 1 && p < nx + 2) {
+      if (g.bc[BOTTOM] == PERIODIC) { PH(p, 0) = PH(p, ny); PH(p, 1) = PH(p, ny + 1); }
+      else if (g.bc[BOTTOM] == OPEN) PH(p, 1) = PH(p, 2);
+      if (g.bc[TOP] == PERIODIC) { PH(p, ny + 2) = PH(p, 2); PH(p, ny + 3) = PH(p, 3); }
+      else if (g.bc[TOP] == OPEN) PH(p, ny + 2) = PH(p, ny + 1);
+    }
+  }
+}
+
+// Convergence test after a sweep (div_b_fix.cpp:370-373): stop when
+// max|update| / max|phi| <= rmax.  The ratio of the last sweep is kept for
+// the final verdict, which the host evaluates as the reference does.
+__global__ void k_sor_check(Ctl* c, double rtol, double max_sweeps, double* last_ratio) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || c->sor_done) return;
+  const double ratio = bits_to_double(c->rmax) / bits_to_double(c->pmax);
+  *last_ratio = ratio;
+  c->rmax = 0ull; c->pmax = 0ull;
+  c->sor_sweeps += 1;
+  if (ratio <= rtol || c->sor_sweeps >= max_sweeps) c->sor_done = 1;
+}
+
+// B += central gradient of phi over [x0-1, x1+1) x [y0-1, y1+1)
+// (div_b_fix.cpp:392-399).
+__global__ void k_sor_correct(Grid g, double* __restrict__ U, const double* __restrict__ phi,
+                              DivRange R, double bxf, double byf) {
+  const int w = R.y1 - R.y0 + 2, h = R.x1 - R.x0 + 2;
+  const long long P = g.pitch;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)w * h;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = R.x0 - 1 + int(e / w), j = R.y0 - 1 + int(e % w);
+    const double* pr = phi + (long long)i * P + g.off;
+    U[g.at(4, i, j)] += (pr[j + P] - pr[j - P]) * bxf;
+    U[g.at(5, i, j)] += (pr[j + 1] - pr[j - 1]) * byf;
+  }
+}
+
+}  // namespace MHD_KNS
+}  // namespace mhd

@@ -33,6 +33,7 @@ struct orc_ctx {
    double *aF, *aG;           /* ENO-LF dissipation [8][NY] / [8][NX] */
    double *U1, *U2, *UL;      /* time-stepper stages */
    double *phi;               /* SOR potential, persists across solves */
+   long long retries;         /* RK3 stage restarts taken so far */
 };
 
 enum { L = 0, R = 1, B = 2, T = 3 };
@@ -609,7 +610,7 @@ int orc_step( orc_ctx* c, double* U, double* dt_inout, int* is_error )
          if( *is_error ) return st;
          st = orc_update_dt( c->dt_min, c->dt_max, c->cfl, &d2, ideal, is_error );
          if( *is_error ) return st;
-         if( d2 < dt ) continue;
+         if( d2 < dt ){ c->retries++; continue; }
          for( k = 0; k < NF; k++ ) for( i = 2; i < nx+2; i++ ) for( j = 2; j < ny+2; j++ )
             AT(c->U2,k,i,j) = (3.0/4.0)*AT(U,k,i,j) + (1.0/4.0)*AT(c->U1,k,i,j)
                             + (1.0/4.0)*dt*AT(c->UL,k,i,j);
@@ -617,7 +618,7 @@ int orc_step( orc_ctx* c, double* U, double* dt_inout, int* is_error )
          if( *is_error ) return st;
          st = orc_update_dt( c->dt_min, c->dt_max, c->cfl, &d3, ideal, is_error );
          if( *is_error ) return st;
-         if( d3 < dt ) continue;
+         if( d3 < dt ){ c->retries++; continue; }
          for( k = 0; k < NF; k++ ) for( i = 2; i < nx+2; i++ ) for( j = 2; j < ny+2; j++ )
             AT(U,k,i,j) = (1.0/3.0)*AT(U,k,i,j) + (2.0/3.0)*AT(c->U2,k,i,j)
                         + (2.0/3.0)*dt*AT(c->UL,k,i,j);
@@ -715,6 +716,11 @@ int orc_divb_sor( orc_ctx* c, const orc_sor_params* sp, double* U, int red_black
             if( fabs(r) > rmax ) rmax = fabs(r);
             if( fabs(PHI(i,j)) > pmax ) pmax = fabs(PHI(i,j));
          }
+         /* Red-black: refresh the ghost copies after each colour.  With
+            periodic sides the ghosts mirror points of the other colour, and
+            one refresh per sweep would feed the second colour stale values
+            across the seam (that mixed ordering diverges for omega >= 1.5). */
+         if( red_black && pass == 0 ) phi_bc( c );
       }
       phi_bc( c );
       if( rmax/pmax <= sp->sor_rmax ){ done = 1; break; }
@@ -731,6 +737,8 @@ int orc_divb_sor( orc_ctx* c, const orc_sor_params* sp, double* U, int red_black
    *is_error = 0;
    return ORC_OK;
 }
+
+long long orc_retries( const orc_ctx* c ){ return c->retries; }
 
 /* main.cpp:174-344 without output (see ref_harness.cpp: ref_run). */
 int orc_run( orc_ctx* c, int nsteps, double t_max, const orc_sor_params* sor, int red_black,

@@ -79,6 +79,9 @@ int  orc_run( orc_ctx* c, int nsteps, double t_max, const orc_sor_params* sor, i
               double* U, double* dt_inout, double* t_inout, int* steps_done,
               double* dt_hist, double* divb_hist, int hist_len, int* is_error );
 
+/* Number of RK3 stage restarts (dt retries) this context has taken. */
+long long orc_retries( const orc_ctx* c );
+
 /* Single-interface and single-cell kernels, exposed for unit tests. */
 int  orc_eigens_f( double gamma, const double* U1, const double* U2, double* lambda,
                    double* lv, double* rv, int* neg_pressure );

@@ -82,6 +82,8 @@ def load_oracle():
                             _dp, _dp, _dp, _ip, _dp, _dp, C.c_int, _ip]
     lib.orc_eigens_f.argtypes = [C.c_double, _dp, _dp, _dp, _dp, _dp, _ip]
     lib.orc_eigenvalues_at.argtypes = [C.c_double, _dp, _dp, _ip]
+    lib.orc_retries.argtypes = [C.c_void_p]
+    lib.orc_retries.restype = C.c_longlong
     return lib
 
 
@@ -139,6 +141,9 @@ class Oracle:
         e = C.c_int(0)
         st = self.lib.orc_apply_bc(self.ctx, _p(U), C.byref(e))
         return st, e.value
+
+    def retries(self):
+        return int(self.lib.orc_retries(self.ctx))
 
     def integrate(self, U, UL=None):
         UL = np.zeros(self.shape()) if UL is None else UL

@@ -271,18 +271,18 @@ int ref_run( int scheme, int time_method, int nx, int ny, double dx, double dy, 
 } // extern "C"
 
 #ifdef MHDREF_BENCH_MAIN
-/* CPU baseline driver: the reference RK3 + ENO scheme on the Orszag-Tang
-   vortex (initial state as in file_access.cpp:578-613 with gamma = 5/3),
-   periodic on all sides, fixed dt (the constant-time mode), for a given
-   number of steps.  Prints one line: "<cells> <steps> <seconds>". */
+/* CPU baseline driver: the reference TimeIntegrationRK3 + SpatialMethodEnoRoe
+   / EnoLF on the Orszag-Tang vortex (initial state as in
+   file_access.cpp:578-613, gamma = 5/3), periodic on all sides, CFL-controlled
+   dt (cfl 0.4, dt_max 0.03125), for `steps` steps.  Prints one line per step:
+   "step <k> <seconds> <dt>", then "cells <n*n>". */
 #include <cstdlib>
 int main( int argc, char** argv ){
    if( argc < 4 ){
-      std::fprintf( stderr, "usage: %s n steps scheme(2=roe,3=lf) [dt]\n", argv[0] );
+      std::fprintf( stderr, "usage: %s n steps scheme(2=roe,3=lf)\n", argv[0] );
       return 2;
    }
    const int n = std::atoi( argv[1] ), steps = std::atoi( argv[2] ), scheme = std::atoi( argv[3] );
-   const double dtc = argc > 4 ? std::atof( argv[4] ) : 1.0/4096.0;
    const int NXt = n+4, NYt = n+4;
    const double gam = 5.0/3.0, L = 2.0*M_PI, dx = L/n, dy = L/n;
    std::vector<double> U( size_t(PRB_DIM)*NXt*NYt, 0.0 );
@@ -296,13 +296,30 @@ int main( int argc, char** argv ){
       at(7,i,j) = p/(gam-1.0) + 0.5*r*(u*u+v*v+w*w) + 0.5*(bx*bx+by*by+bz*bz);
    }
    const int bc[4] = { 1, 1, 1, 1 };
-   double dt = dtc, t = 0.0; int done = 0, err = 0; char msg[256];
-   auto t0 = std::chrono::steady_clock::now();
-   ref_run( scheme, 2, n, n, dx, dy, gam, bc, 0.0, dtc, 0.0, steps, 0.0, nullptr,
-            U.data(), &dt, &t, &done, nullptr, nullptr, 0, nullptr, nullptr, nullptr, nullptr,
-            &err, msg, sizeof msg );
-   std::chrono::duration<double> el = std::chrono::steady_clock::now() - t0;
-   std::printf( "%lld %d %.6f\n", (long long)n*n, done, el.count() );
-   return err;
+   auto method = makeMethod( scheme, n, n, dx, dy, gam, bc );
+   MatView vU( U.data(), PRB_DIM, NXt, NYt );
+   method->initializeDirichletBoundaries( vU.m() );
+   TimeIntegrationRK3 stepper( n, n, 2, 1e-9, 0.03125, 0.4, std::move( method ) );
+   const size_t tot = size_t(PRB_DIM)*NXt*NYt;
+   std::vector<double> cx( tot ), cy( tot ), lx( tot ), ly( tot );
+   MatView vcx( cx.data(), PRB_DIM, NXt, NYt ), vcy( cy.data(), PRB_DIM, NXt, NYt );
+   MatView vlx( lx.data(), PRB_DIM, NXt, NYt ), vly( ly.data(), PRB_DIM, NXt, NYt );
+   // the stepper blends these (timeintegrationrk3.cpp:136-145) although nothing reads them
+   std::vector<double> bfl( size_t(PRB_DIM)*NYt ), bfr( size_t(PRB_DIM)*NYt );
+   std::vector<double> bfu( size_t(PRB_DIM)*NXt ), bfd( size_t(PRB_DIM)*NXt );
+   VecView l( bfl.data(), PRB_DIM, NYt ), r( bfr.data(), PRB_DIM, NYt );
+   VecView u( bfu.data(), PRB_DIM, NXt ), d( bfd.data(), PRB_DIM, NXt );
+   borderVectors bf{ l.v(), r.v(), u.v(), d.v() };
+   double dt = 0.03125;
+   for( int s = 0; s < steps; s++ ){
+      auto t0 = std::chrono::steady_clock::now();
+      t_status st = stepper.step( vU.m(), vcx.m(), vcy.m(), vlx.m(), vly.m(), bf, dt );
+      std::chrono::duration<double> el = std::chrono::steady_clock::now() - t0;
+      if( st.isError ){ std::fprintf( stderr, "step failed: %s\n", st.message.c_str() ); return 1; }
+      std::printf( "step %d %.6f %.10g\n", s, el.count(), dt );
+      std::fflush( stdout );
+   }
+   std::printf( "cells %lld\n", (long long)n*n );
+   return 0;
 }
 #endif

@@ -1,0 +1,253 @@
+"""Parity of the CUDA hot path (libmhd2d_b200.so, parity build) with the
+reference, through the C ABI.
+
+* golden vectors (outputs of the unmodified reference): bit for bit;
+* the oracle at other sizes / boundary mixes (partial tiles, several tiles):
+  bit for bit — the parity build keeps the reference's association order
+  and compiles without FMA contraction;
+* red-black SOR: bit for bit against the oracle's red-black ordering, and
+  the same max|div B| level as the reference's lexicographic sweep;
+* full-size grids: sub-window parity (cells farther than the stencil reach
+  from a window edge depend only on the window) and conservation.
+The only tolerance used is for quantities the reference sums sequentially
+(the integral of |div B|): relative 1e-12.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import mhd2d_b200 as M
+from mhd2d_b200 import problems as P
+from gpu_helpers import gpu_run, interior, make_ctx, same
+from pyoracle import Oracle, SorParams
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _gold(prefix):
+    return sorted(glob.glob(os.path.join(GOLD, prefix + "*.npz")))
+
+
+def _problem(d):
+    U = d["U_in"].copy()
+    return P.Problem(U, float(d["dx"]), float(d["dy"]), float(d.get("gamma", 5.0 / 3.0)),
+                     tuple(int(b) for b in d["bc"]))
+
+
+@pytest.mark.parametrize("path", _gold("integrate_"), ids=os.path.basename)
+def test_integrate_golden_bitwise(path):
+    d = np.load(path)
+    p = _problem(d)
+    ctx = make_ctx(p, scheme=int(d["scheme"]))
+    U = p.U.copy()
+    st, UL, ideal = ctx.integrate_host(U)
+    assert st.status == int(d["status"]) and int(st.isError) == int(d["is_error"])
+    if st.isError:
+        return
+    assert same(U, d["U_out"]), "boundary fill differs"
+    assert same(interior(UL), interior(d["UL"]))
+    assert ideal == float(d["dtIdeal"])
+    cx, cy, LUx, LUy = ctx.characteristics()
+    for name, a in (("cx", cx), ("cy", cy), ("LUx", LUx), ("LUy", LUy)):
+        assert same(a, d[name]), name
+
+
+@pytest.mark.parametrize("path", _gold("run_"), ids=os.path.basename)
+def test_run_golden(path):
+    """Whole main-loop runs.  Without SOR the device result equals the
+    reference bit for bit; with SOR the device's red-black ordering equals
+    the oracle's red-black run bit for bit and meets the same div B level."""
+    d = np.load(path)
+    p = _problem(d)
+    sp = None
+    if d["sor"].size:
+        v = d["sor"]
+        sp = M.SorParams(int(v[0]), int(v[1]), float(v[2]), float(v[3]), float(v[4]), int(v[5]),
+                         float(v[6]))
+    ctx = make_ctx(p, scheme=int(d["scheme"]), time_method=int(d["time_method"]),
+                   dt_min=float(d["dt_min"]), dt_max=float(d["dt_max"]), cfl=float(d["cfl"]),
+                   flags=0)
+    r = gpu_run(ctx, float(d["dt0"]), nsteps=int(d["nsteps"]), t_max=float(d["t_max"]), sor=sp)
+    U = ctx.download()
+    assert r["status"] == int(d["status"]) and r["steps"] == int(d["steps"])
+    assert same(r["dt_hist"], d["dt_hist"])
+    if sp is None:
+        assert same(U, d["U_out"])
+        return
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=int(d["scheme"]),
+               time_method=int(d["time_method"]), dt_min=float(d["dt_min"]),
+               dt_max=float(d["dt_max"]), cfl=float(d["cfl"]))
+    Uo = p.U.copy()
+    osp = SorParams(*[f for f in (sp.divb_skip_steps, sp.sor_steps, sp.sor_rsteps, sp.sor_rmax,
+                                  sp.sor_divbmax, sp.omega_use_static, sp.omega)])
+    q = o.run(Uo, float(d["dt0"]), nsteps=int(d["nsteps"]), sor=osp, red_black=1, hist_len=256)
+    assert same(U, Uo)
+    assert same(r["divb_hist"], q["divb_hist"])
+    # reference (lexicographic) and device (red-black) both clean to divbmax
+    assert np.all(r["divb_hist"] < float(d["sor"][4])) and np.all(d["divb_hist"] < float(d["sor"][4]))
+    assert np.max(np.abs(U - d["U_out"])) < 1e-6 * np.max(np.abs(d["U_out"]))
+
+
+SIZES = [(37, 45), (8, 33), (70, 9), (64, 64), (33, 31)]
+BCS = [(1, 1, 1, 1), (3, 3, 3, 3), (4, 4, 4, 4), (2, 2, 2, 2), (4, 1, 3, 2)]
+
+
+@pytest.mark.parametrize("scheme", [M.ENO_ROE, M.ENO_LF])
+@pytest.mark.parametrize("case", range(len(SIZES)))
+def test_integrate_vs_oracle_tiles(scheme, case):
+    nx, ny = SIZES[case]
+    bc = BCS[case]
+    for mk in (P.random_smooth, P.random_blocky):
+        p = mk(nx, ny, seed=7 * case + scheme, bc=bc)
+        ctx = make_ctx(p, scheme=scheme)
+        U = p.U.copy()
+        st, UL, ideal = ctx.integrate_host(U)
+        o = Oracle(nx, ny, p.dx, p.dy, p.gamma, bc, scheme=scheme)
+        o.init_dirichlet(p.U.copy())
+        Uo = p.U.copy()
+        so, eo, ULo, io = o.integrate(Uo)
+        assert (st.status, int(st.isError)) == (so, eo)
+        assert same(U, Uo) and same(interior(UL), interior(ULo)) and ideal == io
+        for a, b in zip(ctx.characteristics(), o.characteristics()):
+            assert same(a, b)
+
+
+@pytest.mark.parametrize("scheme,tm", [(M.ENO_ROE, M.RK3), (M.ENO_LF, M.RK3), (M.ENO_ROE, M.EULER)])
+def test_steps_vs_oracle_ot128(scheme, tm):
+    p = P.ot_vortex(128)
+    ctx = make_ctx(p, scheme=scheme, time_method=tm, dt_min=1e-7, dt_max=1.0 / 64, cfl=0.4, flags=0)
+    st, dt, dts = ctx.steps(4, 1.0 / 64, record=True)
+    assert not st.isError
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=scheme, time_method=tm,
+               dt_min=1e-7, dt_max=1.0 / 64, cfl=0.4)
+    Uo = p.U.copy()
+    r = o.run(Uo, 1.0 / 64, nsteps=4, hist_len=4)
+    assert same(dts, r["dt_hist"])
+    assert same(ctx.download(), Uo)
+
+
+def test_retry_path_matches_reference():
+    d = np.load(os.path.join(GOLD, "run_explosion_retry.npz"))
+    p = _problem(d)
+    ctx = make_ctx(p, dt_min=float(d["dt_min"]), dt_max=float(d["dt_max"]), cfl=float(d["cfl"]),
+                   flags=0)
+    r = gpu_run(ctx, float(d["dt0"]), nsteps=int(d["nsteps"]))
+    assert same(ctx.download(), d["U_out"]) and same(r["dt_hist"], d["dt_hist"])
+
+
+@pytest.mark.parametrize("bc", [(1, 1, 1, 1), (3, 3, 1, 1), (4, 4, 4, 4), (2, 3, 4, 1)])
+def test_sor_red_black_vs_oracle(bc):
+    p = P.random_smooth(40, 36, seed=sum(bc), bc=bc)
+    sp = M.sor_params(1, 5, 20000, 1e-10, 1e-10, True, 1.7)
+    ctx = make_ctx(p, flags=0)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, bc)
+    osp = SorParams(1, 5, 20000.0, 1e-10, 1e-10, 1, 1.7)
+    Uo = p.U.copy()
+    for _ in range(2):  # the second call warm-starts from the kept potential
+        st, sweeps = ctx.divb_sor(sp)
+        so, eo, swo = o.divb_sor(Uo, osp, red_black=1)
+        assert (st.status, int(st.isError), sweeps) == (so, eo, swo)
+        assert same(ctx.download(), Uo)
+
+
+def test_divb_calc_vs_oracle():
+    p = P.random_blocky(50, 41, seed=3, bc=(1, 1, 3, 4))
+    ctx = make_ctx(p, flags=0)
+    m, t = ctx.divb_calc()
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc)
+    U = p.U.copy()
+    mo, to = o.divb_calc(U)
+    assert m == mo
+    assert abs(t - to) <= 1e-12 * abs(to)
+    assert same(ctx.download(), U)  # periodic B ghosts filled the same way
+
+
+def test_error_paths():
+    d = np.load(os.path.join(GOLD, "integrate_negdensity_2.npz"))
+    p = _problem(d)
+    ctx = make_ctx(p)
+    st, _ = ctx.step(0.01)
+    assert st.status == M.ERR_NEGATIVE_DENSITY and st.isError
+    # dt below dt_min -> ErrorTimeUnderflow, state untouched past stage 1
+    p = P.ot_vortex(32)
+    ctx = make_ctx(p, dt_min=0.5, dt_max=1.0, cfl=0.4)
+    st, _ = ctx.step(1.0)
+    assert st.status == M.ERR_TIME_UNDERFLOW and st.isError
+    # Dirichlet without a snapshot
+    p = P.random_smooth(16, 16, seed=1, bc=(2, 2, 2, 2))
+    c = M.Context(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc)
+    c.upload(p.U)
+    st, _ = c.integrate()
+    assert st.status == M.ERR_WRONG_PARAMETER and st.isError
+    # SOR that cannot converge in one sweep
+    p = P.random_smooth(24, 20, seed=2, bc=(3, 3, 3, 3))
+    ctx = make_ctx(p)
+    st, sw = ctx.divb_sor(M.sor_params(1, 1, 1, 1e-14, 1e-14))
+    assert st.status == M.ERR_NOT_CONVERGED and st.isError and sw == 1
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_full_size_window_parity(seed):
+    """4096^2 Orszag-Tang, one constant-dt RK3 step on the device; random
+    96x96 windows re-run on the oracle agree bit for bit on the cells at
+    least 9 cells (3 stages x 3-cell reach) from the window edge."""
+    n = 4096
+    p = P.ot_vortex(n)
+    dt = 1.0 / 4096
+    ctx = make_ctx(p, dt_max=dt, cfl=0.0, flags=0)
+    st, dt_out = ctx.step(dt)
+    assert not st.isError and dt_out == dt
+    U = ctx.download()
+    rng = np.random.default_rng(seed)
+    w, m = 96, 9
+    for _ in range(3):
+        i0, j0 = (int(v) for v in rng.integers(0, n - w, size=2))
+        win = np.zeros((8, w + 4, w + 4))
+        win[:, 2:-2, 2:-2] = p.U[:, 2 + i0:2 + i0 + w, 2 + j0:2 + j0 + w]
+        o = Oracle(w, w, p.dx, p.dy, p.gamma, (3, 3, 3, 3), dt_max=dt, cfl=0.0)
+        o.init_dirichlet(win)
+        st_o, err, _ = o.step(win, dt)
+        assert not err
+        a = win[:, 2 + m:2 + w - m, 2 + m:2 + w - m]
+        b = U[:, 2 + i0 + m:2 + i0 + w - m, 2 + j0 + m:2 + j0 + w - m]
+        assert same(a, b)
+
+
+def test_full_size_conservation():
+    """Periodic 4096^2: the flux form telescopes, so sum(UL) vanishes up to
+    the rounding of the sum itself."""
+    p = P.ot_vortex(4096)
+    ctx = make_ctx(p, flags=0)
+    st, ideal = ctx.integrate()
+    assert not st.isError and 0 < ideal < 1
+    UL = interior(ctx.download_ul())
+    for k in range(8):
+        tot = np.sum(UL[k])
+        scale = np.sum(np.abs(UL[k])) + 1e-300
+        assert abs(tot) <= 1e-11 * scale, (k, tot, scale)
+
+
+def test_plugin_interface_like_reference():
+    """Drive the device through the reference-shaped classes, as main.cpp
+    does (method -> initializeDirichletBoundaries -> stepper -> step)."""
+    p = P.brio_wu(64, 8)
+    method = M.SpatialMethodEnoRoe(p.nx, p.ny, 2, p.dx, p.dy, p.bc, p.gamma)
+    method.initializeDirichletBoundaries(p.U)
+    stepper = M.TimeIntegrationRK3(p.nx, p.ny, 2, 1e-6, 0.0078125, 0.4, method)
+    U = p.U.copy()
+    shape = U.shape
+    cx, cy, LUx, LUy = (np.zeros(shape) for _ in range(4))
+    dt, t = 0.0078125, 0.0
+    for _ in range(5):
+        st, dt = stepper.step(U, cx, cy, LUx, LUy, None, dt)
+        assert not st.isError
+        t += dt
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-6, dt_max=0.0078125, cfl=0.4)
+    Uo = p.U.copy()
+    o.run(Uo, 0.0078125, nsteps=5)
+    assert same(U, Uo)
+    ocx, ocy, oLx, oLy = o.characteristics()
+    assert same(cx, ocx) and same(LUy, oLy)
