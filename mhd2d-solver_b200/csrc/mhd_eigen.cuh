@@ -106,6 +106,20 @@ __device__ __forceinline__ bool midpoint(double gm, const double* U1, const doub
   return true;
 }
 
+// Makes the midpoint scalars opaque to the optimiser at the top of each
+// characteristic iteration (an empty asm that "may modify" them, no
+// instruction emitted).  Without it the compiler hoists every row's
+// coefficient products out of the loop, which needs far more registers
+// than one row at a time and ends in local-memory spills.
+__device__ __forceinline__ void opaque(Mid& e) {
+  asm volatile("" : "+d"(e.u), "+d"(e.v), "+d"(e.w), "+d"(e.uu), "+d"(e.a2), "+d"(e.a),
+                    "+d"(e.ca), "+d"(e.cs), "+d"(e.cs2), "+d"(e.cf), "+d"(e.cf2), "+d"(e.rr),
+                    "+d"(e.sbx));
+  asm volatile("" : "+d"(e.af), "+d"(e.as), "+d"(e.af2), "+d"(e.as2), "+d"(e.bty), "+d"(e.btz),
+                    "+d"(e.th1), "+d"(e.th2), "+d"(e.g1), "+d"(e.g21), "+d"(e.vb), "+d"(e.fcf),
+                    "+d"(e.fcs));
+}
+
 __device__ __forceinline__ double eigenvalue(const Mid& e, int k) {
   switch (k) {
     case 0: return e.u - e.cf;

@@ -52,9 +52,9 @@ struct TileGeom {
   static constexpr int OFF_U = 0;
   static constexpr int OFF_F = OFF_U + NF * RU * CU;       // sF[7][RU][TJ]
   static constexpr int OFF_G = OFF_F + 7 * RU * TJ;        // sG[7][TI][CU], slots in y frame order
-  static constexpr int OFF_FX = OFF_G + 7 * TI * CU;       // sFx[7][TI+1][TJ]
-  static constexpr int OFF_GY = OFF_FX + 7 * (TI + 1) * TJ;  // sGy[7][TI][TJ+1], y frame order
-  static constexpr int TOTAL = OFF_GY + 7 * TI * (TJ + 1);
+  static constexpr int OFF_FX = OFF_G + 7 * TI * CU;       // sFx[8][TI+1][TJ]
+  static constexpr int OFF_GY = OFF_FX + 8 * (TI + 1) * TJ;  // sGy[8][TI][TJ+1], y frame order
+  static constexpr int TOTAL = OFF_GY + 8 * TI * (TJ + 1);
   static constexpr size_t BYTES = size_t(TOTAL) * sizeof(double);
 };
 
@@ -102,18 +102,29 @@ struct Lane {
   int qplane, qstep;
   bool swp;          // y interface: x/y roles swapped
   int l1, l2;        // stencil points of U1 / U2 (1 / 2, or open-boundary substitutes)
-  __device__ __forceinline__ double F(int m, int l) const { return f[slot_of(m) * fplane + l * fstep]; }
+  // component 4 of a frame flux is identically zero (F[4], G[5]) and not stored
+  __device__ __forceinline__ double F(int m, int l) const {
+    return m == 4 ? 0.0 : f[slot_of(m) * fplane + l * fstep];
+  }
   __device__ __forceinline__ double Q(int k, int l) const {
     return q[(swp ? swap_xy(k) : k) * qplane + l * qstep];
   }
 };
 
-// Numerical flux of one interface in the lane's frame.  Fn gets the 7
-// non-zero components (slot order), lam / LU the characteristic outputs.
-template <int SCHEME, bool CHARS>
+// Numerical flux of one interface in the lane's frame: Fn[m], m = 0..7 (Fn[4]
+// is the structurally zero component), lam / LU the characteristic outputs.
+//
+// DENSE = false, the fast form: characteristics 0..6 only, structurally
+// zero products skipped.  Skipping a product 0*x changes nothing while every
+// x is finite; *nonfinite reports a characteristic flux that is not (the
+// reference's 0*inf, 0*NaN would then turn "zero" components into NaN).
+// DENSE = true performs every product of the reference's dense 8x8 loops,
+// the dummy wave 7 included, and so reproduces its NaN / inf propagation
+// exactly; the kernel recomputes flagged interfaces this way.
+template <int SCHEME, bool CHARS, bool DENSE>
 __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const double* alpha,
                                                double* Fn, double& smax, int& negp,
-                                               double* lam, double* LU) {
+                                               double* lam, double* LU, bool& nonfinite) {
   double U1[NF], U2[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
@@ -131,31 +142,35 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
     smax = take_max(smax, fabs(lk));
   }
 #pragma unroll
-  for (int s = 0; s < 7; s++) Fn[s] = 0.0;
+  for (int m = 0; m < NF; m++) Fn[m] = 0.0;
 
+  constexpr int KN = DENSE ? 8 : 7;
 #pragma unroll 1
-  for (int k = 0; k < 7; k++) {
+  for (int k = 0; k < KN; k++) {
+    opaque(e);
     double l[NF];
+    if (DENSE) {
+#pragma unroll
+      for (int m = 0; m < NF; m++) l[m] = 0.0;
+    }
     lv_row(e, k, l);
-    const unsigned lm = lv_mask(k);
+    const unsigned lm = DENSE ? 0xFFu : lv_mask(k);
     double fw;
     if (SCHEME == 2) {  // ENO-Roe: project F and its undivided differences
-      double w[4], vw[3];
+      // w = lv.F at the 4 points, Vw = lv.(F[p+1] - F[p]) at 3 points; each
+      // sum runs over m in ascending order, like the reference's loops
+      double w[4] = {0.0, 0.0, 0.0, 0.0}, vw[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-      for (int p = 0; p < 4; p++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int m = 0; m < NF; m++)
-          if (lm & (1u << m)) acc += l[m] * L.F(m, p);
-        w[p] = acc;
-      }
-#pragma unroll
-      for (int p = 0; p < 3; p++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int m = 0; m < NF; m++)
-          if (lm & (1u << m)) acc += l[m] * (L.F(m, p + 1) - L.F(m, p));
-        vw[p] = acc;
+      for (int m = 0; m < NF; m++) {
+        if (!(lm & (1u << m))) continue;
+        const double f0 = L.F(m, 0), f1 = L.F(m, 1), f2 = L.F(m, 2), f3 = L.F(m, 3);
+        w[0] += l[m] * f0;
+        w[1] += l[m] * f1;
+        w[2] += l[m] * f2;
+        w[3] += l[m] * f3;
+        vw[0] += l[m] * (f1 - f0);
+        vw[1] += l[m] * (f2 - f1);
+        vw[2] += l[m] * (f3 - f2);
       }
       const double wm = eno_minus(w[0], w[1], w[2], vw[0], vw[1]);
       const double wp = eno_plus(w[1], w[2], w[3], vw[1], vw[2]);
@@ -186,6 +201,7 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
       fw = wm + wp;
       if (CHARS) LU[k] = ru[1];
     }
+    if (!DENSE && !isfinite(fw)) nonfinite = true;
     if (CHARS && SCHEME == 2) {
       double acc = 0.0;
 #pragma unroll
@@ -194,16 +210,23 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
       LU[k] = acc;
     }
     double q[NF];
+    if (DENSE) {
+#pragma unroll
+      for (int m = 0; m < NF; m++) q[m] = 0.0;
+    }
     rv_row(e, k, q);
-    const unsigned rm = rv_mask(k);
+    const unsigned rm = DENSE ? 0xFFu : rv_mask(k);
 #pragma unroll
     for (int m = 0; m < NF; m++)
-      if (rm & (1u << m)) Fn[slot_of(m)] += q[m] * fw;
+      if (rm & (1u << m)) Fn[m] += q[m] * fw;
   }
-  // The dummy wave 7 contributes +0 * +0 last in the reference's sums.
+  if (!DENSE) {
+    // the dummy wave 7 contributes +0 * +0 last in the reference's sums
 #pragma unroll
-  for (int s = 0; s < 7; s++) Fn[s] = Fn[s] + 0.0;
-  if (CHARS) LU[7] = 0.0;
+    for (int m = 0; m < NF; m++)
+      if (m != 4) Fn[m] = Fn[m] + 0.0;
+    if (CHARS) LU[7] = 0.0;
+  }
   return true;
 }
 
@@ -224,6 +247,8 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int i0 = 2 + blockIdx.y * TI, j0 = 2 + blockIdx.x * TJ;
   const double gm = g.gamma;
+  __shared__ int tile_nonfinite;  // some stencil state or flux value is inf / NaN
+  if (tid == 0) tile_nonfinite = 0;
 
   // 0. stage the state box
   for (int e = tid; e < NF * RU * CU; e += NW * 32) {
@@ -249,6 +274,14 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
 #pragma unroll
       for (int k = 0; k < NF; k++) { F[k] = 0.0; G[k] = 0.0; }
     }
+    bool fin = true;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      fin = fin && isfinite(q[k]);
+      if (k != 4) fin = fin && (!needF || isfinite(F[k]));
+      if (k != 5) fin = fin && (!needG || isfinite(G[k]));
+    }
+    if (!fin) tile_nonfinite = 1;
     if (needF) {
 #pragma unroll
       for (int m = 0; m < NF; m++)
@@ -304,9 +337,16 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
       }
     }
     if (!valid) continue;
-    double Fn[7], lam[NF], LU[NF], smax;
+    double Fn[NF], lam[NF], LU[NF], smax;
     int negp = 0;
-    if (!interface_flux<SCHEME, CHARS>(gm, L, al, Fn, smax, negp, lam, LU)) {
+    bool nonfinite = tile_nonfinite != 0, ok = true;
+    if (!nonfinite)
+      ok = interface_flux<SCHEME, CHARS, false>(gm, L, al, Fn, smax, negp, lam, LU, nonfinite);
+    if (ok && nonfinite) {
+      bool unused = false;
+      ok = interface_flux<SCHEME, CHARS, true>(gm, L, al, Fn, smax, negp, lam, LU, unused);
+    }
+    if (!ok) {
       atomicExch(&ctl->error, 6);  // ErrorNegativeDensity
       atomicAdd(&ctl->negd_count, 1ull);
       continue;
@@ -315,11 +355,11 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
     if (isx) {
       smaxX = take_max(smaxX, smax);
 #pragma unroll
-      for (int s = 0; s < 7; s++) sFx[(s * (TI + 1) + (ii + 1)) * TJ + jj] = Fn[s];
+      for (int m = 0; m < NF; m++) sFx[(m * (TI + 1) + (ii + 1)) * TJ + jj] = Fn[m];
     } else {
       smaxY = take_max(smaxY, smax);
 #pragma unroll
-      for (int s = 0; s < 7; s++) sGy[(s * TI + ii) * (TJ + 1) + (jj + 1)] = Fn[s];
+      for (int m = 0; m < NF; m++) sGy[(m * TI + ii) * (TJ + 1) + (jj + 1)] = Fn[m];
       if (gi == g.nx + 1 && gj == g.ny + 1) ctl->neg_last = negp;  // last interface of the sweep
     }
     if (CHARS) {
@@ -341,16 +381,11 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
     if (i >= g.nx + 2 || j >= g.ny + 2) continue;
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      double fr = 0.0, fl = 0.0, gr = 0.0, gl = 0.0;
-      if (k != 4) {
-        fr = sFx[(slot_of(k) * (TI + 1) + (r + 1)) * TJ + c];
-        fl = sFx[(slot_of(k) * (TI + 1) + r) * TJ + c];
-      }
-      const int fk = swap_xy(k);
-      if (fk != 4) {
-        gr = sGy[(slot_of(fk) * TI + r) * (TJ + 1) + (c + 1)];
-        gl = sGy[(slot_of(fk) * TI + r) * (TJ + 1) + c];
-      }
+      const double fr = sFx[(k * (TI + 1) + (r + 1)) * TJ + c];
+      const double fl = sFx[(k * (TI + 1) + r) * TJ + c];
+      const int fk = swap_xy(k);  // y numerical fluxes are stored in the y frame
+      const double gr = sGy[(fk * TI + r) * (TJ + 1) + (c + 1)];
+      const double gl = sGy[(fk * TI + r) * (TJ + 1) + c];
       UL[g.at(k, i, j)] = -(inv_dx) * (fr - fl) - (inv_dy) * (gr - gl);
     }
   }
