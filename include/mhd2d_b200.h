@@ -91,6 +91,13 @@ int mhd_download_ul( mhd_ctx* ctx, double* UL );
    state currently on the device. */
 int mhd_init_dirichlet( mhd_ctx* ctx );
 
+/* The same snapshot handed over from the host, as the reference keeps it in
+   SpatialIntegrationMethod::dirichletBoundaryLeft/Right/Bottom/Top
+   (spatialintegrationmethod.hpp:55-58): left / right are [8][NY], bottom /
+   top [8][NX] blocks (only the interior entries are read). */
+int mhd_set_dirichlet( mhd_ctx* ctx, const double* left, const double* right,
+                       const double* bottom, const double* top );
+
 /* Replaces SpatialMethodEnoRoe::integrate (spatialmethodenoroe.cpp:33-179)
    and SpatialMethodEnoLF::integrate (spatialmethodenolf.cpp:33-230) on the
    device state: boundary fill (in place), fluxes, dtIdeal, UL. */

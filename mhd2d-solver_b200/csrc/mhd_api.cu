@@ -406,6 +406,20 @@ int mhd_init_dirichlet(mhd_ctx* c) {
   return set_status(c, MHD_OK, false, "");
 }
 
+int mhd_set_dirichlet(mhd_ctx* c, const double* left, const double* right, const double* bottom,
+                      const double* top) {
+  if (!c || !left || !right || !bottom || !top) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  const size_t ny = size_t(NF) * c->g.NY * sizeof(double), nx = size_t(NF) * c->g.NX * sizeof(double);
+  CK(cudaMemcpyAsync(c->snap[0], left, ny, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->snap[1], right, ny, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->snap[2], bottom, nx, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->snap[3], top, nx, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->dirichlet_ready = true;
+  return set_status(c, MHD_OK, false, "");
+}
+
 int mhd_integrate(mhd_ctx* c, double* dtIdeal) {
   if (!c) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));

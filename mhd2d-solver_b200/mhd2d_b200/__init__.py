@@ -80,6 +80,7 @@ def library():
         "mhd_download": [vp, _dp],
         "mhd_download_ul": [vp, _dp],
         "mhd_init_dirichlet": [vp],
+        "mhd_set_dirichlet": [vp, _dp, _dp, _dp, _dp],
         "mhd_integrate": [vp, _dp],
         "mhd_integrate_host": [vp, _dp, _dp, _dp],
         "mhd_set_stepper": [vp, C.c_int, C.c_double, C.c_double, C.c_double],
