@@ -160,6 +160,29 @@ int mhd_time_integrate( mhd_ctx* ctx, int n, double* avg_ms );
    The denominator of the FP64 roofline of the flux kernels. */
 int mhd_fp64_peak( int device, double* tflops );
 
+/* No counterpart in the reference.  The div B diagnostic of mhd_divb_calc
+   for callers that cannot allocate device memory (code running under CUDA
+   graph capture, plug-ins inside an application that owns all device
+   memory, runtimes that forbid allocation after start-up).  It allocates
+   nothing: its scratch (one partial max and sum per grid row) is a fixed
+   file-scope device array of 2 x 16384 doubles that every GPU loading the
+   library keeps until exit, so nx may not exceed 16384
+   (MHD_ERR_WRONG_PARAMETER otherwise).
+     U       device state block, element (k,i,j) at
+             k*(nx+4)*pitch + i*pitch + row_offset + j (pitch = ny+4,
+             row_offset = 0 is the reference's own layout); the periodic Bx,
+             By ghost layers are written, as divBCalculation does;
+     result  device pointer to 2 doubles: max|div B|, integral of |div B|;
+     stream  a cudaStream_t (NULL: the default stream).
+   The work is enqueued on `stream` and the call returns without waiting.
+   The first call on a device looks up the scratch array's device address
+   (cudaGetSymbolAddress, with that device current); make that first call
+   before any stream capture.  All calls share the scratch array: calls
+   whose work overlaps on the GPU race, so serialise them. */
+int mhd_divb_calc_noalloc( double* U, int nx, int ny, int pitch, int row_offset,
+                           double dx, double dy, const int bc[4], double* result,
+                           void* stream );
+
 #ifdef __cplusplus
 }
 #endif

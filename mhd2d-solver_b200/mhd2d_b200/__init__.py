@@ -96,6 +96,8 @@ def library():
         "mhd_stream": [vp, C.POINTER(vp)],
         "mhd_time_integrate": [vp, C.c_int, _dp],
         "mhd_fp64_peak": [C.c_int, _dp],
+        "mhd_divb_calc_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                  C.c_double, _ip, C.c_void_p, C.c_void_p],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
