@@ -8,13 +8,16 @@
 // and the sign flips that keep the fast and slow vectors continuous across
 // By = 0.  Row 7 (the dummy wave) and column 4 (Bx) are structurally zero
 // and never formed; the other rows are produced on demand, so a thread holds
-// ~30 midpoint scalars plus one row instead of two dense 8x8 matrices.
+// ~25 midpoint scalars plus one row instead of two dense 8x8 matrices.
 //
 // Every expression keeps the reference's association order; the parity
 // build compiles this with -fmad=false, which makes each entry bit-identical
 // to the reference's x86-64 double arithmetic (IEEE division and sqrt on
-// both sides).  The y direction uses the same code on x/y-swapped inputs,
-// as getEigensG / getNumericalFluxG do (spatialmethodeno.cpp:574-598).
+// both sides).  Products with the sign factors sgn(Bx), cffactor and
+// csfactor (exactly +-1) are applied as sign-bit flips, which give the same
+// bits as the multiplication and keep the FP64 pipe free.  The y direction
+// uses the same code on x/y-swapped inputs, as getEigensG /
+// getNumericalFluxG do (spatialmethodeno.cpp:574-598).
 #pragma once
 
 #include "mhd_common.cuh"
@@ -26,17 +29,30 @@
 namespace mhd {
 namespace MHD_KNS {
 
+// gamma and the gamma-only quantities the formulas use, computed once on
+// the host in the same IEEE arithmetic: g1 = gamma - 1, g21 = (gamma - 2) /
+// (gamma - 1), rs2 = 1 / sqrt(2).
+struct Gas {
+  double gm, g1, g21, rs2;
+};
+
 struct Mid {
   double u, v, w, uu;
   double a2, a, ca2, ca, cs2, cs, cf2, cf;
-  double rr, sbx, af2, af, as2, as, bty, btz, th1, th2, g1, g21, vb;
-  double fcf, fcs;  // sign factors of the fast / slow rows
-  int negp;         // midpoint pressure was negative and clamped
+  double rr, af2, af, as2, as, bty, btz, th1, th2, vb;
+  unsigned sbxm, fcfm, fcsm;  // sign-bit masks of sgn(Bx), cffactor, csfactor
+  int negp;                   // midpoint pressure was negative and clamped
 };
+
+// x * s for s = +-1 given as a mask of the sign bit of the high word.
+__device__ __forceinline__ double flip(double x, unsigned m) {
+  return __hiloint2double(__double2hiint(x) ^ (int)m, __double2loint(x));
+}
 
 // Returns false on non-positive midpoint density (the reference's
 // ErrorNegativeDensity, spatialmethodeno.cpp:307-310).
-__device__ __forceinline__ bool midpoint(double gm, const double* U1, const double* U2, Mid& e) {
+__device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const double* U2, Mid& e) {
+  const double gm = G.gm;
   const double r = 0.5 * (U1[0] + U2[0]);
   e.u = 0.5 * (U1[1] / U1[0] + U2[1] / U2[0]);
   e.v = 0.5 * (U1[2] / U1[0] + U2[2] / U2[0]);
@@ -78,7 +94,7 @@ __device__ __forceinline__ bool midpoint(double gm, const double* U1, const doub
 
   e.rr = sqrt(r);
   const double bp2 = by * by + bz * bz;
-  e.sbx = (bx < 0.0) ? -1.0 : 1.0;
+  e.sbxm = (bx < 0.0) ? 0x80000000u : 0u;
   const bool deg = (bp2 < SMALL) && (fabs(e.ca2 - a2) < SMALL);
   double af2 = deg ? 1.0 : (cf2 - e.ca2) / (cf2 - cs2);
   if (af2 < 0.0) af2 = 0.0;
@@ -91,18 +107,18 @@ __device__ __forceinline__ bool midpoint(double gm, const double* U1, const doub
     e.bty = by / sb;
     e.btz = bz / sb;
   } else {
-    e.bty = 1.0 / sqrt(2.0);
-    e.btz = 1.0 / sqrt(2.0);
+    e.bty = G.rs2;
+    e.btz = G.rs2;
   }
-  e.g1 = gm - 1.0;
-  e.g21 = (gm - 2.0) / (gm - 1.0);
-  e.th1 = 1.0 / (af2 * a2 * (cf2 - e.g21 * a2) + as2 * cf2 * (cs2 - e.g21 * a2));
-  e.th2 = 1.0 / (af2 * e.cf * e.a * e.sbx + as2 * e.cs * e.ca * e.sbx);
+  const double g21 = G.g21;
+  e.th1 = 1.0 / (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2));
+  e.th2 = 1.0 / (flip(af2 * e.cf * e.a, e.sbxm) + flip(as2 * e.cs * e.ca, e.sbxm));
   e.vb = e.bty * v + e.btz * w;
 
-  const double sgnbt = ((by > 0.0) || (fabs(by) < SMALL && (bz > 0.0))) ? 1.0 : -1.0;
-  e.fcs = a2 > e.ca2 ? sgnbt : 1.0;
-  e.fcf = a2 < e.ca2 ? sgnbt : 1.0;
+  const bool sgnbt_pos = (by > 0.0) || (fabs(by) < SMALL && (bz > 0.0));
+  const unsigned bt = sgnbt_pos ? 0u : 0x80000000u;
+  e.fcsm = a2 > e.ca2 ? bt : 0u;
+  e.fcfm = a2 < e.ca2 ? bt : 0u;
   return true;
 }
 
@@ -113,11 +129,10 @@ __device__ __forceinline__ bool midpoint(double gm, const double* U1, const doub
 // than one row at a time and ends in local-memory spills.
 __device__ __forceinline__ void opaque(Mid& e) {
   asm volatile("" : "+d"(e.u), "+d"(e.v), "+d"(e.w), "+d"(e.uu), "+d"(e.a2), "+d"(e.a),
-                    "+d"(e.ca), "+d"(e.cs), "+d"(e.cs2), "+d"(e.cf), "+d"(e.cf2), "+d"(e.rr),
-                    "+d"(e.sbx));
+                    "+d"(e.ca), "+d"(e.cs), "+d"(e.cs2), "+d"(e.cf), "+d"(e.cf2), "+d"(e.rr));
   asm volatile("" : "+d"(e.af), "+d"(e.as), "+d"(e.af2), "+d"(e.as2), "+d"(e.bty), "+d"(e.btz),
-                    "+d"(e.th1), "+d"(e.th2), "+d"(e.g1), "+d"(e.g21), "+d"(e.vb), "+d"(e.fcf),
-                    "+d"(e.fcs));
+                    "+d"(e.th1), "+d"(e.th2), "+d"(e.vb), "+r"(e.sbxm), "+r"(e.fcfm),
+                    "+r"(e.fcsm));
 }
 
 __device__ __forceinline__ double eigenvalue(const Mid& e, int k) {
@@ -143,57 +158,60 @@ __host__ __device__ constexpr unsigned rv_mask(int k) {
 }
 
 // Left eigenvector row k (spatialmethodeno.cpp:473-552, sign flips 554-568).
-__device__ __forceinline__ void lv_row(const Mid& e, int k, double* l) {
+__device__ __forceinline__ void lv_row(const Mid& e, const Gas& G, int k, double* l) {
   const double u = e.u, v = e.v, w = e.w, uu = e.uu, a2 = e.a2, a = e.a, ca = e.ca;
-  const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr, sbx = e.sbx;
+  const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr;
   const double af = e.af, as = e.as, af2 = e.af2, as2 = e.as2, bty = e.bty, btz = e.btz;
-  const double th1 = e.th1, th2 = e.th2, g21 = e.g21, vb = e.vb;
+  const double th1 = e.th1, th2 = e.th2, g21 = G.g21, vb = e.vb;
+  const unsigned sb = e.sbxm;
   switch (k) {
     case 0:
     case 6: {
-      const double f = e.fcf;
       if (k == 0) {
-        l[0] = 0.25 * th1 * af * a2 * uu + 0.5 * th2 * (af * a * u * sbx - as * cs * vb);
-        l[1] = -0.5 * th1 * af * a2 * u - 0.5 * th2 * af * a * sbx;
+        l[0] = 0.25 * th1 * af * a2 * uu + 0.5 * th2 * (flip(af * a * u, sb) - as * cs * vb);
+        l[1] = -0.5 * th1 * af * a2 * u - flip(0.5 * th2 * af * a, sb);
         l[2] = -0.5 * th1 * af * a2 * v + 0.5 * th2 * as * bty * cs;
         l[3] = -0.5 * th1 * af * a2 * w + 0.5 * th2 * as * btz * cs;
       } else {
-        l[0] = 0.25 * th1 * af * a2 * uu - 0.5 * th2 * (af * a * u * sbx - as * cs * vb);
-        l[1] = -0.5 * th1 * af * a2 * u + 0.5 * th2 * af * a * sbx;
+        l[0] = 0.25 * th1 * af * a2 * uu - 0.5 * th2 * (flip(af * a * u, sb) - as * cs * vb);
+        l[1] = -0.5 * th1 * af * a2 * u + flip(0.5 * th2 * af * a, sb);
         l[2] = -0.5 * th1 * af * a2 * v - 0.5 * th2 * as * bty * cs;
         l[3] = -0.5 * th1 * af * a2 * w - 0.5 * th2 * as * btz * cs;
       }
       l[5] = 0.5 * th1 * as * bty * cf * rr * (cs2 - g21 * a2);
       l[6] = 0.5 * th1 * as * btz * cf * rr * (cs2 - g21 * a2);
       l[7] = 0.5 * th1 * af * a2;
-      l[0] *= f; l[1] *= f; l[2] *= f; l[3] *= f; l[5] *= f; l[6] *= f; l[7] *= f;
+      const unsigned f = e.fcfm;
+      l[0] = flip(l[0], f); l[1] = flip(l[1], f); l[2] = flip(l[2], f); l[3] = flip(l[3], f);
+      l[5] = flip(l[5], f); l[6] = flip(l[6], f); l[7] = flip(l[7], f);
       break;
     }
     case 1:
-      l[0] = -0.5 * (btz * v - bty * w) * sbx;
-      l[2] = 0.5 * btz * sbx;
-      l[3] = -0.5 * bty * sbx;
+      l[0] = flip(-0.5 * (btz * v - bty * w), sb);
+      l[2] = flip(0.5 * btz, sb);
+      l[3] = flip(-0.5 * bty, sb);
       l[5] = 0.5 * btz * rr;
       l[6] = -0.5 * bty * rr;
       break;
     case 2:
     case 4: {
-      const double f = e.fcs;
       if (k == 2) {
-        l[0] = 0.25 * th1 * as * cf2 * uu + 0.5 * th2 * (as * ca * u * sbx + af * cf * vb);
-        l[1] = -0.5 * th1 * as * cf2 * u - 0.5 * th2 * as * ca * sbx;
+        l[0] = 0.25 * th1 * as * cf2 * uu + 0.5 * th2 * (flip(as * ca * u, sb) + af * cf * vb);
+        l[1] = -0.5 * th1 * as * cf2 * u - flip(0.5 * th2 * as * ca, sb);
         l[2] = -0.5 * th1 * as * cf2 * v - 0.5 * th2 * af * bty * cf;
         l[3] = -0.5 * th1 * as * cf2 * w - 0.5 * th2 * af * btz * cf;
       } else {
-        l[0] = 0.25 * th1 * as * cf2 * uu - 0.5 * th2 * (as * ca * u * sbx + af * cf * vb);
-        l[1] = -0.5 * th1 * as * cf2 * u + 0.5 * th2 * as * ca * sbx;
+        l[0] = 0.25 * th1 * as * cf2 * uu - 0.5 * th2 * (flip(as * ca * u, sb) + af * cf * vb);
+        l[1] = -0.5 * th1 * as * cf2 * u + flip(0.5 * th2 * as * ca, sb);
         l[2] = -0.5 * th1 * as * cf2 * v + 0.5 * th2 * af * bty * cf;
         l[3] = -0.5 * th1 * as * cf2 * w + 0.5 * th2 * af * btz * cf;
       }
       l[5] = -0.5 * th1 * af * bty * cf * rr * (cf2 - g21 * a2);
       l[6] = -0.5 * th1 * af * btz * cf * rr * (cf2 - g21 * a2);
       l[7] = 0.5 * th1 * as * cf2;
-      l[0] *= f; l[1] *= f; l[2] *= f; l[3] *= f; l[5] *= f; l[6] *= f; l[7] *= f;
+      const unsigned f = e.fcsm;
+      l[0] = flip(l[0], f); l[1] = flip(l[1], f); l[2] = flip(l[2], f); l[3] = flip(l[3], f);
+      l[5] = flip(l[5], f); l[6] = flip(l[6], f); l[7] = flip(l[7], f);
       break;
     }
     case 3: {
@@ -207,9 +225,9 @@ __device__ __forceinline__ void lv_row(const Mid& e, int k, double* l) {
       break;
     }
     case 5:
-      l[0] = +0.5 * (btz * v - bty * w) * sbx;
-      l[2] = -0.5 * btz * sbx;
-      l[3] = 0.5 * bty * sbx;
+      l[0] = flip(+0.5 * (btz * v - bty * w), sb);
+      l[2] = flip(-0.5 * btz, sb);
+      l[3] = flip(0.5 * bty, sb);
       l[5] = 0.5 * btz * rr;
       l[6] = -0.5 * bty * rr;
       break;
@@ -219,41 +237,62 @@ __device__ __forceinline__ void lv_row(const Mid& e, int k, double* l) {
 }
 
 // Right eigenvector row k (spatialmethodeno.cpp:392-471, sign flips 554-568).
-__device__ __forceinline__ void rv_row(const Mid& e, int k, double* q) {
+__device__ __forceinline__ void rv_row(const Mid& e, const Gas& G, int k, double* q) {
   const double u = e.u, v = e.v, w = e.w, uu = e.uu, a2 = e.a2, a = e.a, ca = e.ca;
-  const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr, sbx = e.sbx;
-  const double af = e.af, as = e.as, bty = e.bty, btz = e.btz, g1 = e.g1, g21 = e.g21;
+  const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr;
+  const double af = e.af, as = e.as, bty = e.bty, btz = e.btz, g1 = G.g1, g21 = G.g21;
   const double vb = e.vb;
+  const unsigned sb = e.sbxm;
   switch (k) {
-    case 0: {
-      const double f = e.fcf;
-      q[0] = af;
-      q[1] = af * (u - cf);
-      q[2] = af * v + as * bty * ca * sbx;
-      q[3] = af * w + as * btz * ca * sbx;
+    case 0:
+    case 6: {
+      if (k == 0) {
+        q[0] = af;
+        q[1] = af * (u - cf);
+        q[2] = af * v + flip(as * bty * ca, sb);
+        q[3] = af * w + flip(as * btz * ca, sb);
+        q[7] = 0.5 * af * uu + af * cf2 / g1 - af * cf * u + flip(as * ca, sb) * vb + g21 * af * (cf2 - a2);
+      } else {
+        q[0] = af;
+        q[1] = af * (u + cf);
+        q[2] = af * v - flip(as * bty * ca, sb);
+        q[3] = af * w - flip(as * btz * ca, sb);
+        q[7] = 0.5 * af * uu + af * cf2 / g1 + af * cf * u - flip(as * ca, sb) * vb + g21 * af * (cf2 - a2);
+      }
       q[5] = as * bty * cf / rr;
       q[6] = as * btz * cf / rr;
-      q[7] = 0.5 * af * uu + af * cf2 / g1 - af * cf * u + as * ca * sbx * vb + g21 * af * (cf2 - a2);
-      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
+      const unsigned f = e.fcfm;
+      q[0] = flip(q[0], f); q[1] = flip(q[1], f); q[2] = flip(q[2], f); q[3] = flip(q[3], f);
+      q[5] = flip(q[5], f); q[6] = flip(q[6], f); q[7] = flip(q[7], f);
       break;
     }
     case 1:
-      q[2] = btz * sbx;
-      q[3] = -bty * sbx;
+      q[2] = flip(btz, sb);
+      q[3] = flip(-bty, sb);
       q[5] = btz / rr;
       q[6] = -bty / rr;
-      q[7] = (btz * v - bty * w) * sbx;
+      q[7] = flip(btz * v - bty * w, sb);
       break;
-    case 2: {
-      const double f = e.fcs;
-      q[0] = as;
-      q[1] = as * (u - cs);
-      q[2] = as * v - af * bty * a * sbx;
-      q[3] = as * w - af * btz * a * sbx;
+    case 2:
+    case 4: {
+      if (k == 2) {
+        q[0] = as;
+        q[1] = as * (u - cs);
+        q[2] = as * v - flip(af * bty * a, sb);
+        q[3] = as * w - flip(af * btz * a, sb);
+        q[7] = 0.5 * as * uu + as * cs2 / g1 - as * cs * u - flip(af * a, sb) * vb + g21 * as * (cs2 - a2);
+      } else {
+        q[0] = as;
+        q[1] = as * (u + cs);
+        q[2] = as * v + flip(af * bty * a, sb);
+        q[3] = as * w + flip(af * btz * a, sb);
+        q[7] = 0.5 * as * uu + as * cs2 / g1 + as * cs * u + flip(af * a, sb) * vb + g21 * as * (cs2 - a2);
+      }
       q[5] = -af * bty * a2 / (cf * rr);
       q[6] = -af * btz * a2 / (cf * rr);
-      q[7] = 0.5 * as * uu + as * cs2 / g1 - as * cs * u - af * a * sbx * vb + g21 * as * (cs2 - a2);
-      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
+      const unsigned f = e.fcsm;
+      q[0] = flip(q[0], f); q[1] = flip(q[1], f); q[2] = flip(q[2], f); q[3] = flip(q[3], f);
+      q[5] = flip(q[5], f); q[6] = flip(q[6], f); q[7] = flip(q[7], f);
       break;
     }
     case 3:
@@ -263,37 +302,13 @@ __device__ __forceinline__ void rv_row(const Mid& e, int k, double* q) {
       q[3] = w;
       q[7] = 0.5 * uu;
       break;
-    case 4: {
-      const double f = e.fcs;
-      q[0] = as;
-      q[1] = as * (u + cs);
-      q[2] = as * v + af * bty * a * sbx;
-      q[3] = as * w + af * btz * a * sbx;
-      q[5] = -af * bty * a2 / (cf * rr);
-      q[6] = -af * btz * a2 / (cf * rr);
-      q[7] = 0.5 * as * uu + as * cs2 / g1 + as * cs * u + af * a * sbx * vb + g21 * as * (cs2 - a2);
-      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
-      break;
-    }
     case 5:
-      q[2] = -btz * sbx;
-      q[3] = +bty * sbx;
+      q[2] = flip(-btz, sb);
+      q[3] = flip(+bty, sb);
       q[5] = btz / rr;
       q[6] = -bty / rr;
-      q[7] = -(btz * v - bty * w) * sbx;
+      q[7] = flip(-(btz * v - bty * w), sb);
       break;
-    case 6: {
-      const double f = e.fcf;
-      q[0] = af;
-      q[1] = af * (u + cf);
-      q[2] = af * v - as * bty * ca * sbx;
-      q[3] = af * w - as * btz * ca * sbx;
-      q[5] = as * bty * cf / rr;
-      q[6] = as * btz * cf / rr;
-      q[7] = 0.5 * af * uu + af * cf2 / g1 + af * cf * u - as * ca * sbx * vb + g21 * af * (cf2 - a2);
-      q[0] *= f; q[1] *= f; q[2] *= f; q[3] *= f; q[5] *= f; q[6] *= f; q[7] *= f;
-      break;
-    }
     default:
       break;
   }

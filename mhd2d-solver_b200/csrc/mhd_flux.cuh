@@ -122,7 +122,7 @@ struct Lane {
 // the dummy wave 7 included, and so reproduces its NaN / inf propagation
 // exactly; the kernel recomputes flagged interfaces this way.
 template <int SCHEME, bool CHARS, bool DENSE>
-__device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const double* alpha,
+__device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, const double* alpha,
                                                double* Fn, double& smax, int& negp,
                                                double* lam, double* LU, bool& nonfinite) {
   double U1[NF], U2[NF];
@@ -132,7 +132,7 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
     U2[k] = L.Q(k, L.l2);
   }
   Mid e;
-  if (!midpoint(gm, U1, U2, e)) return false;
+  if (!midpoint(G, U1, U2, e)) return false;
   negp = e.negp;
   smax = 0.0;
 #pragma unroll
@@ -145,7 +145,11 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
   for (int m = 0; m < NF; m++) Fn[m] = 0.0;
 
   constexpr int KN = DENSE ? 8 : 7;
-#pragma unroll 1
+#ifndef MHD_K_UNROLL
+#define MHD_K_UNROLL 7
+#endif
+  constexpr int kUnroll = MHD_K_UNROLL;
+#pragma unroll kUnroll
   for (int k = 0; k < KN; k++) {
     opaque(e);
     double l[NF];
@@ -153,7 +157,7 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
 #pragma unroll
       for (int m = 0; m < NF; m++) l[m] = 0.0;
     }
-    lv_row(e, k, l);
+    lv_row(e, G, k, l);
     const unsigned lm = DENSE ? 0xFFu : lv_mask(k);
     double fw;
     if (SCHEME == 2) {  // ENO-Roe: project F and its undivided differences
@@ -214,7 +218,7 @@ __device__ __forceinline__ bool interface_flux(double gm, const Lane& L, const d
 #pragma unroll
       for (int m = 0; m < NF; m++) q[m] = 0.0;
     }
-    rv_row(e, k, q);
+    rv_row(e, G, k, q);
     const unsigned rm = DENSE ? 0xFFu : rv_mask(k);
 #pragma unroll
     for (int m = 0; m < NF; m++)
@@ -234,7 +238,7 @@ template <int SCHEME, bool CHARS, int TI, int TJ, int NW>
 __global__ void __launch_bounds__(NW * 32, MHD_MINB)
 k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
        const double* __restrict__ alphaF, const double* __restrict__ alphaG,
-       double inv_dx, double inv_dy, Ctl* ctl, CharOut co) {
+       double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co) {
   using T = TileGeom<TI, TJ>;
   constexpr int RU = T::RU, CU = T::CU;
   if (ctl->skip) return;
@@ -341,10 +345,10 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
     int negp = 0;
     bool nonfinite = tile_nonfinite != 0, ok = true;
     if (!nonfinite)
-      ok = interface_flux<SCHEME, CHARS, false>(gm, L, al, Fn, smax, negp, lam, LU, nonfinite);
+      ok = interface_flux<SCHEME, CHARS, false>(G, L, al, Fn, smax, negp, lam, LU, nonfinite);
     if (ok && nonfinite) {
       bool unused = false;
-      ok = interface_flux<SCHEME, CHARS, true>(gm, L, al, Fn, smax, negp, lam, LU, unused);
+      ok = interface_flux<SCHEME, CHARS, true>(G, L, al, Fn, smax, negp, lam, LU, unused);
     }
     if (!ok) {
       atomicExch(&ctl->error, 6);  // ErrorNegativeDensity

@@ -1,6 +1,8 @@
 // Kernel instantiations and launchers.  Built twice from this one source:
 //   MHD_KSET = kExact  with -fmad=false  (bit-identical to the reference)
 //   MHD_KSET = kFast   with -fmad=true   (FMA contraction)
+#include <cmath>
+
 #include "mhd_flux.cuh"
 #include "mhd_launch.h"
 #include "mhd_misc.cuh"
@@ -13,7 +15,18 @@
 namespace mhd {
 namespace MHD_KNS {
 
-constexpr int TI = 8, TJ = 32, NW = 6;
+// 7 x 32 tiles, 8 warps: 16 warp tasks per tile = 2 rounds, 90 KB of shared
+// memory and at most 128 registers per thread, so 2 CTAs = 16 warps per SM
+// (measured best against 8x32/6 warps, 15x32 or 11x32/8 warps with one CTA,
+// and smaller tiles at 96 registers).
+#ifndef MHD_TI
+#define MHD_TI 7
+#endif
+#ifndef MHD_NW
+#define MHD_NW 8
+#endif
+// tile rows x columns and warps per CTA of the fused flux kernel
+constexpr int TI = MHD_TI, TJ = 32, NW = MHD_NW;
 using Geom = TileGeom<TI, TJ>;
 
 int grid1d(long long n, int block) {
@@ -53,7 +66,8 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
   dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + TI - 1) / TI);
   CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
              ch ? ch[3] : nullptr};
-  kern<<<grid, NW * 32, Geom::BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, ctl, co);
+  const Gas G{g.gamma, g.gamma - 1.0, (g.gamma - 2.0) / (g.gamma - 1.0), 1.0 / std::sqrt(2.0)};
+  kern<<<grid, NW * 32, Geom::BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co);
 }
 
 void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
