@@ -254,13 +254,22 @@ k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
   __shared__ int tile_nonfinite;  // some stencil state or flux value is inf / NaN
   if (tid == 0) tile_nonfinite = 0;
 
-  // 0. stage the state box
+  // 0. stage the state box: all copies are issued asynchronously
+  //    (global -> shared without a register round trip), then waited for
+  //    once; a plain load-then-store loop waits one HBM latency per element
   for (int e = tid; e < NF * RU * CU; e += NW * 32) {
     const int k = e / (RU * CU), rem = e - k * (RU * CU);
     const int r = rem / CU, c = rem - r * CU;
     const int i = i0 - 2 + r, j = j0 - 2 + c;
-    sU[e] = (i < g.NX && j < g.NY) ? U[g.at(k, i, j)] : 0.0;
+    if (i < g.NX && j < g.NY) {
+      const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(sU + e));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(U + g.at(k, i, j))
+                   : "memory");
+    } else {
+      sU[e] = 0.0;
+    }
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 
   // 1. physical fluxes: F on rows [0,RU) x cols [2,TJ+2), G on rows [2,TI+2) x cols [0,CU)
