@@ -42,6 +42,10 @@ REF_SAMPLE = 512
 # extrapolated to 4096^2 (tests/test_flop_constants.py re-derives them).
 FLOPS_PER_CELL_INTEGRATE = {2: 3011.9, 3: 3514.0}
 FLOPS_PER_CELL_STEP = {2: 9147.6, 3: 10653.9}
+# DRAM bytes (read + write) of one k_flux launch per interior cell, from one
+# ncu capture of the 2048^2 ENO-Roe case (545.2 MB; profiles/
+# k_flux_eno_roe_ot2048_ncu.md), scaled to a launch by its cell count.
+DRAM_BYTES_PER_CELL_FLUX = 545.17e6 / 2048 ** 2
 
 
 def parse():
@@ -130,11 +134,13 @@ def barrier(world):
 
 
 def allreduce_max(world, x):
+    """Max over ranks (the slowest rank's time); NCCL on GPUs, gloo on CPU."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -279,6 +285,20 @@ def run_ours(args):
     peak = M.fp64_peak_tflops(dev)
     flops = FLOPS_PER_CELL_INTEGRATE[scheme] * cells
     achieved = flops / (t_int * 1e-3) / 1e12
+
+    # SOR div-B cleaning, measured separately: a fixed number of red-black
+    # sweeps on the evolved 4096^2 state (the convergence test never fires:
+    # rmax 0), timed with CUDA events on the library stream.
+    sor_sweeps = 200
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    st_sor, done = ctx.divb_sor(M.sor_params(1, 1, sor_sweeps, 0.0, 0.0, True, 1.7))
+    s1.record(stream)
+    torch.cuda.synchronize()
+    sor_ms = s0.elapsed_time(s1) / max(done, 1)
+    # minimum traffic of one sweep: phi read + written once, Bx and By read once
+    sor_bytes = 32.0 * cells
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -295,12 +315,19 @@ def run_ours(args):
                     "call": "mhd_step_host (pinned host state)"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": DRAM_BYTES_PER_CELL_FLUX * cells,
+                         "traffic_note": "dram bytes per k_flux launch, ncu 2048^2 capture scaled "
+                                         "by cells; algorithmic 128 B/cell",
                          "kernel": "k_flux (fused spatial operator) + boundary fill",
                          "flops_per_launch": flops, "launch_ms": t_int,
                          "peak_source": "measured live: FP64 FMA-chain probe (mhd_fp64_peak); "
                                         "MEASURED_PEAKS.json has no FP64 figure"},
             "clocks": clocks,
+            "sor": {"ms_per_sweep": sor_ms, "sweeps": done, "status": st_sor.status,
+                    "gbs_min_traffic": sor_bytes / (sor_ms * 1e-3) / 1e9,
+                    "note": "red-black sweep (2 colours + ghost refresh + convergence test), "
+                            "32 B/cell minimum traffic; not part of the timed step"},
         }
         if world == 1:
             line["cpu_baseline"] = cpu_baseline_sample(scheme)

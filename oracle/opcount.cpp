@@ -1,6 +1,8 @@
 // ORACLE — TEST INFRASTRUCTURE ONLY.  Floating-point operation count of the
 // hot path, from the oracle restatement (mhd_oracle.c) compiled with a
-// counting scalar type: +, -, *, /, sqrt count 1 each.
+// counting scalar type: +, -, *, /, sqrt count 1 each.  Divisions and square
+// roots with a nonzero operand are also counted on their own (each costs a
+// multi-instruction correctly rounded sequence on the GPU).
 //
 // Two counts are kept:
 //   dense   — every operation the reference formulas perform as written;
@@ -17,7 +19,7 @@
 #include <cstring>
 #include <random>
 
-static unsigned long long g_dense = 0, g_nonzero = 0;
+static unsigned long long g_dense = 0, g_nonzero = 0, g_div = 0, g_sqrt = 0;
 
 struct CountedDouble {
   double v;
@@ -39,14 +41,20 @@ static inline CountedDouble op(double r, double a, double b) {
 static inline CountedDouble operator+(CountedDouble a, CountedDouble b) { return op(a.v + b.v, a.v, b.v); }
 static inline CountedDouble operator-(CountedDouble a, CountedDouble b) { return op(a.v - b.v, a.v, b.v); }
 static inline CountedDouble operator*(CountedDouble a, CountedDouble b) { return op(a.v * b.v, a.v, b.v); }
-static inline CountedDouble operator/(CountedDouble a, CountedDouble b) { return op(a.v / b.v, a.v, b.v); }
+static inline CountedDouble operator/(CountedDouble a, CountedDouble b) {
+  if (a.v != 0.0) g_div++;
+  return op(a.v / b.v, a.v, b.v);
+}
 static inline CountedDouble operator-(CountedDouble a) { return CountedDouble(-a.v); }
 static inline CountedDouble operator+(CountedDouble a) { return a; }
 static inline CountedDouble& operator+=(CountedDouble& a, CountedDouble b) { a = a + b; return a; }
 static inline CountedDouble& operator-=(CountedDouble& a, CountedDouble b) { a = a - b; return a; }
 static inline CountedDouble& operator*=(CountedDouble& a, CountedDouble b) { a = a * b; return a; }
 static inline CountedDouble& operator/=(CountedDouble& a, CountedDouble b) { a = a / b; return a; }
-static inline CountedDouble sqrt(CountedDouble a) { return op(std::sqrt(a.v), a.v, 1.0); }
+static inline CountedDouble sqrt(CountedDouble a) {
+  if (a.v != 0.0) g_sqrt++;
+  return op(std::sqrt(a.v), a.v, 1.0);
+}
 static inline CountedDouble fabs(CountedDouble a) { return CountedDouble(std::fabs(a.v)); }
 static inline CountedDouble cos(CountedDouble a) { return op(std::cos(a.v), a.v, 1.0); }
 static inline bool isnan(CountedDouble a) { return std::isnan(a.v); }
@@ -89,15 +97,17 @@ int main(int argc, char** argv) {
     orc_ctx* c = orc_create(scheme, 2, n, n, dx, dx, gm, bc, 0.0, 1e-4, 0.0);
     CountedDouble ideal = 0.0, dt = 1e-4;
     int err = 0;
-    g_dense = g_nonzero = 0;
+    g_dense = g_nonzero = g_div = g_sqrt = 0;
     orc_integrate(c, U, UL, &ideal, &err);
     const double id = double(g_dense) / (n * n), inz = double(g_nonzero) / (n * n);
+    const double idiv = double(g_div) / (n * n), isq = double(g_sqrt) / (n * n);
     g_dense = g_nonzero = 0;
     orc_step(c, U, &dt, &err);
     const double sd = double(g_dense) / (n * n), snz = double(g_nonzero) / (n * n);
     std::printf(", \"%s\": {\"integrate_dense\": %.2f, \"integrate_nonzero\": %.2f, "
+                "\"integrate_div\": %.2f, \"integrate_sqrt\": %.2f, "
                 "\"step_dense\": %.2f, \"step_nonzero\": %.2f}",
-                scheme == 2 ? "eno_roe" : "eno_lf", id, inz, sd, snz);
+                scheme == 2 ? "eno_roe" : "eno_lf", id, inz, idiv, isq, sd, snz);
     orc_destroy(c);
     std::free(U); std::free(UL); std::free(Ud);
   }
