@@ -183,6 +183,90 @@ int mhd_divb_calc_noalloc( double* U, int nx, int ny, int pitch, int row_offset,
                            double dx, double dy, const int bc[4], double* result,
                            void* stream );
 
+/* ------------------------------------------------------------------------
+ * Batched runs.  The reference runs one problem per process; its
+ * "batching" is starting several copies with different INI files.  A batch
+ * holds many independent runs of uneven grid sizes, schemes, boundary
+ * conditions and end times on one GPU and advances all of them together:
+ * each stage is one boundary fill, one ENO-LF dissipation pass, ONE
+ * persistent flux launch over the tiles of every active run, one
+ * controller pass (a per-run CFL reduction and dt control, the retry logic
+ * of TimeIntegrationRK3::step included) and one stage update, replayed
+ * from a CUDA graph.  Every run follows the reference main loop
+ * (main.cpp:174-344) without file output and SOR: step, t += dt, stop when
+ * t >= t_end, on a NaN at U[0][2][2], on a fatal status, or after
+ * max_steps steps when max_steps > 0.  Each run's arithmetic is the same as
+ * a context's (bit-identical results). */
+typedef struct mhd_batch mhd_batch;
+
+typedef struct {
+   int    nx, ny;
+   double dx, dy, gamma;
+   int    bc[4];          /* left, right, bottom, top */
+   int    scheme;         /* 2 ENO-Roe, 3 ENO-LF */
+   int    time_method;    /* 1 Euler, 2 RK3-TVD */
+   double dt_min, dt_max, cfl;
+   double dt0;            /* dt entering the first step */
+   double t_end;          /* simulated end time ([time] t_max) */
+   int    max_steps;      /* 0: no step limit */
+} mhd_batch_desc;
+
+typedef struct {
+   double    t, dt;
+   int       steps;
+   int       active;       /* 1 while the run continues */
+   int       status;       /* ReturnStatus that stopped it (0: reached its end) */
+   int       phase;        /* RK3 stage the next spatial operator belongs to */
+   long long retries;      /* RK3 stage-loop restarts (dt reductions) */
+   long long neg_pressure; /* midpoint pressures clamped to zero */
+} mhd_batch_state;
+
+/* Tile shapes of the persistent flux launch the autotuner chooses from. */
+enum { MHD_BATCH_TILE_7x32 = 0, MHD_BATCH_TILE_3x32 = 1, MHD_BATCH_TILE_COUNT = 2 };
+
+int mhd_batch_create( int n, const mhd_batch_desc* runs, int device, mhd_batch** out );
+int mhd_batch_destroy( mhd_batch* b );
+int mhd_batch_last_error( mhd_batch* b, char* buf, size_t len, int* is_error );
+
+/* Load run `idx` from a host [8][NX][NY] block (ghosts ignored) and re-arm it:
+   t = 0, dt = dt0, no steps; Dirichlet sides take their edge snapshot
+   (initializeDirichletBoundaries) from this state. */
+int mhd_batch_upload( mhd_batch* b, int idx, const double* U );
+int mhd_batch_download( mhd_batch* b, int idx, double* U );
+
+/* Advance every active run by up to `stages` spatial-operator stages (an
+   RK3 step is 3 stages, an Euler step 1; a dt retry adds stages).  The
+   host looks at the active count every `check_every` stages (<= 0: only at
+   the end) and returns early when no run is active. */
+int mhd_batch_advance( mhd_batch* b, int stages, int check_every, int* n_active );
+
+/* Per-run progress, read back after the last advance. */
+int mhd_batch_get_state( mhd_batch* b, int idx, mhd_batch_state* out );
+
+/* Autotuner: times the persistent flux launch of every tile shape (and two
+   persistent grid sizes) on the batch's current states, keeps the fastest
+   and returns its MHD_BATCH_TILE_* code and CTAs per SM.  The states are
+   left exactly as they were. */
+int mhd_batch_tune( mhd_batch* b, int reps, int* tile, int* ctas_per_sm, double* best_ms );
+/* Use a given tile shape / persistent grid (ctas_per_sm <= 0: the occupancy limit). */
+int mhd_batch_set_tile( mhd_batch* b, int tile, int ctas_per_sm );
+
+/* Device-side initial states (problem setups of file_access.cpp), written
+   straight into run idx and re-arming it like mhd_batch_upload.
+   kind MHD_PROBLEM_EXPLOSION, p[0..8]: x0, y0 (lower-left corner), r,
+     rho_in, p_in, rho_out, p_out, Bx, By  (Bz = 0, velocity 0; "jump" transition)
+   kind MHD_PROBLEM_WAVE, p[0..15]: x0, y0, Lx, Ly, rho, u, v, w, Bx, By, Bz, p,
+     epsilon, wave (0..6 = right eigenvector index), kx, ky  (readProblemWaveTest)
+   kind MHD_PROBLEM_ORSZAG_TANG: no parameters (gamma from the run)
+   kind MHD_PROBLEM_PLASMA_SHEET, p[0..3+K]: x0, y0, delta, K, a_1..a_K */
+enum { MHD_PROBLEM_EXPLOSION = 1, MHD_PROBLEM_WAVE = 2, MHD_PROBLEM_ORSZAG_TANG = 3,
+       MHD_PROBLEM_PLASMA_SHEET = 4 };
+int mhd_batch_init_problem( mhd_batch* b, int idx, int kind, const double* p, int np );
+
+int mhd_batch_stream( mhd_batch* b, void** stream );
+/* Kernel launches issued so far (graph nodes counted per replay). */
+int mhd_batch_launches( mhd_batch* b, long long* launches );
+
 #ifdef __cplusplus
 }
 #endif

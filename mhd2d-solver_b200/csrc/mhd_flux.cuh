@@ -234,197 +234,44 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
   return true;
 }
 
+// One tile of the spatial operator: interior cells i0 = 2 + ti*TI .. +TI,
+// j0 = 2 + tj*TJ .. +TJ.  Every thread of the CTA calls it with the same
+// (tj, ti); the kernel provides TileGeom::BYTES of dynamic shared memory.  A
+// caller that runs several tiles in a row separates them with
+// __syncthreads().
+template <int SCHEME, bool CHARS, int TI, int TJ, int NW>
+__device__ __forceinline__ void flux_tile(const Grid& g, const double* __restrict__ U,
+                                          double* __restrict__ UL,
+                                          const double* __restrict__ alphaF,
+                                          const double* __restrict__ alphaG, double inv_dx,
+                                          double inv_dy, const Gas& G, Ctl* ctl, const CharOut& co,
+                                          int tj, int ti) {
+#include "mhd_flux_tile.inc"
+}
+
 template <int SCHEME, bool CHARS, int TI, int TJ, int NW>
 __global__ void __launch_bounds__(NW * 32, MHD_MINB)
 k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
        const double* __restrict__ alphaF, const double* __restrict__ alphaG,
        double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co) {
-  using T = TileGeom<TI, TJ>;
-  constexpr int RU = T::RU, CU = T::CU;
   if (ctl->skip) return;
-  extern __shared__ double sm[];
-  double* sU = sm + T::OFF_U;
-  double* sF = sm + T::OFF_F;
-  double* sG = sm + T::OFF_G;
-  double* sFx = sm + T::OFF_FX;
-  double* sGy = sm + T::OFF_GY;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int i0 = 2 + blockIdx.y * TI, j0 = 2 + blockIdx.x * TJ;
-  const double gm = g.gamma;
-  __shared__ int tile_nonfinite;  // some stencil state or flux value is inf / NaN
-  if (tid == 0) tile_nonfinite = 0;
-
-  // 0. stage the state box: all copies are issued asynchronously
-  //    (global -> shared without a register round trip), then waited for
-  //    once; a plain load-then-store loop waits one HBM latency per element
-  for (int e = tid; e < NF * RU * CU; e += NW * 32) {
-    const int k = e / (RU * CU), rem = e - k * (RU * CU);
-    const int r = rem / CU, c = rem - r * CU;
-    const int i = i0 - 2 + r, j = j0 - 2 + c;
-    if (i < g.NX && j < g.NY) {
-      const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(sU + e));
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(U + g.at(k, i, j))
-                   : "memory");
-    } else {
-      sU[e] = 0.0;
-    }
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();
-
-  // 1. physical fluxes: F on rows [0,RU) x cols [2,TJ+2), G on rows [2,TI+2) x cols [0,CU)
-  for (int e = tid; e < RU * CU; e += NW * 32) {
-    const int r = e / CU, c = e - r * CU;
-    const bool needF = (c >= 2 && c < TJ + 2), needG = (r >= 2 && r < TI + 2);
-    if (!needF && !needG) continue;
-    const int i = i0 - 2 + r, j = j0 - 2 + c;
-    double q[NF], F[NF], G[NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) q[k] = sU[(k * RU + r) * CU + c];
-    if (i < g.NX && j < g.NY) {
-      phys_flux(gm, q, F, G);
-    } else {
-#pragma unroll
-      for (int k = 0; k < NF; k++) { F[k] = 0.0; G[k] = 0.0; }
-    }
-    bool fin = true;
-#pragma unroll
-    for (int k = 0; k < NF; k++) {
-      fin = fin && isfinite(q[k]);
-      if (k != 4) fin = fin && (!needF || isfinite(F[k]));
-      if (k != 5) fin = fin && (!needG || isfinite(G[k]));
-    }
-    if (!fin) tile_nonfinite = 1;
-    if (needF) {
-#pragma unroll
-      for (int m = 0; m < NF; m++)
-        if (m != 4) sF[(slot_of(m) * RU + r) * TJ + (c - 2)] = F[m];
-    }
-    if (needG) {
-#pragma unroll
-      for (int m = 0; m < NF; m++)  // y frame: slot s holds G[swap_xy(frame m)]
-        if (m != 4) sG[(slot_of(m) * TI + (r - 2)) * CU + c] = G[swap_xy(m)];
-    }
-  }
-  __syncthreads();
-
-  // 2. interfaces
-  double smaxX = 0.0, smaxY = 0.0;
-  int negc = 0;
-  constexpr int NTASK = 2 * TI + 2;
-  for (int t = warp; t < NTASK; t += NW) {
-    Lane L;
-    int ii, jj, gi, gj;
-    bool valid, isx;
-    double al[NF];
-    if (t <= TI) {  // x interfaces between rows i0+ii and i0+ii+1
-      isx = true;
-      ii = t - 1; jj = lane;
-      gi = i0 + ii; gj = j0 + jj;
-      valid = (gi <= g.nx + 1) && (gj < g.ny + 2);
-      L.f = sF + (ii + 1) * TJ + jj; L.fplane = RU * TJ; L.fstep = TJ;
-      L.q = sU + (ii + 1) * CU + (jj + 2); L.qplane = RU * CU; L.qstep = CU;
-      L.swp = false;
-      L.l1 = (g.bc[LEFT] == OPEN && gi < 2) ? 2 : 1;
-      L.l2 = (g.bc[RIGHT] == OPEN && gi > g.nx) ? 1 : 2;
-      if (SCHEME == 3 && valid) {
-#pragma unroll
-        for (int k = 0; k < NF; k++) al[k] = alphaF[k * g.NY + gj];
-      }
-    } else {  // y interfaces between columns j and j+1
-      isx = false;
-      int rr;
-      if (t < NTASK - 1) { rr = t - (TI + 1); jj = lane; }
-      else { rr = lane; jj = -1; }
-      ii = rr;
-      gi = i0 + rr; gj = j0 + jj;
-      valid = (rr < TI) && (gi < g.nx + 2) && (gj < g.ny + 2);
-      L.f = sG + rr * CU + (jj + 1); L.fplane = TI * CU; L.fstep = 1;
-      L.q = sU + (rr + 2) * CU + (jj + 1); L.qplane = RU * CU; L.qstep = 1;
-      L.swp = true;
-      L.l1 = (g.bc[BOTTOM] == OPEN && gj < 2) ? 2 : 1;
-      L.l2 = (g.bc[TOP] == OPEN && gj > g.ny) ? 1 : 2;
-      if (SCHEME == 3 && valid) {
-#pragma unroll
-        for (int k = 0; k < NF; k++) al[k] = alphaG[k * g.NX + gi];
-      }
-    }
-    if (!valid) continue;
-    double Fn[NF], lam[NF], LU[NF], smax;
-    int negp = 0;
-    bool nonfinite = tile_nonfinite != 0, ok = true;
-    if (!nonfinite)
-      ok = interface_flux<SCHEME, CHARS, false>(G, L, al, Fn, smax, negp, lam, LU, nonfinite);
-    if (ok && nonfinite) {
-      bool unused = false;
-      ok = interface_flux<SCHEME, CHARS, true>(G, L, al, Fn, smax, negp, lam, LU, unused);
-    }
-    if (!ok) {
-      atomicExch(&ctl->error, 6);  // ErrorNegativeDensity
-      atomicAdd(&ctl->negd_count, 1ull);
-      continue;
-    }
-    negc += negp;
-    if (isx) {
-      smaxX = take_max(smaxX, smax);
-#pragma unroll
-      for (int m = 0; m < NF; m++) sFx[(m * (TI + 1) + (ii + 1)) * TJ + jj] = Fn[m];
-    } else {
-      smaxY = take_max(smaxY, smax);
-#pragma unroll
-      for (int m = 0; m < NF; m++) sGy[(m * TI + ii) * (TJ + 1) + (jj + 1)] = Fn[m];
-      if (gi == g.nx + 1 && gj == g.ny + 1) ctl->neg_last = negp;  // last interface of the sweep
-    }
-    if (CHARS) {
-      double* cdst = isx ? co.cx : co.cy;
-      double* ldst = isx ? co.LUx : co.LUy;
-#pragma unroll
-      for (int k = 0; k < NF; k++) {
-        cdst[g.at(k, gi, gj)] = lam[k];
-        ldst[g.at(k, gi, gj)] = LU[k];
-      }
-    }
-  }
-  __syncthreads();
-
-  // 3. UL of the tile's cells
-  for (int e = tid; e < TI * TJ; e += NW * 32) {
-    const int r = e / TJ, c = e - r * TJ;
-    const int i = i0 + r, j = j0 + c;
-    if (i >= g.nx + 2 || j >= g.ny + 2) continue;
-#pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const double fr = sFx[(k * (TI + 1) + (r + 1)) * TJ + c];
-      const double fl = sFx[(k * (TI + 1) + r) * TJ + c];
-      const int fk = swap_xy(k);  // y numerical fluxes are stored in the y frame
-      const double gr = sGy[(fk * TI + r) * (TJ + 1) + (c + 1)];
-      const double gl = sGy[(fk * TI + r) * (TJ + 1) + c];
-      UL[g.at(k, i, j)] = -(inv_dx) * (fr - fl) - (inv_dy) * (gr - gl);
-    }
-  }
-
-  // CFL maxima and counters
-  smaxX = warp_max(smaxX);
-  smaxY = warp_max(smaxY);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) negc += __shfl_xor_sync(0xffffffffu, negc, o);
-  if (lane == 0) {
-    atomic_max_pos(&ctl->maxX, smaxX);
-    atomic_max_pos(&ctl->maxY, smaxY);
-    if (negc) atomicAdd(&ctl->neg_count, (unsigned long long)negc);
-  }
+  const int tj = blockIdx.x, ti = blockIdx.y;
+#include "mhd_flux_tile.inc"
 }
 
 // ENO-LF dissipation coefficients (spatialmethodenolf.cpp:66-125):
 // alphaF[k][j] = max_i |lambda_k(U_ij)|, alphaG[k][i] = max_j |lambda_k(swap U_ij)|
 // over i in [1, nx+2), j in [1, ny+2) without the (i < 2 && j < 2) corner.
-// The arrays must be zero on entry.  Block = 32 (j) x 8 (i) cells.
-__global__ void __launch_bounds__(256)
-k_lf_alpha(Grid g, const double* __restrict__ U, double* alphaF, double* alphaG, Ctl* ctl) {
-  if (ctl->skip) return;
-  __shared__ double col[8][NF][33];
+// The arrays must be zero on entry.  Block = 32 (j) x 8 (i) cells.  Like the
+// reference's "if( alphaabs > alpha ) alpha = alphaabs" a NaN eigenvalue
+// never enters a maximum: each cell contributes max(0, |lambda|) first.
+// One 32 x 8 block of cells (bx, by); all 256 threads call it with the same
+// block, col is a shared [8][NF][33] scratch.
+__device__ __forceinline__ void lf_alpha_block(const Grid& g, const double* __restrict__ U,
+                                               double* alphaF, double* alphaG, Ctl* ctl, int bx,
+                                               int by, double (*col)[NF][33]) {
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int j = 1 + blockIdx.x * 32 + tx, i = 1 + blockIdx.y * 8 + ty;
+  const int j = 1 + bx * 32 + tx, i = 1 + by * 8 + ty;
   double lx[NF], ly[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) { lx[k] = 0.0; ly[k] = 0.0; }
@@ -441,14 +288,14 @@ k_lf_alpha(Grid g, const double* __restrict__ U, double* alphaF, double* alphaG,
     } else {
       negp += np;
 #pragma unroll
-      for (int k = 0; k < NF; k++) lx[k] = fabs(lam[k]);
+      for (int k = 0; k < NF; k++) lx[k] = take_max(0.0, fabs(lam[k]));
       double s[NF];
 #pragma unroll
       for (int k = 0; k < NF; k++) s[k] = q[swap_xy(k)];
       eigenvalues_at(g.gamma, s, lam, np);
       negp += np;
 #pragma unroll
-      for (int k = 0; k < NF; k++) ly[k] = fabs(lam[k]);
+      for (int k = 0; k < NF; k++) ly[k] = take_max(0.0, fabs(lam[k]));
     }
   }
   // per-row (alphaG, over j = lanes) maxima
@@ -471,6 +318,13 @@ k_lf_alpha(Grid g, const double* __restrict__ U, double* alphaF, double* alphaG,
     }
   }
   (void)negp;
+}
+
+__global__ void __launch_bounds__(256)
+k_lf_alpha(Grid g, const double* __restrict__ U, double* alphaF, double* alphaG, Ctl* ctl) {
+  if (ctl->skip) return;
+  __shared__ double col[8][NF][33];
+  lf_alpha_block(g, U, alphaF, alphaG, ctl, blockIdx.x, blockIdx.y, col);
 }
 
 }  // namespace MHD_KNS

@@ -25,13 +25,18 @@ struct Snap {
   const double *l, *r, *b, *t;  // Dirichlet edge snapshots [8][NY], [8][NX]
 };
 
-__global__ void k_bc(Grid g, double* __restrict__ U, Snap d, const Ctl* ctl) {
-  if (ctl->skip) return;
+// Number of ghost values one fill writes: 2 layers x 8 fields on 4 sides.
+__host__ __device__ __forceinline__ long long bc_count(const Grid& g) {
+  return 4LL * NF * g.ny + 4LL * NF * g.nx;
+}
+
+// Ghost value e in [0, bc_count(g)).
+__device__ __forceinline__ void bc_elem(const Grid& g, double* __restrict__ U, const Snap& d,
+                                        long long e) {
   const int nx = g.nx, ny = g.ny;
-  const long long nlr = 2LL * 2 * NF * ny, nbt = 2LL * 2 * NF * nx;
+  const long long nlr = 2LL * 2 * NF * ny;
   const double rxy = g.dx / g.dy, ryx = g.dy / g.dx;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nlr + nbt;
-       e += (long long)gridDim.x * blockDim.x) {
+  {
     if (e < nlr) {  // left / right: side, layer, field, row j (fastest)
       const int j = 2 + int(e % ny);
       long long q = e / ny;
@@ -104,6 +109,14 @@ __global__ void k_bc(Grid g, double* __restrict__ U, Snap d, const Ctl* ctl) {
   }
 }
 
+__global__ void k_bc(Grid g, double* __restrict__ U, Snap d, const Ctl* ctl) {
+  if (ctl->skip) return;
+  const long long n = bc_count(g);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    bc_elem(g, U, d, e);
+}
+
 // Dirichlet edge snapshot (spatialintegrationmethod.cpp:39-59).
 __global__ void k_snapshot(Grid g, const double* __restrict__ U, double* l, double* r, double* b,
                            double* t) {
@@ -129,6 +142,18 @@ __global__ void k_snapshot(Grid g, const double* __restrict__ U, double* l, doub
 //   mode 1: U1 = U + dt*UL
 //   mode 2: U2 = (3/4)U + (1/4)U1 + (1/4)dt*UL
 //   mode 3: U  = (1/3)U + (2/3)U2 + (2/3)dt*UL
+__device__ __forceinline__ void combine_at(int mode, double dt, long long a,
+                                           double* __restrict__ U, double* __restrict__ U1,
+                                           double* __restrict__ U2,
+                                           const double* __restrict__ UL) {
+  switch (mode) {
+    case 0: U[a] = U[a] + dt * UL[a]; break;
+    case 1: U1[a] = U[a] + dt * UL[a]; break;
+    case 2: U2[a] = (3.0 / 4.0) * U[a] + (1.0 / 4.0) * U1[a] + (1.0 / 4.0) * dt * UL[a]; break;
+    default: U[a] = (1.0 / 3.0) * U[a] + (2.0 / 3.0) * U2[a] + (2.0 / 3.0) * dt * UL[a]; break;
+  }
+}
+
 __global__ void k_combine(Grid g, int mode, double* __restrict__ U, double* __restrict__ U1,
                           double* __restrict__ U2, const double* __restrict__ UL, const Ctl* ctl) {
   if (ctl->skip) return;
@@ -137,13 +162,7 @@ __global__ void k_combine(Grid g, int mode, double* __restrict__ U, double* __re
   const int i = 2 + blockIdx.y;
   const int k = blockIdx.z;
   if (j >= g.ny + 2) return;
-  const long long a = g.at(k, i, j);
-  switch (mode) {
-    case 0: U[a] = U[a] + dt * UL[a]; break;
-    case 1: U1[a] = U[a] + dt * UL[a]; break;
-    case 2: U2[a] = (3.0 / 4.0) * U[a] + (1.0 / 4.0) * U1[a] + (1.0 / 4.0) * dt * UL[a]; break;
-    default: U[a] = (1.0 / 3.0) * U[a] + (2.0 / 3.0) * U2[a] + (2.0 / 3.0) * dt * UL[a]; break;
-  }
+  combine_at(mode, dt, g.at(k, i, j), U, U1, U2, UL);
 }
 
 // ---------------------------------------------------------------------------

@@ -47,6 +47,24 @@ _ip = C.POINTER(C.c_int)
 _lib = None
 
 
+class BatchDesc(C.Structure):
+    """mhd_batch_desc: one run of a batch."""
+
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("gamma", C.c_double), ("bc", C.c_int * 4), ("scheme", C.c_int),
+                ("time_method", C.c_int), ("dt_min", C.c_double), ("dt_max", C.c_double),
+                ("cfl", C.c_double), ("dt0", C.c_double), ("t_end", C.c_double),
+                ("max_steps", C.c_int)]
+
+
+class BatchState(C.Structure):
+    """mhd_batch_state: progress of one run."""
+
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("steps", C.c_int), ("active", C.c_int),
+                ("status", C.c_int), ("phase", C.c_int), ("retries", C.c_longlong),
+                ("neg_pressure", C.c_longlong)]
+
+
 class SorParams(C.Structure):
     """mhd_sor_params: the [divb corrector] keys (file_access.cpp:273-299)."""
 
@@ -98,6 +116,18 @@ def library():
         "mhd_fp64_peak": [C.c_int, _dp],
         "mhd_divb_calc_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                   C.c_double, _ip, C.c_void_p, C.c_void_p],
+        "mhd_batch_create": [C.c_int, C.POINTER(BatchDesc), C.c_int, C.POINTER(vp)],
+        "mhd_batch_destroy": [vp],
+        "mhd_batch_last_error": [vp, C.c_char_p, C.c_size_t, _ip],
+        "mhd_batch_upload": [vp, C.c_int, _dp],
+        "mhd_batch_download": [vp, C.c_int, _dp],
+        "mhd_batch_advance": [vp, C.c_int, C.c_int, _ip],
+        "mhd_batch_get_state": [vp, C.c_int, C.POINTER(BatchState)],
+        "mhd_batch_tune": [vp, C.c_int, _ip, _ip, _dp],
+        "mhd_batch_set_tile": [vp, C.c_int, C.c_int],
+        "mhd_batch_init_problem": [vp, C.c_int, C.c_int, _dp, C.c_int],
+        "mhd_batch_stream": [vp, C.POINTER(vp)],
+        "mhd_batch_launches": [vp, C.POINTER(C.c_longlong)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

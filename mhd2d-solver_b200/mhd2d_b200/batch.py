@@ -1,0 +1,176 @@
+"""Batched runs (mhd_batch_* in include/mhd2d_b200.h).
+
+The reference runs one problem per process (main.cpp); running many is
+starting several copies with different INI files.  ``Batch`` holds many
+independent runs of uneven grid sizes, schemes, boundary conditions and end
+times on one GPU and advances all of them together, each following the
+reference main loop (step, t += dt, stop at t >= t_end, on a NaN or on a
+fatal status).  Each run's result is bit-identical to the same problem
+advanced alone through a ``Context``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import (ENO_ROE, OK, RK3, STATUS_NAMES, BatchDesc, BatchState, MhdError, TStatus, _p,
+               library)
+
+PROBLEM_EXPLOSION, PROBLEM_WAVE, PROBLEM_ORSZAG_TANG, PROBLEM_PLASMA_SHEET = 1, 2, 3, 4
+TILE_7x32, TILE_3x32 = 0, 1
+WAVES = ("negative fast magnetosonic", "negative alfven", "negative slow magnetosonic",
+         "entropy", "positive slow magnetosonic", "positive alfven",
+         "positive fast magnetosonic")
+
+
+@dataclass
+class Run:
+    """One run of a batch (the [problem] / [time] / [method] keys that matter)."""
+
+    nx: int
+    ny: int
+    dx: float
+    dy: float
+    gamma: float
+    bc: tuple
+    scheme: int = ENO_ROE
+    time_method: int = RK3
+    dt_min: float = 1e-9
+    dt_max: float = 1.0
+    cfl: float = 0.4
+    dt0: float = 1e-3
+    t_end: float = 1.0
+    max_steps: int = 0
+
+    def desc(self):
+        d = BatchDesc()
+        d.nx, d.ny, d.dx, d.dy, d.gamma = self.nx, self.ny, self.dx, self.dy, self.gamma
+        for s in range(4):
+            d.bc[s] = int(self.bc[s])
+        d.scheme, d.time_method = self.scheme, self.time_method
+        d.dt_min, d.dt_max, d.cfl = self.dt_min, self.dt_max, self.cfl
+        d.dt0, d.t_end, d.max_steps = self.dt0, self.t_end, self.max_steps
+        return d
+
+
+class Batch:
+    def __init__(self, runs, device=0):
+        self.lib = library()
+        self.runs = list(runs)
+        arr = (BatchDesc * len(self.runs))(*[r.desc() for r in self.runs])
+        h = C.c_void_p()
+        st = self.lib.mhd_batch_create(len(self.runs), arr, device, C.byref(h))
+        if st != OK:
+            msg = ""
+            if h:
+                msg = self._message(h)
+                self.lib.mhd_batch_destroy(h)
+            raise MhdError(f"mhd_batch_create failed: {STATUS_NAMES.get(st, st)} {msg}")
+        self.h = h
+
+    def _message(self, h=None):
+        buf = C.create_string_buffer(1024)
+        e = C.c_int(0)
+        self.lib.mhd_batch_last_error(h or self.h, buf, 1024, C.byref(e))
+        return buf.value.decode()
+
+    def _check(self, st, what):
+        if st != OK:
+            raise MhdError(f"{what}: {STATUS_NAMES.get(st, st)} {self._message()}")
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mhd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return len(self.runs)
+
+    def shape(self, i):
+        r = self.runs[i]
+        return (8, r.nx + 4, r.ny + 4)
+
+    # -- data ------------------------------------------------------------------------
+    def upload(self, i, U):
+        self._check(self.lib.mhd_batch_upload(self.h, i, _p(np.ascontiguousarray(U))), "upload")
+
+    def download(self, i, out=None):
+        out = np.empty(self.shape(i)) if out is None else out
+        self._check(self.lib.mhd_batch_download(self.h, i, _p(out)), "download")
+        return out
+
+    def init_problem(self, i, kind, params=()):
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        ptr = _p(p) if p.size else None
+        self._check(self.lib.mhd_batch_init_problem(self.h, i, kind, ptr, int(p.size)),
+                    "init_problem")
+
+    def init_explosion(self, i, r=0.1, rho_in=1.0, p_in=10.0, rho_out=0.125, p_out=1.0,
+                       bx=2 ** -0.5, by=2 ** -0.5):
+        self.init_problem(i, PROBLEM_EXPLOSION, [0.0, 0.0, r, rho_in, p_in, rho_out, p_out, bx, by])
+
+    def init_wave(self, i, wave, kx, ky, eps=1e-6, rho=1.0, u=0.0, v=0.0, w=0.0, bx=1.0,
+                  by=2 ** 0.5, bz=0.5, p=None, lx=1.0, ly=1.0, x0=-0.5, y0=-0.5):
+        p = 1.0 / self.runs[i].gamma if p is None else p
+        self.init_problem(i, PROBLEM_WAVE, [x0, y0, lx, ly, rho, u, v, w, bx, by, bz, p, eps,
+                                            float(wave), float(kx), float(ky)])
+
+    def init_orszag_tang(self, i):
+        self.init_problem(i, PROBLEM_ORSZAG_TANG, [])
+
+    def init_plasma_sheet(self, i, amps, delta=0.1, x0=-2.0, y0=-1.0):
+        a = list(amps)
+        self.init_problem(i, PROBLEM_PLASMA_SHEET, [x0, y0, delta, float(len(a))] + a)
+
+    # -- stepping --------------------------------------------------------------------
+    def advance(self, stages, check_every=0):
+        """Advance every active run by up to `stages` stages; returns the active count."""
+        n = C.c_int(0)
+        self._check(self.lib.mhd_batch_advance(self.h, int(stages), int(check_every),
+                                               C.byref(n)), "advance")
+        return n.value
+
+    def run(self, max_stages=10 ** 9, check_every=48):
+        """Advance until every run stopped (or max_stages)."""
+        return self.advance(max_stages, check_every)
+
+    def state(self, i):
+        s = BatchState()
+        self._check(self.lib.mhd_batch_get_state(self.h, i, C.byref(s)), "get_state")
+        return {"t": s.t, "dt": s.dt, "steps": s.steps, "active": bool(s.active),
+                "status": TStatus(s.status not in (0, 1, 2, 7), s.status), "phase": s.phase,
+                "retries": s.retries, "neg_pressure": s.neg_pressure}
+
+    def states(self):
+        return [self.state(i) for i in range(len(self))]
+
+    def tune(self, reps=2):
+        t, c, ms = C.c_int(0), C.c_int(0), C.c_double(0)
+        self._check(self.lib.mhd_batch_tune(self.h, reps, C.byref(t), C.byref(c), C.byref(ms)),
+                    "tune")
+        return {"tile": t.value, "ctas_per_sm": c.value, "ms_per_stage": ms.value}
+
+    def set_tile(self, tile, ctas_per_sm=0):
+        self._check(self.lib.mhd_batch_set_tile(self.h, tile, ctas_per_sm), "set_tile")
+
+    def stream(self):
+        s = C.c_void_p()
+        self.lib.mhd_batch_stream(self.h, C.byref(s))
+        return s.value or 0
+
+    def launches(self):
+        n = C.c_longlong(0)
+        self.lib.mhd_batch_launches(self.h, C.byref(n))
+        return n.value

@@ -158,6 +158,22 @@ def test_steps_vs_oracle_ot128(scheme, tm):
     assert same(ctx.download(), Uo)
 
 
+def test_lf_run_into_nan_matches_oracle():
+    """ENO-LF blocky state with Neumann sides that blows up into NaNs: the
+    dissipation maxima skip NaN eigenvalues like the reference's
+    "if( alphaabs > alpha )" and the run stops at the same step."""
+    p = P.random_blocky(20, 30, seed=5, bc=(M.NEUMANN,) * 4)
+    ctx = make_ctx(p, scheme=M.ENO_LF, dt_min=1e-9, dt_max=0.01, cfl=0.4, flags=0)
+    r = gpu_run(ctx, 1e-3, t_max=0.02)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=M.ENO_LF, dt_min=1e-9,
+               dt_max=0.01, cfl=0.4)
+    Uo = p.U.copy()
+    ro = o.run(Uo, 1e-3, t_max=0.02)
+    assert np.isnan(Uo[0, 2, 2])  # the case really reaches the NaN stop
+    assert (r["steps"], r["t"], r["dt"]) == (ro["steps"], ro["t"], ro["dt"])
+    assert same(interior(ctx.download()), interior(Uo))
+
+
 def test_retry_path_matches_reference():
     d = np.load(os.path.join(GOLD, "run_explosion_retry.npz"))
     p = _problem(d)
