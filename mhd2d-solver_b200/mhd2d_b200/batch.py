@@ -174,3 +174,63 @@ class Batch:
         n = C.c_longlong(0)
         self.lib.mhd_batch_launches(self.h, C.byref(n))
         return n.value
+
+    def cells(self):
+        return np.array([r.nx * r.ny for r in self.runs], dtype=np.int64)
+
+    def steps(self):
+        return np.array([self.state(i)["steps"] for i in range(len(self))], dtype=np.int64)
+
+
+@dataclass
+class MixedRun:
+    """One run of the mixed benchmark batch and its device-side initial state."""
+
+    run: Run
+    kind: str       # "explosion" or "wave"
+    wave: int = 0
+    kx: int = 1
+    ky: int = 0
+
+    def init(self, b, i):
+        if self.kind == "explosion":
+            b.init_explosion(i)
+        else:
+            b.init_wave(i, self.wave, self.kx, self.ky, eps=1e-6)
+
+
+def mixed_runs(n=512, seed=0, side_min=64, side_max=1024, gamma=5.0 / 3.0):
+    """The mixed batch of independent runs (seeded):
+
+    * grid sides drawn log-uniformly in [side_min, side_max], nx and ny
+      independently;
+    * ENO-LF or ENO-Roe with probability 1/2, RK3, CFL 0.4, t_end ~ U[0.1, 1];
+    * half 2-D explosions on [-0.5, 0.5]^2 with open sides (rho 1, p 10
+      inside r < 0.1; rho 0.125, p 1 outside; B = (1, 1, 0)/sqrt 2);
+    * half linear waves on the periodic unit box (rho 1, p 1/gamma,
+      B = (1, sqrt 2, 0.5), a 1e-6 right-eigenvector perturbation of one of
+      the 7 waves), integer wave vector (kx, ky) close to an angle drawn
+      uniformly in [0, pi/2).
+    """
+    import math
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(side_min), math.log(side_max)
+    out = []
+    for r in range(n):
+        nx = int(round(math.exp(rng.uniform(lo, hi))))
+        ny = int(round(math.exp(rng.uniform(lo, hi))))
+        scheme = 3 if rng.uniform() < 0.5 else 2
+        t_end = float(rng.uniform(0.1, 1.0))
+        common = dict(scheme=scheme, time_method=RK3, dt_min=1e-10, dt_max=2.0 ** -6,
+                      cfl=0.4, dt0=2.0 ** -10, t_end=t_end)
+        if r % 2 == 0:
+            run = Run(nx, ny, 1.0 / nx, 1.0 / ny, gamma, (4, 4, 4, 4), **common)
+            out.append(MixedRun(run, "explosion"))
+        else:
+            run = Run(nx, ny, 1.0 / nx, 1.0 / ny, gamma, (1, 1, 1, 1), **common)
+            ang = rng.uniform(0.0, 0.5 * math.pi)
+            kx, ky = int(round(4 * math.cos(ang))), int(round(4 * math.sin(ang)))
+            if kx == 0 and ky == 0:
+                kx = 1
+            out.append(MixedRun(run, "wave", int(rng.integers(0, 7)), kx, ky))
+    return out
