@@ -267,6 +267,61 @@ int mhd_batch_stream( mhd_batch* b, void** stream );
 /* Kernel launches issued so far (graph nodes counted per replay). */
 int mhd_batch_launches( mhd_batch* b, long long* launches );
 
+/* ------------------------------------------------------------------------
+ * Discrete adjoint of the ENO-Roe time step.  The reference has no
+ * differentiation; this is the gradient of its discrete forward map.
+ * J = sum over the final interior of |m|^2 / (2 rho) dx dy (kinetic energy).
+ *
+ * mhd_adj_forward advances the initial state nsteps steps exactly as a
+ * context does (TimeIntegrationRK3::step / TimeIntegrationEuler::step with
+ * updateDt and the RK3 retry rule, ENO-Roe fluxes; bit-identical results),
+ * recording every executed stage (input buffer, stage update, dt), the ENO
+ * stencil and upwind choices of every interface and characteristic (4-bit
+ * codes), and a checkpoint of U every `checkpoint_every` steps.
+ * mhd_adj_backward computes dJ/dU0 of that discrete map with the recorded
+ * choices and dt frozen: per checkpoint segment, last first, the segment is
+ * replayed from its checkpoint and its stages are differentiated in reverse.
+ * mhd_adj_replay runs the same frozen map from another initial state (the
+ * frozen-stencil, frozen-dt forward that central finite differences of J
+ * need). */
+typedef struct mhd_adj mhd_adj;
+
+typedef struct {
+   int       steps, stages, checkpoints, retries;
+   double    t, dt;              /* simulated time and last dt of the recording */
+   double    ms_forward;         /* device time of the recording forward */
+   double    ms_backward;        /* device time of the last backward (replays included) */
+   double    ms_replay;          /* device time of the last full replay */
+   long long launches;
+} mhd_adj_stats;
+
+int mhd_adj_create( int nx, int ny, double dx, double dy, double gamma, const int bc[4],
+                    int time_method, double dt_min, double dt_max, double cfl,
+                    int checkpoint_every, int device, mhd_adj** out );
+int mhd_adj_destroy( mhd_adj* a );
+int mhd_adj_last_error( mhd_adj* a, char* buf, size_t len, int* is_error );
+/* Initial state from the host (Dirichlet sides take their edges from it). */
+int mhd_adj_upload( mhd_adj* a, const double* U0 );
+/* Initial state generated on the device (kinds of mhd_batch_init_problem). */
+int mhd_adj_init_problem( mhd_adj* a, int kind, const double* p, int np );
+/* Recording forward run; *J (optional) = J of the final state. */
+int mhd_adj_forward( mhd_adj* a, int nsteps, double dt0, double* J );
+/* Frozen replay from a host initial state (NULL: the recorded one); Dirichlet
+   sides take their edges from that state, so dJ/dU0 includes the edge
+   snapshot's dependence on U0. */
+int mhd_adj_replay( mhd_adj* a, const double* U0, double* J );
+/* Frozen replay from a device-generated initial state. */
+int mhd_adj_replay_problem( mhd_adj* a, int kind, const double* p, int np, double* J );
+int mhd_adj_backward( mhd_adj* a );
+/* dJ/dU0 as a host [8][NX][NY] block (ghost entries 0). */
+int mhd_adj_gradient( mhd_adj* a, double* dJdU0 );
+/* dJ/da_k, k = 1..K, of the plasma-sheet initial state (MHD_PROBLEM_PLASMA_SHEET
+   with corner x0, y0): contraction of dJ/dU0 with dU0/da_k. */
+int mhd_adj_sheet_gradient( mhd_adj* a, double x0, double y0, int K, double* dJda );
+/* which: 0 initial state, 1 final state of the recording, 2 working state. */
+int mhd_adj_download( mhd_adj* a, int which, double* U );
+int mhd_adj_info( mhd_adj* a, mhd_adj_stats* out );
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,1178 @@
+// Discrete adjoint of the ENO-Roe RK3-TVD (or Euler) time step
+// (include/mhd2d_b200.h, mhd_adj_*).
+//
+// Forward (recording) run — the reference main loop's stepping
+// (TimeIntegrationRK3::step with its retry rule, updateDt) on the device:
+//   * every executed spatial operator ("stage") is logged by the controller
+//     kernel: which buffer it read (U, U1, U2), the stage update that
+//     followed (k_combine mode) and its dt;
+//   * the flux kernel records, per interface and characteristic, the ENO-2
+//     stencil choices of w- and w+ and the upwind choice as 4-bit codes
+//     (one 32-bit word per interface);
+//   * U is checkpointed at the start of every K-th step.
+// Replay — the same stage sequence with the recorded choices and dt frozen
+// (k_flux MASK = 2): bit-identical to the recording on the same initial
+// state; on a perturbed one it is the frozen-stencil, frozen-dt map whose
+// derivative the adjoint computes (central finite differences use it).
+// Backward — for each checkpoint segment, last first: replay the segment
+// from its checkpoint keeping every stage input, then walk its stages in
+// reverse: adjoint of the stage update (linear), then the adjoint of the
+// spatial operator L at the stored stage input:
+//   1. ka_adj_iface: per x / y interface, recompute the midpoint
+//      eigen-system and the frozen ENO combination, and form the adjoints
+//      of the 4 stencil fluxes and of the two midpoint states
+//      (mhd_adjoint_gen.cuh, generated reverse-mode code);
+//   2. ka_adj_gather: per cell, sum the contributions of every interface
+//      that used it and apply the transposed flux Jacobians;
+//   3. ka_adj_bc: transpose of the boundary fill (ghost -> interior; the
+//      Dirichlet edges, snapshots of U0, collect their own adjoints).
+// The result is dJ/dU0 for J = sum of the kinetic energy |m|^2 / (2 rho)
+// dx dy over the final interior.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mhd2d_b200.h"
+#include "mhd_adjoint_gen.cuh"
+#include "mhd_flux.cuh"
+#include "mhd_misc.cuh"
+#include "mhd_problems.cuh"
+
+namespace mhd {
+namespace MHD_KNS {
+
+constexpr int ATI = 7, ATJ = 32, ANW = 8;  // flux tile of the forward runs
+using AGeom = TileGeom<ATI, ATJ>;
+constexpr int NSC = 44;  // scratch words per interface: 4 x 7 flux adjoints, 2 x 8 state adjoints
+
+struct StageRec {
+  int in_buf;  // 0 U, 1 U1, 2 U2
+  int mode;    // k_combine mode that followed
+  double dt;
+};
+
+// The step controller with a log of the executed stages.
+__global__ void ka_control(Ctl* c, StepParams p, int phase, double arg, StageRec* log, int* nlog,
+                           int cap) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const bool ran = !c->skip && !c->error;  // the stage's flux ran
+  control_step(c, p, phase, arg);
+  if (!ran || c->error) return;
+  int in_buf = -1, mode = -1;
+  double dt = c->dt;
+  switch (phase) {
+    case PH_RK_FIRST: in_buf = 0; mode = 1; break;
+    case PH_EULER: in_buf = 0; mode = 0; break;
+    case PH_RK_SECOND:
+    case PH_RK_FINAL:
+      in_buf = phase == PH_RK_SECOND ? 1 : 2;
+      if (c->retry) {  // the retry tail starts with U1 = U + dt*UL, dt = min(dt1, dt2, dt3)
+        mode = 1;
+        dt = min3(c->dt1, c->dt2, c->dt3);
+      } else {
+        mode = phase == PH_RK_SECOND ? 2 : 3;
+      }
+      break;
+    default: return;
+  }
+  const int n = *nlog;
+  if (n >= cap) {  // the host sized the log; running past it stops the run
+    c->error = 10;
+    c->skip = 1;
+    return;
+  }
+  log[n] = StageRec{in_buf, mode, dt};
+  *nlog = n + 1;
+}
+
+// Stage update with an explicit dt (replay).
+__global__ void ka_combine(Grid g, int mode, double dt, double* __restrict__ U,
+                           double* __restrict__ U1, double* __restrict__ U2,
+                           const double* __restrict__ UL) {
+  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = 2 + blockIdx.y;
+  const int k = blockIdx.z;
+  if (j >= g.ny + 2) return;
+  combine_at(mode, dt, g.at(k, i, j), U, U1, U2, UL);
+}
+
+// Adjoint of one stage update (interior, elementwise); lUL receives the
+// adjoint of UL.
+__global__ void ka_combine_adj(Grid g, int mode, double dt, double* __restrict__ lU,
+                               double* __restrict__ lU1, double* __restrict__ lU2,
+                               double* __restrict__ lUL) {
+  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = 2 + blockIdx.y;
+  const int k = blockIdx.z;
+  if (j >= g.ny + 2) return;
+  const long long a = g.at(k, i, j);
+  switch (mode) {
+    case 0:  // U = U + dt*UL
+      lUL[a] = dt * lU[a];
+      break;
+    case 1: {  // U1 = U + dt*UL
+      const double b = lU1[a];
+      lUL[a] = dt * b;
+      lU[a] += b;
+      lU1[a] = 0.0;
+      break;
+    }
+    case 2: {  // U2 = (3/4)U + (1/4)U1 + (1/4)dt*UL
+      const double b = lU2[a];
+      lUL[a] = (1.0 / 4.0) * dt * b;
+      lU[a] += (3.0 / 4.0) * b;
+      lU1[a] += (1.0 / 4.0) * b;
+      lU2[a] = 0.0;
+      break;
+    }
+    default: {  // U = (1/3)U + (2/3)U2 + (2/3)dt*UL
+      const double b = lU[a];
+      lUL[a] = (2.0 / 3.0) * dt * b;
+      lU2[a] += (2.0 / 3.0) * b;
+      lU[a] = (1.0 / 3.0) * b;
+      break;
+    }
+  }
+}
+
+// Stencil of interface f (between cells f and f+1 along the direction) at
+// transverse index t: cell of stencil point p.
+__device__ __forceinline__ long long cell_at(const Grid& g, bool ydir, int k, int f, int t, int p) {
+  return ydir ? g.at(k, t, f - 1 + p) : g.at(k, f - 1 + p, t);
+}
+
+constexpr int AIB = 64;  // threads per block of ka_adj_iface (37 KB of shared memory)
+
+// Adjoint of the numerical flux of every interface of one direction.  One
+// thread per interface; the interface's frame is the x frame (y interfaces
+// work on x/y-swapped states, as the forward does).  Writes NSC scratch
+// words per interface: S[c][f][t] (x) or S[c][t][f] (y) with c = 7p +
+// slot(m) for the adjoint of the frame flux component m at stencil point p,
+// 28 + k for the adjoint of the frame state U1[k], 36 + k for U2[k].
+template <bool YDIR>
+__global__ void __launch_bounds__(AIB) ka_adj_iface(Grid g, Gas G, const double* __restrict__ X,
+                                                    const unsigned* __restrict__ mask,
+                                                    const double* __restrict__ lUL,
+                                                    double* __restrict__ S, double inv_d) {
+  __shared__ double sF[28][AIB];   // frame fluxes of the 4 stencil points
+  __shared__ double sFb[28][AIB];  // their adjoints
+  __shared__ double sQ[16][AIB];   // U1, U2 (frame)
+  const int tid = threadIdx.x;
+  const int nf = YDIR ? g.ny + 1 : g.nx + 1;  // faces 1..n+1 along the direction
+  const int nt = YDIR ? g.nx : g.ny;          // interior transverse cells 2..n+1
+  const long long n = (long long)nf * nt;
+  const long long NXY = (long long)g.NX * g.NY;
+  const long long e = blockIdx.x * (long long)blockDim.x + tid;
+  if (e >= n) return;
+  // consecutive threads walk the contiguous j direction
+  const int f = YDIR ? 1 + int(e % nf) : 1 + int(e / nt);
+  const int t = YDIR ? 2 + int(e / nf) : 2 + int(e % nt);
+  const int ncell = YDIR ? g.ny : g.nx;
+  const int lo_bc = YDIR ? BOTTOM : LEFT, hi_bc = YDIR ? TOP : RIGHT;
+  const int l1 = (g.bc[lo_bc] == OPEN && f < 2) ? 2 : 1;
+  const int l2 = (g.bc[hi_bc] == OPEN && f > ncell) ? 1 : 2;
+  // frame states of the stencil and their fluxes
+  for (int p = 0; p < 4; p++) {
+    double q[NF], F[NF], Gy[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      const int kk = YDIR ? swap_xy(k) : k;
+      q[k] = X[cell_at(g, YDIR, kk, f, t, p)];
+    }
+    phys_flux(G.gm, q, F, Gy);
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      if (m == 4) continue;
+      sF[p * 7 + slot_of(m)][tid] = F[m];
+      sFb[p * 7 + slot_of(m)][tid] = 0.0;
+    }
+    if (p == l1) {
+#pragma unroll
+      for (int k = 0; k < NF; k++) sQ[k][tid] = q[k];
+    }
+    if (p == l2) {
+#pragma unroll
+      for (int k = 0; k < NF; k++) sQ[8 + k][tid] = q[k];
+    }
+  }
+  // adjoint of the frame numerical flux: UL = -(F_f - F_{f-1}) / d - ...
+  double lF[NF];
+  const int cell_lo = f, cell_hi = f + 1;  // the two cells sharing the face
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    const int kk = YDIR ? swap_xy(m) : m;
+    double v = 0.0;
+    if (cell_lo >= 2 && cell_lo <= ncell + 1)
+      v -= inv_d * lUL[YDIR ? g.at(kk, t, cell_lo) : g.at(kk, cell_lo, t)];
+    if (cell_hi >= 2 && cell_hi <= ncell + 1)
+      v += inv_d * lUL[YDIR ? g.at(kk, t, cell_hi) : g.at(kk, cell_hi, t)];
+    lF[m] = v;
+  }
+  double U1[NF], U2[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    U1[k] = sQ[k][tid];
+    U2[k] = sQ[8 + k][tid];
+  }
+  double* out = YDIR ? S + (long long)t * g.NY + f : S + (long long)f * g.NY + t;
+  Mid e0;
+  if (!midpoint(G, U1, U2, e0)) {
+    for (int c = 0; c < NSC; c++) out[c * NXY] = 0.0;
+    return;
+  }
+  const unsigned mw = mask[YDIR ? (long long)t * g.NY + f : (long long)f * g.NY + t];
+  MidBar mb{};
+#pragma unroll 1
+  for (int k = 0; k < 7; k++) {
+    double l[NF], r[NF];
+#pragma unroll
+    for (int m = 0; m < NF; m++) { l[m] = 0.0; r[m] = 0.0; }
+    lv_row(e0, G, k, l);
+    rv_row(e0, G, k, r);
+    const unsigned code = (mw >> (4 * k)) & 0xFu;
+    const int up = int(code >> 2);
+    double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;  // frozen ENO combination of the 4 points
+    if (up == 0) {
+      if (code & 1u) { c0 = -0.5; c1 = 1.5; } else { c1 = 0.5; c2 = 0.5; }
+    } else if (up == 1) {
+      if (code & 2u) { c1 = 0.5; c2 = 0.5; } else { c2 = 1.5; c3 = -0.5; }
+    }
+    double phi[NF], fw = 0.0, gk = 0.0;
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      if (m == 4) { phi[m] = 0.0; continue; }
+      const int s = slot_of(m);
+      phi[m] = c0 * sF[s][tid] + c1 * sF[7 + s][tid] + c2 * sF[14 + s][tid] + c3 * sF[21 + s][tid];
+      fw += l[m] * phi[m];
+    }
+#pragma unroll
+    for (int m = 0; m < NF; m++) gk += lF[m] * r[m];
+    double lb[NF], rb[NF];
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      lb[m] = gk * phi[m];
+      rb[m] = fw * lF[m];
+    }
+    row_adjoint(e0, G, k, lb, rb, mb);
+    if (gk != 0.0) {
+#pragma unroll
+      for (int m = 0; m < NF; m++) {
+        if (m == 4) continue;
+        const int s = slot_of(m);
+        const double v = gk * l[m];
+        sFb[s][tid] += c0 * v;
+        sFb[7 + s][tid] += c1 * v;
+        sFb[14 + s][tid] += c2 * v;
+        sFb[21 + s][tid] += c3 * v;
+      }
+    }
+  }
+  double U1b[NF], U2b[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) { U1b[k] = 0.0; U2b[k] = 0.0; }
+  midpoint_adjoint(G, e0, U1, U2, mb, U1b, U2b);
+  for (int c = 0; c < 28; c++) out[c * NXY] = sFb[c][tid];
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    out[(28 + k) * NXY] = U1b[k];
+    out[(36 + k) * NXY] = U2b[k];
+  }
+}
+
+// Per cell: sum the interface contributions of both directions, apply the
+// transposed flux Jacobians; T gets the adjoint of the stage input incl.
+// ghost cells (before the boundary-fill transpose).
+__global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double* __restrict__ X,
+                                                     const double* __restrict__ SX,
+                                                     const double* __restrict__ SY,
+                                                     double* __restrict__ T) {
+  const long long NXY = (long long)g.NX * g.NY;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= NXY) return;
+  const int i = int(e / g.NY), j = int(e % g.NY);
+  double lu[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) lu[k] = 0.0;
+  for (int dir = 0; dir < 2; dir++) {
+    const bool yd = dir == 1;
+    const int a = yd ? j : i;  // position along the direction
+    const int t = yd ? i : j;  // transverse position
+    const int ncell = yd ? g.ny : g.nx, ntr = yd ? g.nx : g.ny;
+    if (t < 2 || t > ntr + 1) continue;
+    const double* S = yd ? SY : SX;
+    const int lo_bc = yd ? BOTTOM : LEFT, hi_bc = yd ? TOP : RIGHT;
+    double fb[NF], qb[NF];
+    bool any = false;
+#pragma unroll
+    for (int m = 0; m < NF; m++) { fb[m] = 0.0; qb[m] = 0.0; }
+    for (int p = 0; p < 4; p++) {
+      const int f = a + 1 - p;
+      if (f < 1 || f > ncell + 1) continue;
+      const long long off = yd ? (long long)t * g.NY + f : (long long)f * g.NY + t;
+      any = true;
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (m != 4) fb[m] += S[(7 * p + slot_of(m)) * NXY + off];
+      const int l1 = (g.bc[lo_bc] == OPEN && f < 2) ? 2 : 1;
+      const int l2 = (g.bc[hi_bc] == OPEN && f > ncell) ? 1 : 2;
+      if (p == l1) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) qb[k] += S[(28 + k) * NXY + off];
+      }
+      if (p == l2) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) qb[k] += S[(36 + k) * NXY + off];
+      }
+    }
+    if (!any) continue;
+    double q[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) q[k] = X[g.at(yd ? swap_xy(k) : k, i, j)];
+    flux_x_adjoint(G.gm, q, fb, qb);
+#pragma unroll
+    for (int k = 0; k < NF; k++) lu[yd ? swap_xy(k) : k] += qb[k];
+  }
+#pragma unroll
+  for (int k = 0; k < NF; k++) T[g.at(k, i, j)] = lu[k];
+}
+
+// Transpose of the boundary fill (k_bc / bc_elem) for one side: adds the
+// adjoints of the side's two ghost layers to the interior cells they were
+// copied from.  pass 0: the copies (one thread per field and boundary cell,
+// both layers); Dirichlet ghosts hold the edge snapshot of the initial
+// state, so their adjoints go to lsnap (the side's [8][NY] or [8][NX]
+// array).  pass 1: the div B terms of Neumann Bx / By ghosts, gathered per
+// target cell so no two threads add to the same cell.
+__global__ void ka_adj_bc(Grid g, int side, int pass, double* __restrict__ T,
+                          double* __restrict__ lsnap) {
+  const bool xs = side == LEFT || side == RIGHT;
+  const int nb = xs ? g.ny : g.nx;  // boundary cells along the side
+  const int b = g.bc[side];
+  const double rxy = g.dx / g.dy, ryx = g.dy / g.dx;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pass == 0) {
+    if (e >= NF * nb) return;
+    const int k = e / nb, c = 2 + e % nb;  // c: j (x sides) or i (y sides)
+    if (b == DIRICHLET) {
+      const int len = xs ? g.NY : g.NX;
+      double acc = 0.0;
+      for (int gl = 1; gl <= 2; gl++) {
+        if (side == LEFT) acc += T[g.at(k, 2 - gl, c)];
+        else if (side == RIGHT) acc += T[g.at(k, g.nx + 1 + gl, c)];
+        else if (side == BOTTOM) acc += T[g.at(k, c, 2 - gl)];
+        else acc += T[g.at(k, c, g.ny + 1 + gl)];
+      }
+      lsnap[k * len + c] += acc;
+      return;
+    }
+    for (int gl = 1; gl <= 2; gl++) {
+      int gi, gj, si, sj;  // ghost cell, its source
+      if (side == LEFT) {
+        gi = 2 - gl; gj = c; sj = c;
+        si = b == PERIODIC ? g.nx + 2 - gl : 2 + gl;
+        if (b == NEUMANN && k == 4 && c >= 3 && c < g.ny + 1) si = gi + 2;
+      } else if (side == RIGHT) {
+        gi = g.nx + 1 + gl; gj = c; sj = c;
+        si = b == PERIODIC ? 1 + gl : g.nx + 1 - gl;
+        if (b == NEUMANN && k == 4 && c >= 3 && c < g.ny + 1) si = gi - 2;
+      } else if (side == BOTTOM) {
+        gj = 2 - gl; gi = c; si = c;
+        sj = b == PERIODIC ? g.ny + 2 - gl : 2 + gl;
+        if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj + 2;
+      } else {
+        gj = g.ny + 1 + gl; gi = c; si = c;
+        sj = b == PERIODIC ? 1 + gl : g.ny + 1 - gl;
+        if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj - 2;
+      }
+      T[g.at(k, si, sj)] += T[g.at(k, gi, gj)];
+    }
+    return;
+  }
+  // pass 1: Neumann div B terms.  A left ghost Bx at row it, column c' reads
+  // By at row s5, columns c'-1 (coefficient -rxy) and c'+1 (+rxy); the
+  // target (By, s5, c) therefore collects -rxy * ghost(c+1) and
+  // +rxy * ghost(c-1).  The other sides mirror this.
+  if (b != NEUMANN || e >= nb) return;
+  const int c = 2 + e;
+  for (int layer = 0; layer < 2; layer++) {
+    if (xs) {
+      int gi, s5;
+      double cm, cp;  // coefficients of the ghosts at columns c+1 and c-1
+      if (side == LEFT) {
+        gi = layer;
+        s5 = gi == 1 ? 2 : 3;
+        cm = -rxy; cp = rxy;
+      } else {  // right: -rxy * (By[j+1] - By[j-1])
+        gi = g.nx + 2 + layer;
+        s5 = gi == g.nx + 2 ? g.nx + 1 : g.nx;
+        cm = rxy; cp = -rxy;
+      }
+      double acc = 0.0;
+      if (c + 1 >= 3 && c + 1 < g.ny + 1) acc += cm * T[g.at(4, gi, c + 1)];
+      if (c - 1 >= 3 && c - 1 < g.ny + 1) acc += cp * T[g.at(4, gi, c - 1)];
+      T[g.at(5, s5, c)] += acc;
+    } else {
+      int gj, s4;
+      double cm, cp;
+      if (side == BOTTOM) {  // -ryx * (Bx[i-1] - Bx[i+1])
+        gj = layer;
+        s4 = gj == 1 ? 2 : 3;
+        cm = -ryx; cp = ryx;
+      } else {  // top: -ryx * (Bx[i+1] - Bx[i-1])
+        gj = g.ny + 2 + layer;
+        s4 = gj == g.ny + 2 ? g.ny + 1 : g.ny;
+        cm = ryx; cp = -ryx;
+      }
+      double acc = 0.0;
+      if (c + 1 >= 3 && c + 1 < g.nx + 1) acc += cm * T[g.at(5, c + 1, gj)];
+      if (c - 1 >= 3 && c - 1 < g.nx + 1) acc += cp * T[g.at(5, c - 1, gj)];
+      T[g.at(4, c, s4)] += acc;
+    }
+  }
+}
+
+// Transpose of k_snapshot for one side: the edge row / column of U0 gets
+// the accumulated adjoint of its snapshot.
+__global__ void ka_snap_adj(Grid g, int side, const double* __restrict__ lsnap,
+                            double* __restrict__ lU) {
+  const bool xs = side == LEFT || side == RIGHT;
+  const int nb = xs ? g.ny : g.nx, len = xs ? g.NY : g.NX;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= NF * nb) return;
+  const int k = e / nb, c = 2 + e % nb;
+  const double v = lsnap[k * len + c];
+  if (side == LEFT) lU[g.at(k, 2, c)] += v;
+  else if (side == RIGHT) lU[g.at(k, g.nx + 1, c)] += v;
+  else if (side == BOTTOM) lU[g.at(k, c, 2)] += v;
+  else lU[g.at(k, c, g.ny + 1)] += v;
+}
+
+// dst[interior] += T[interior]
+__global__ void ka_accum(Grid g, const double* __restrict__ T, double* __restrict__ dst) {
+  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = 2 + blockIdx.y;
+  const int k = blockIdx.z;
+  if (j >= g.ny + 2) return;
+  const long long a = g.at(k, i, j);
+  dst[a] += T[a];
+}
+
+// J = sum over the interior of |m|^2 / (2 rho): per-block partial sums in a
+// fixed order (the host adds the partials in block order and scales by dx dy).
+__global__ void __launch_bounds__(256) ka_objective(Grid g, const double* __restrict__ U,
+                                                   double* partial) {
+  __shared__ double sm[256];
+  const long long n = (long long)g.nx * g.ny;
+  double s = 0.0;
+  for (long long e = blockIdx.x * 256LL + threadIdx.x; e < n; e += (long long)gridDim.x * 256) {
+    const int i = 2 + int(e / g.ny), j = 2 + int(e % g.ny);
+    const double r = U[g.at(0, i, j)], mx = U[g.at(1, i, j)], my = U[g.at(2, i, j)],
+                 mz = U[g.at(3, i, j)];
+    s += 0.5 * (mx * mx + my * my + mz * mz) / r;
+  }
+  sm[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+
+// lU = dJ/dU on the interior.
+__global__ void ka_seed(Grid g, const double* __restrict__ U, double* __restrict__ lU,
+                        double dxdy) {
+  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = 2 + blockIdx.y;
+  if (j >= g.ny + 2) return;
+  const double r = U[g.at(0, i, j)], mx = U[g.at(1, i, j)], my = U[g.at(2, i, j)],
+               mz = U[g.at(3, i, j)];
+  const double mm = mx * mx + my * my + mz * mz;
+  lU[g.at(0, i, j)] = -0.5 * mm / (r * r) * dxdy;
+  lU[g.at(1, i, j)] = mx / r * dxdy;
+  lU[g.at(2, i, j)] = my / r * dxdy;
+  lU[g.at(3, i, j)] = mz / r * dxdy;
+  for (int k = 4; k < NF; k++) lU[g.at(k, i, j)] = 0.0;
+}
+
+// dJ/da_k of the plasma-sheet setup (kb_problem): v = sum_k a_k s_k with
+// s_k = sin(k pi y) exp(-x^2/0.04); my = rho v and E = ... + rho v^2 / 2, so
+// dU0/da_k = (0, 0, rho s_k, 0, 0, 0, 0, rho v s_k).  Per-block partials.
+__global__ void __launch_bounds__(256) ka_sheet_grad(Grid g, const double* __restrict__ U0,
+                                                    const double* __restrict__ lU, double x0,
+                                                    double y0, int K, double* partial) {
+  __shared__ double sm[256];
+  const long long n = (long long)g.nx * g.ny;
+  for (int kk = 1; kk <= K; kk++) {
+    double s = 0.0;
+    for (long long e = blockIdx.x * 256LL + threadIdx.x; e < n; e += (long long)gridDim.x * 256) {
+      const int ii = int(e / g.ny), jj = int(e % g.ny);
+      const int i = 2 + ii, j = 2 + jj;
+      const double x = x0 + ii * g.dx, y = y0 + jj * g.dy;
+      const double sk = sin(kk * M_PI * y) * exp(-x * x / 0.04);
+      const double r = U0[g.at(0, i, j)], v = U0[g.at(2, i, j)] / r;
+      s += lU[g.at(2, i, j)] * r * sk + lU[g.at(7, i, j)] * r * v * sk;
+    }
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[(kk - 1) * gridDim.x + blockIdx.x] = sm[0];
+    __syncthreads();
+  }
+}
+
+}  // namespace MHD_KNS
+}  // namespace mhd
+
+using namespace mhd;
+using namespace mhd::MHD_KNS;
+
+namespace {
+constexpr int kObjBlocks = 296;
+constexpr int kSlotsPerChunk = 64;
+}  // namespace
+
+struct mhd_adj {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Grid g{};
+  Gas G{};
+  StepParams sp{};
+  int time_method = 2, K = 64;
+  size_t blk = 0;  // doubles per state block
+  double *U = nullptr, *U1 = nullptr, *U2 = nullptr, *UL = nullptr;
+  double *U0 = nullptr, *Ufinal = nullptr;
+  double* snap[4] = {nullptr, nullptr, nullptr, nullptr};   // Dirichlet edges of U0
+  double* snapr[4] = {nullptr, nullptr, nullptr, nullptr};  // ... of a replay's own U0
+  double* lsnap[4] = {nullptr, nullptr, nullptr, nullptr};  // their adjoints
+  double** cur_snap = snap;
+  double *aF = nullptr, *aG = nullptr;  // unused by ENO-Roe, passed to the flux kernel
+  Ctl *ctl = nullptr, *hctl = nullptr;
+  StageRec* dlog = nullptr;
+  int* dnlog = nullptr;
+  int* hnlog = nullptr;
+  int log_cap = 0;
+  std::vector<StageRec> log;      // executed stages of the recording
+  std::vector<int> step_stage;    // first stage of every step (+ the end)
+  std::vector<double*> ckpt;      // U at steps 0, K, 2K, ...
+  std::vector<unsigned*> chunks;  // mask slots (2 x NX x NY words per stage)
+  size_t slot_words = 0;
+  double *lU = nullptr, *lU1 = nullptr, *lU2 = nullptr, *lUL = nullptr, *T = nullptr;
+  double *SX = nullptr, *SY = nullptr;
+  std::vector<double*> seg;  // stage inputs of one segment
+  double *partial = nullptr, *hpartial = nullptr;
+  bool recorded = false, have_grad = false;
+  int steps = 0;
+  double t = 0.0, dt = 0.0;
+  double ms_forward = 0.0, ms_backward = 0.0, ms_replay = 0.0;
+  std::string msg;
+  bool is_error = false;
+  long long launches = 0;
+};
+
+namespace {
+
+int aset(mhd_adj* a, int st, bool err, const std::string& m) {
+  a->is_error = err;
+  a->msg = m;
+  return st;
+}
+
+int afail(mhd_adj* a, cudaError_t e, const char* where) {
+  return aset(a, MHD_ERR_CUDA, true,
+              std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e));
+}
+
+#define AK(call)                                          \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return afail(a, e_, #call);    \
+  } while (0)
+
+int pitch_for(int NY) { return ((NY + ROW_OFF + 15) / 16) * 16; }
+
+cudaError_t alloc_block(mhd_adj* a, double** p) {
+  cudaError_t e = cudaMalloc(p, a->blk * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, a->blk * sizeof(double), a->stream);
+  return e;
+}
+
+unsigned* mask_slot(mhd_adj* a, int s) {
+  return a->chunks[s / kSlotsPerChunk] + (size_t)(s % kSlotsPerChunk) * a->slot_words;
+}
+
+// Room for stages [0, n): mask slots and the device stage log.
+int ensure_slots(mhd_adj* a, int n) {
+  while ((int)a->chunks.size() * kSlotsPerChunk < n) {
+    unsigned* p = nullptr;
+    AK(cudaMalloc(&p, (size_t)kSlotsPerChunk * a->slot_words * sizeof(unsigned)));
+    a->chunks.push_back(p);
+  }
+  if (n > a->log_cap) {
+    const int cap = std::max(n, 2 * a->log_cap + 64);
+    StageRec* d = nullptr;
+    AK(cudaMalloc(&d, sizeof(StageRec) * cap));
+    if (a->dlog) {
+      AK(cudaMemcpyAsync(d, a->dlog, sizeof(StageRec) * a->log_cap, cudaMemcpyDeviceToDevice,
+                         a->stream));
+      AK(cudaStreamSynchronize(a->stream));
+      cudaFree(a->dlog);
+    }
+    a->dlog = d;
+    a->log_cap = cap;
+  }
+  return MHD_OK;
+}
+
+double* buf(mhd_adj* a, int id) { return id == 0 ? a->U : (id == 1 ? a->U1 : a->U2); }
+
+void launch_bc(mhd_adj* a, double* X) {
+  double** sn = a->cur_snap;
+  const Snap d{sn[0], sn[1], sn[2], sn[3]};
+  const long long n = bc_count(a->g);
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_bc<<<int(blocks), 256, 0, a->stream>>>(a->g, X, d, a->ctl);
+  a->launches++;
+}
+
+template <int MASK>
+void launch_flux(mhd_adj* a, const double* X, unsigned* slot) {
+  auto kern = k_flux<2, false, ATI, ATJ, ANW, MASK>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(AGeom::BYTES));
+    attr = true;
+  }
+  const Grid& g = a->g;
+  dim3 grid((g.ny + ATJ - 1) / ATJ, (g.nx + ATI - 1) / ATI);
+  const CharOut co{nullptr, nullptr, nullptr, nullptr};
+  kern<<<grid, ANW * 32, AGeom::BYTES, a->stream>>>(g, X, a->UL, a->aF, a->aG, 1.0 / g.dx,
+                                                     1.0 / g.dy, a->G, a->ctl, co, slot,
+                                                     slot + (size_t)g.NX * g.NY);
+  a->launches++;
+}
+
+void launch_control(mhd_adj* a, int phase, double arg = 0.0) {
+  ka_control<<<1, 32, 0, a->stream>>>(a->ctl, a->sp, phase, arg, a->dlog, a->dnlog, a->log_cap);
+  a->launches++;
+}
+
+void launch_combine_ctl(mhd_adj* a, int mode) {
+  const Grid& g = a->g;
+  dim3 grid((g.ny + 255) / 256, g.nx, NF);
+  k_combine<<<grid, 256, 0, a->stream>>>(g, mode, a->U, a->U1, a->U2, a->UL, a->ctl);
+  a->launches++;
+}
+
+int read_ctl(mhd_adj* a) {
+  AK(cudaMemcpyAsync(a->hctl, a->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, a->stream));
+  AK(cudaMemcpyAsync(a->hnlog, a->dnlog, sizeof(int), cudaMemcpyDeviceToHost, a->stream));
+  AK(cudaStreamSynchronize(a->stream));
+  AK(cudaGetLastError());
+  return MHD_OK;
+}
+
+// One recorded time step from U (TimeIntegrationRK3::step /
+// TimeIntegrationEuler::step, as a context runs it).  The i-th flux launched
+// since the last synchronisation, if it runs, is logged as stage base + i,
+// so its choices go to that mask slot.
+int record_step(mhd_adj* a, double* dt_inout) {
+  int base = *a->hnlog, st;
+  if ((st = ensure_slots(a, base + 3))) return st;
+  launch_control(a, PH_RESET_STEP, *dt_inout);
+  launch_bc(a, a->U);
+  launch_flux<1>(a, a->U, mask_slot(a, base));
+  if (a->time_method == 1) {
+    launch_control(a, PH_EULER);
+    launch_combine_ctl(a, 0);
+    launch_control(a, PH_DONE);
+    if ((st = read_ctl(a))) return st;
+  } else {
+    launch_control(a, PH_RK_FIRST);
+    int guard = 0;
+    for (;;) {
+      launch_combine_ctl(a, 1);
+      launch_bc(a, a->U1);
+      launch_flux<1>(a, a->U1, mask_slot(a, base + 1));
+      launch_control(a, PH_RK_SECOND);
+      launch_combine_ctl(a, 2);
+      launch_bc(a, a->U2);
+      launch_flux<1>(a, a->U2, mask_slot(a, base + 2));
+      launch_control(a, PH_RK_FINAL);
+      launch_combine_ctl(a, 3);
+      launch_control(a, PH_DONE);
+      if ((st = read_ctl(a))) return st;
+      if (!a->hctl->retry || a->hctl->error) break;
+      if (++guard > 64)
+        return aset(a, MHD_ERR_WRONG_PARAMETER, true, "RK3 retry loop did not settle");
+      base = *a->hnlog - 1;  // the retry tail's first flux takes the next slot
+      if ((st = ensure_slots(a, base + 3))) return st;
+      launch_control(a, PH_RK_RETRY);
+    }
+  }
+  const Ctl& h = *a->hctl;
+  if (h.error == 6)
+    return aset(a, MHD_ERR_NEGATIVE_DENSITY, true, "negative density encountered\n! getEigens_F");
+  if (h.error == 4)
+    return aset(a, MHD_ERR_TIME_UNDERFLOW, true, "CFL condition violated!\n! updateDt");
+  if (h.error)
+    return aset(a, MHD_ERR_WRONG_PARAMETER, true, "updateDt: no power-of-two time step fits");
+  *dt_inout = h.dt;
+  return MHD_OK;
+}
+
+// J of a device state (deterministic: fixed grid, partials summed in order).
+int objective(mhd_adj* a, const double* U, double* J) {
+  ka_objective<<<kObjBlocks, 256, 0, a->stream>>>(a->g, U, a->partial);
+  a->launches++;
+  AK(cudaMemcpyAsync(a->hpartial, a->partial, kObjBlocks * sizeof(double),
+                     cudaMemcpyDeviceToHost, a->stream));
+  AK(cudaStreamSynchronize(a->stream));
+  double s = 0.0;
+  for (int b = 0; b < kObjBlocks; b++) s += a->hpartial[b];
+  *J = s * (a->g.dx * a->g.dy);
+  return MHD_OK;
+}
+
+// Replays stages [s0, s1) on the working buffers; with keep, the input of
+// stage s (after its boundary fill) is copied to a->seg[s - s0].
+void replay_stages(mhd_adj* a, int s0, int s1, bool keep) {
+  const Grid& g = a->g;
+  dim3 cgrid((g.ny + 255) / 256, g.nx, NF);
+  for (int s = s0; s < s1; s++) {
+    const StageRec& r = a->log[s];
+    double* X = buf(a, r.in_buf);
+    launch_bc(a, X);
+    if (keep)
+      cudaMemcpyAsync(a->seg[s - s0], X, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                      a->stream);
+    launch_flux<2>(a, X, mask_slot(a, s));
+    ka_combine<<<cgrid, 256, 0, a->stream>>>(g, r.mode, r.dt, a->U, a->U1, a->U2, a->UL);
+    a->launches++;
+  }
+}
+
+int reset_ctl(mhd_adj* a) {
+  AK(cudaMemsetAsync(a->ctl, 0, sizeof(Ctl), a->stream));
+  return MHD_OK;
+}
+
+void snapshot_into(mhd_adj* a, const double* U, double* const* dst) {
+  const int m = std::max(a->g.nx, a->g.ny);
+  k_snapshot<<<(NF * m + 255) / 256, 256, 0, a->stream>>>(a->g, U, dst[0], dst[1], dst[2],
+                                                          dst[3]);
+  a->launches++;
+}
+
+// Adjoint of the spatial operator of stage s at its stored input X:
+// lbuf += L'(X)^T lUL.
+void adjoint_L(mhd_adj* a, int s, const double* X, double* lbuf) {
+  const Grid& g = a->g;
+  unsigned* mx = mask_slot(a, s);
+  unsigned* my = mx + (size_t)g.NX * g.NY;
+  const long long nx_faces = (long long)(g.nx + 1) * g.ny, ny_faces = (long long)(g.ny + 1) * g.nx;
+  ka_adj_iface<false><<<int((nx_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
+      g, a->G, X, mx, a->lUL, a->SX, 1.0 / g.dx);
+  ka_adj_iface<true><<<int((ny_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
+      g, a->G, X, my, a->lUL, a->SY, 1.0 / g.dy);
+  const long long ncell = (long long)g.NX * g.NY;
+  ka_adj_gather<<<int((ncell + 127) / 128), 128, 0, a->stream>>>(g, a->G, X, a->SX, a->SY, a->T);
+  for (int side = 0; side < 4; side++) {
+    const int nb = (side < 2) ? g.ny : g.nx;
+    ka_adj_bc<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, 0, a->T, a->lsnap[side]);
+    ka_adj_bc<<<(nb + 127) / 128, 128, 0, a->stream>>>(g, side, 1, a->T, a->lsnap[side]);
+  }
+  dim3 cgrid((g.ny + 255) / 256, g.nx, NF);
+  ka_accum<<<cgrid, 256, 0, a->stream>>>(g, a->T, lbuf);
+  a->launches += 12;
+}
+
+int check_ready(mhd_adj* a) {
+  if (!a->recorded)
+    return aset(a, MHD_ERR_WRONG_PARAMETER, true, "no recorded forward run (call mhd_adj_forward)");
+  return MHD_OK;
+}
+
+int timed_ms(cudaEvent_t e0, cudaEvent_t e1, double* out) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *out = ms;
+  return MHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhd_adj_create(int nx, int ny, double dx, double dy, double gamma, const int bc[4],
+                   int time_method, double dt_min, double dt_max, double cfl,
+                   int checkpoint_every, int device, mhd_adj** out) {
+  if (!out) return MHD_ERR_WRONG_PARAMETER;
+  *out = nullptr;
+  if (nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0) || !bc || (time_method != 1 && time_method != 2) ||
+      checkpoint_every < 1)
+    return MHD_ERR_WRONG_PARAMETER;
+  for (int s = 0; s < 4; s++)
+    if (bc[s] < 1 || bc[s] > 4) return MHD_ERR_WRONG_PARAMETER;
+  mhd_adj* a = new (std::nothrow) mhd_adj;
+  if (!a) return MHD_ERR_WRONG_PARAMETER;
+  *out = a;
+  a->device = device;
+  a->time_method = time_method;
+  a->K = checkpoint_every;
+  AK(cudaSetDevice(device));
+  AK(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+  Grid& g = a->g;
+  g.nx = nx; g.ny = ny; g.NX = nx + 4; g.NY = ny + 4;
+  g.pitch = pitch_for(g.NY);
+  g.off = ROW_OFF;
+  g.fstride = (long long)g.NX * g.pitch;
+  g.dx = dx; g.dy = dy; g.gamma = gamma;
+  for (int s = 0; s < 4; s++) g.bc[s] = bc[s];
+  a->G = Gas{gamma, gamma - 1.0, (gamma - 2.0) / (gamma - 1.0), 1.0 / std::sqrt(2.0)};
+  a->sp = StepParams{dx, dy, dt_min, dt_max, cfl};
+  a->blk = size_t(NF) * g.fstride + 16;
+  a->slot_words = 2 * (size_t)g.NX * g.NY;
+  for (double** p : {&a->U, &a->U1, &a->U2, &a->UL, &a->U0, &a->Ufinal, &a->lU, &a->lU1, &a->lU2,
+                     &a->lUL, &a->T})
+    AK(alloc_block(a, p));
+  const size_t sn = sizeof(double) * NF * std::max(g.NX, g.NY);
+  for (int s = 0; s < 4; s++) {
+    for (double** p : {&a->snap[s], &a->snapr[s], &a->lsnap[s]}) {
+      AK(cudaMalloc(p, sn));
+      AK(cudaMemsetAsync(*p, 0, sn, a->stream));
+    }
+  }
+  AK(cudaMalloc(&a->aF, sizeof(double) * NF * g.NY));
+  AK(cudaMalloc(&a->aG, sizeof(double) * NF * g.NX));
+  const size_t sc = (size_t)NSC * g.NX * g.NY;
+  AK(cudaMalloc(&a->SX, sc * sizeof(double)));
+  AK(cudaMalloc(&a->SY, sc * sizeof(double)));
+  AK(cudaMemsetAsync(a->SX, 0, sc * sizeof(double), a->stream));
+  AK(cudaMemsetAsync(a->SY, 0, sc * sizeof(double), a->stream));
+  AK(cudaMalloc(&a->ctl, sizeof(Ctl)));
+  AK(cudaMemsetAsync(a->ctl, 0, sizeof(Ctl), a->stream));
+  AK(cudaMallocHost(&a->hctl, sizeof(Ctl)));
+  AK(cudaMalloc(&a->dnlog, sizeof(int)));
+  AK(cudaMallocHost(&a->hnlog, sizeof(int)));
+  AK(cudaMalloc(&a->partial, sizeof(double) * kObjBlocks * 40));
+  AK(cudaMallocHost(&a->hpartial, sizeof(double) * kObjBlocks * 40));
+  AK(cudaStreamSynchronize(a->stream));
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_destroy(mhd_adj* a) {
+  if (!a) return MHD_OK;
+  cudaSetDevice(a->device);
+  if (a->stream) cudaStreamSynchronize(a->stream);
+  for (double* p : {a->U, a->U1, a->U2, a->UL, a->U0, a->Ufinal, a->lU, a->lU1, a->lU2, a->lUL,
+                    a->T, a->SX, a->SY, a->aF, a->aG, a->partial})
+    cudaFree(p);
+  for (int s = 0; s < 4; s++) {
+    cudaFree(a->snap[s]);
+    cudaFree(a->snapr[s]);
+    cudaFree(a->lsnap[s]);
+  }
+  for (double* p : a->ckpt) cudaFree(p);
+  for (double* p : a->seg) cudaFree(p);
+  for (unsigned* p : a->chunks) cudaFree(p);
+  cudaFree(a->dlog);
+  cudaFree(a->dnlog);
+  cudaFree(a->ctl);
+  if (a->hctl) cudaFreeHost(a->hctl);
+  if (a->hnlog) cudaFreeHost(a->hnlog);
+  if (a->hpartial) cudaFreeHost(a->hpartial);
+  if (a->stream) cudaStreamDestroy(a->stream);
+  delete a;
+  return MHD_OK;
+}
+
+int mhd_adj_last_error(mhd_adj* a, char* buf, size_t len, int* is_error) {
+  if (!a) return MHD_ERR_WRONG_PARAMETER;
+  if (buf && len) {
+    std::strncpy(buf, a->msg.c_str(), len - 1);
+    buf[len - 1] = 0;
+  }
+  if (is_error) *is_error = a->is_error ? 1 : 0;
+  return MHD_OK;
+}
+
+int mhd_adj_upload(mhd_adj* a, const double* U0) {
+  if (!a || !U0) return MHD_ERR_WRONG_PARAMETER;
+  AK(cudaSetDevice(a->device));
+  const Grid& g = a->g;
+  AK(cudaMemcpy2DAsync(a->U0 + g.off, g.pitch * sizeof(double), U0, g.NY * sizeof(double),
+                       g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyHostToDevice,
+                       a->stream));
+  snapshot_into(a, a->U0, a->snap);
+  AK(cudaStreamSynchronize(a->stream));
+  a->recorded = false;
+  a->have_grad = false;
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_init_problem(mhd_adj* a, int kind, const double* p, int np) {
+  if (!a) return MHD_ERR_WRONG_PARAMETER;
+  AK(cudaSetDevice(a->device));
+  ProblemArgs pa{};
+  std::string err;
+  cudaError_t ce = cudaSuccess;
+  const int st = problem_args(kind, p, np, a->g.gamma, a->stream, pa, err, ce);
+  if (ce != cudaSuccess) return afail(a, ce, "problem_args");
+  if (st) return aset(a, st, true, err);
+  AK(cudaMemsetAsync(a->U0, 0, a->blk * sizeof(double), a->stream));
+  enqueue_problem(a->g, a->U0, pa, a->stream);
+  snapshot_into(a, a->U0, a->snap);
+  a->launches++;
+  AK(cudaStreamSynchronize(a->stream));
+  AK(cudaGetLastError());
+  a->recorded = false;
+  a->have_grad = false;
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_forward(mhd_adj* a, int nsteps, double dt0, double* J) {
+  if (!a || nsteps < 1) return MHD_ERR_WRONG_PARAMETER;
+  AK(cudaSetDevice(a->device));
+  for (double* p : a->ckpt) cudaFree(p);
+  a->ckpt.clear();
+  a->log.clear();
+  a->step_stage.clear();
+  a->recorded = false;
+  a->have_grad = false;
+  a->cur_snap = a->snap;
+  int st;
+  if ((st = reset_ctl(a))) return st;
+  AK(cudaMemsetAsync(a->dnlog, 0, sizeof(int), a->stream));
+  *a->hnlog = 0;
+  AK(cudaMemcpyAsync(a->U, a->U0, a->blk * sizeof(double), cudaMemcpyDeviceToDevice, a->stream));
+  cudaEvent_t e0, e1;
+  AK(cudaEventCreate(&e0));
+  AK(cudaEventCreate(&e1));
+  AK(cudaEventRecord(e0, a->stream));
+  double dt = dt0, t = 0.0;
+  int done = 0;
+  for (int s = 0; s < nsteps; s++) {
+    if (s % a->K == 0) {
+      double* c = nullptr;
+      AK(cudaMalloc(&c, a->blk * sizeof(double)));
+      AK(cudaMemcpyAsync(c, a->U, a->blk * sizeof(double), cudaMemcpyDeviceToDevice, a->stream));
+      a->ckpt.push_back(c);
+    }
+    a->step_stage.push_back(*a->hnlog);
+    if ((st = record_step(a, &dt))) break;
+    t += dt;
+    done++;
+  }
+  AK(cudaEventRecord(e1, a->stream));
+  AK(cudaEventSynchronize(e1));
+  timed_ms(e0, e1, &a->ms_forward);
+  if (st) return st;
+  a->step_stage.push_back(*a->hnlog);
+  a->log.resize(*a->hnlog);
+  AK(cudaMemcpy(a->log.data(), a->dlog, sizeof(StageRec) * a->log.size(),
+                cudaMemcpyDeviceToHost));
+  AK(cudaMemcpyAsync(a->Ufinal, a->U, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                     a->stream));
+  a->steps = done;
+  a->t = t;
+  a->dt = dt;
+  a->recorded = true;
+  if (J && (st = objective(a, a->U, J))) return st;
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_replay(mhd_adj* a, const double* U0, double* J) {
+  if (!a) return MHD_ERR_WRONG_PARAMETER;
+  int st = check_ready(a);
+  if (st) return st;
+  AK(cudaSetDevice(a->device));
+  const Grid& g = a->g;
+  if (U0) {
+    AK(cudaMemcpy2DAsync(a->U + g.off, g.pitch * sizeof(double), U0, g.NY * sizeof(double),
+                         g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyHostToDevice,
+                         a->stream));
+    // Dirichlet sides take their edges from this initial state, as a run
+    // set up from it would
+    snapshot_into(a, a->U, a->snapr);
+    a->cur_snap = a->snapr;
+  } else {
+    AK(cudaMemcpyAsync(a->U, a->U0, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                       a->stream));
+  }
+  if ((st = reset_ctl(a))) return st;
+  cudaEvent_t e0, e1;
+  AK(cudaEventCreate(&e0));
+  AK(cudaEventCreate(&e1));
+  AK(cudaEventRecord(e0, a->stream));
+  replay_stages(a, 0, int(a->log.size()), false);
+  a->cur_snap = a->snap;
+  AK(cudaEventRecord(e1, a->stream));
+  AK(cudaEventSynchronize(e1));
+  AK(cudaGetLastError());
+  timed_ms(e0, e1, &a->ms_replay);
+  if (J && (st = objective(a, a->U, J))) return st;
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_replay_problem(mhd_adj* a, int kind, const double* p, int np, double* J) {
+  if (!a) return MHD_ERR_WRONG_PARAMETER;
+  int st = check_ready(a);
+  if (st) return st;
+  AK(cudaSetDevice(a->device));
+  ProblemArgs pa{};
+  std::string err;
+  cudaError_t ce = cudaSuccess;
+  st = problem_args(kind, p, np, a->g.gamma, a->stream, pa, err, ce);
+  if (ce != cudaSuccess) return afail(a, ce, "problem_args");
+  if (st) return aset(a, st, true, err);
+  AK(cudaMemsetAsync(a->U, 0, a->blk * sizeof(double), a->stream));
+  enqueue_problem(a->g, a->U, pa, a->stream);
+  a->launches++;
+  snapshot_into(a, a->U, a->snapr);
+  a->cur_snap = a->snapr;
+  if ((st = reset_ctl(a))) return st;
+  replay_stages(a, 0, int(a->log.size()), false);
+  a->cur_snap = a->snap;
+  AK(cudaGetLastError());
+  if (J && (st = objective(a, a->U, J))) return st;
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_backward(mhd_adj* a) {
+  if (!a) return MHD_ERR_WRONG_PARAMETER;
+  int st = check_ready(a);
+  if (st) return st;
+  AK(cudaSetDevice(a->device));
+  const Grid& g = a->g;
+  a->cur_snap = a->snap;
+  // the largest segment sizes the stage-input store
+  const int nseg = int(a->ckpt.size());
+  int maxst = 0;
+  for (int q = 0; q < nseg; q++) {
+    const int s0 = a->step_stage[q * a->K];
+    const int s1 = a->step_stage[std::min((q + 1) * a->K, a->steps)];
+    maxst = std::max(maxst, s1 - s0);
+  }
+  while ((int)a->seg.size() < maxst) {
+    double* p = nullptr;
+    AK(cudaMalloc(&p, a->blk * sizeof(double)));
+    a->seg.push_back(p);
+  }
+  cudaEvent_t e0, e1;
+  AK(cudaEventCreate(&e0));
+  AK(cudaEventCreate(&e1));
+  AK(cudaEventRecord(e0, a->stream));
+  for (double* p : {a->lU, a->lU1, a->lU2, a->lUL, a->T})
+    AK(cudaMemsetAsync(p, 0, a->blk * sizeof(double), a->stream));
+  for (int side = 0; side < 4; side++)
+    AK(cudaMemsetAsync(a->lsnap[side], 0, sizeof(double) * NF * std::max(g.NX, g.NY), a->stream));
+  dim3 cgrid((g.ny + 255) / 256, g.nx, NF);
+  dim3 sgrid((g.ny + 255) / 256, g.nx);
+  ka_seed<<<sgrid, 256, 0, a->stream>>>(g, a->Ufinal, a->lU, g.dx * g.dy);
+  a->launches++;
+  double* lb[3] = {a->lU, a->lU1, a->lU2};
+  for (int q = nseg - 1; q >= 0; q--) {
+    const int s0 = a->step_stage[q * a->K];
+    const int s1 = a->step_stage[std::min((q + 1) * a->K, a->steps)];
+    AK(cudaMemcpyAsync(a->U, a->ckpt[q], a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                       a->stream));
+    if ((st = reset_ctl(a))) return st;
+    replay_stages(a, s0, s1, true);
+    for (int s = s1 - 1; s >= s0; s--) {
+      const StageRec& r = a->log[s];
+      ka_combine_adj<<<cgrid, 256, 0, a->stream>>>(g, r.mode, r.dt, a->lU, a->lU1, a->lU2,
+                                                   a->lUL);
+      a->launches++;
+      adjoint_L(a, s, a->seg[s - s0], lb[r.in_buf]);
+    }
+  }
+  for (int side = 0; side < 4; side++) {
+    if (g.bc[side] != DIRICHLET) continue;
+    const int nb = (side < 2) ? g.ny : g.nx;
+    ka_snap_adj<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, a->lsnap[side], a->lU);
+    a->launches++;
+  }
+  AK(cudaEventRecord(e1, a->stream));
+  AK(cudaEventSynchronize(e1));
+  AK(cudaGetLastError());
+  timed_ms(e0, e1, &a->ms_backward);
+  a->have_grad = true;
+  return aset(a, MHD_OK, false, "");
+}
+
+int mhd_adj_gradient(mhd_adj* a, double* dJdU0) {
+  if (!a || !dJdU0) return MHD_ERR_WRONG_PARAMETER;
+  if (!a->have_grad)
+    return aset(a, MHD_ERR_WRONG_PARAMETER, true, "no adjoint (call mhd_adj_backward)");
+  AK(cudaSetDevice(a->device));
+  const Grid& g = a->g;
+  AK(cudaMemcpy2DAsync(dJdU0, g.NY * sizeof(double), a->lU + g.off, g.pitch * sizeof(double),
+                       g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyDeviceToHost,
+                       a->stream));
+  AK(cudaStreamSynchronize(a->stream));
+  return MHD_OK;
+}
+
+int mhd_adj_sheet_gradient(mhd_adj* a, double x0, double y0, int K, double* dJda) {
+  if (!a || !dJda || K < 1 || K > 40) return MHD_ERR_WRONG_PARAMETER;
+  if (!a->have_grad)
+    return aset(a, MHD_ERR_WRONG_PARAMETER, true, "no adjoint (call mhd_adj_backward)");
+  AK(cudaSetDevice(a->device));
+  ka_sheet_grad<<<kObjBlocks, 256, 0, a->stream>>>(a->g, a->U0, a->lU, x0, y0, K, a->partial);
+  a->launches++;
+  AK(cudaMemcpyAsync(a->hpartial, a->partial, sizeof(double) * kObjBlocks * K,
+                     cudaMemcpyDeviceToHost, a->stream));
+  AK(cudaStreamSynchronize(a->stream));
+  AK(cudaGetLastError());
+  for (int k = 0; k < K; k++) {
+    double s = 0.0;
+    for (int b = 0; b < kObjBlocks; b++) s += a->hpartial[k * kObjBlocks + b];
+    dJda[k] = s;
+  }
+  return MHD_OK;
+}
+
+int mhd_adj_download(mhd_adj* a, int which, double* U) {
+  if (!a || !U || which < 0 || which > 2) return MHD_ERR_WRONG_PARAMETER;
+  AK(cudaSetDevice(a->device));
+  const Grid& g = a->g;
+  const double* src = which == 0 ? a->U0 : (which == 1 ? a->Ufinal : a->U);
+  AK(cudaMemcpy2DAsync(U, g.NY * sizeof(double), src + g.off, g.pitch * sizeof(double),
+                       g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyDeviceToHost,
+                       a->stream));
+  AK(cudaStreamSynchronize(a->stream));
+  return MHD_OK;
+}
+
+int mhd_adj_info(mhd_adj* a, mhd_adj_stats* out) {
+  if (!a || !out) return MHD_ERR_WRONG_PARAMETER;
+  out->steps = a->steps;
+  out->stages = int(a->log.size());
+  out->checkpoints = int(a->ckpt.size());
+  int retries = 0;
+  for (size_t s = 0; s < a->log.size(); s++)
+    if (a->log[s].mode == 1 && a->log[s].in_buf != 0) retries++;
+  out->retries = retries;
+  out->t = a->t;
+  out->dt = a->dt;
+  out->ms_forward = a->ms_forward;
+  out->ms_backward = a->ms_backward;
+  out->ms_replay = a->ms_replay;
+  out->launches = a->launches;
+  return MHD_OK;
+}
+
+}  // extern "C"

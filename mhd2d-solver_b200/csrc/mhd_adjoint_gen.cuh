@@ -1,0 +1,1019 @@
+// GENERATED by gen_adjoint.py from the formulas restated there; do not edit.
+// Reverse-mode adjoints of the ENO-Roe interface algebra with frozen branches.
+#pragma once
+
+#include "mhd_eigen.cuh"
+
+namespace mhd {
+namespace MHD_KNS {
+
+// d sqrt(v) / dv, 0 at v = 0 (frozen one-sided branch)
+__device__ __forceinline__ double inv2sqrt(double v) {
+  return v > 0.0 ? 0.5 / sqrt(v) : 0.0;
+}
+
+// Adjoints of the Mid scalars.
+struct MidBar {
+  double u, v, w, uu, a2, a, ca2, ca, cs2, cs, cf2, cf, rr, af2, af, as2, as, bty, btz, th1, th2, vb;
+};
+
+// Adds the adjoint of left row k (lb) and right row k (rb) to mb.
+__device__ __forceinline__ void row_adjoint(const Mid& e, const Gas& G, int k,
+                                            const double* lb, const double* rb,
+                                            MidBar& mb) {
+  const double sb = (e.sbxm ? -1.0 : 1.0), fcf = (e.fcfm ? -1.0 : 1.0),
+               fcs = (e.fcsm ? -1.0 : 1.0);
+  (void)fcf; (void)fcs; (void)sb;
+  switch (k) {
+    case 0: {
+      mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
+      mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
+      mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
+      mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
+      mb.th2 += lb[0] * fcf * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
+      mb.af += lb[0] * fcf * (0.5 * e.th2) * e.u * e.a * sb;
+      mb.a += lb[0] * fcf * (0.5 * e.th2) * e.u * (sb * e.af);
+      mb.u += lb[0] * fcf * (0.5 * e.th2) * (sb * e.af * e.a);
+      mb.as += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.cs;
+      mb.cs += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.as;
+      mb.vb += -(lb[0] * fcf * (0.5 * e.th2)) * (e.as * e.cs);
+      mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
+      mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
+      mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
+      mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+      mb.th2 += -(lb[1] * fcf) * e.a * e.af * (sb * 0.5);
+      mb.af += -(lb[1] * fcf) * e.a * (sb * 0.5 * e.th2);
+      mb.a += -(lb[1] * fcf) * (sb * 0.5 * e.th2 * e.af);
+      mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
+      mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
+      mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
+      mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+      mb.th2 += lb[2] * fcf * e.cs * e.bty * e.as * 0.5;
+      mb.as += lb[2] * fcf * e.cs * e.bty * (0.5 * e.th2);
+      mb.bty += lb[2] * fcf * e.cs * (0.5 * e.th2 * e.as);
+      mb.cs += lb[2] * fcf * (0.5 * e.th2 * e.as * e.bty);
+      mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
+      mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
+      mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
+      mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+      mb.th2 += lb[3] * fcf * e.cs * e.btz * e.as * 0.5;
+      mb.as += lb[3] * fcf * e.cs * e.btz * (0.5 * e.th2);
+      mb.btz += lb[3] * fcf * e.cs * (0.5 * e.th2 * e.as);
+      mb.cs += lb[3] * fcf * (0.5 * e.th2 * e.as * e.btz);
+      mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
+      mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
+      mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+      mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
+      mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
+      mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
+      mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
+      mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
+      mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+      mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
+      mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
+      mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
+      mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
+      mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
+      mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
+      mb.af += rb[0] * fcf;
+      mb.af += rb[1] * fcf * (e.u - e.cf);
+      mb.u += rb[1] * fcf * e.af;
+      mb.cf += -(rb[1] * fcf * e.af);
+      mb.af += rb[2] * fcf * e.v;
+      mb.v += rb[2] * fcf * e.af;
+      mb.as += rb[2] * fcf * e.ca * e.bty * sb;
+      mb.bty += rb[2] * fcf * e.ca * (sb * e.as);
+      mb.ca += rb[2] * fcf * (sb * e.as * e.bty);
+      mb.af += rb[3] * fcf * e.w;
+      mb.w += rb[3] * fcf * e.af;
+      mb.as += rb[3] * fcf * e.ca * e.btz * sb;
+      mb.btz += rb[3] * fcf * e.ca * (sb * e.as);
+      mb.ca += rb[3] * fcf * (sb * e.as * e.btz);
+      mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
+      mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
+      mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
+      mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
+      mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
+      mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
+      mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
+      mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
+      mb.af += rb[7] * fcf * e.uu * 0.5;
+      mb.uu += rb[7] * fcf * (0.5 * e.af);
+      mb.af += rb[7] * fcf / G.g1 * e.cf2;
+      mb.cf2 += rb[7] * fcf / G.g1 * e.af;
+      mb.af += -(rb[7] * fcf) * e.u * e.cf;
+      mb.cf += -(rb[7] * fcf) * e.u * e.af;
+      mb.u += -(rb[7] * fcf) * (e.af * e.cf);
+      mb.as += rb[7] * fcf * e.vb * e.ca * sb;
+      mb.ca += rb[7] * fcf * e.vb * (sb * e.as);
+      mb.vb += rb[7] * fcf * (sb * e.as * e.ca);
+      mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
+      mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
+      mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
+      break;
+    }
+    case 1: {
+      mb.btz += lb[0] * sb * -0.5 * e.v;
+      mb.v += lb[0] * sb * -0.5 * e.btz;
+      mb.bty += -(lb[0] * sb * -0.5) * e.w;
+      mb.w += -(lb[0] * sb * -0.5) * e.bty;
+      mb.btz += lb[2] * sb * 0.5;
+      mb.bty += lb[3] * sb * -0.5;
+      mb.btz += lb[5] * e.rr * 0.5;
+      mb.rr += lb[5] * (0.5 * e.btz);
+      mb.bty += lb[6] * e.rr * -0.5;
+      mb.rr += lb[6] * (-0.5 * e.bty);
+      mb.btz += rb[2] * sb;
+      mb.bty += -rb[3] * sb;
+      mb.btz += rb[5] / e.rr;
+      mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
+      mb.bty += -(rb[6] / e.rr);
+      mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
+      mb.btz += rb[7] * sb * e.v;
+      mb.v += rb[7] * sb * e.btz;
+      mb.bty += -(rb[7] * sb) * e.w;
+      mb.w += -(rb[7] * sb) * e.bty;
+      break;
+    }
+    case 2: {
+      mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
+      mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
+      mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
+      mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
+      mb.th2 += lb[0] * fcs * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
+      mb.as += lb[0] * fcs * (0.5 * e.th2) * e.u * e.ca * sb;
+      mb.ca += lb[0] * fcs * (0.5 * e.th2) * e.u * (sb * e.as);
+      mb.u += lb[0] * fcs * (0.5 * e.th2) * (sb * e.as * e.ca);
+      mb.af += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.cf;
+      mb.cf += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.af;
+      mb.vb += lb[0] * fcs * (0.5 * e.th2) * (e.af * e.cf);
+      mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
+      mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
+      mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
+      mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+      mb.th2 += -(lb[1] * fcs) * e.ca * e.as * (sb * 0.5);
+      mb.as += -(lb[1] * fcs) * e.ca * (sb * 0.5 * e.th2);
+      mb.ca += -(lb[1] * fcs) * (sb * 0.5 * e.th2 * e.as);
+      mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
+      mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
+      mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
+      mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+      mb.th2 += -(lb[2] * fcs) * e.cf * e.bty * e.af * 0.5;
+      mb.af += -(lb[2] * fcs) * e.cf * e.bty * (0.5 * e.th2);
+      mb.bty += -(lb[2] * fcs) * e.cf * (0.5 * e.th2 * e.af);
+      mb.cf += -(lb[2] * fcs) * (0.5 * e.th2 * e.af * e.bty);
+      mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
+      mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
+      mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
+      mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+      mb.th2 += -(lb[3] * fcs) * e.cf * e.btz * e.af * 0.5;
+      mb.af += -(lb[3] * fcs) * e.cf * e.btz * (0.5 * e.th2);
+      mb.btz += -(lb[3] * fcs) * e.cf * (0.5 * e.th2 * e.af);
+      mb.cf += -(lb[3] * fcs) * (0.5 * e.th2 * e.af * e.btz);
+      mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
+      mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
+      mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+      mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
+      mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
+      mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
+      mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
+      mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
+      mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+      mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
+      mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
+      mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
+      mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
+      mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
+      mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
+      mb.as += rb[0] * fcs;
+      mb.as += rb[1] * fcs * (e.u - e.cs);
+      mb.u += rb[1] * fcs * e.as;
+      mb.cs += -(rb[1] * fcs * e.as);
+      mb.as += rb[2] * fcs * e.v;
+      mb.v += rb[2] * fcs * e.as;
+      mb.af += -(rb[2] * fcs) * e.a * e.bty * sb;
+      mb.bty += -(rb[2] * fcs) * e.a * (sb * e.af);
+      mb.a += -(rb[2] * fcs) * (sb * e.af * e.bty);
+      mb.as += rb[3] * fcs * e.w;
+      mb.w += rb[3] * fcs * e.as;
+      mb.af += -(rb[3] * fcs) * e.a * e.btz * sb;
+      mb.btz += -(rb[3] * fcs) * e.a * (sb * e.af);
+      mb.a += -(rb[3] * fcs) * (sb * e.af * e.btz);
+      mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
+      mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+      mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
+      mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+      mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
+      mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+      mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
+      mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+      mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      mb.as += rb[7] * fcs * e.uu * 0.5;
+      mb.uu += rb[7] * fcs * (0.5 * e.as);
+      mb.as += rb[7] * fcs / G.g1 * e.cs2;
+      mb.cs2 += rb[7] * fcs / G.g1 * e.as;
+      mb.as += -(rb[7] * fcs) * e.u * e.cs;
+      mb.cs += -(rb[7] * fcs) * e.u * e.as;
+      mb.u += -(rb[7] * fcs) * (e.as * e.cs);
+      mb.af += -(rb[7] * fcs) * e.vb * e.a * sb;
+      mb.a += -(rb[7] * fcs) * e.vb * (sb * e.af);
+      mb.vb += -(rb[7] * fcs) * (sb * e.af * e.a);
+      mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
+      mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
+      mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
+      break;
+    }
+    case 3: {
+      mb.th1 += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * e.uu * 0.5;
+      mb.uu += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * (0.5 * e.th1);
+      mb.af2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.a2;
+      mb.a2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.af2;
+      mb.as2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.cf2;
+      mb.cf2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.as2;
+      mb.th1 += lb[1] * e.u * (e.af2 * e.a2 + e.as2 * e.cf2);
+      mb.af2 += lb[1] * e.u * e.th1 * e.a2;
+      mb.a2 += lb[1] * e.u * e.th1 * e.af2;
+      mb.as2 += lb[1] * e.u * e.th1 * e.cf2;
+      mb.cf2 += lb[1] * e.u * e.th1 * e.as2;
+      mb.u += lb[1] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      mb.th1 += lb[2] * e.v * (e.af2 * e.a2 + e.as2 * e.cf2);
+      mb.af2 += lb[2] * e.v * e.th1 * e.a2;
+      mb.a2 += lb[2] * e.v * e.th1 * e.af2;
+      mb.as2 += lb[2] * e.v * e.th1 * e.cf2;
+      mb.cf2 += lb[2] * e.v * e.th1 * e.as2;
+      mb.v += lb[2] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      mb.th1 += lb[3] * e.w * (e.af2 * e.a2 + e.as2 * e.cf2);
+      mb.af2 += lb[3] * e.w * e.th1 * e.a2;
+      mb.a2 += lb[3] * e.w * e.th1 * e.af2;
+      mb.as2 += lb[3] * e.w * e.th1 * e.cf2;
+      mb.cf2 += lb[3] * e.w * e.th1 * e.as2;
+      mb.w += lb[3] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      mb.th1 += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.af;
+      mb.af += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.th1;
+      mb.as += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * (e.th1 * e.af);
+      mb.bty += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
+      mb.cf += lb[5] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.bty);
+      mb.rr += lb[5] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.bty * e.cf);
+      mb.cf2 += lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr);
+      mb.cs2 += -(lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr));
+      mb.th1 += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.af;
+      mb.af += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.th1;
+      mb.as += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * (e.th1 * e.af);
+      mb.btz += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
+      mb.cf += lb[6] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.btz);
+      mb.rr += lb[6] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.btz * e.cf);
+      mb.cf2 += lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr);
+      mb.cs2 += -(lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr));
+      mb.th1 += -(lb[7] * (e.af2 * e.a2 + e.as2 * e.cf2));
+      mb.af2 += lb[7] * -e.th1 * e.a2;
+      mb.a2 += lb[7] * -e.th1 * e.af2;
+      mb.as2 += lb[7] * -e.th1 * e.cf2;
+      mb.cf2 += lb[7] * -e.th1 * e.as2;
+      mb.u += rb[1];
+      mb.v += rb[2];
+      mb.w += rb[3];
+      mb.uu += rb[7] * 0.5;
+      break;
+    }
+    case 4: {
+      mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
+      mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
+      mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
+      mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
+      mb.th2 += -(lb[0] * fcs) * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
+      mb.as += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * e.ca * sb;
+      mb.ca += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * (sb * e.as);
+      mb.u += -(lb[0] * fcs) * (0.5 * e.th2) * (sb * e.as * e.ca);
+      mb.af += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.cf;
+      mb.cf += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.af;
+      mb.vb += -(lb[0] * fcs) * (0.5 * e.th2) * (e.af * e.cf);
+      mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
+      mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
+      mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
+      mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+      mb.th2 += lb[1] * fcs * e.ca * e.as * (sb * 0.5);
+      mb.as += lb[1] * fcs * e.ca * (sb * 0.5 * e.th2);
+      mb.ca += lb[1] * fcs * (sb * 0.5 * e.th2 * e.as);
+      mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
+      mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
+      mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
+      mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+      mb.th2 += lb[2] * fcs * e.cf * e.bty * e.af * 0.5;
+      mb.af += lb[2] * fcs * e.cf * e.bty * (0.5 * e.th2);
+      mb.bty += lb[2] * fcs * e.cf * (0.5 * e.th2 * e.af);
+      mb.cf += lb[2] * fcs * (0.5 * e.th2 * e.af * e.bty);
+      mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
+      mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
+      mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
+      mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+      mb.th2 += lb[3] * fcs * e.cf * e.btz * e.af * 0.5;
+      mb.af += lb[3] * fcs * e.cf * e.btz * (0.5 * e.th2);
+      mb.btz += lb[3] * fcs * e.cf * (0.5 * e.th2 * e.af);
+      mb.cf += lb[3] * fcs * (0.5 * e.th2 * e.af * e.btz);
+      mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
+      mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
+      mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+      mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
+      mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
+      mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
+      mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
+      mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
+      mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+      mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
+      mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
+      mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
+      mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
+      mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
+      mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
+      mb.as += rb[0] * fcs;
+      mb.as += rb[1] * fcs * (e.u + e.cs);
+      mb.u += rb[1] * fcs * e.as;
+      mb.cs += rb[1] * fcs * e.as;
+      mb.as += rb[2] * fcs * e.v;
+      mb.v += rb[2] * fcs * e.as;
+      mb.af += rb[2] * fcs * e.a * e.bty * sb;
+      mb.bty += rb[2] * fcs * e.a * (sb * e.af);
+      mb.a += rb[2] * fcs * (sb * e.af * e.bty);
+      mb.as += rb[3] * fcs * e.w;
+      mb.w += rb[3] * fcs * e.as;
+      mb.af += rb[3] * fcs * e.a * e.btz * sb;
+      mb.btz += rb[3] * fcs * e.a * (sb * e.af);
+      mb.a += rb[3] * fcs * (sb * e.af * e.btz);
+      mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
+      mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+      mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
+      mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+      mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
+      mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+      mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
+      mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+      mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      mb.as += rb[7] * fcs * e.uu * 0.5;
+      mb.uu += rb[7] * fcs * (0.5 * e.as);
+      mb.as += rb[7] * fcs / G.g1 * e.cs2;
+      mb.cs2 += rb[7] * fcs / G.g1 * e.as;
+      mb.as += rb[7] * fcs * e.u * e.cs;
+      mb.cs += rb[7] * fcs * e.u * e.as;
+      mb.u += rb[7] * fcs * (e.as * e.cs);
+      mb.af += rb[7] * fcs * e.vb * e.a * sb;
+      mb.a += rb[7] * fcs * e.vb * (sb * e.af);
+      mb.vb += rb[7] * fcs * (sb * e.af * e.a);
+      mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
+      mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
+      mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
+      break;
+    }
+    case 5: {
+      mb.btz += lb[0] * sb * 0.5 * e.v;
+      mb.v += lb[0] * sb * 0.5 * e.btz;
+      mb.bty += -(lb[0] * sb * 0.5) * e.w;
+      mb.w += -(lb[0] * sb * 0.5) * e.bty;
+      mb.btz += lb[2] * sb * -0.5;
+      mb.bty += lb[3] * sb * 0.5;
+      mb.btz += lb[5] * e.rr * 0.5;
+      mb.rr += lb[5] * (0.5 * e.btz);
+      mb.bty += lb[6] * e.rr * -0.5;
+      mb.rr += lb[6] * (-0.5 * e.bty);
+      mb.btz += -rb[2] * sb;
+      mb.bty += rb[3] * sb;
+      mb.btz += rb[5] / e.rr;
+      mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
+      mb.bty += -(rb[6] / e.rr);
+      mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
+      mb.btz += -rb[7] * sb * e.v;
+      mb.v += -rb[7] * sb * e.btz;
+      mb.bty += -(-rb[7] * sb) * e.w;
+      mb.w += -(-rb[7] * sb) * e.bty;
+      break;
+    }
+    case 6: {
+      mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
+      mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
+      mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
+      mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
+      mb.th2 += -(lb[0] * fcf) * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
+      mb.af += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * e.a * sb;
+      mb.a += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * (sb * e.af);
+      mb.u += -(lb[0] * fcf) * (0.5 * e.th2) * (sb * e.af * e.a);
+      mb.as += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.cs;
+      mb.cs += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.as;
+      mb.vb += -(-(lb[0] * fcf) * (0.5 * e.th2)) * (e.as * e.cs);
+      mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
+      mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
+      mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
+      mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+      mb.th2 += lb[1] * fcf * e.a * e.af * (sb * 0.5);
+      mb.af += lb[1] * fcf * e.a * (sb * 0.5 * e.th2);
+      mb.a += lb[1] * fcf * (sb * 0.5 * e.th2 * e.af);
+      mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
+      mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
+      mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
+      mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+      mb.th2 += -(lb[2] * fcf) * e.cs * e.bty * e.as * 0.5;
+      mb.as += -(lb[2] * fcf) * e.cs * e.bty * (0.5 * e.th2);
+      mb.bty += -(lb[2] * fcf) * e.cs * (0.5 * e.th2 * e.as);
+      mb.cs += -(lb[2] * fcf) * (0.5 * e.th2 * e.as * e.bty);
+      mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
+      mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
+      mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
+      mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+      mb.th2 += -(lb[3] * fcf) * e.cs * e.btz * e.as * 0.5;
+      mb.as += -(lb[3] * fcf) * e.cs * e.btz * (0.5 * e.th2);
+      mb.btz += -(lb[3] * fcf) * e.cs * (0.5 * e.th2 * e.as);
+      mb.cs += -(lb[3] * fcf) * (0.5 * e.th2 * e.as * e.btz);
+      mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
+      mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
+      mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+      mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
+      mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
+      mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
+      mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
+      mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
+      mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+      mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
+      mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
+      mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
+      mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
+      mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
+      mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
+      mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
+      mb.af += rb[0] * fcf;
+      mb.af += rb[1] * fcf * (e.u + e.cf);
+      mb.u += rb[1] * fcf * e.af;
+      mb.cf += rb[1] * fcf * e.af;
+      mb.af += rb[2] * fcf * e.v;
+      mb.v += rb[2] * fcf * e.af;
+      mb.as += -(rb[2] * fcf) * e.ca * e.bty * sb;
+      mb.bty += -(rb[2] * fcf) * e.ca * (sb * e.as);
+      mb.ca += -(rb[2] * fcf) * (sb * e.as * e.bty);
+      mb.af += rb[3] * fcf * e.w;
+      mb.w += rb[3] * fcf * e.af;
+      mb.as += -(rb[3] * fcf) * e.ca * e.btz * sb;
+      mb.btz += -(rb[3] * fcf) * e.ca * (sb * e.as);
+      mb.ca += -(rb[3] * fcf) * (sb * e.as * e.btz);
+      mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
+      mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
+      mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
+      mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
+      mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
+      mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
+      mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
+      mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
+      mb.af += rb[7] * fcf * e.uu * 0.5;
+      mb.uu += rb[7] * fcf * (0.5 * e.af);
+      mb.af += rb[7] * fcf / G.g1 * e.cf2;
+      mb.cf2 += rb[7] * fcf / G.g1 * e.af;
+      mb.af += rb[7] * fcf * e.u * e.cf;
+      mb.cf += rb[7] * fcf * e.u * e.af;
+      mb.u += rb[7] * fcf * (e.af * e.cf);
+      mb.as += -(rb[7] * fcf) * e.vb * e.ca * sb;
+      mb.ca += -(rb[7] * fcf) * e.vb * (sb * e.as);
+      mb.vb += -(rb[7] * fcf) * (sb * e.as * e.ca);
+      mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
+      mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
+      mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// Adds d(Mid)/d(U1, U2)^T mb to U1b, U2b (midpoint() of mhd_eigen.cuh).
+__device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, const double* U1, const double* U2, const MidBar& mb, double* U1b, double* U2b) {
+  const double a0 = U1[0];
+  const double a1 = U1[1];
+  const double a2_ = U1[2];
+  const double a3 = U1[3];
+  const double a4 = U1[4];
+  const double a5 = U1[5];
+  const double a6 = U1[6];
+  const double a7 = U1[7];
+  const double b0 = U2[0];
+  const double b1 = U2[1];
+  const double b2 = U2[2];
+  const double b3 = U2[3];
+  const double b4 = U2[4];
+  const double b5 = U2[5];
+  const double b6 = U2[6];
+  const double b7 = U2[7];
+  const double gm = G.gm, gm1 = gm - 1.0, g21 = G.g21;
+  const double sb = (e.sbxm ? -1.0 : 1.0);
+  [[maybe_unused]] double r = 0.5 * (a0 + b0);
+  [[maybe_unused]] double u = 0.5 * (a1 / a0 + b1 / b0);
+  [[maybe_unused]] double v = 0.5 * (a2_ / a0 + b2 / b0);
+  [[maybe_unused]] double w = 0.5 * (a3 / a0 + b3 / b0);
+  [[maybe_unused]] double bx = 0.5 * (a4 + b4);
+  [[maybe_unused]] double by = 0.5 * (a5 + b5);
+  [[maybe_unused]] double bz = 0.5 * (a6 + b6);
+  [[maybe_unused]] double uu = u * u + v * v + w * w;
+  [[maybe_unused]] double bb = bx * bx + by * by + bz * bz;
+  [[maybe_unused]] double mml = a1 * a1 + a2_ * a2_ + a3 * a3;
+  [[maybe_unused]] double bbl = a4 * a4 + a5 * a5 + a6 * a6;
+  [[maybe_unused]] double mmr = b1 * b1 + b2 * b2 + b3 * b3;
+  [[maybe_unused]] double bbr = b4 * b4 + b5 * b5 + b6 * b6;
+  [[maybe_unused]] double ptl = gm1 * (a7 - 0.5 * mml / a0 - 0.5 * bbl) + 0.5 * bbl;
+  [[maybe_unused]] double ptr = gm1 * (b7 - 0.5 * mmr / b0 - 0.5 * bbr) + 0.5 * bbr;
+  [[maybe_unused]] double pt = 0.5 * (ptl + ptr);
+  [[maybe_unused]] double p = pt - 0.5 * bb;
+  const bool p_fz = p < 0.0;
+  if (p_fz) p = 0.0;
+  [[maybe_unused]] double a2 = gm * p / r;
+  const bool a2_fz = a2 < 0.0;
+  if (a2_fz) a2 = 0.0;
+  [[maybe_unused]] double a = sqrt(a2);
+  [[maybe_unused]] double ca2 = bx * bx / r;
+  [[maybe_unused]] double ca = sqrt(ca2);
+  [[maybe_unused]] double c2 = 0.5 * (bb / r + a2);
+  [[maybe_unused]] double ct = c2 * c2 - a2 * ca2;
+  const bool ct_fz = ct < 0.0;
+  if (ct_fz) ct = 0.0;
+  [[maybe_unused]] double sct = sqrt(ct);
+  [[maybe_unused]] double cs2 = c2 - sct;
+  const bool cs2_fz = cs2 < 0.0;
+  if (cs2_fz) cs2 = SMALL;
+  [[maybe_unused]] double cf2 = c2 + sct;
+  const bool cf2_fz = cf2 < 0.0;
+  if (cf2_fz) cf2 = SMALL;
+  [[maybe_unused]] double cs = sqrt(cs2);
+  [[maybe_unused]] double cf = sqrt(cf2);
+  [[maybe_unused]] double rr = sqrt(r);
+  [[maybe_unused]] double bp2 = by * by + bz * bz;
+  const bool deg = (bp2 < SMALL) && (fabs(ca2 - a2) < SMALL);
+  [[maybe_unused]] double af2 = (cf2 - ca2) / (cf2 - cs2);
+  const bool af2_fz = deg || af2 < 0.0;
+  if (af2_fz) af2 = deg ? 1.0 : 0.0;
+  [[maybe_unused]] double as2 = (cf2 - a2) / (cf2 - cs2);
+  const bool as2_fz = deg || as2 < 0.0;
+  if (as2_fz) as2 = deg ? 1.0 : 0.0;
+  [[maybe_unused]] double af = sqrt(af2);
+  [[maybe_unused]] double as_ = sqrt(as2);
+  [[maybe_unused]] double sbp = sqrt(bp2);
+  const bool sbp_fz = !(bp2 > SMALL);
+  if (sbp_fz) sbp = 1.0;
+  [[maybe_unused]] double bty = by / sbp;
+  const bool bty_fz = !(bp2 > SMALL);
+  if (bty_fz) bty = G.rs2;
+  [[maybe_unused]] double btz = bz / sbp;
+  const bool btz_fz = !(bp2 > SMALL);
+  if (btz_fz) btz = G.rs2;
+  [[maybe_unused]] double th1 = 1.0 / (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2));
+  [[maybe_unused]] double th2 = 1.0 / (sb * af2 * cf * a + sb * as2 * cs * ca);
+  [[maybe_unused]] double vb = bty * v + btz * w;
+  // reverse sweep
+  double r_b = 0.0;
+  double u_b = 0.0;
+  double v_b = 0.0;
+  double w_b = 0.0;
+  double bx_b = 0.0;
+  double by_b = 0.0;
+  double bz_b = 0.0;
+  double uu_b = 0.0;
+  double bb_b = 0.0;
+  double mml_b = 0.0;
+  double bbl_b = 0.0;
+  double mmr_b = 0.0;
+  double bbr_b = 0.0;
+  double ptl_b = 0.0;
+  double ptr_b = 0.0;
+  double pt_b = 0.0;
+  double p_b = 0.0;
+  double a2_b = 0.0;
+  double a_b = 0.0;
+  double ca2_b = 0.0;
+  double ca_b = 0.0;
+  double c2_b = 0.0;
+  double ct_b = 0.0;
+  double sct_b = 0.0;
+  double cs2_b = 0.0;
+  double cf2_b = 0.0;
+  double cs_b = 0.0;
+  double cf_b = 0.0;
+  double rr_b = 0.0;
+  double bp2_b = 0.0;
+  double af2_b = 0.0;
+  double as2_b = 0.0;
+  double af_b = 0.0;
+  double as__b = 0.0;
+  double sbp_b = 0.0;
+  double bty_b = 0.0;
+  double btz_b = 0.0;
+  double th1_b = 0.0;
+  double th2_b = 0.0;
+  double vb_b = 0.0;
+  double a0_b = 0.0;
+  double a1_b = 0.0;
+  double a2__b = 0.0;
+  double a3_b = 0.0;
+  double a4_b = 0.0;
+  double a5_b = 0.0;
+  double a6_b = 0.0;
+  double a7_b = 0.0;
+  double b0_b = 0.0;
+  double b1_b = 0.0;
+  double b2_b = 0.0;
+  double b3_b = 0.0;
+  double b4_b = 0.0;
+  double b5_b = 0.0;
+  double b6_b = 0.0;
+  double b7_b = 0.0;
+  u_b += mb.u;
+  v_b += mb.v;
+  w_b += mb.w;
+  uu_b += mb.uu;
+  a2_b += mb.a2;
+  a_b += mb.a;
+  ca2_b += mb.ca2;
+  ca_b += mb.ca;
+  cs2_b += mb.cs2;
+  cs_b += mb.cs;
+  cf2_b += mb.cf2;
+  cf_b += mb.cf;
+  rr_b += mb.rr;
+  af2_b += mb.af2;
+  af_b += mb.af;
+  as2_b += mb.as2;
+  as__b += mb.as;
+  bty_b += mb.bty;
+  btz_b += mb.btz;
+  th1_b += mb.th1;
+  th2_b += mb.th2;
+  vb_b += mb.vb;
+  {
+    bty_b += (vb_b) * (v);
+    v_b += (vb_b) * (bty);
+    btz_b += (vb_b) * (w);
+    w_b += (vb_b) * (btz);
+  }
+  {
+    af2_b += (((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (a)) * (cf)) * (sb);
+    cf_b += ((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (a)) * (sb * af2);
+    a_b += (-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (sb * af2 * cf);
+    as2_b += (((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (ca)) * (cs)) * (sb);
+    cs_b += ((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (ca)) * (sb * as2);
+    ca_b += (-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (sb * as2 * cs);
+  }
+  {
+    af2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cf2 - g21 * a2)) * (a2);
+    a2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cf2 - g21 * a2)) * (af2);
+    cf2_b += (-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (af2 * a2);
+    a2_b += (-((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (af2 * a2))) * (g21);
+    as2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cs2 - g21 * a2)) * (cf2);
+    cf2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cs2 - g21 * a2)) * (as2);
+    cs2_b += (-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (as2 * cf2);
+    a2_b += (-((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (as2 * cf2))) * (g21);
+  }
+  if (!btz_fz) {
+    bz_b += (btz_b) / (sbp);
+    sbp_b += -(btz_b) * (bz) / ((sbp) * (sbp));
+  }
+  if (!bty_fz) {
+    by_b += (bty_b) / (sbp);
+    sbp_b += -(bty_b) * (by) / ((sbp) * (sbp));
+  }
+  if (!sbp_fz) {
+    bp2_b += (sbp_b) * inv2sqrt(bp2);
+  }
+  {
+    as2_b += (as__b) * inv2sqrt(as2);
+  }
+  {
+    af2_b += (af_b) * inv2sqrt(af2);
+  }
+  if (!as2_fz) {
+    cf2_b += (as2_b) / (cf2 - cs2);
+    a2_b += -((as2_b) / (cf2 - cs2));
+    cf2_b += -(as2_b) * (cf2 - a2) / ((cf2 - cs2) * (cf2 - cs2));
+    cs2_b += -(-(as2_b) * (cf2 - a2) / ((cf2 - cs2) * (cf2 - cs2)));
+  }
+  if (!af2_fz) {
+    cf2_b += (af2_b) / (cf2 - cs2);
+    ca2_b += -((af2_b) / (cf2 - cs2));
+    cf2_b += -(af2_b) * (cf2 - ca2) / ((cf2 - cs2) * (cf2 - cs2));
+    cs2_b += -(-(af2_b) * (cf2 - ca2) / ((cf2 - cs2) * (cf2 - cs2)));
+  }
+  {
+    by_b += (bp2_b) * (by);
+    by_b += (bp2_b) * (by);
+    bz_b += (bp2_b) * (bz);
+    bz_b += (bp2_b) * (bz);
+  }
+  {
+    r_b += (rr_b) * inv2sqrt(r);
+  }
+  {
+    cf2_b += (cf_b) * inv2sqrt(cf2);
+  }
+  {
+    cs2_b += (cs_b) * inv2sqrt(cs2);
+  }
+  if (!cf2_fz) {
+    c2_b += cf2_b;
+    sct_b += cf2_b;
+  }
+  if (!cs2_fz) {
+    c2_b += cs2_b;
+    sct_b += -(cs2_b);
+  }
+  {
+    ct_b += (sct_b) * inv2sqrt(ct);
+  }
+  if (!ct_fz) {
+    c2_b += (ct_b) * (c2);
+    c2_b += (ct_b) * (c2);
+    a2_b += (-(ct_b)) * (ca2);
+    ca2_b += (-(ct_b)) * (a2);
+  }
+  {
+    bb_b += ((c2_b) * (0.5)) / (r);
+    r_b += -((c2_b) * (0.5)) * (bb) / ((r) * (r));
+    a2_b += (c2_b) * (0.5);
+  }
+  {
+    ca2_b += (ca_b) * inv2sqrt(ca2);
+  }
+  {
+    bx_b += ((ca2_b) / (r)) * (bx);
+    bx_b += ((ca2_b) / (r)) * (bx);
+    r_b += -(ca2_b) * (bx * bx) / ((r) * (r));
+  }
+  {
+    a2_b += (a_b) * inv2sqrt(a2);
+  }
+  if (!a2_fz) {
+    p_b += ((a2_b) / (r)) * (gm);
+    r_b += -(a2_b) * (gm * p) / ((r) * (r));
+  }
+  if (!p_fz) {
+    pt_b += p_b;
+    bb_b += (-(p_b)) * (0.5);
+  }
+  {
+    ptl_b += (pt_b) * (0.5);
+    ptr_b += (pt_b) * (0.5);
+  }
+  {
+    b7_b += (ptr_b) * (gm1);
+    mmr_b += ((-((ptr_b) * (gm1))) / (b0)) * (0.5);
+    b0_b += -(-((ptr_b) * (gm1))) * (0.5 * mmr) / ((b0) * (b0));
+    bbr_b += (-((ptr_b) * (gm1))) * (0.5);
+    bbr_b += (ptr_b) * (0.5);
+  }
+  {
+    a7_b += (ptl_b) * (gm1);
+    mml_b += ((-((ptl_b) * (gm1))) / (a0)) * (0.5);
+    a0_b += -(-((ptl_b) * (gm1))) * (0.5 * mml) / ((a0) * (a0));
+    bbl_b += (-((ptl_b) * (gm1))) * (0.5);
+    bbl_b += (ptl_b) * (0.5);
+  }
+  {
+    b4_b += (bbr_b) * (b4);
+    b4_b += (bbr_b) * (b4);
+    b5_b += (bbr_b) * (b5);
+    b5_b += (bbr_b) * (b5);
+    b6_b += (bbr_b) * (b6);
+    b6_b += (bbr_b) * (b6);
+  }
+  {
+    b1_b += (mmr_b) * (b1);
+    b1_b += (mmr_b) * (b1);
+    b2_b += (mmr_b) * (b2);
+    b2_b += (mmr_b) * (b2);
+    b3_b += (mmr_b) * (b3);
+    b3_b += (mmr_b) * (b3);
+  }
+  {
+    a4_b += (bbl_b) * (a4);
+    a4_b += (bbl_b) * (a4);
+    a5_b += (bbl_b) * (a5);
+    a5_b += (bbl_b) * (a5);
+    a6_b += (bbl_b) * (a6);
+    a6_b += (bbl_b) * (a6);
+  }
+  {
+    a1_b += (mml_b) * (a1);
+    a1_b += (mml_b) * (a1);
+    a2__b += (mml_b) * (a2_);
+    a2__b += (mml_b) * (a2_);
+    a3_b += (mml_b) * (a3);
+    a3_b += (mml_b) * (a3);
+  }
+  {
+    bx_b += (bb_b) * (bx);
+    bx_b += (bb_b) * (bx);
+    by_b += (bb_b) * (by);
+    by_b += (bb_b) * (by);
+    bz_b += (bb_b) * (bz);
+    bz_b += (bb_b) * (bz);
+  }
+  {
+    u_b += (uu_b) * (u);
+    u_b += (uu_b) * (u);
+    v_b += (uu_b) * (v);
+    v_b += (uu_b) * (v);
+    w_b += (uu_b) * (w);
+    w_b += (uu_b) * (w);
+  }
+  {
+    a6_b += (bz_b) * (0.5);
+    b6_b += (bz_b) * (0.5);
+  }
+  {
+    a5_b += (by_b) * (0.5);
+    b5_b += (by_b) * (0.5);
+  }
+  {
+    a4_b += (bx_b) * (0.5);
+    b4_b += (bx_b) * (0.5);
+  }
+  {
+    a3_b += ((w_b) * (0.5)) / (a0);
+    a0_b += -((w_b) * (0.5)) * (a3) / ((a0) * (a0));
+    b3_b += ((w_b) * (0.5)) / (b0);
+    b0_b += -((w_b) * (0.5)) * (b3) / ((b0) * (b0));
+  }
+  {
+    a2__b += ((v_b) * (0.5)) / (a0);
+    a0_b += -((v_b) * (0.5)) * (a2_) / ((a0) * (a0));
+    b2_b += ((v_b) * (0.5)) / (b0);
+    b0_b += -((v_b) * (0.5)) * (b2) / ((b0) * (b0));
+  }
+  {
+    a1_b += ((u_b) * (0.5)) / (a0);
+    a0_b += -((u_b) * (0.5)) * (a1) / ((a0) * (a0));
+    b1_b += ((u_b) * (0.5)) / (b0);
+    b0_b += -((u_b) * (0.5)) * (b1) / ((b0) * (b0));
+  }
+  {
+    a0_b += (r_b) * (0.5);
+    b0_b += (r_b) * (0.5);
+  }
+  U1b[0] += a0_b; U1b[1] += a1_b; U1b[2] += a2__b; U1b[3] += a3_b; U1b[4] += a4_b; U1b[5] += a5_b; U1b[6] += a6_b; U1b[7] += a7_b;
+  U2b[0] += b0_b; U2b[1] += b1_b; U2b[2] += b2_b; U2b[3] += b3_b; U2b[4] += b4_b; U2b[5] += b5_b; U2b[6] += b6_b; U2b[7] += b7_b;
+}
+
+// Adds (dF/dq)^T Fb to qb for the physical x flux F(q) (F[4] = 0).
+__device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const double* Fb, double* qb) {
+  const double q0 = q[0];
+  const double q1 = q[1];
+  const double q2 = q[2];
+  const double q3 = q[3];
+  const double q4 = q[4];
+  const double q5 = q[5];
+  const double q6 = q[6];
+  const double q7 = q[7];
+  const double gm1 = gm - 1.0;
+  [[maybe_unused]] double fu = q1 / q0;
+  [[maybe_unused]] double fv = q2 / q0;
+  [[maybe_unused]] double fw = q3 / q0;
+  [[maybe_unused]] double fuu = fu * fu + fv * fv + fw * fw;
+  [[maybe_unused]] double fub = fu * q4 + fv * q5 + fw * q6;
+  [[maybe_unused]] double fbb = q4 * q4 + q5 * q5 + q6 * q6;
+  [[maybe_unused]] double fp = gm1 * (q7 - 0.5 * q0 * fuu - 0.5 * fbb);
+  [[maybe_unused]] double fpt = fp + 0.5 * fbb;
+  [[maybe_unused]] double fo0 = q1;
+  [[maybe_unused]] double fo1 = q1 * fu - q4 * q4 + fpt;
+  [[maybe_unused]] double fo2 = q2 * fu - q4 * q5;
+  [[maybe_unused]] double fo3 = q3 * fu - q4 * q6;
+  [[maybe_unused]] double fo5 = q5 * fu - q4 * fv;
+  [[maybe_unused]] double fo6 = q6 * fu - q4 * fw;
+  [[maybe_unused]] double fo7 = (q7 + fpt) * fu - q4 * fub;
+  // reverse sweep
+  double fu_b = 0.0;
+  double fv_b = 0.0;
+  double fw_b = 0.0;
+  double fuu_b = 0.0;
+  double fub_b = 0.0;
+  double fbb_b = 0.0;
+  double fp_b = 0.0;
+  double fpt_b = 0.0;
+  double fo0_b = 0.0;
+  double fo1_b = 0.0;
+  double fo2_b = 0.0;
+  double fo3_b = 0.0;
+  double fo5_b = 0.0;
+  double fo6_b = 0.0;
+  double fo7_b = 0.0;
+  double q0_b = 0.0;
+  double q1_b = 0.0;
+  double q2_b = 0.0;
+  double q3_b = 0.0;
+  double q4_b = 0.0;
+  double q5_b = 0.0;
+  double q6_b = 0.0;
+  double q7_b = 0.0;
+  fo0_b = Fb[0];
+  fo1_b = Fb[1];
+  fo2_b = Fb[2];
+  fo3_b = Fb[3];
+  fo5_b = Fb[5];
+  fo6_b = Fb[6];
+  fo7_b = Fb[7];
+  {
+    q7_b += (fo7_b) * (fu);
+    fpt_b += (fo7_b) * (fu);
+    fu_b += (fo7_b) * (q7 + fpt);
+    q4_b += (-(fo7_b)) * (fub);
+    fub_b += (-(fo7_b)) * (q4);
+  }
+  {
+    q6_b += (fo6_b) * (fu);
+    fu_b += (fo6_b) * (q6);
+    q4_b += (-(fo6_b)) * (fw);
+    fw_b += (-(fo6_b)) * (q4);
+  }
+  {
+    q5_b += (fo5_b) * (fu);
+    fu_b += (fo5_b) * (q5);
+    q4_b += (-(fo5_b)) * (fv);
+    fv_b += (-(fo5_b)) * (q4);
+  }
+  {
+    q3_b += (fo3_b) * (fu);
+    fu_b += (fo3_b) * (q3);
+    q4_b += (-(fo3_b)) * (q6);
+    q6_b += (-(fo3_b)) * (q4);
+  }
+  {
+    q2_b += (fo2_b) * (fu);
+    fu_b += (fo2_b) * (q2);
+    q4_b += (-(fo2_b)) * (q5);
+    q5_b += (-(fo2_b)) * (q4);
+  }
+  {
+    q1_b += (fo1_b) * (fu);
+    fu_b += (fo1_b) * (q1);
+    q4_b += (-(fo1_b)) * (q4);
+    q4_b += (-(fo1_b)) * (q4);
+    fpt_b += fo1_b;
+  }
+  {
+    q1_b += fo0_b;
+  }
+  {
+    fp_b += fpt_b;
+    fbb_b += (fpt_b) * (0.5);
+  }
+  {
+    q7_b += (fp_b) * (gm1);
+    q0_b += ((-((fp_b) * (gm1))) * (fuu)) * (0.5);
+    fuu_b += (-((fp_b) * (gm1))) * (0.5 * q0);
+    fbb_b += (-((fp_b) * (gm1))) * (0.5);
+  }
+  {
+    q4_b += (fbb_b) * (q4);
+    q4_b += (fbb_b) * (q4);
+    q5_b += (fbb_b) * (q5);
+    q5_b += (fbb_b) * (q5);
+    q6_b += (fbb_b) * (q6);
+    q6_b += (fbb_b) * (q6);
+  }
+  {
+    fu_b += (fub_b) * (q4);
+    q4_b += (fub_b) * (fu);
+    fv_b += (fub_b) * (q5);
+    q5_b += (fub_b) * (fv);
+    fw_b += (fub_b) * (q6);
+    q6_b += (fub_b) * (fw);
+  }
+  {
+    fu_b += (fuu_b) * (fu);
+    fu_b += (fuu_b) * (fu);
+    fv_b += (fuu_b) * (fv);
+    fv_b += (fuu_b) * (fv);
+    fw_b += (fuu_b) * (fw);
+    fw_b += (fuu_b) * (fw);
+  }
+  {
+    q3_b += (fw_b) / (q0);
+    q0_b += -(fw_b) * (q3) / ((q0) * (q0));
+  }
+  {
+    q2_b += (fv_b) / (q0);
+    q0_b += -(fv_b) * (q2) / ((q0) * (q0));
+  }
+  {
+    q1_b += (fu_b) / (q0);
+    q0_b += -(fu_b) * (q1) / ((q0) * (q0));
+  }
+  qb[0] += q0_b;
+  qb[1] += q1_b;
+  qb[2] += q2_b;
+  qb[3] += q3_b;
+  qb[4] += q4_b;
+  qb[5] += q5_b;
+  qb[6] += q6_b;
+  qb[7] += q7_b;
+}
+
+}  // namespace MHD_KNS
+}  // namespace mhd

@@ -33,6 +33,7 @@
 #include "../../include/mhd2d_b200.h"
 #include "mhd_flux.cuh"
 #include "mhd_misc.cuh"
+#include "mhd_problems.cuh"
 
 namespace mhd {
 namespace MHD_KNS {
@@ -276,103 +277,6 @@ __global__ void kb_arm(const BInst* __restrict__ I, BState* S, int b, double dt0
   s.mode = -1;
   s.active = 1;
   if (!was) atomicAdd(n_active, 1);
-}
-
-// ---------------------------------------------------------------------------
-// Device-side initial states (interior cells; ghosts are filled by the
-// first boundary pass).  Conversions follow conversions.cpp:20-35.
-__device__ __forceinline__ void to_conserved(double gm, double rho, double u, double v, double w,
-                                             double bx, double by, double bz, double p,
-                                             double* q) {
-  q[0] = rho;
-  q[1] = u * rho;
-  q[2] = v * rho;
-  q[3] = w * rho;
-  q[4] = bx;
-  q[5] = by;
-  q[6] = bz;
-  const double uu = u * u + v * v + w * w;
-  const double bb = bx * bx + by * by + bz * bz;
-  q[7] = p / (gm - 1.0) + 0.5 * rho * uu + 0.5 * bb;
-}
-
-struct ProblemArgs {
-  int kind;
-  int K;
-  double p[40];
-  double ev[NF];  // wave: the chosen right eigenvector
-  double avg[NF]; // wave: conserved background state
-};
-
-__global__ void kb_problem(Grid g, double* __restrict__ U, ProblemArgs a) {
-  const long long n = (long long)g.nx * g.ny;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int ii = int(e / g.ny), jj = int(e - (long long)ii * g.ny);
-    const int i = ii + 2, j = jj + 2;
-    double q[NF];
-    const double gm = g.gamma;
-    if (a.kind == MHD_PROBLEM_EXPLOSION) {
-      // readProblemExplosion (file_access.cpp:398-470): centre at index (NX/2, NY/2)
-      const double di = double(i - g.NX / 2), dj = double(j - g.NY / 2);
-      const double r = a.p[2];
-      const bool inside = di * di * g.dx * g.dx + dj * dj * g.dy * g.dy < r * r;
-      const double rho = inside ? a.p[3] : a.p[5];
-      const double p = inside ? a.p[4] : a.p[6];
-      to_conserved(gm, rho, 0.0, 0.0, 0.0, a.p[7], a.p[8], 0.0, p, q);
-    } else if (a.kind == MHD_PROBLEM_WAVE) {
-      // readProblemWaveTest (file_access.cpp:922-1045)
-      const double x = a.p[0] + ii * g.dx, y = a.p[1] + jj * g.dy;
-      const double kx = a.p[14], ky = a.p[15];
-      const double sx = 2.0 * M_PI / a.p[2], sy = 2.0 * M_PI / a.p[3];
-      const double cphase = cos(sx * kx * x + sy * ky * y);
-      double c[NF];
-#pragma unroll
-      for (int k = 0; k < NF; k++) c[k] = a.avg[k] + a.p[12] * a.ev[k] * cphase;
-      // natural variables, rotation by atan2(ky, kx), back to conserved
-      const double u = c[1] / c[0], v = c[2] / c[0], w = c[3] / c[0];
-      const double mm = c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
-      const double bb = c[4] * c[4] + c[5] * c[5] + c[6] * c[6];
-      const double p = (gm - 1.0) * (c[7] - 0.5 * mm / c[0] - 0.5 * bb);
-      const double ang = atan2(ky, kx), ct = cos(ang), st = sin(ang);
-      const double ru = ct * u - st * v, rv = st * u + ct * v;
-      const double rbx = ct * c[4] - st * c[5], rby = st * c[4] + ct * c[5];
-      to_conserved(gm, c[0], ru, rv, w, rbx, rby, c[6], p, q);
-    } else if (a.kind == MHD_PROBLEM_ORSZAG_TANG) {
-      // readProblemOTVortex (file_access.cpp:578-613)
-      const double x = ii * g.dx, y = jj * g.dy;
-      to_conserved(gm, gm * gm, -sin(y), sin(x), 0.0, -sin(y), sin(2 * x), 0.0, gm, q);
-    } else {
-      // plasma sheet: By = tanh(x/delta), T = 0.5, p = 1.25 - By^2/2, rho = p/T,
-      // v = sum_k a_k sin(k pi y) exp(-x^2/0.04)
-      const double x = a.p[0] + ii * g.dx, y = a.p[1] + jj * g.dy;
-      const double by = tanh(x / a.p[2]);
-      const double p = 1.25 - 0.5 * by * by;
-      const double rho = p / 0.5;
-      double v = 0.0;
-      const double env = exp(-x * x / 0.04);
-      for (int k = 1; k <= a.K; k++) v += a.p[3 + k] * sin(k * M_PI * y) * env;
-      to_conserved(gm, rho, 0.0, v, 0.0, 0.0, by, 0.0, p, q);
-    }
-#pragma unroll
-    for (int k = 0; k < NF; k++) U[g.at(k, i, j)] = q[k];
-  }
-}
-
-// Right eigenvector `wave` at the state (avg, avg) (getEigens_F with
-// break_on_neg_pressure = true, as readProblemWaveTest calls it).
-__global__ void kb_wave_eigen(double gamma, const double* avg, int wave, double* out, int* err) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const Gas G{gamma, gamma - 1.0, (gamma - 2.0) / (gamma - 1.0), 1.0 / sqrt(2.0)};
-  double U[NF];
-  for (int k = 0; k < NF; k++) U[k] = avg[k];
-  Mid e;
-  if (!midpoint(G, U, U, e) || e.negp) { *err = 1; return; }
-  double q[NF];
-  for (int k = 0; k < NF; k++) q[k] = 0.0;
-  rv_row(e, G, wave, q);
-  for (int k = 0; k < NF; k++) out[k] = q[k];
-  *err = 0;
 }
 
 }  // namespace MHD_KNS
@@ -809,51 +713,13 @@ int mhd_batch_init_problem(mhd_batch* b, int idx, int kind, const double* p, int
   if (check_idx(b, idx)) return MHD_ERR_WRONG_PARAMETER;
   BK(cudaSetDevice(b->device));
   ProblemArgs a{};
-  a.kind = kind;
-  const mhd_batch_desc& d = b->desc[idx];
-  const BInst& in = b->hinst[idx];
-  if (kind == MHD_PROBLEM_EXPLOSION) {
-    if (!p || np < 9) return MHD_ERR_WRONG_PARAMETER;
-  } else if (kind == MHD_PROBLEM_WAVE) {
-    if (!p || np < 16) return MHD_ERR_WRONG_PARAMETER;
-    const int wave = int(p[13]);
-    if (wave < 0 || wave > 6 || p[14] < 0 || p[15] < 0) return MHD_ERR_WRONG_PARAMETER;
-  } else if (kind == MHD_PROBLEM_PLASMA_SHEET) {
-    if (!p || np < 4 || int(p[3]) < 0 || 4 + int(p[3]) > np || 4 + int(p[3]) > 40)
-      return MHD_ERR_WRONG_PARAMETER;
-    a.K = int(p[3]);
-  } else if (kind != MHD_PROBLEM_ORSZAG_TANG) {
-    return MHD_ERR_WRONG_PARAMETER;
-  }
-  for (int q = 0; q < np && q < 40; q++) a.p[q] = p[q];
-  if (kind == MHD_PROBLEM_WAVE) {
-    // conserved background (toConservationPoint), then its right eigenvector
-    const double rho = p[4], u = p[5], v = p[6], w = p[7], bx = p[8], by = p[9], bz = p[10];
-    const double pr = p[11], gm = d.gamma;
-    a.avg[0] = rho;
-    a.avg[1] = u * rho; a.avg[2] = v * rho; a.avg[3] = w * rho;
-    a.avg[4] = bx; a.avg[5] = by; a.avg[6] = bz;
-    const double uu = u * u + v * v + w * w, bb = bx * bx + by * by + bz * bz;
-    a.avg[7] = pr / (gm - 1.0) + 0.5 * rho * uu + 0.5 * bb;
-    double* dtmp = nullptr;
-    BK(cudaMalloc(&dtmp, 2 * NF * sizeof(double) + sizeof(int)));
-    BK(cudaMemcpyAsync(dtmp, a.avg, NF * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-    int* derr = reinterpret_cast<int*>(dtmp + 2 * NF);
-    kb_wave_eigen<<<1, 32, 0, b->stream>>>(gm, dtmp, int(p[13]), dtmp + NF, derr);
-    int herr = 0;
-    cudaMemcpyAsync(a.ev, dtmp + NF, NF * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
-    cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
-    cudaError_t e = cudaStreamSynchronize(b->stream);
-    cudaFree(dtmp);
-    if (e != cudaSuccess) return bfail(b, e, "kb_wave_eigen");
-    if (herr)
-      return bset(b, MHD_ERR_WRONG_PARAMETER, true,
-                  "readProblemWaveTest: failed to calculate eigensystem from average values.");
-    b->launches += 1;
-  }
-  const long long cells = (long long)d.nx * d.ny;
-  int blocks = int(std::min<long long>((cells + 255) / 256, 148LL * 16));
-  kb_problem<<<blocks, 256, 0, b->stream>>>(in.g, in.U, a);
+  std::string err;
+  cudaError_t ce = cudaSuccess;
+  const int st = problem_args(kind, p, np, b->desc[idx].gamma, b->stream, a, err, ce);
+  if (ce != cudaSuccess) return bfail(b, ce, "problem_args");
+  if (st) return bset(b, st, true, err);
+  if (kind == MHD_PROBLEM_WAVE) b->launches += 1;
+  enqueue_problem(b->hinst[idx].g, b->hinst[idx].U, a, b->stream);
   b->launches += 1;
   BK(cudaGetLastError());
   return arm(b, idx);

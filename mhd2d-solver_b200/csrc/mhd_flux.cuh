@@ -121,10 +121,16 @@ struct Lane {
 // DENSE = true performs every product of the reference's dense 8x8 loops,
 // the dummy wave 7 included, and so reproduces its NaN / inf propagation
 // exactly; the kernel recomputes flagged interfaces this way.
-template <int SCHEME, bool CHARS, bool DENSE>
+// MASK (ENO-Roe only): 0 plain; 1 records, per characteristic k, a 4-bit
+// code in bits 4k..4k+3 of *mw (bit 0: the ENO- stencil took the left
+// pair, bit 1: the ENO+ stencil took the left pair, bits 2-3: upwind choice
+// 0 wm, 1 wp, 2 zero); 2 replays the choices stored in *mw instead of
+// comparing (the frozen-stencil forward of the adjoint).
+template <int SCHEME, bool CHARS, bool DENSE, int MASK = 0>
 __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, const double* alpha,
                                                double* Fn, double& smax, int& negp,
-                                               double* lam, double* LU, bool& nonfinite) {
+                                               double* lam, double* LU, bool& nonfinite,
+                                               unsigned* mw = nullptr) {
   double U1[NF], U2[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
@@ -176,10 +182,35 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
         vw[1] += l[m] * (f2 - f1);
         vw[2] += l[m] * (f3 - f2);
       }
-      const double wm = eno_minus(w[0], w[1], w[2], vw[0], vw[1]);
-      const double wp = eno_plus(w[1], w[2], w[3], vw[1], vw[2]);
-      const double ak = eigenvalue(e, k);
-      fw = (ak >= 0 && wm < 1.0e10) ? wm : ((ak <= 0 && wp < 1.0e10) ? wp : 0.0);
+      if constexpr (MASK == 0) {
+        const double wm = eno_minus(w[0], w[1], w[2], vw[0], vw[1]);
+        const double wp = eno_plus(w[1], w[2], w[3], vw[1], vw[2]);
+        const double ak = eigenvalue(e, k);
+        fw = (ak >= 0 && wm < 1.0e10) ? wm : ((ak <= 0 && wp < 1.0e10) ? wp : 0.0);
+      } else {
+        bool em, ep;
+        int up;
+        if constexpr (MASK == 1) {
+          em = fabs(vw[0]) < fabs(vw[1]);
+          ep = fabs(vw[1]) < fabs(vw[2]);
+        } else {
+          const unsigned c = (*mw >> (4 * k)) & 0xFu;
+          em = (c & 1u) != 0;
+          ep = (c & 2u) != 0;
+        }
+        const double wm = em ? (-(1.0 / 2.0) * w[0] + (3.0 / 2.0) * w[1])
+                             : ((1.0 / 2.0) * w[1] + (1.0 / 2.0) * w[2]);
+        const double wp = ep ? ((1.0 / 2.0) * w[1] + (1.0 / 2.0) * w[2])
+                             : ((3.0 / 2.0) * w[2] - (1.0 / 2.0) * w[3]);
+        if constexpr (MASK == 1) {
+          const double ak = eigenvalue(e, k);
+          up = (ak >= 0 && wm < 1.0e10) ? 0 : ((ak <= 0 && wp < 1.0e10) ? 1 : 2);
+          *mw |= (unsigned(em) | (unsigned(ep) << 1) | (unsigned(up) << 2)) << (4 * k);
+        } else {
+          up = int((*mw >> (4 * k + 2)) & 3u);
+        }
+        fw = up == 0 ? wm : (up == 1 ? wp : 0.0);
+      }
     } else {  // ENO-LF: split w = (RF +- alpha RU)/2, ENO on each half
       double ru[4], rf[4];
 #pragma unroll
@@ -239,21 +270,25 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
 // (tj, ti); the kernel provides TileGeom::BYTES of dynamic shared memory.  A
 // caller that runs several tiles in a row separates them with
 // __syncthreads().
-template <int SCHEME, bool CHARS, int TI, int TJ, int NW>
+template <int SCHEME, bool CHARS, int TI, int TJ, int NW, int MASK = 0>
 __device__ __forceinline__ void flux_tile(const Grid& g, const double* __restrict__ U,
                                           double* __restrict__ UL,
                                           const double* __restrict__ alphaF,
                                           const double* __restrict__ alphaG, double inv_dx,
                                           double inv_dy, const Gas& G, Ctl* ctl, const CharOut& co,
-                                          int tj, int ti) {
+                                          int tj, int ti, unsigned* maskX = nullptr,
+                                          unsigned* maskY = nullptr) {
 #include "mhd_flux_tile.inc"
 }
 
-template <int SCHEME, bool CHARS, int TI, int TJ, int NW>
+// maskX / maskY: ENO choice words of the x / y interfaces ([NX][NY] by the
+// interface's left / lower cell), written (MASK 1) or read (MASK 2).
+template <int SCHEME, bool CHARS, int TI, int TJ, int NW, int MASK = 0>
 __global__ void __launch_bounds__(NW * 32, MHD_MINB)
 k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
        const double* __restrict__ alphaF, const double* __restrict__ alphaG,
-       double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co) {
+       double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co, unsigned* maskX,
+       unsigned* maskY) {
   if (ctl->skip) return;
   const int tj = blockIdx.x, ti = blockIdx.y;
 #include "mhd_flux_tile.inc"

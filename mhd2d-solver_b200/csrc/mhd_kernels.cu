@@ -67,7 +67,8 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
   CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
              ch ? ch[3] : nullptr};
   const Gas G{g.gamma, g.gamma - 1.0, (g.gamma - 2.0) / (g.gamma - 1.0), 1.0 / std::sqrt(2.0)};
-  kern<<<grid, NW * 32, Geom::BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co);
+  kern<<<grid, NW * 32, Geom::BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co,
+                                          nullptr, nullptr);
 }
 
 void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double* aF,

@@ -203,8 +203,7 @@ __device__ __forceinline__ double min3(double a, double b, double c) {
 }
 
 
-__global__ void k_control(Ctl* c, StepParams p, int phase, double arg) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void control_step(Ctl* c, const StepParams& p, int phase, double arg) {
   if (phase == PH_RESET_STEP || phase == PH_RESET_INTEGRATE) {
     c->skip = 0; c->retry = 0; c->error = 0; c->neg_last = 0; c->step_done = 0;
     c->maxX = 0ull; c->maxY = 0ull;
@@ -255,6 +254,11 @@ __global__ void k_control(Ctl* c, StepParams p, int phase, double arg) {
   }
   c->upd_status = st;
   if (st == 4 || st == 10) { c->error = st; c->skip = 1; }
+}
+
+__global__ void k_control(Ctl* c, StepParams p, int phase, double arg) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  control_step(c, p, phase, arg);
 }
 
 // ---------------------------------------------------------------------------

@@ -47,6 +47,15 @@ _ip = C.POINTER(C.c_int)
 _lib = None
 
 
+class AdjStats(C.Structure):
+    """mhd_adj_stats."""
+
+    _fields_ = [("steps", C.c_int), ("stages", C.c_int), ("checkpoints", C.c_int),
+                ("retries", C.c_int), ("t", C.c_double), ("dt", C.c_double),
+                ("ms_forward", C.c_double), ("ms_backward", C.c_double),
+                ("ms_replay", C.c_double), ("launches", C.c_longlong)]
+
+
 class BatchDesc(C.Structure):
     """mhd_batch_desc: one run of a batch."""
 
@@ -128,6 +137,20 @@ def library():
         "mhd_batch_init_problem": [vp, C.c_int, C.c_int, _dp, C.c_int],
         "mhd_batch_stream": [vp, C.POINTER(vp)],
         "mhd_batch_launches": [vp, C.POINTER(C.c_longlong)],
+        "mhd_adj_create": [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _ip, C.c_int,
+                           C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(vp)],
+        "mhd_adj_destroy": [vp],
+        "mhd_adj_last_error": [vp, C.c_char_p, C.c_size_t, _ip],
+        "mhd_adj_upload": [vp, _dp],
+        "mhd_adj_init_problem": [vp, C.c_int, _dp, C.c_int],
+        "mhd_adj_forward": [vp, C.c_int, C.c_double, _dp],
+        "mhd_adj_replay": [vp, _dp, _dp],
+        "mhd_adj_replay_problem": [vp, C.c_int, _dp, C.c_int, _dp],
+        "mhd_adj_backward": [vp],
+        "mhd_adj_gradient": [vp, _dp],
+        "mhd_adj_sheet_gradient": [vp, C.c_double, C.c_double, C.c_int, _dp],
+        "mhd_adj_download": [vp, C.c_int, _dp],
+        "mhd_adj_info": [vp, C.POINTER(AdjStats)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

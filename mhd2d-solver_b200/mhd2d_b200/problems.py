@@ -15,7 +15,10 @@ The problem descriptions follow the reference's problem setups
                     (file_access.cpp:302-395 with angle 0);
 * ``explosion``   — circular blast, open boundaries;
 * ``random_smooth`` / ``random_blocky`` — seeded synthetic states for
-                    parity tests (smooth and discontinuous).
+                    parity tests (smooth and discontinuous);
+* ``plasma_sheet`` — the current sheet of the adjoint benchmark
+                    (By = tanh(x/delta), a velocity perturbation with
+                    amplitudes a_k) and its tangents dU0/da_k.
 """
 from __future__ import annotations
 
@@ -136,3 +139,41 @@ def random_blocky(nx, ny, seed=0, gamma=5.0 / 3.0, bc=(PERIODIC,) * 4, nblocks=4
     p = field(0.1, 2.0)
     U = to_conserved(rho, u, v, w, bx, by, bz, p, gamma)
     return Problem(U, dx, dy, gamma, tuple(bc), f"random_blocky[{seed}]")
+
+
+def plasma_sheet(nx, ny, amps, delta=0.1, gamma=5.0 / 3.0, lx=4.0, ly=2.0, x0=-2.0, y0=-1.0,
+                 bc=(NEUMANN, NEUMANN, PERIODIC, PERIODIC)):
+    """By = tanh(x/delta), Bx = Bz = 0, T = 0.5, p = 1.25 - By^2/2, rho = p/T,
+    v = sum_k a_k sin(k pi y) exp(-x^2/0.04); cell i at x0 + i dx (the
+    reference's coordinate convention, file_access.cpp:598-599)."""
+    dx, dy = lx / nx, ly / ny
+    x = (x0 + np.arange(nx) * dx)[:, None] * np.ones((1, ny))
+    y = np.ones((nx, 1)) * (y0 + np.arange(ny) * dy)[None, :]
+    by = np.tanh(x / delta)
+    p = 1.25 - 0.5 * by * by
+    rho = p / 0.5
+    env = np.exp(-x * x / 0.04)
+    v = np.zeros_like(x)
+    for k, a in enumerate(amps, start=1):
+        v = v + a * np.sin(k * math.pi * y) * env
+    z = np.zeros_like(x)
+    U = to_conserved(rho, z, v, z, z, by, z, p, gamma)
+    return Problem(U, dx, dy, gamma, tuple(bc), "plasma_sheet",
+                   extra={"amps": list(amps), "delta": delta, "x0": x0, "y0": y0})
+
+
+def plasma_sheet_tangents(p):
+    """dU0/da_k of plasma_sheet, shape (K, 8, nx+4, ny+4)."""
+    nx, ny = p.nx, p.ny
+    x = (p.extra["x0"] + np.arange(nx) * p.dx)[:, None] * np.ones((1, ny))
+    y = np.ones((nx, 1)) * (p.extra["y0"] + np.arange(ny) * p.dy)[None, :]
+    rho = p.U[0, 2:-2, 2:-2]
+    v = p.U[2, 2:-2, 2:-2] / rho
+    env = np.exp(-x * x / 0.04)
+    K = len(p.extra["amps"])
+    T = np.zeros((K,) + p.U.shape)
+    for k in range(1, K + 1):
+        s = np.sin(k * math.pi * y) * env
+        T[k - 1, 2, 2:-2, 2:-2] = rho * s
+        T[k - 1, 7, 2:-2, 2:-2] = rho * v * s
+    return T

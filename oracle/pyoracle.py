@@ -24,6 +24,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libmhdoracle.so")
+TLM_SO = os.path.join(HERE, "_build", "libmhdtlm.so")
 REF_SO = os.path.join(HERE, "_ref", "libmhdref.so")
 REF_BENCH = os.path.join(HERE, "_ref", "ref_bench")
 
@@ -85,6 +86,34 @@ def load_oracle():
     lib.orc_retries.argtypes = [C.c_void_p]
     lib.orc_retries.restype = C.c_longlong
     return lib
+
+
+TLM_NT = 17  # tangent directions of one tlm_run call (tlm.cpp)
+
+
+def tlm_run(U0, dU0, nx, ny, dx, dy, gamma, bc, nsteps, dt0, time_method=2, dt_min=0.0,
+            dt_max=1.0, cfl=0.4, scheme=2):
+    """Tangent-linear run of the oracle (tlm.cpp): J and dJ/dU0 . dU0[r] for each
+    of up to 17 directions dU0[r] (shape (ndir, 8, nx+4, ny+4)), frozen branches."""
+    if not os.path.exists(TLM_SO):
+        raise FileNotFoundError(f"{TLM_SO} missing: run `make -C oracle`")
+    lib = C.CDLL(TLM_SO)
+    lib.tlm_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                            C.c_double, _ip, C.c_double, C.c_double, C.c_double, C.c_int,
+                            C.c_double, _dp, C.c_int, _dp, _dp, _dp, _dp, _ip]
+    U0 = np.ascontiguousarray(U0, dtype=np.float64)
+    dU0 = np.ascontiguousarray(dU0, dtype=np.float64).reshape(-1, *U0.shape)
+    nd = dU0.shape[0]
+    if nd > TLM_NT:
+        raise ValueError("at most 17 directions per call")
+    J = C.c_double(0.0)
+    dJ = np.zeros(max(nd, 1))
+    Uout = np.zeros_like(U0)
+    steps = C.c_int(0)
+    st = lib.tlm_run(scheme, time_method, nx, ny, dx, dy, gamma, _bc(bc), dt_min, dt_max, cfl,
+                     nsteps, dt0, _p(U0), nd, _p(dU0), C.byref(J), _p(dJ), _p(Uout),
+                     C.byref(steps))
+    return dict(status=st, J=J.value, dJ=dJ[:nd], U=Uout, steps=steps.value)
 
 
 def reference_available():

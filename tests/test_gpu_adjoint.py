@@ -1,0 +1,193 @@
+"""Discrete adjoint of the ENO-Roe step (mhd_adj_*) against the tangent-linear
+oracle (oracle/tlm.cpp: forward-mode derivative of the same discrete map with
+the same frozen branches) and against frozen-stencil central differences of
+the GPU replay."""
+import os
+
+import numpy as np
+import pytest
+
+import mhd2d_b200 as M
+from mhd2d_b200 import problems as P
+from mhd2d_b200.adjoint import Adjoint
+from gpu_helpers import make_ctx, same
+from pyoracle import tlm_run
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _interior_dirs(shape, n, seed):
+    d = np.random.default_rng(seed).normal(0, 1, (n,) + shape)
+    d[:, :, :2], d[:, :, -2:], d[:, :, :, :2], d[:, :, :, -2:] = 0, 0, 0, 0
+    return d
+
+
+def _adjoint(p, nsteps, dt0=1e-3, dt_max=0.01, tm=M.RK3, K=4, cfl=0.4, dt_min=1e-9):
+    a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, time_method=tm, dt_min=dt_min,
+                dt_max=dt_max, cfl=cfl, checkpoint_every=K)
+    a.upload(p.U)
+    J = a.forward(nsteps, dt0)
+    return a, J
+
+
+def _dot(g, d):
+    return float((g[:, 2:-2, 2:-2] * d[:, 2:-2, 2:-2]).sum())
+
+
+CASES = [
+    ("sheet", lambda: P.plasma_sheet(32, 16, np.random.default_rng(1).normal(0, 1e-2, 6))),
+    ("smooth-periodic", lambda: P.random_smooth(24, 20, seed=2)),
+    ("smooth-open", lambda: P.random_smooth(20, 24, seed=3, bc=(M.OPEN,) * 4)),
+    ("smooth-mixed", lambda: P.random_smooth(22, 18, seed=4,
+                                            bc=(M.DIRICHLET, M.NEUMANN, M.NEUMANN, M.OPEN))),
+    ("blocky-neumann", lambda: P.random_blocky(20, 20, seed=6, bc=(M.NEUMANN,) * 4)),
+]
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_recording_forward_and_replay_match_context(name, make):
+    p = make()
+    a, J = _adjoint(p, 6)
+    c = make_ctx(p, dt_min=1e-9, dt_max=0.01, flags=0)
+    dt = 1e-3
+    for _ in range(6):
+        st, dt = c.step(dt)
+        assert not st.isError
+    Uc = c.download()
+    assert same(a.download(1)[:, 2:-2, 2:-2], Uc[:, 2:-2, 2:-2])
+    assert a.info()["dt"] == dt
+    assert a.replay() == J  # frozen replay of the recorded initial state
+    assert same(a.download(2)[:, 2:-2, 2:-2], Uc[:, 2:-2, 2:-2])
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+def test_adjoint_matches_tangent_linear(name, make):
+    p = make()
+    nsteps = 6
+    a, J = _adjoint(p, nsteps)
+    a.backward()
+    g = a.gradient()
+    d = _interior_dirs(p.U.shape, 4, seed=7)
+    r = tlm_run(p.U, d, p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, nsteps=nsteps, dt0=1e-3,
+                dt_min=1e-9, dt_max=0.01)
+    assert r["steps"] == nsteps
+    assert abs(r["J"] - J) <= 1e-12 * abs(J)
+    for q in range(d.shape[0]):
+        adj = _dot(g, d[q])
+        assert abs(adj - r["dJ"][q]) <= 1e-9 * max(abs(r["dJ"][q]), 1e-30), (q, adj, r["dJ"][q])
+
+
+def test_sheet_amplitude_gradient_matches_tangent_linear():
+    amps = np.random.default_rng(5).normal(0, 1e-3, 16)
+    p = P.plasma_sheet(40, 20, amps)
+    a, J = _adjoint(p, 12)
+    a.sheet = (p.extra["x0"], p.extra["y0"], 16)
+    a.backward()
+    dJda = a.sheet_gradient()
+    T = P.plasma_sheet_tangents(p)
+    r = tlm_run(p.U, T, p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, nsteps=12, dt0=1e-3,
+                dt_min=1e-9, dt_max=0.01)
+    scale = np.abs(r["dJ"]).max()
+    assert np.all(np.abs(dJda - r["dJ"]) <= 1e-9 * scale), (dJda, r["dJ"])
+
+
+def test_frozen_stencil_central_differences():
+    """(J(U0 + h d) - J(U0 - h d)) / 2h of the frozen replay, h = 1e-7, against
+    the adjoint's dJ/dU0 . d, within 1e-6 relative."""
+    amps = np.random.default_rng(9).normal(0, 1e-3, 16)
+    p = P.plasma_sheet(64, 32, amps)
+    a, J = _adjoint(p, 30, K=8)
+    a.backward()
+    g = a.gradient()
+    T = P.plasma_sheet_tangents(p)
+    dirs = [T[0], T[3], T[15]] + list(_interior_dirs(p.U.shape, 2, seed=11) * 1e-3)
+    h = 1e-7
+    for d in dirs:
+        fd = (a.replay(p.U + h * d) - a.replay(p.U - h * d)) / (2 * h)
+        adj = _dot(g, d)
+        assert abs(fd - adj) <= 1e-6 * abs(adj), (fd, adj)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    p = P.random_blocky(24, 16, seed=8, bc=(M.PERIODIC, M.PERIODIC, M.NEUMANN, M.NEUMANN))
+    grads = []
+    for K in (1, 3, 100):
+        a, _ = _adjoint(p, 7, K=K)
+        a.backward()
+        grads.append(a.gradient())
+        assert a.info()["checkpoints"] == -(-7 // K)
+    assert same(grads[0], grads[1]) and same(grads[0], grads[2])
+
+
+def test_retry_steps_and_euler_match_tangent_linear():
+    d = np.load(os.path.join(GOLD, "run_explosion_retry.npz"))
+    p = P.Problem(d["U_in"].copy(), float(d["dx"]), float(d["dy"]), float(d["gamma"]),
+                  tuple(int(b) for b in d["bc"]))
+    n = int(d["nsteps"])
+    kw = dict(dt0=float(d["dt0"]), dt_max=float(d["dt_max"]), cfl=float(d["cfl"]),
+              dt_min=float(d["dt_min"]))
+    a, J = _adjoint(p, n, **kw)
+    assert a.info()["retries"] > 0  # the case really restarts RK3 stage loops
+    a.backward()
+    g = a.gradient()
+    dirs = _interior_dirs(p.U.shape, 3, seed=12)
+    r = tlm_run(p.U, dirs, p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, nsteps=n, dt0=kw["dt0"],
+                dt_min=kw["dt_min"], dt_max=kw["dt_max"], cfl=kw["cfl"])
+    for q in range(3):
+        assert abs(_dot(g, dirs[q]) - r["dJ"][q]) <= 1e-9 * abs(r["dJ"][q])
+    pe = P.random_smooth(20, 20, seed=13)
+    a, J = _adjoint(pe, 5, tm=M.EULER)
+    a.backward()
+    g = a.gradient()
+    dirs = _interior_dirs(pe.U.shape, 2, seed=14)
+    r = tlm_run(pe.U, dirs, pe.nx, pe.ny, pe.dx, pe.dy, pe.gamma, pe.bc, nsteps=5, dt0=1e-3,
+                time_method=1, dt_min=1e-9, dt_max=0.01)
+    for q in range(2):
+        assert abs(_dot(g, dirs[q]) - r["dJ"][q]) <= 1e-9 * abs(r["dJ"][q])
+
+
+def test_device_plasma_sheet_and_its_gradient():
+    amps = np.random.default_rng(2).normal(0, 1e-3, 16)
+    p = P.plasma_sheet(48, 24, amps)
+    a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-9, dt_max=0.01,
+                checkpoint_every=5)
+    a.init_plasma_sheet(amps)
+    U0 = a.download(0)
+    np.testing.assert_allclose(U0[:, 2:-2, 2:-2], p.U[:, 2:-2, 2:-2], rtol=1e-13, atol=1e-17)
+    a.forward(8, 1e-3)
+    a.backward()
+    dJda = a.sheet_gradient()
+    # the same state uploaded from the host gives the same dJ/da
+    b = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-9, dt_max=0.01,
+                checkpoint_every=5)
+    b.upload(U0)
+    b.forward(8, 1e-3)
+    b.backward()
+    b.sheet = a.sheet
+    assert same(dJda, b.sheet_gradient())
+    # frozen central differences in the amplitudes (replays of the device setup)
+    h = 1e-7
+    for k in (0, 7):
+        ap, am = amps.copy(), amps.copy()
+        ap[k] += h
+        am[k] -= h
+        fd = (a.replay_plasma_sheet(ap) - a.replay_plasma_sheet(am)) / (2 * h)
+        assert abs(fd - dJda[k]) <= 1e-6 * np.abs(dJda).max(), (k, fd, dJda[k])
+
+
+def test_autograd_function_wrapper():
+    import torch
+
+    from adjoint_autograd import kinetic_energy_after_steps
+    p = P.plasma_sheet(32, 16, np.random.default_rng(4).normal(0, 1e-2, 4))
+    a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-9, dt_max=0.01,
+                checkpoint_every=3)
+    U0 = torch.tensor(p.U, dtype=torch.float64, requires_grad=True)
+    J = kinetic_energy_after_steps(U0, a, 9, 1e-3)
+    J.backward()
+    d = _interior_dirs(p.U.shape, 1, seed=21)[0] * 1e-3
+    h = 1e-7
+    fd = (a.replay(p.U + h * d) - a.replay(p.U - h * d)) / (2 * h)
+    adj = float((U0.grad.numpy() * d).sum())
+    assert abs(fd - adj) <= 1e-6 * abs(adj)
