@@ -12,7 +12,10 @@ statement t = f(x, y, ...) in reverse order the generator emits
 walking the expression tree (sum, difference, product, quotient, square
 root, negation).  Clamps and degenerate-case branches are frozen: a
 statement whose frozen condition held in the forward evaluation passes no
-adjoint on (its value was a constant there).  The derivative of sqrt(v) is
+adjoint on (its value was a constant there), and neither does a statement
+whose adjoint is exactly zero (degenerate midpoints, e.g. a pressure clamped
+to zero, give infinite partial derivatives that a zero seed must not turn
+into NaN).  The derivative of sqrt(v) is
 taken as 0 at v = 0, the one-sided convention of a frozen branch (it only
 arises where the forward value is exactly zero, e.g. B_x = 0).
 """
@@ -242,12 +245,19 @@ def emit_rows():
         o.append(f"    case {k}: {{")
         for rows, seedname in ((LROWS, "lb"), (RROWS, "rb")):
             for m, expr in sorted(rows[k].items()):
+                lines = []
                 for var, coef in reverse_of(expr, f"{seedname}[{m}]"):
                     if var in CONSTS:
                         continue
                     assert var in MID_FIELDS, var
                     field = "as" if var == "as_" else var
-                    o.append(f"      mb.{field} += {c_expr(coef, MID_NAMES)};")
+                    lines.append(f"        mb.{field} += {c_expr(coef, MID_NAMES)};")
+                if lines:
+                    # a zero seed adds nothing (and must not meet an infinite
+                    # partial derivative: 0 * inf would be NaN)
+                    o.append(f"      if ({seedname}[{m}] != 0.0) {{")
+                    o.extend(lines)
+                    o.append("      }")
         o.append("      break;")
         o.append("    }")
     o.append("    default:")
@@ -287,7 +297,7 @@ def emit_program(name, decl, stmts, inputs, prologue, seeds, epilogue):
             lines.append(f"    {var}_b += {coef};")
         if not lines:
             continue
-        o.append(f"  if (!{t}_fz) {{" if len(st) > 2 else "  {")
+        o.append(f"  if (!{t}_fz && {t}_b != 0.0) {{" if len(st) > 2 else f"  if ({t}_b != 0.0) {{")
         o.extend(lines)
         o.append("  }")
     o.extend(epilogue)

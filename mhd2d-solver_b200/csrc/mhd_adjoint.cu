@@ -237,10 +237,13 @@ __global__ void __launch_bounds__(AIB) ka_adj_iface(Grid g, Gas G, const double*
     rv_row(e0, G, k, r);
     const unsigned code = (mw >> (4 * k)) & 0xFu;
     const int up = int(code >> 2);
+    // upwind choice "zero": the characteristic's flux is the constant 0 (its
+    // row may even be non-finite, as at a midpoint whose pressure was clamped)
+    if (up == 2) continue;
     double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;  // frozen ENO combination of the 4 points
     if (up == 0) {
       if (code & 1u) { c0 = -0.5; c1 = 1.5; } else { c1 = 0.5; c2 = 0.5; }
-    } else if (up == 1) {
+    } else {
       if (code & 2u) { c1 = 0.5; c2 = 0.5; } else { c2 = 1.5; c3 = -0.5; }
     }
     double phi[NF], fw = 0.0, gk = 0.0;

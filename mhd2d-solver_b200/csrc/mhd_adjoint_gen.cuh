@@ -26,461 +26,635 @@ __device__ __forceinline__ void row_adjoint(const Mid& e, const Gas& G, int k,
   (void)fcf; (void)fcs; (void)sb;
   switch (k) {
     case 0: {
-      mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
-      mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
-      mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
-      mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
-      mb.th2 += lb[0] * fcf * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
-      mb.af += lb[0] * fcf * (0.5 * e.th2) * e.u * e.a * sb;
-      mb.a += lb[0] * fcf * (0.5 * e.th2) * e.u * (sb * e.af);
-      mb.u += lb[0] * fcf * (0.5 * e.th2) * (sb * e.af * e.a);
-      mb.as += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.cs;
-      mb.cs += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.as;
-      mb.vb += -(lb[0] * fcf * (0.5 * e.th2)) * (e.as * e.cs);
-      mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
-      mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
-      mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
-      mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-      mb.th2 += -(lb[1] * fcf) * e.a * e.af * (sb * 0.5);
-      mb.af += -(lb[1] * fcf) * e.a * (sb * 0.5 * e.th2);
-      mb.a += -(lb[1] * fcf) * (sb * 0.5 * e.th2 * e.af);
-      mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
-      mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
-      mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
-      mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-      mb.th2 += lb[2] * fcf * e.cs * e.bty * e.as * 0.5;
-      mb.as += lb[2] * fcf * e.cs * e.bty * (0.5 * e.th2);
-      mb.bty += lb[2] * fcf * e.cs * (0.5 * e.th2 * e.as);
-      mb.cs += lb[2] * fcf * (0.5 * e.th2 * e.as * e.bty);
-      mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
-      mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
-      mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
-      mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-      mb.th2 += lb[3] * fcf * e.cs * e.btz * e.as * 0.5;
-      mb.as += lb[3] * fcf * e.cs * e.btz * (0.5 * e.th2);
-      mb.btz += lb[3] * fcf * e.cs * (0.5 * e.th2 * e.as);
-      mb.cs += lb[3] * fcf * (0.5 * e.th2 * e.as * e.btz);
-      mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
-      mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
-      mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-      mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
-      mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
-      mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
-      mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
-      mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
-      mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-      mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
-      mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
-      mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
-      mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
-      mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
-      mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
-      mb.af += rb[0] * fcf;
-      mb.af += rb[1] * fcf * (e.u - e.cf);
-      mb.u += rb[1] * fcf * e.af;
-      mb.cf += -(rb[1] * fcf * e.af);
-      mb.af += rb[2] * fcf * e.v;
-      mb.v += rb[2] * fcf * e.af;
-      mb.as += rb[2] * fcf * e.ca * e.bty * sb;
-      mb.bty += rb[2] * fcf * e.ca * (sb * e.as);
-      mb.ca += rb[2] * fcf * (sb * e.as * e.bty);
-      mb.af += rb[3] * fcf * e.w;
-      mb.w += rb[3] * fcf * e.af;
-      mb.as += rb[3] * fcf * e.ca * e.btz * sb;
-      mb.btz += rb[3] * fcf * e.ca * (sb * e.as);
-      mb.ca += rb[3] * fcf * (sb * e.as * e.btz);
-      mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
-      mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
-      mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
-      mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
-      mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
-      mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
-      mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
-      mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
-      mb.af += rb[7] * fcf * e.uu * 0.5;
-      mb.uu += rb[7] * fcf * (0.5 * e.af);
-      mb.af += rb[7] * fcf / G.g1 * e.cf2;
-      mb.cf2 += rb[7] * fcf / G.g1 * e.af;
-      mb.af += -(rb[7] * fcf) * e.u * e.cf;
-      mb.cf += -(rb[7] * fcf) * e.u * e.af;
-      mb.u += -(rb[7] * fcf) * (e.af * e.cf);
-      mb.as += rb[7] * fcf * e.vb * e.ca * sb;
-      mb.ca += rb[7] * fcf * e.vb * (sb * e.as);
-      mb.vb += rb[7] * fcf * (sb * e.as * e.ca);
-      mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
-      mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
-      mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
+      if (lb[0] != 0.0) {
+        mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
+        mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
+        mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
+        mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
+        mb.th2 += lb[0] * fcf * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
+        mb.af += lb[0] * fcf * (0.5 * e.th2) * e.u * e.a * sb;
+        mb.a += lb[0] * fcf * (0.5 * e.th2) * e.u * (sb * e.af);
+        mb.u += lb[0] * fcf * (0.5 * e.th2) * (sb * e.af * e.a);
+        mb.as += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.cs;
+        mb.cs += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.as;
+        mb.vb += -(lb[0] * fcf * (0.5 * e.th2)) * (e.as * e.cs);
+      }
+      if (lb[1] != 0.0) {
+        mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
+        mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
+        mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
+        mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+        mb.th2 += -(lb[1] * fcf) * e.a * e.af * (sb * 0.5);
+        mb.af += -(lb[1] * fcf) * e.a * (sb * 0.5 * e.th2);
+        mb.a += -(lb[1] * fcf) * (sb * 0.5 * e.th2 * e.af);
+      }
+      if (lb[2] != 0.0) {
+        mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
+        mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
+        mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
+        mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+        mb.th2 += lb[2] * fcf * e.cs * e.bty * e.as * 0.5;
+        mb.as += lb[2] * fcf * e.cs * e.bty * (0.5 * e.th2);
+        mb.bty += lb[2] * fcf * e.cs * (0.5 * e.th2 * e.as);
+        mb.cs += lb[2] * fcf * (0.5 * e.th2 * e.as * e.bty);
+      }
+      if (lb[3] != 0.0) {
+        mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
+        mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
+        mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
+        mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+        mb.th2 += lb[3] * fcf * e.cs * e.btz * e.as * 0.5;
+        mb.as += lb[3] * fcf * e.cs * e.btz * (0.5 * e.th2);
+        mb.btz += lb[3] * fcf * e.cs * (0.5 * e.th2 * e.as);
+        mb.cs += lb[3] * fcf * (0.5 * e.th2 * e.as * e.btz);
+      }
+      if (lb[5] != 0.0) {
+        mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
+        mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
+        mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+        mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
+        mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
+        mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
+        mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[6] != 0.0) {
+        mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
+        mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
+        mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+        mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
+        mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
+        mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
+        mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[7] != 0.0) {
+        mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
+        mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
+        mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
+      }
+      if (rb[0] != 0.0) {
+        mb.af += rb[0] * fcf;
+      }
+      if (rb[1] != 0.0) {
+        mb.af += rb[1] * fcf * (e.u - e.cf);
+        mb.u += rb[1] * fcf * e.af;
+        mb.cf += -(rb[1] * fcf * e.af);
+      }
+      if (rb[2] != 0.0) {
+        mb.af += rb[2] * fcf * e.v;
+        mb.v += rb[2] * fcf * e.af;
+        mb.as += rb[2] * fcf * e.ca * e.bty * sb;
+        mb.bty += rb[2] * fcf * e.ca * (sb * e.as);
+        mb.ca += rb[2] * fcf * (sb * e.as * e.bty);
+      }
+      if (rb[3] != 0.0) {
+        mb.af += rb[3] * fcf * e.w;
+        mb.w += rb[3] * fcf * e.af;
+        mb.as += rb[3] * fcf * e.ca * e.btz * sb;
+        mb.btz += rb[3] * fcf * e.ca * (sb * e.as);
+        mb.ca += rb[3] * fcf * (sb * e.as * e.btz);
+      }
+      if (rb[5] != 0.0) {
+        mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
+        mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
+        mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
+        mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
+      }
+      if (rb[6] != 0.0) {
+        mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
+        mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
+        mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
+        mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
+      }
+      if (rb[7] != 0.0) {
+        mb.af += rb[7] * fcf * e.uu * 0.5;
+        mb.uu += rb[7] * fcf * (0.5 * e.af);
+        mb.af += rb[7] * fcf / G.g1 * e.cf2;
+        mb.cf2 += rb[7] * fcf / G.g1 * e.af;
+        mb.af += -(rb[7] * fcf) * e.u * e.cf;
+        mb.cf += -(rb[7] * fcf) * e.u * e.af;
+        mb.u += -(rb[7] * fcf) * (e.af * e.cf);
+        mb.as += rb[7] * fcf * e.vb * e.ca * sb;
+        mb.ca += rb[7] * fcf * e.vb * (sb * e.as);
+        mb.vb += rb[7] * fcf * (sb * e.as * e.ca);
+        mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
+        mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
+        mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
+      }
       break;
     }
     case 1: {
-      mb.btz += lb[0] * sb * -0.5 * e.v;
-      mb.v += lb[0] * sb * -0.5 * e.btz;
-      mb.bty += -(lb[0] * sb * -0.5) * e.w;
-      mb.w += -(lb[0] * sb * -0.5) * e.bty;
-      mb.btz += lb[2] * sb * 0.5;
-      mb.bty += lb[3] * sb * -0.5;
-      mb.btz += lb[5] * e.rr * 0.5;
-      mb.rr += lb[5] * (0.5 * e.btz);
-      mb.bty += lb[6] * e.rr * -0.5;
-      mb.rr += lb[6] * (-0.5 * e.bty);
-      mb.btz += rb[2] * sb;
-      mb.bty += -rb[3] * sb;
-      mb.btz += rb[5] / e.rr;
-      mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
-      mb.bty += -(rb[6] / e.rr);
-      mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
-      mb.btz += rb[7] * sb * e.v;
-      mb.v += rb[7] * sb * e.btz;
-      mb.bty += -(rb[7] * sb) * e.w;
-      mb.w += -(rb[7] * sb) * e.bty;
+      if (lb[0] != 0.0) {
+        mb.btz += lb[0] * sb * -0.5 * e.v;
+        mb.v += lb[0] * sb * -0.5 * e.btz;
+        mb.bty += -(lb[0] * sb * -0.5) * e.w;
+        mb.w += -(lb[0] * sb * -0.5) * e.bty;
+      }
+      if (lb[2] != 0.0) {
+        mb.btz += lb[2] * sb * 0.5;
+      }
+      if (lb[3] != 0.0) {
+        mb.bty += lb[3] * sb * -0.5;
+      }
+      if (lb[5] != 0.0) {
+        mb.btz += lb[5] * e.rr * 0.5;
+        mb.rr += lb[5] * (0.5 * e.btz);
+      }
+      if (lb[6] != 0.0) {
+        mb.bty += lb[6] * e.rr * -0.5;
+        mb.rr += lb[6] * (-0.5 * e.bty);
+      }
+      if (rb[2] != 0.0) {
+        mb.btz += rb[2] * sb;
+      }
+      if (rb[3] != 0.0) {
+        mb.bty += -rb[3] * sb;
+      }
+      if (rb[5] != 0.0) {
+        mb.btz += rb[5] / e.rr;
+        mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
+      }
+      if (rb[6] != 0.0) {
+        mb.bty += -(rb[6] / e.rr);
+        mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
+      }
+      if (rb[7] != 0.0) {
+        mb.btz += rb[7] * sb * e.v;
+        mb.v += rb[7] * sb * e.btz;
+        mb.bty += -(rb[7] * sb) * e.w;
+        mb.w += -(rb[7] * sb) * e.bty;
+      }
       break;
     }
     case 2: {
-      mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
-      mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
-      mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
-      mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
-      mb.th2 += lb[0] * fcs * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
-      mb.as += lb[0] * fcs * (0.5 * e.th2) * e.u * e.ca * sb;
-      mb.ca += lb[0] * fcs * (0.5 * e.th2) * e.u * (sb * e.as);
-      mb.u += lb[0] * fcs * (0.5 * e.th2) * (sb * e.as * e.ca);
-      mb.af += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.cf;
-      mb.cf += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.af;
-      mb.vb += lb[0] * fcs * (0.5 * e.th2) * (e.af * e.cf);
-      mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
-      mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
-      mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
-      mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-      mb.th2 += -(lb[1] * fcs) * e.ca * e.as * (sb * 0.5);
-      mb.as += -(lb[1] * fcs) * e.ca * (sb * 0.5 * e.th2);
-      mb.ca += -(lb[1] * fcs) * (sb * 0.5 * e.th2 * e.as);
-      mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
-      mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
-      mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
-      mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-      mb.th2 += -(lb[2] * fcs) * e.cf * e.bty * e.af * 0.5;
-      mb.af += -(lb[2] * fcs) * e.cf * e.bty * (0.5 * e.th2);
-      mb.bty += -(lb[2] * fcs) * e.cf * (0.5 * e.th2 * e.af);
-      mb.cf += -(lb[2] * fcs) * (0.5 * e.th2 * e.af * e.bty);
-      mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
-      mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
-      mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
-      mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-      mb.th2 += -(lb[3] * fcs) * e.cf * e.btz * e.af * 0.5;
-      mb.af += -(lb[3] * fcs) * e.cf * e.btz * (0.5 * e.th2);
-      mb.btz += -(lb[3] * fcs) * e.cf * (0.5 * e.th2 * e.af);
-      mb.cf += -(lb[3] * fcs) * (0.5 * e.th2 * e.af * e.btz);
-      mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
-      mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
-      mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-      mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
-      mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
-      mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
-      mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
-      mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
-      mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-      mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
-      mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
-      mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
-      mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
-      mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
-      mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
-      mb.as += rb[0] * fcs;
-      mb.as += rb[1] * fcs * (e.u - e.cs);
-      mb.u += rb[1] * fcs * e.as;
-      mb.cs += -(rb[1] * fcs * e.as);
-      mb.as += rb[2] * fcs * e.v;
-      mb.v += rb[2] * fcs * e.as;
-      mb.af += -(rb[2] * fcs) * e.a * e.bty * sb;
-      mb.bty += -(rb[2] * fcs) * e.a * (sb * e.af);
-      mb.a += -(rb[2] * fcs) * (sb * e.af * e.bty);
-      mb.as += rb[3] * fcs * e.w;
-      mb.w += rb[3] * fcs * e.as;
-      mb.af += -(rb[3] * fcs) * e.a * e.btz * sb;
-      mb.btz += -(rb[3] * fcs) * e.a * (sb * e.af);
-      mb.a += -(rb[3] * fcs) * (sb * e.af * e.btz);
-      mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
-      mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-      mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
-      mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-      mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
-      mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-      mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
-      mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-      mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      mb.as += rb[7] * fcs * e.uu * 0.5;
-      mb.uu += rb[7] * fcs * (0.5 * e.as);
-      mb.as += rb[7] * fcs / G.g1 * e.cs2;
-      mb.cs2 += rb[7] * fcs / G.g1 * e.as;
-      mb.as += -(rb[7] * fcs) * e.u * e.cs;
-      mb.cs += -(rb[7] * fcs) * e.u * e.as;
-      mb.u += -(rb[7] * fcs) * (e.as * e.cs);
-      mb.af += -(rb[7] * fcs) * e.vb * e.a * sb;
-      mb.a += -(rb[7] * fcs) * e.vb * (sb * e.af);
-      mb.vb += -(rb[7] * fcs) * (sb * e.af * e.a);
-      mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
-      mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
-      mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
+      if (lb[0] != 0.0) {
+        mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
+        mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
+        mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
+        mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
+        mb.th2 += lb[0] * fcs * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
+        mb.as += lb[0] * fcs * (0.5 * e.th2) * e.u * e.ca * sb;
+        mb.ca += lb[0] * fcs * (0.5 * e.th2) * e.u * (sb * e.as);
+        mb.u += lb[0] * fcs * (0.5 * e.th2) * (sb * e.as * e.ca);
+        mb.af += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.cf;
+        mb.cf += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.af;
+        mb.vb += lb[0] * fcs * (0.5 * e.th2) * (e.af * e.cf);
+      }
+      if (lb[1] != 0.0) {
+        mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
+        mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
+        mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+        mb.th2 += -(lb[1] * fcs) * e.ca * e.as * (sb * 0.5);
+        mb.as += -(lb[1] * fcs) * e.ca * (sb * 0.5 * e.th2);
+        mb.ca += -(lb[1] * fcs) * (sb * 0.5 * e.th2 * e.as);
+      }
+      if (lb[2] != 0.0) {
+        mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
+        mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
+        mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+        mb.th2 += -(lb[2] * fcs) * e.cf * e.bty * e.af * 0.5;
+        mb.af += -(lb[2] * fcs) * e.cf * e.bty * (0.5 * e.th2);
+        mb.bty += -(lb[2] * fcs) * e.cf * (0.5 * e.th2 * e.af);
+        mb.cf += -(lb[2] * fcs) * (0.5 * e.th2 * e.af * e.bty);
+      }
+      if (lb[3] != 0.0) {
+        mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
+        mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
+        mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+        mb.th2 += -(lb[3] * fcs) * e.cf * e.btz * e.af * 0.5;
+        mb.af += -(lb[3] * fcs) * e.cf * e.btz * (0.5 * e.th2);
+        mb.btz += -(lb[3] * fcs) * e.cf * (0.5 * e.th2 * e.af);
+        mb.cf += -(lb[3] * fcs) * (0.5 * e.th2 * e.af * e.btz);
+      }
+      if (lb[5] != 0.0) {
+        mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
+        mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
+        mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+        mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
+        mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
+        mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
+        mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[6] != 0.0) {
+        mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
+        mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
+        mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+        mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
+        mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
+        mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
+        mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[7] != 0.0) {
+        mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
+        mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
+        mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
+      }
+      if (rb[0] != 0.0) {
+        mb.as += rb[0] * fcs;
+      }
+      if (rb[1] != 0.0) {
+        mb.as += rb[1] * fcs * (e.u - e.cs);
+        mb.u += rb[1] * fcs * e.as;
+        mb.cs += -(rb[1] * fcs * e.as);
+      }
+      if (rb[2] != 0.0) {
+        mb.as += rb[2] * fcs * e.v;
+        mb.v += rb[2] * fcs * e.as;
+        mb.af += -(rb[2] * fcs) * e.a * e.bty * sb;
+        mb.bty += -(rb[2] * fcs) * e.a * (sb * e.af);
+        mb.a += -(rb[2] * fcs) * (sb * e.af * e.bty);
+      }
+      if (rb[3] != 0.0) {
+        mb.as += rb[3] * fcs * e.w;
+        mb.w += rb[3] * fcs * e.as;
+        mb.af += -(rb[3] * fcs) * e.a * e.btz * sb;
+        mb.btz += -(rb[3] * fcs) * e.a * (sb * e.af);
+        mb.a += -(rb[3] * fcs) * (sb * e.af * e.btz);
+      }
+      if (rb[5] != 0.0) {
+        mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
+        mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+        mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
+        mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+        mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      }
+      if (rb[6] != 0.0) {
+        mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
+        mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+        mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
+        mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+        mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      }
+      if (rb[7] != 0.0) {
+        mb.as += rb[7] * fcs * e.uu * 0.5;
+        mb.uu += rb[7] * fcs * (0.5 * e.as);
+        mb.as += rb[7] * fcs / G.g1 * e.cs2;
+        mb.cs2 += rb[7] * fcs / G.g1 * e.as;
+        mb.as += -(rb[7] * fcs) * e.u * e.cs;
+        mb.cs += -(rb[7] * fcs) * e.u * e.as;
+        mb.u += -(rb[7] * fcs) * (e.as * e.cs);
+        mb.af += -(rb[7] * fcs) * e.vb * e.a * sb;
+        mb.a += -(rb[7] * fcs) * e.vb * (sb * e.af);
+        mb.vb += -(rb[7] * fcs) * (sb * e.af * e.a);
+        mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
+        mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
+        mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
+      }
       break;
     }
     case 3: {
-      mb.th1 += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * e.uu * 0.5;
-      mb.uu += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * (0.5 * e.th1);
-      mb.af2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.a2;
-      mb.a2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.af2;
-      mb.as2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.cf2;
-      mb.cf2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.as2;
-      mb.th1 += lb[1] * e.u * (e.af2 * e.a2 + e.as2 * e.cf2);
-      mb.af2 += lb[1] * e.u * e.th1 * e.a2;
-      mb.a2 += lb[1] * e.u * e.th1 * e.af2;
-      mb.as2 += lb[1] * e.u * e.th1 * e.cf2;
-      mb.cf2 += lb[1] * e.u * e.th1 * e.as2;
-      mb.u += lb[1] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
-      mb.th1 += lb[2] * e.v * (e.af2 * e.a2 + e.as2 * e.cf2);
-      mb.af2 += lb[2] * e.v * e.th1 * e.a2;
-      mb.a2 += lb[2] * e.v * e.th1 * e.af2;
-      mb.as2 += lb[2] * e.v * e.th1 * e.cf2;
-      mb.cf2 += lb[2] * e.v * e.th1 * e.as2;
-      mb.v += lb[2] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
-      mb.th1 += lb[3] * e.w * (e.af2 * e.a2 + e.as2 * e.cf2);
-      mb.af2 += lb[3] * e.w * e.th1 * e.a2;
-      mb.a2 += lb[3] * e.w * e.th1 * e.af2;
-      mb.as2 += lb[3] * e.w * e.th1 * e.cf2;
-      mb.cf2 += lb[3] * e.w * e.th1 * e.as2;
-      mb.w += lb[3] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
-      mb.th1 += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.af;
-      mb.af += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.th1;
-      mb.as += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * (e.th1 * e.af);
-      mb.bty += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
-      mb.cf += lb[5] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.bty);
-      mb.rr += lb[5] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.bty * e.cf);
-      mb.cf2 += lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr);
-      mb.cs2 += -(lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr));
-      mb.th1 += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.af;
-      mb.af += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.th1;
-      mb.as += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * (e.th1 * e.af);
-      mb.btz += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
-      mb.cf += lb[6] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.btz);
-      mb.rr += lb[6] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.btz * e.cf);
-      mb.cf2 += lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr);
-      mb.cs2 += -(lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr));
-      mb.th1 += -(lb[7] * (e.af2 * e.a2 + e.as2 * e.cf2));
-      mb.af2 += lb[7] * -e.th1 * e.a2;
-      mb.a2 += lb[7] * -e.th1 * e.af2;
-      mb.as2 += lb[7] * -e.th1 * e.cf2;
-      mb.cf2 += lb[7] * -e.th1 * e.as2;
-      mb.u += rb[1];
-      mb.v += rb[2];
-      mb.w += rb[3];
-      mb.uu += rb[7] * 0.5;
+      if (lb[0] != 0.0) {
+        mb.th1 += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * e.uu * 0.5;
+        mb.uu += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * (0.5 * e.th1);
+        mb.af2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.a2;
+        mb.a2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.af2;
+        mb.as2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.cf2;
+        mb.cf2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.as2;
+      }
+      if (lb[1] != 0.0) {
+        mb.th1 += lb[1] * e.u * (e.af2 * e.a2 + e.as2 * e.cf2);
+        mb.af2 += lb[1] * e.u * e.th1 * e.a2;
+        mb.a2 += lb[1] * e.u * e.th1 * e.af2;
+        mb.as2 += lb[1] * e.u * e.th1 * e.cf2;
+        mb.cf2 += lb[1] * e.u * e.th1 * e.as2;
+        mb.u += lb[1] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      }
+      if (lb[2] != 0.0) {
+        mb.th1 += lb[2] * e.v * (e.af2 * e.a2 + e.as2 * e.cf2);
+        mb.af2 += lb[2] * e.v * e.th1 * e.a2;
+        mb.a2 += lb[2] * e.v * e.th1 * e.af2;
+        mb.as2 += lb[2] * e.v * e.th1 * e.cf2;
+        mb.cf2 += lb[2] * e.v * e.th1 * e.as2;
+        mb.v += lb[2] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      }
+      if (lb[3] != 0.0) {
+        mb.th1 += lb[3] * e.w * (e.af2 * e.a2 + e.as2 * e.cf2);
+        mb.af2 += lb[3] * e.w * e.th1 * e.a2;
+        mb.a2 += lb[3] * e.w * e.th1 * e.af2;
+        mb.as2 += lb[3] * e.w * e.th1 * e.cf2;
+        mb.cf2 += lb[3] * e.w * e.th1 * e.as2;
+        mb.w += lb[3] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      }
+      if (lb[5] != 0.0) {
+        mb.th1 += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.af;
+        mb.af += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.th1;
+        mb.as += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * (e.th1 * e.af);
+        mb.bty += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
+        mb.cf += lb[5] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.bty);
+        mb.rr += lb[5] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.bty * e.cf);
+        mb.cf2 += lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr);
+        mb.cs2 += -(lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr));
+      }
+      if (lb[6] != 0.0) {
+        mb.th1 += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.af;
+        mb.af += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.th1;
+        mb.as += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * (e.th1 * e.af);
+        mb.btz += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
+        mb.cf += lb[6] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.btz);
+        mb.rr += lb[6] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.btz * e.cf);
+        mb.cf2 += lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr);
+        mb.cs2 += -(lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr));
+      }
+      if (lb[7] != 0.0) {
+        mb.th1 += -(lb[7] * (e.af2 * e.a2 + e.as2 * e.cf2));
+        mb.af2 += lb[7] * -e.th1 * e.a2;
+        mb.a2 += lb[7] * -e.th1 * e.af2;
+        mb.as2 += lb[7] * -e.th1 * e.cf2;
+        mb.cf2 += lb[7] * -e.th1 * e.as2;
+      }
+      if (rb[1] != 0.0) {
+        mb.u += rb[1];
+      }
+      if (rb[2] != 0.0) {
+        mb.v += rb[2];
+      }
+      if (rb[3] != 0.0) {
+        mb.w += rb[3];
+      }
+      if (rb[7] != 0.0) {
+        mb.uu += rb[7] * 0.5;
+      }
       break;
     }
     case 4: {
-      mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
-      mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
-      mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
-      mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
-      mb.th2 += -(lb[0] * fcs) * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
-      mb.as += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * e.ca * sb;
-      mb.ca += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * (sb * e.as);
-      mb.u += -(lb[0] * fcs) * (0.5 * e.th2) * (sb * e.as * e.ca);
-      mb.af += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.cf;
-      mb.cf += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.af;
-      mb.vb += -(lb[0] * fcs) * (0.5 * e.th2) * (e.af * e.cf);
-      mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
-      mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
-      mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
-      mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-      mb.th2 += lb[1] * fcs * e.ca * e.as * (sb * 0.5);
-      mb.as += lb[1] * fcs * e.ca * (sb * 0.5 * e.th2);
-      mb.ca += lb[1] * fcs * (sb * 0.5 * e.th2 * e.as);
-      mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
-      mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
-      mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
-      mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-      mb.th2 += lb[2] * fcs * e.cf * e.bty * e.af * 0.5;
-      mb.af += lb[2] * fcs * e.cf * e.bty * (0.5 * e.th2);
-      mb.bty += lb[2] * fcs * e.cf * (0.5 * e.th2 * e.af);
-      mb.cf += lb[2] * fcs * (0.5 * e.th2 * e.af * e.bty);
-      mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
-      mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
-      mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
-      mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-      mb.th2 += lb[3] * fcs * e.cf * e.btz * e.af * 0.5;
-      mb.af += lb[3] * fcs * e.cf * e.btz * (0.5 * e.th2);
-      mb.btz += lb[3] * fcs * e.cf * (0.5 * e.th2 * e.af);
-      mb.cf += lb[3] * fcs * (0.5 * e.th2 * e.af * e.btz);
-      mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
-      mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
-      mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-      mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
-      mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
-      mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
-      mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
-      mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
-      mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-      mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
-      mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
-      mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
-      mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
-      mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
-      mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
-      mb.as += rb[0] * fcs;
-      mb.as += rb[1] * fcs * (e.u + e.cs);
-      mb.u += rb[1] * fcs * e.as;
-      mb.cs += rb[1] * fcs * e.as;
-      mb.as += rb[2] * fcs * e.v;
-      mb.v += rb[2] * fcs * e.as;
-      mb.af += rb[2] * fcs * e.a * e.bty * sb;
-      mb.bty += rb[2] * fcs * e.a * (sb * e.af);
-      mb.a += rb[2] * fcs * (sb * e.af * e.bty);
-      mb.as += rb[3] * fcs * e.w;
-      mb.w += rb[3] * fcs * e.as;
-      mb.af += rb[3] * fcs * e.a * e.btz * sb;
-      mb.btz += rb[3] * fcs * e.a * (sb * e.af);
-      mb.a += rb[3] * fcs * (sb * e.af * e.btz);
-      mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
-      mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-      mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
-      mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-      mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
-      mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-      mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
-      mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-      mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      mb.as += rb[7] * fcs * e.uu * 0.5;
-      mb.uu += rb[7] * fcs * (0.5 * e.as);
-      mb.as += rb[7] * fcs / G.g1 * e.cs2;
-      mb.cs2 += rb[7] * fcs / G.g1 * e.as;
-      mb.as += rb[7] * fcs * e.u * e.cs;
-      mb.cs += rb[7] * fcs * e.u * e.as;
-      mb.u += rb[7] * fcs * (e.as * e.cs);
-      mb.af += rb[7] * fcs * e.vb * e.a * sb;
-      mb.a += rb[7] * fcs * e.vb * (sb * e.af);
-      mb.vb += rb[7] * fcs * (sb * e.af * e.a);
-      mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
-      mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
-      mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
+      if (lb[0] != 0.0) {
+        mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
+        mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
+        mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
+        mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
+        mb.th2 += -(lb[0] * fcs) * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
+        mb.as += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * e.ca * sb;
+        mb.ca += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * (sb * e.as);
+        mb.u += -(lb[0] * fcs) * (0.5 * e.th2) * (sb * e.as * e.ca);
+        mb.af += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.cf;
+        mb.cf += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.af;
+        mb.vb += -(lb[0] * fcs) * (0.5 * e.th2) * (e.af * e.cf);
+      }
+      if (lb[1] != 0.0) {
+        mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
+        mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
+        mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+        mb.th2 += lb[1] * fcs * e.ca * e.as * (sb * 0.5);
+        mb.as += lb[1] * fcs * e.ca * (sb * 0.5 * e.th2);
+        mb.ca += lb[1] * fcs * (sb * 0.5 * e.th2 * e.as);
+      }
+      if (lb[2] != 0.0) {
+        mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
+        mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
+        mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+        mb.th2 += lb[2] * fcs * e.cf * e.bty * e.af * 0.5;
+        mb.af += lb[2] * fcs * e.cf * e.bty * (0.5 * e.th2);
+        mb.bty += lb[2] * fcs * e.cf * (0.5 * e.th2 * e.af);
+        mb.cf += lb[2] * fcs * (0.5 * e.th2 * e.af * e.bty);
+      }
+      if (lb[3] != 0.0) {
+        mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
+        mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
+        mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
+        mb.th2 += lb[3] * fcs * e.cf * e.btz * e.af * 0.5;
+        mb.af += lb[3] * fcs * e.cf * e.btz * (0.5 * e.th2);
+        mb.btz += lb[3] * fcs * e.cf * (0.5 * e.th2 * e.af);
+        mb.cf += lb[3] * fcs * (0.5 * e.th2 * e.af * e.btz);
+      }
+      if (lb[5] != 0.0) {
+        mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
+        mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
+        mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+        mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
+        mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
+        mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
+        mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[6] != 0.0) {
+        mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
+        mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
+        mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+        mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
+        mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
+        mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
+        mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[7] != 0.0) {
+        mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
+        mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
+        mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
+      }
+      if (rb[0] != 0.0) {
+        mb.as += rb[0] * fcs;
+      }
+      if (rb[1] != 0.0) {
+        mb.as += rb[1] * fcs * (e.u + e.cs);
+        mb.u += rb[1] * fcs * e.as;
+        mb.cs += rb[1] * fcs * e.as;
+      }
+      if (rb[2] != 0.0) {
+        mb.as += rb[2] * fcs * e.v;
+        mb.v += rb[2] * fcs * e.as;
+        mb.af += rb[2] * fcs * e.a * e.bty * sb;
+        mb.bty += rb[2] * fcs * e.a * (sb * e.af);
+        mb.a += rb[2] * fcs * (sb * e.af * e.bty);
+      }
+      if (rb[3] != 0.0) {
+        mb.as += rb[3] * fcs * e.w;
+        mb.w += rb[3] * fcs * e.as;
+        mb.af += rb[3] * fcs * e.a * e.btz * sb;
+        mb.btz += rb[3] * fcs * e.a * (sb * e.af);
+        mb.a += rb[3] * fcs * (sb * e.af * e.btz);
+      }
+      if (rb[5] != 0.0) {
+        mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
+        mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+        mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
+        mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+        mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      }
+      if (rb[6] != 0.0) {
+        mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
+        mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+        mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
+        mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+        mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      }
+      if (rb[7] != 0.0) {
+        mb.as += rb[7] * fcs * e.uu * 0.5;
+        mb.uu += rb[7] * fcs * (0.5 * e.as);
+        mb.as += rb[7] * fcs / G.g1 * e.cs2;
+        mb.cs2 += rb[7] * fcs / G.g1 * e.as;
+        mb.as += rb[7] * fcs * e.u * e.cs;
+        mb.cs += rb[7] * fcs * e.u * e.as;
+        mb.u += rb[7] * fcs * (e.as * e.cs);
+        mb.af += rb[7] * fcs * e.vb * e.a * sb;
+        mb.a += rb[7] * fcs * e.vb * (sb * e.af);
+        mb.vb += rb[7] * fcs * (sb * e.af * e.a);
+        mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
+        mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
+        mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
+      }
       break;
     }
     case 5: {
-      mb.btz += lb[0] * sb * 0.5 * e.v;
-      mb.v += lb[0] * sb * 0.5 * e.btz;
-      mb.bty += -(lb[0] * sb * 0.5) * e.w;
-      mb.w += -(lb[0] * sb * 0.5) * e.bty;
-      mb.btz += lb[2] * sb * -0.5;
-      mb.bty += lb[3] * sb * 0.5;
-      mb.btz += lb[5] * e.rr * 0.5;
-      mb.rr += lb[5] * (0.5 * e.btz);
-      mb.bty += lb[6] * e.rr * -0.5;
-      mb.rr += lb[6] * (-0.5 * e.bty);
-      mb.btz += -rb[2] * sb;
-      mb.bty += rb[3] * sb;
-      mb.btz += rb[5] / e.rr;
-      mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
-      mb.bty += -(rb[6] / e.rr);
-      mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
-      mb.btz += -rb[7] * sb * e.v;
-      mb.v += -rb[7] * sb * e.btz;
-      mb.bty += -(-rb[7] * sb) * e.w;
-      mb.w += -(-rb[7] * sb) * e.bty;
+      if (lb[0] != 0.0) {
+        mb.btz += lb[0] * sb * 0.5 * e.v;
+        mb.v += lb[0] * sb * 0.5 * e.btz;
+        mb.bty += -(lb[0] * sb * 0.5) * e.w;
+        mb.w += -(lb[0] * sb * 0.5) * e.bty;
+      }
+      if (lb[2] != 0.0) {
+        mb.btz += lb[2] * sb * -0.5;
+      }
+      if (lb[3] != 0.0) {
+        mb.bty += lb[3] * sb * 0.5;
+      }
+      if (lb[5] != 0.0) {
+        mb.btz += lb[5] * e.rr * 0.5;
+        mb.rr += lb[5] * (0.5 * e.btz);
+      }
+      if (lb[6] != 0.0) {
+        mb.bty += lb[6] * e.rr * -0.5;
+        mb.rr += lb[6] * (-0.5 * e.bty);
+      }
+      if (rb[2] != 0.0) {
+        mb.btz += -rb[2] * sb;
+      }
+      if (rb[3] != 0.0) {
+        mb.bty += rb[3] * sb;
+      }
+      if (rb[5] != 0.0) {
+        mb.btz += rb[5] / e.rr;
+        mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
+      }
+      if (rb[6] != 0.0) {
+        mb.bty += -(rb[6] / e.rr);
+        mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
+      }
+      if (rb[7] != 0.0) {
+        mb.btz += -rb[7] * sb * e.v;
+        mb.v += -rb[7] * sb * e.btz;
+        mb.bty += -(-rb[7] * sb) * e.w;
+        mb.w += -(-rb[7] * sb) * e.bty;
+      }
       break;
     }
     case 6: {
-      mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
-      mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
-      mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
-      mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
-      mb.th2 += -(lb[0] * fcf) * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
-      mb.af += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * e.a * sb;
-      mb.a += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * (sb * e.af);
-      mb.u += -(lb[0] * fcf) * (0.5 * e.th2) * (sb * e.af * e.a);
-      mb.as += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.cs;
-      mb.cs += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.as;
-      mb.vb += -(-(lb[0] * fcf) * (0.5 * e.th2)) * (e.as * e.cs);
-      mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
-      mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
-      mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
-      mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-      mb.th2 += lb[1] * fcf * e.a * e.af * (sb * 0.5);
-      mb.af += lb[1] * fcf * e.a * (sb * 0.5 * e.th2);
-      mb.a += lb[1] * fcf * (sb * 0.5 * e.th2 * e.af);
-      mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
-      mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
-      mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
-      mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-      mb.th2 += -(lb[2] * fcf) * e.cs * e.bty * e.as * 0.5;
-      mb.as += -(lb[2] * fcf) * e.cs * e.bty * (0.5 * e.th2);
-      mb.bty += -(lb[2] * fcf) * e.cs * (0.5 * e.th2 * e.as);
-      mb.cs += -(lb[2] * fcf) * (0.5 * e.th2 * e.as * e.bty);
-      mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
-      mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
-      mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
-      mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-      mb.th2 += -(lb[3] * fcf) * e.cs * e.btz * e.as * 0.5;
-      mb.as += -(lb[3] * fcf) * e.cs * e.btz * (0.5 * e.th2);
-      mb.btz += -(lb[3] * fcf) * e.cs * (0.5 * e.th2 * e.as);
-      mb.cs += -(lb[3] * fcf) * (0.5 * e.th2 * e.as * e.btz);
-      mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
-      mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
-      mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-      mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
-      mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
-      mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
-      mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
-      mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
-      mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-      mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
-      mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
-      mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
-      mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
-      mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
-      mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
-      mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
-      mb.af += rb[0] * fcf;
-      mb.af += rb[1] * fcf * (e.u + e.cf);
-      mb.u += rb[1] * fcf * e.af;
-      mb.cf += rb[1] * fcf * e.af;
-      mb.af += rb[2] * fcf * e.v;
-      mb.v += rb[2] * fcf * e.af;
-      mb.as += -(rb[2] * fcf) * e.ca * e.bty * sb;
-      mb.bty += -(rb[2] * fcf) * e.ca * (sb * e.as);
-      mb.ca += -(rb[2] * fcf) * (sb * e.as * e.bty);
-      mb.af += rb[3] * fcf * e.w;
-      mb.w += rb[3] * fcf * e.af;
-      mb.as += -(rb[3] * fcf) * e.ca * e.btz * sb;
-      mb.btz += -(rb[3] * fcf) * e.ca * (sb * e.as);
-      mb.ca += -(rb[3] * fcf) * (sb * e.as * e.btz);
-      mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
-      mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
-      mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
-      mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
-      mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
-      mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
-      mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
-      mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
-      mb.af += rb[7] * fcf * e.uu * 0.5;
-      mb.uu += rb[7] * fcf * (0.5 * e.af);
-      mb.af += rb[7] * fcf / G.g1 * e.cf2;
-      mb.cf2 += rb[7] * fcf / G.g1 * e.af;
-      mb.af += rb[7] * fcf * e.u * e.cf;
-      mb.cf += rb[7] * fcf * e.u * e.af;
-      mb.u += rb[7] * fcf * (e.af * e.cf);
-      mb.as += -(rb[7] * fcf) * e.vb * e.ca * sb;
-      mb.ca += -(rb[7] * fcf) * e.vb * (sb * e.as);
-      mb.vb += -(rb[7] * fcf) * (sb * e.as * e.ca);
-      mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
-      mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
-      mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
+      if (lb[0] != 0.0) {
+        mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
+        mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
+        mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
+        mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
+        mb.th2 += -(lb[0] * fcf) * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
+        mb.af += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * e.a * sb;
+        mb.a += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * (sb * e.af);
+        mb.u += -(lb[0] * fcf) * (0.5 * e.th2) * (sb * e.af * e.a);
+        mb.as += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.cs;
+        mb.cs += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.as;
+        mb.vb += -(-(lb[0] * fcf) * (0.5 * e.th2)) * (e.as * e.cs);
+      }
+      if (lb[1] != 0.0) {
+        mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
+        mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
+        mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
+        mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+        mb.th2 += lb[1] * fcf * e.a * e.af * (sb * 0.5);
+        mb.af += lb[1] * fcf * e.a * (sb * 0.5 * e.th2);
+        mb.a += lb[1] * fcf * (sb * 0.5 * e.th2 * e.af);
+      }
+      if (lb[2] != 0.0) {
+        mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
+        mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
+        mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
+        mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+        mb.th2 += -(lb[2] * fcf) * e.cs * e.bty * e.as * 0.5;
+        mb.as += -(lb[2] * fcf) * e.cs * e.bty * (0.5 * e.th2);
+        mb.bty += -(lb[2] * fcf) * e.cs * (0.5 * e.th2 * e.as);
+        mb.cs += -(lb[2] * fcf) * (0.5 * e.th2 * e.as * e.bty);
+      }
+      if (lb[3] != 0.0) {
+        mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
+        mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
+        mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
+        mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
+        mb.th2 += -(lb[3] * fcf) * e.cs * e.btz * e.as * 0.5;
+        mb.as += -(lb[3] * fcf) * e.cs * e.btz * (0.5 * e.th2);
+        mb.btz += -(lb[3] * fcf) * e.cs * (0.5 * e.th2 * e.as);
+        mb.cs += -(lb[3] * fcf) * (0.5 * e.th2 * e.as * e.btz);
+      }
+      if (lb[5] != 0.0) {
+        mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
+        mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
+        mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+        mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
+        mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
+        mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
+        mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[6] != 0.0) {
+        mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
+        mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
+        mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+        mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
+        mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
+        mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
+        mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
+      }
+      if (lb[7] != 0.0) {
+        mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
+        mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
+        mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
+      }
+      if (rb[0] != 0.0) {
+        mb.af += rb[0] * fcf;
+      }
+      if (rb[1] != 0.0) {
+        mb.af += rb[1] * fcf * (e.u + e.cf);
+        mb.u += rb[1] * fcf * e.af;
+        mb.cf += rb[1] * fcf * e.af;
+      }
+      if (rb[2] != 0.0) {
+        mb.af += rb[2] * fcf * e.v;
+        mb.v += rb[2] * fcf * e.af;
+        mb.as += -(rb[2] * fcf) * e.ca * e.bty * sb;
+        mb.bty += -(rb[2] * fcf) * e.ca * (sb * e.as);
+        mb.ca += -(rb[2] * fcf) * (sb * e.as * e.bty);
+      }
+      if (rb[3] != 0.0) {
+        mb.af += rb[3] * fcf * e.w;
+        mb.w += rb[3] * fcf * e.af;
+        mb.as += -(rb[3] * fcf) * e.ca * e.btz * sb;
+        mb.btz += -(rb[3] * fcf) * e.ca * (sb * e.as);
+        mb.ca += -(rb[3] * fcf) * (sb * e.as * e.btz);
+      }
+      if (rb[5] != 0.0) {
+        mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
+        mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
+        mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
+        mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
+      }
+      if (rb[6] != 0.0) {
+        mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
+        mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
+        mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
+        mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
+      }
+      if (rb[7] != 0.0) {
+        mb.af += rb[7] * fcf * e.uu * 0.5;
+        mb.uu += rb[7] * fcf * (0.5 * e.af);
+        mb.af += rb[7] * fcf / G.g1 * e.cf2;
+        mb.cf2 += rb[7] * fcf / G.g1 * e.af;
+        mb.af += rb[7] * fcf * e.u * e.cf;
+        mb.cf += rb[7] * fcf * e.u * e.af;
+        mb.u += rb[7] * fcf * (e.af * e.cf);
+        mb.as += -(rb[7] * fcf) * e.vb * e.ca * sb;
+        mb.ca += -(rb[7] * fcf) * e.vb * (sb * e.as);
+        mb.vb += -(rb[7] * fcf) * (sb * e.as * e.ca);
+        mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
+        mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
+        mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
+      }
       break;
     }
     default:
@@ -648,13 +822,13 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
   th1_b += mb.th1;
   th2_b += mb.th2;
   vb_b += mb.vb;
-  {
+  if (vb_b != 0.0) {
     bty_b += (vb_b) * (v);
     v_b += (vb_b) * (bty);
     btz_b += (vb_b) * (w);
     w_b += (vb_b) * (btz);
   }
-  {
+  if (th2_b != 0.0) {
     af2_b += (((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (a)) * (cf)) * (sb);
     cf_b += ((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (a)) * (sb * af2);
     a_b += (-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (sb * af2 * cf);
@@ -662,7 +836,7 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     cs_b += ((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (ca)) * (sb * as2);
     ca_b += (-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (sb * as2 * cs);
   }
-  {
+  if (th1_b != 0.0) {
     af2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cf2 - g21 * a2)) * (a2);
     a2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cf2 - g21 * a2)) * (af2);
     cf2_b += (-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (af2 * a2);
@@ -672,110 +846,110 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     cs2_b += (-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (as2 * cf2);
     a2_b += (-((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (as2 * cf2))) * (g21);
   }
-  if (!btz_fz) {
+  if (!btz_fz && btz_b != 0.0) {
     bz_b += (btz_b) / (sbp);
     sbp_b += -(btz_b) * (bz) / ((sbp) * (sbp));
   }
-  if (!bty_fz) {
+  if (!bty_fz && bty_b != 0.0) {
     by_b += (bty_b) / (sbp);
     sbp_b += -(bty_b) * (by) / ((sbp) * (sbp));
   }
-  if (!sbp_fz) {
+  if (!sbp_fz && sbp_b != 0.0) {
     bp2_b += (sbp_b) * inv2sqrt(bp2);
   }
-  {
+  if (as__b != 0.0) {
     as2_b += (as__b) * inv2sqrt(as2);
   }
-  {
+  if (af_b != 0.0) {
     af2_b += (af_b) * inv2sqrt(af2);
   }
-  if (!as2_fz) {
+  if (!as2_fz && as2_b != 0.0) {
     cf2_b += (as2_b) / (cf2 - cs2);
     a2_b += -((as2_b) / (cf2 - cs2));
     cf2_b += -(as2_b) * (cf2 - a2) / ((cf2 - cs2) * (cf2 - cs2));
     cs2_b += -(-(as2_b) * (cf2 - a2) / ((cf2 - cs2) * (cf2 - cs2)));
   }
-  if (!af2_fz) {
+  if (!af2_fz && af2_b != 0.0) {
     cf2_b += (af2_b) / (cf2 - cs2);
     ca2_b += -((af2_b) / (cf2 - cs2));
     cf2_b += -(af2_b) * (cf2 - ca2) / ((cf2 - cs2) * (cf2 - cs2));
     cs2_b += -(-(af2_b) * (cf2 - ca2) / ((cf2 - cs2) * (cf2 - cs2)));
   }
-  {
+  if (bp2_b != 0.0) {
     by_b += (bp2_b) * (by);
     by_b += (bp2_b) * (by);
     bz_b += (bp2_b) * (bz);
     bz_b += (bp2_b) * (bz);
   }
-  {
+  if (rr_b != 0.0) {
     r_b += (rr_b) * inv2sqrt(r);
   }
-  {
+  if (cf_b != 0.0) {
     cf2_b += (cf_b) * inv2sqrt(cf2);
   }
-  {
+  if (cs_b != 0.0) {
     cs2_b += (cs_b) * inv2sqrt(cs2);
   }
-  if (!cf2_fz) {
+  if (!cf2_fz && cf2_b != 0.0) {
     c2_b += cf2_b;
     sct_b += cf2_b;
   }
-  if (!cs2_fz) {
+  if (!cs2_fz && cs2_b != 0.0) {
     c2_b += cs2_b;
     sct_b += -(cs2_b);
   }
-  {
+  if (sct_b != 0.0) {
     ct_b += (sct_b) * inv2sqrt(ct);
   }
-  if (!ct_fz) {
+  if (!ct_fz && ct_b != 0.0) {
     c2_b += (ct_b) * (c2);
     c2_b += (ct_b) * (c2);
     a2_b += (-(ct_b)) * (ca2);
     ca2_b += (-(ct_b)) * (a2);
   }
-  {
+  if (c2_b != 0.0) {
     bb_b += ((c2_b) * (0.5)) / (r);
     r_b += -((c2_b) * (0.5)) * (bb) / ((r) * (r));
     a2_b += (c2_b) * (0.5);
   }
-  {
+  if (ca_b != 0.0) {
     ca2_b += (ca_b) * inv2sqrt(ca2);
   }
-  {
+  if (ca2_b != 0.0) {
     bx_b += ((ca2_b) / (r)) * (bx);
     bx_b += ((ca2_b) / (r)) * (bx);
     r_b += -(ca2_b) * (bx * bx) / ((r) * (r));
   }
-  {
+  if (a_b != 0.0) {
     a2_b += (a_b) * inv2sqrt(a2);
   }
-  if (!a2_fz) {
+  if (!a2_fz && a2_b != 0.0) {
     p_b += ((a2_b) / (r)) * (gm);
     r_b += -(a2_b) * (gm * p) / ((r) * (r));
   }
-  if (!p_fz) {
+  if (!p_fz && p_b != 0.0) {
     pt_b += p_b;
     bb_b += (-(p_b)) * (0.5);
   }
-  {
+  if (pt_b != 0.0) {
     ptl_b += (pt_b) * (0.5);
     ptr_b += (pt_b) * (0.5);
   }
-  {
+  if (ptr_b != 0.0) {
     b7_b += (ptr_b) * (gm1);
     mmr_b += ((-((ptr_b) * (gm1))) / (b0)) * (0.5);
     b0_b += -(-((ptr_b) * (gm1))) * (0.5 * mmr) / ((b0) * (b0));
     bbr_b += (-((ptr_b) * (gm1))) * (0.5);
     bbr_b += (ptr_b) * (0.5);
   }
-  {
+  if (ptl_b != 0.0) {
     a7_b += (ptl_b) * (gm1);
     mml_b += ((-((ptl_b) * (gm1))) / (a0)) * (0.5);
     a0_b += -(-((ptl_b) * (gm1))) * (0.5 * mml) / ((a0) * (a0));
     bbl_b += (-((ptl_b) * (gm1))) * (0.5);
     bbl_b += (ptl_b) * (0.5);
   }
-  {
+  if (bbr_b != 0.0) {
     b4_b += (bbr_b) * (b4);
     b4_b += (bbr_b) * (b4);
     b5_b += (bbr_b) * (b5);
@@ -783,7 +957,7 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     b6_b += (bbr_b) * (b6);
     b6_b += (bbr_b) * (b6);
   }
-  {
+  if (mmr_b != 0.0) {
     b1_b += (mmr_b) * (b1);
     b1_b += (mmr_b) * (b1);
     b2_b += (mmr_b) * (b2);
@@ -791,7 +965,7 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     b3_b += (mmr_b) * (b3);
     b3_b += (mmr_b) * (b3);
   }
-  {
+  if (bbl_b != 0.0) {
     a4_b += (bbl_b) * (a4);
     a4_b += (bbl_b) * (a4);
     a5_b += (bbl_b) * (a5);
@@ -799,7 +973,7 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     a6_b += (bbl_b) * (a6);
     a6_b += (bbl_b) * (a6);
   }
-  {
+  if (mml_b != 0.0) {
     a1_b += (mml_b) * (a1);
     a1_b += (mml_b) * (a1);
     a2__b += (mml_b) * (a2_);
@@ -807,7 +981,7 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     a3_b += (mml_b) * (a3);
     a3_b += (mml_b) * (a3);
   }
-  {
+  if (bb_b != 0.0) {
     bx_b += (bb_b) * (bx);
     bx_b += (bb_b) * (bx);
     by_b += (bb_b) * (by);
@@ -815,7 +989,7 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     bz_b += (bb_b) * (bz);
     bz_b += (bb_b) * (bz);
   }
-  {
+  if (uu_b != 0.0) {
     u_b += (uu_b) * (u);
     u_b += (uu_b) * (u);
     v_b += (uu_b) * (v);
@@ -823,37 +997,37 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     w_b += (uu_b) * (w);
     w_b += (uu_b) * (w);
   }
-  {
+  if (bz_b != 0.0) {
     a6_b += (bz_b) * (0.5);
     b6_b += (bz_b) * (0.5);
   }
-  {
+  if (by_b != 0.0) {
     a5_b += (by_b) * (0.5);
     b5_b += (by_b) * (0.5);
   }
-  {
+  if (bx_b != 0.0) {
     a4_b += (bx_b) * (0.5);
     b4_b += (bx_b) * (0.5);
   }
-  {
+  if (w_b != 0.0) {
     a3_b += ((w_b) * (0.5)) / (a0);
     a0_b += -((w_b) * (0.5)) * (a3) / ((a0) * (a0));
     b3_b += ((w_b) * (0.5)) / (b0);
     b0_b += -((w_b) * (0.5)) * (b3) / ((b0) * (b0));
   }
-  {
+  if (v_b != 0.0) {
     a2__b += ((v_b) * (0.5)) / (a0);
     a0_b += -((v_b) * (0.5)) * (a2_) / ((a0) * (a0));
     b2_b += ((v_b) * (0.5)) / (b0);
     b0_b += -((v_b) * (0.5)) * (b2) / ((b0) * (b0));
   }
-  {
+  if (u_b != 0.0) {
     a1_b += ((u_b) * (0.5)) / (a0);
     a0_b += -((u_b) * (0.5)) * (a1) / ((a0) * (a0));
     b1_b += ((u_b) * (0.5)) / (b0);
     b0_b += -((u_b) * (0.5)) * (b1) / ((b0) * (b0));
   }
-  {
+  if (r_b != 0.0) {
     a0_b += (r_b) * (0.5);
     b0_b += (r_b) * (0.5);
   }
@@ -918,58 +1092,58 @@ __device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const
   fo5_b = Fb[5];
   fo6_b = Fb[6];
   fo7_b = Fb[7];
-  {
+  if (fo7_b != 0.0) {
     q7_b += (fo7_b) * (fu);
     fpt_b += (fo7_b) * (fu);
     fu_b += (fo7_b) * (q7 + fpt);
     q4_b += (-(fo7_b)) * (fub);
     fub_b += (-(fo7_b)) * (q4);
   }
-  {
+  if (fo6_b != 0.0) {
     q6_b += (fo6_b) * (fu);
     fu_b += (fo6_b) * (q6);
     q4_b += (-(fo6_b)) * (fw);
     fw_b += (-(fo6_b)) * (q4);
   }
-  {
+  if (fo5_b != 0.0) {
     q5_b += (fo5_b) * (fu);
     fu_b += (fo5_b) * (q5);
     q4_b += (-(fo5_b)) * (fv);
     fv_b += (-(fo5_b)) * (q4);
   }
-  {
+  if (fo3_b != 0.0) {
     q3_b += (fo3_b) * (fu);
     fu_b += (fo3_b) * (q3);
     q4_b += (-(fo3_b)) * (q6);
     q6_b += (-(fo3_b)) * (q4);
   }
-  {
+  if (fo2_b != 0.0) {
     q2_b += (fo2_b) * (fu);
     fu_b += (fo2_b) * (q2);
     q4_b += (-(fo2_b)) * (q5);
     q5_b += (-(fo2_b)) * (q4);
   }
-  {
+  if (fo1_b != 0.0) {
     q1_b += (fo1_b) * (fu);
     fu_b += (fo1_b) * (q1);
     q4_b += (-(fo1_b)) * (q4);
     q4_b += (-(fo1_b)) * (q4);
     fpt_b += fo1_b;
   }
-  {
+  if (fo0_b != 0.0) {
     q1_b += fo0_b;
   }
-  {
+  if (fpt_b != 0.0) {
     fp_b += fpt_b;
     fbb_b += (fpt_b) * (0.5);
   }
-  {
+  if (fp_b != 0.0) {
     q7_b += (fp_b) * (gm1);
     q0_b += ((-((fp_b) * (gm1))) * (fuu)) * (0.5);
     fuu_b += (-((fp_b) * (gm1))) * (0.5 * q0);
     fbb_b += (-((fp_b) * (gm1))) * (0.5);
   }
-  {
+  if (fbb_b != 0.0) {
     q4_b += (fbb_b) * (q4);
     q4_b += (fbb_b) * (q4);
     q5_b += (fbb_b) * (q5);
@@ -977,7 +1151,7 @@ __device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const
     q6_b += (fbb_b) * (q6);
     q6_b += (fbb_b) * (q6);
   }
-  {
+  if (fub_b != 0.0) {
     fu_b += (fub_b) * (q4);
     q4_b += (fub_b) * (fu);
     fv_b += (fub_b) * (q5);
@@ -985,7 +1159,7 @@ __device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const
     fw_b += (fub_b) * (q6);
     q6_b += (fub_b) * (fw);
   }
-  {
+  if (fuu_b != 0.0) {
     fu_b += (fuu_b) * (fu);
     fu_b += (fuu_b) * (fu);
     fv_b += (fuu_b) * (fv);
@@ -993,15 +1167,15 @@ __device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const
     fw_b += (fuu_b) * (fw);
     fw_b += (fuu_b) * (fw);
   }
-  {
+  if (fw_b != 0.0) {
     q3_b += (fw_b) / (q0);
     q0_b += -(fw_b) * (q3) / ((q0) * (q0));
   }
-  {
+  if (fv_b != 0.0) {
     q2_b += (fv_b) / (q0);
     q0_b += -(fv_b) * (q2) / ((q0) * (q0));
   }
-  {
+  if (fu_b != 0.0) {
     q1_b += (fu_b) / (q0);
     q0_b += -(fu_b) * (q1) / ((q0) * (q0));
   }

@@ -92,21 +92,40 @@ def test_sheet_amplitude_gradient_matches_tangent_linear():
     assert np.all(np.abs(dJda - r["dJ"]) <= 1e-9 * scale), (dJda, r["dJ"])
 
 
-def test_frozen_stencil_central_differences():
+@pytest.mark.parametrize("bc", [(M.PERIODIC,) * 4, (M.OPEN, M.OPEN, M.NEUMANN, M.NEUMANN)])
+def test_frozen_stencil_central_differences(bc):
     """(J(U0 + h d) - J(U0 - h d)) / 2h of the frozen replay, h = 1e-7, against
-    the adjoint's dJ/dU0 . d, within 1e-6 relative."""
+    the adjoint's dJ/dU0 . d, within 1e-6 relative, on a smooth state."""
+    p = P.random_smooth(48, 40, seed=9, bc=bc)
+    a, J = _adjoint(p, 20, K=6)
+    a.backward()
+    g = a.gradient()
+    h = 1e-7
+    for d in _interior_dirs(p.U.shape, 3, seed=11):
+        fd = (a.replay(p.U + h * d) - a.replay(p.U - h * d)) / (2 * h)
+        adj = _dot(g, d)
+        assert abs(fd - adj) <= 1e-6 * abs(adj), (fd, adj)
+
+
+def test_plasma_sheet_amplitude_differences():
+    """The current sheet starts with B_x = 0, where the slow speed
+    c_s = sqrt(c^2 - sqrt(c^4 - a^2 c_a^2)) ~ |B_x| a / sqrt(2 rho c^2) has a
+    kink (and its computed value a rounding-level cancellation): the discrete
+    map is not differentiable there, so central differences in the
+    amplitudes a_k agree with the frozen-branch derivative only to ~1e-3 at
+    h = 1e-5 and not better at smaller h.  The tangent-linear comparison
+    above checks the same derivative to 1e-9."""
     amps = np.random.default_rng(9).normal(0, 1e-3, 16)
     p = P.plasma_sheet(64, 32, amps)
     a, J = _adjoint(p, 30, K=8)
     a.backward()
     g = a.gradient()
     T = P.plasma_sheet_tangents(p)
-    dirs = [T[0], T[3], T[15]] + list(_interior_dirs(p.U.shape, 2, seed=11) * 1e-3)
-    h = 1e-7
-    for d in dirs:
-        fd = (a.replay(p.U + h * d) - a.replay(p.U - h * d)) / (2 * h)
-        adj = _dot(g, d)
-        assert abs(fd - adj) <= 1e-6 * abs(adj), (fd, adj)
+    h = 1e-5
+    for k in (0, 3):
+        fd = (a.replay(p.U + h * T[k]) - a.replay(p.U - h * T[k])) / (2 * h)
+        adj = _dot(g, T[k])
+        assert abs(fd - adj) <= 5e-3 * abs(adj), (k, fd, adj)
 
 
 def test_checkpoint_interval_does_not_change_the_gradient():
@@ -180,13 +199,13 @@ def test_autograd_function_wrapper():
     import torch
 
     from adjoint_autograd import kinetic_energy_after_steps
-    p = P.plasma_sheet(32, 16, np.random.default_rng(4).normal(0, 1e-2, 4))
+    p = P.random_smooth(32, 24, seed=4)
     a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-9, dt_max=0.01,
                 checkpoint_every=3)
     U0 = torch.tensor(p.U, dtype=torch.float64, requires_grad=True)
     J = kinetic_energy_after_steps(U0, a, 9, 1e-3)
     J.backward()
-    d = _interior_dirs(p.U.shape, 1, seed=21)[0] * 1e-3
+    d = _interior_dirs(p.U.shape, 1, seed=21)[0]
     h = 1e-7
     fd = (a.replay(p.U + h * d) - a.replay(p.U - h * d)) / (2 * h)
     adj = float((U0.grad.numpy() * d).sum())
