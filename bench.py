@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--batch-runs", type=int, default=512,
                     help="runs of the batched-vs-sequential measurement (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--adjoint-steps", type=int, default=2000,
+                    help="steps of the plasma-sheet adjoint measurement (0: skip it)")
     return ap.parse_args()
 
 
@@ -277,6 +279,82 @@ def batched_measure(dev, n_runs, steps, seed=0):
                         "log-uniform 64..1024, eno-roe/eno-lf, rk3, generated on the device"}
 
 
+def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1):
+    """Cost of the discrete adjoint on the plasma sheet (1024 x 512 on
+    [-2, 2] x [-1, 1], Neumann in x, periodic in y, By = tanh(x/0.1), 16
+    velocity amplitudes a_k ~ N(0, 1e-3), ENO-Roe RK3, `steps` steps,
+    checkpoints every K steps): a plain forward run (mhd_steps), the
+    recording forward, the backward sweep (segment replays included), and
+    central differences of J in two amplitudes through the frozen replay."""
+    import numpy as np
+    import torch
+
+    import mhd2d_b200 as M
+    from mhd2d_b200 import problems as P
+    from mhd2d_b200.adjoint import Adjoint
+
+    amps = np.random.default_rng(seed).normal(0, 1e-3, 16)
+    p = P.plasma_sheet(nx, ny, amps)
+    kw = dict(dt_min=1e-9, dt_max=2.0 ** -6, cfl=0.4)
+    dt0 = 2.0 ** -12
+    ctx = M.Context(nx, ny, p.dx, p.dy, p.gamma, p.bc, scheme=M.ENO_ROE, time_method=M.RK3,
+                    flags=0, device=dev, **kw)
+    ctx.upload(p.U)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.steps(2, dt0)  # warm-up
+    ctx.upload(p.U)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    st, _, _ = ctx.steps(steps, dt0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1)
+    ctx.close()
+    a = Adjoint(nx, ny, p.dx, p.dy, p.gamma, p.bc, checkpoint_every=K, device=dev, **kw)
+    a.init_plasma_sheet(amps)
+    J = a.forward(steps, dt0)
+    a.backward()
+    dJda = a.sheet_gradient()
+    info = a.info()
+    # gradient check on a shorter window of the same run: over the full
+    # window the frozen-stencil linearisation of the sheet grows without
+    # bound (perturbed frozen replays diverge), so it is checked where the
+    # linearisation holds
+    fd_steps = min(steps, 200)
+    J_short = a.forward(fd_steps, dt0)
+    a.backward()
+    g_short = a.sheet_gradient()
+    fd = {}
+    for h in (1e-5, 1e-7):
+        for k in (0, 1):
+            ap, am = amps.copy(), amps.copy()
+            ap[k] += h
+            am[k] -= h
+            d = (a.replay_plasma_sheet(ap) - a.replay_plasma_sheet(am)) / (2 * h)
+            fd[f"a{k + 1}_h{h:g}"] = {"fd": d, "adjoint": float(g_short[k]),
+                                     "rel_err": abs(d - g_short[k]) / abs(g_short[k])}
+    a.close()
+    cell_updates = float(nx) * ny * info["steps"]
+    return {"workload": f"plasma sheet {nx}x{ny}, eno-roe, rk3, {info['steps']} steps, "
+                        f"checkpoints every {K} steps, J = kinetic energy",
+            "J": J, "dJda": [float(x) for x in dJda],
+            "ms_forward_plain": ms_plain, "ms_forward_recording": info["ms_forward"],
+            "ms_backward": info["ms_backward"],
+            "adjoint_over_forward": info["ms_backward"] / ms_plain,
+            "forward_plus_adjoint_over_forward": (info["ms_forward"] + info["ms_backward"]) / ms_plain,
+            "forward_cell_updates_per_s": cell_updates / (ms_plain * 1e-3),
+            "stages": info["stages"], "checkpoints": info["checkpoints"],
+            "central_differences": {"steps": fd_steps, "J": J_short, "checks": fd},
+            "note": "backward = segment replays from checkpoints + reverse sweep.  The "
+                    "frozen-stencil linearisation of the sheet is unstable over the full "
+                    "window (dJ/da grows to ~1e6 and perturbed frozen replays diverge by "
+                    "t ~ 1), so central differences check the gradient on the first "
+                    f"{fd_steps} steps; the tangent-linear oracle checks the same "
+                    "derivative to 1e-9 at small sizes (tests/test_gpu_adjoint.py)"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -400,6 +478,10 @@ def run_ours(args):
         bm = batched_measure(dev, args.batch_runs, args.batch_steps)
         if rank == 0:
             line["batched"] = bm
+    if args.adjoint_steps > 0:
+        am = adjoint_measure(dev, args.adjoint_steps)
+        if rank == 0:
+            line["adjoint"] = am
     if rank == 0:
         if world == 1:
             line["cpu_baseline"] = cpu_baseline_sample(scheme)
