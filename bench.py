@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--adjoint-steps", type=int, default=2000,
                     help="steps of the plasma-sheet adjoint measurement (0: skip it)")
+    ap.add_argument("--adjoint-grid", default="1024x512")
     return ap.parse_args()
 
 
@@ -479,7 +480,8 @@ def run_ours(args):
         if rank == 0:
             line["batched"] = bm
     if args.adjoint_steps > 0:
-        am = adjoint_measure(dev, args.adjoint_steps)
+        anx, any_ = (int(v) for v in args.adjoint_grid.split("x"))
+        am = adjoint_measure(dev, args.adjoint_steps, nx=anx, ny=any_)
         if rank == 0:
             line["adjoint"] = am
     if rank == 0:
