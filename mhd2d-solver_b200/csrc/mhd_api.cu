@@ -46,6 +46,7 @@ struct mhd_ctx {
   double *aF = nullptr, *aG = nullptr;
   double *snap[4] = {nullptr, nullptr, nullptr, nullptr};  // left, right, bottom, top
   double *phi = nullptr, *partial = nullptr, *ratio = nullptr;
+  double* sor_xy = nullptr;  // source terms of the current SOR solve (allocated on first use)
   int npartial = 0;
   Ctl* ctl = nullptr;
   Ctl* hctl = nullptr;  // pinned mirror
@@ -231,6 +232,12 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
   const double coef[6] = {pxf, pyf, 4.0 / (2.0 * g.dx), 4.0 / (2.0 * g.dy),
                           1.0 / (2 * (pxf + pyf)), omega};
   double nan_ratio = std::numeric_limits<double>::quiet_NaN();  // no sweep: 0/0, "converged"
+  if (!c->sor_xy) {  // 2 colours x rows x pairs x 4 doubles covers every range of this grid
+    const size_t n = 2ull * g.nx * ((g.ny + 2 + 3) / 4 + 1) * 4;
+    CK(cudaMalloc(&c->sor_xy, n * sizeof(double)));
+  }
+  c->ks->sor_rhs(g, c->U, r, coef, c->sor_xy, c->stream);
+  c->launches += 1;
   CK(cudaMemsetAsync(&c->ctl->rmax, 0, 2 * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(&c->ctl->sor_done, 0, 2 * sizeof(int), c->stream));
   CK(cudaMemcpyAsync(c->ratio, &nan_ratio, sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -239,8 +246,8 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
   if (p->sor_rsteps > 0) {
     for (;;) {
       for (int s = 0; s < chunk; s++) {
-        c->ks->sor_sweep(g, c->phi, c->U, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio, c->ctl,
-                         c->stream);
+        c->ks->sor_sweep(g, c->phi, c->sor_xy, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio,
+                         c->ctl, c->stream);
         c->launches += 5;
       }
       issued += chunk;
@@ -337,7 +344,7 @@ int mhd_ctx_destroy(mhd_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   double* bufs[] = {c->U, c->U1, c->U2, c->UL, c->ch[0], c->ch[1], c->ch[2], c->ch[3], c->aF,
                     c->aG, c->snap[0], c->snap[1], c->snap[2], c->snap[3], c->phi, c->partial,
-                    c->ratio};
+                    c->ratio, c->sor_xy};
   for (double* b : bufs)
     if (b) cudaFree(b);
   if (c->ctl) cudaFree(c->ctl);

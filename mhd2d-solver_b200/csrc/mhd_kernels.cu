@@ -108,19 +108,28 @@ void l_divb(const Grid& g, double* U, const int range[4], double* partial, int n
   k_divb_finish<<<1, 32, 0, s>>>(partial, nb, g.dx * g.dy, ctl);
 }
 
-void l_sor_sweep(const Grid& g, double* phi, const double* U, const int range[4],
+void l_sor_rhs(const Grid& g, const double* U, const int range[4], const double coef[6],
+               double* xy, cudaStream_t s) {
+  DivRange R{range[0], range[1], range[2], range[3]};
+  SorCoef c{coef[0], coef[1], coef[2], coef[3], coef[4], coef[5]};
+  const long long n = 2LL * (R.x1 - R.x0) * sor_pairs(R);
+  k_sor_rhs<<<grid1d(n, 256), 256, 0, s>>>(g, U, R, c, reinterpret_cast<double4*>(xy));
+}
+
+void l_sor_sweep(const Grid& g, double* phi, const double* xy, const int range[4],
                  const double coef[6], double rtol, double max_sweeps, double* last_ratio,
                  Ctl* ctl, cudaStream_t s) {
   DivRange R{range[0], range[1], range[2], range[3]};
   SorCoef c{coef[0], coef[1], coef[2], coef[3], coef[4], coef[5]};
-  const int q = (R.y1 + 3) / 4 + 1;
-  dim3 grid((q + 127) / 128, R.x1 - R.x0);
+  dim3 grid((sor_pairs(R) + SOR_THREADS - 1) / SOR_THREADS,
+            (R.x1 - R.x0 + SOR_ROWS - 1) / SOR_ROWS);
   const int m = g.nx > g.ny ? g.nx : g.ny;
+  const double4* f = reinterpret_cast<const double4*>(xy);
   // ghosts are refreshed after each colour: with periodic sides they mirror
   // points of the other colour (see k_sor_half)
-  k_sor_half<<<grid, 128, 0, s>>>(g, phi, U, R, c, 0, ctl);
+  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl);
   k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl);
-  k_sor_half<<<grid, 128, 0, s>>>(g, phi, U, R, c, 1, ctl);
+  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl);
   k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl);
   k_sor_check<<<1, 32, 0, s>>>(ctl, rtol, max_sweeps, last_ratio);
 }
@@ -139,7 +148,7 @@ int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
 
 using namespace MHD_KNS;
 extern const KernelSet MHD_KSET = {MHD_KSET_NAME, l_bc, l_snapshot, l_lf_alpha, l_flux,
-                                   l_combine, l_control, l_divb, l_sor_sweep, l_sor_correct,
-                                   l_smem, l_launches};
+                                   l_combine, l_control, l_divb, l_sor_rhs, l_sor_sweep,
+                                   l_sor_correct, l_smem, l_launches};
 
 }  // namespace mhd

@@ -35,8 +35,12 @@ struct KernelSet {
   // div B: wrap periodic B ghosts, reduce max / sum over [x0,x1) x [y0,y1)
   void (*divb)(const Grid& g, double* U, const int range[4], double* partial, int npartial,
                Ctl* ctl, cudaStream_t s);
+  // the fixed source terms of one SOR solve (xy: 4 doubles per same-colour
+  // column pair, sor_xy_doubles of them)
+  void (*sor_rhs)(const Grid& g, const double* U, const int range[4], const double coef[6],
+                  double* xy, cudaStream_t s);
   // one SOR sweep (both colours, potential ghosts, convergence check)
-  void (*sor_sweep)(const Grid& g, double* phi, const double* U, const int range[4],
+  void (*sor_sweep)(const Grid& g, double* phi, const double* xy, const int range[4],
                     const double coef[6], double rtol, double max_sweeps, double* last_ratio,
                     Ctl* ctl, cudaStream_t s);
   void (*sor_correct)(const Grid& g, double* U, const double* phi, const int range[4],

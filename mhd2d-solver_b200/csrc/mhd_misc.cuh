@@ -345,36 +345,106 @@ struct SorCoef {
   double pxf, pyf, bxf, byf, coef, omega;
 };
 
-__global__ void __launch_bounds__(256) k_sor_half(Grid g, double* __restrict__ phi,
-                                                  const double* __restrict__ U, DivRange R,
-                                                  SorCoef s, int color, Ctl* c) {
+// Rows per block of k_sor_half: each block reduces its update / potential
+// maxima over SOR_ROWS rows before its two atomics.
+constexpr int SOR_ROWS = 8;
+constexpr int SOR_THREADS = 128;
+
+// Same-colour column pairs per row: thread q of a row owns columns
+// jb = 2*(2q + b), jb + 1 with b = (colour + (i>>1)) & 1.
+__host__ __device__ __forceinline__ int sor_pairs(const DivRange& R) { return (R.y1 + 3) / 4 + 1; }
+
+// The divergence source terms of the SOR update are fixed during a solve:
+// X = bxf*(Bx[i+1][j] - Bx[i-1][j]), Y = byf*(By[i][j+1] - By[i][j-1]), the
+// same products the per-point update forms (so it stays bit-identical).  They
+// are stored once per solve, per colour and pair, as {X(jb), X(jb+1), Y(jb),
+// Y(jb+1)}: a warp's half sweep reads them as contiguous 32-byte items.
+__global__ void k_sor_rhs(Grid g, const double* __restrict__ U, DivRange R, SorCoef s,
+                          double4* __restrict__ xy) {
+  const int Q = sor_pairs(R), H = R.x1 - R.x0;
+  const long long n = 2LL * H * Q;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int q = int(e % Q);
+    const int ir = int((e / Q) % H);
+    const int color = int(e / ((long long)Q * H));
+    const int i = R.x0 + ir;
+    const int jb = 2 * (2 * q + ((color + (i >> 1)) & 1));
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int t = 0; t < 2; t++) {
+      const int j = jb + t;
+      if (j >= R.y0 && j < R.y1) {
+        v[t] = s.bxf * (U[g.at(4, i + 1, j)] - U[g.at(4, i - 1, j)]);
+        v[2 + t] = s.byf * (U[g.at(5, i, j + 1)] - U[g.at(5, i, j - 1)]);
+      }
+    }
+    xy[e] = make_double4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// One colour of a red-black sweep.  The potential pairs are read and written
+// as 16-byte items (jb is even, the padded row offset is even).
+__global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __restrict__ phi,
+                                                          const double4* __restrict__ xy,
+                                                          DivRange R, SorCoef s, int color,
+                                                          Ctl* c) {
   if (c->sor_done) return;
-  const int i = R.x0 + blockIdx.y;
+  __shared__ double red[2][SOR_THREADS / 32];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  // even column blocks jb = 2*(2q + b) with b chosen so the block has this colour
-  const int b = (color + (i >> 1)) & 1;
-  const int jb = 2 * (2 * q + b);
-  double rmax = 0.0, pmax = 0.0;
+  const int Q = sor_pairs(R), H = R.x1 - R.x0;
   const long long P = g.pitch;
-  double* prow = phi + (long long)i * P + g.off;
+  double rmax = 0.0, pmax = 0.0;
+  if (q < Q) {
+    for (int rr = 0; rr < SOR_ROWS; rr++) {
+      const int ir = blockIdx.y * SOR_ROWS + rr;
+      const int i = R.x0 + ir;
+      if (i >= R.x1) break;
+      const int jb = 2 * (2 * q + ((color + (i >> 1)) & 1));
+      if (jb + 1 < R.y0 || jb >= R.y1) continue;
+      double* prow = phi + (long long)i * P + g.off;
+      const double4 f = xy[((long long)color * H + ir) * Q + q];
+      const double2 up = *reinterpret_cast<const double2*>(prow + jb + 2 * P);
+      const double2 dn = *reinterpret_cast<const double2*>(prow + jb - 2 * P);
+      const double2 lf = *reinterpret_cast<const double2*>(prow + jb - 2);
+      const double2 rt = *reinterpret_cast<const double2*>(prow + jb + 2);
+      double2 me = *reinterpret_cast<const double2*>(prow + jb);
+      const double ax[2] = {up.x, up.y}, bx[2] = {dn.x, dn.y};
+      const double ay[2] = {rt.x, rt.y}, by[2] = {lf.x, lf.y};
+      const double X[2] = {f.x, f.y}, Y[2] = {f.z, f.w};
+      double out[2] = {me.x, me.y};
 #pragma unroll
-  for (int t = 0; t < 2; t++) {
-    const int j = jb + t;
-    if (i < R.x1 && j >= R.y0 && j < R.y1) {
-      double r = s.pxf * (prow[j + 2 * P] + prow[j - 2 * P]);
-      r += s.pyf * (prow[j + 2] + prow[j - 2]);
-      r += s.bxf * (U[g.at(4, i + 1, j)] - U[g.at(4, i - 1, j)]);
-      r += s.byf * (U[g.at(5, i, j + 1)] - U[g.at(5, i, j - 1)]);
-      r *= s.coef;
-      r -= prow[j];
-      prow[j] += s.omega * r;
-      rmax = take_max(rmax, fabs(r));
-      pmax = take_max(pmax, fabs(prow[j]));
+      for (int t = 0; t < 2; t++) {
+        const int j = jb + t;
+        if (j >= R.y0 && j < R.y1) {
+          double r = s.pxf * (ax[t] + bx[t]);
+          r += s.pyf * (ay[t] + by[t]);
+          r += X[t];
+          r += Y[t];
+          r *= s.coef;
+          r -= out[t];
+          out[t] += s.omega * r;
+          rmax = take_max(rmax, fabs(r));
+          pmax = take_max(pmax, fabs(out[t]));
+        }
+      }
+      me.x = out[0];
+      me.y = out[1];
+      *reinterpret_cast<double2*>(prow + jb) = me;
     }
   }
   rmax = warp_max(rmax);
   pmax = warp_max(pmax);
-  if ((threadIdx.x & 31) == 0) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][w] = rmax;
+    red[1][w] = pmax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q2 = 1; q2 < SOR_THREADS / 32; q2++) {
+      rmax = take_max(rmax, red[0][q2]);
+      pmax = take_max(pmax, red[1][q2]);
+    }
     atomic_max_pos(&c->rmax, rmax);
     atomic_max_pos(&c->pmax, pmax);
   }
