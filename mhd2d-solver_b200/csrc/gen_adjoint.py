@@ -209,6 +209,69 @@ R4.update({1: "fcs * (as_ * (u + cs))", 2: "fcs * (as_ * v + sb * af * bty * a)"
 R3 = {0: "1.0", 1: "u", 2: "v", 3: "w", 7: "0.5 * uu"}
 RROWS = [R0, R1, R2, R3, R4, R5, R6]
 
+# The same rows split by pair: rows k and 6 - k (k = 0, 1, 2) are A + B and
+# A - B (left) and C + D and C - D (right).  Row 3 is its own "pair" (A, C).
+# The adjoint of both rows of a pair is then one pass over A, B, C, D with
+# the seeds lb_k + lb_{6-k} (A), lb_k - lb_{6-k} (B), and likewise for C, D.
+PAIRS = [
+    (0, 6,
+     {0: "fcf * (0.25 * th1 * af * a2 * uu)", 1: "fcf * (-0.5 * th1 * af * a2 * u)",
+      2: "fcf * (-0.5 * th1 * af * a2 * v)", 3: "fcf * (-0.5 * th1 * af * a2 * w)",
+      5: "fcf * (0.5 * th1 * as_ * bty * cf * rr * (cs2 - g21 * a2))",
+      6: "fcf * (0.5 * th1 * as_ * btz * cf * rr * (cs2 - g21 * a2))",
+      7: "fcf * (0.5 * th1 * af * a2)"},
+     {0: "fcf * (0.5 * th2 * (sb * af * a * u - as_ * cs * vb))",
+      1: "fcf * (-(sb * 0.5 * th2 * af * a))", 2: "fcf * (0.5 * th2 * as_ * bty * cs)",
+      3: "fcf * (0.5 * th2 * as_ * btz * cs)"},
+     {0: "fcf * af", 1: "fcf * (af * u)", 2: "fcf * (af * v)", 3: "fcf * (af * w)",
+      5: "fcf * (as_ * bty * cf / rr)", 6: "fcf * (as_ * btz * cf / rr)",
+      7: "fcf * (0.5 * af * uu + af * cf2 / g1 + g21 * af * (cf2 - a2))"},
+     {1: "fcf * (-(af * cf))", 2: "fcf * (sb * as_ * bty * ca)",
+      3: "fcf * (sb * as_ * btz * ca)", 7: "fcf * (-(af * cf * u) + sb * as_ * ca * vb)"}),
+    (2, 4,
+     {0: "fcs * (0.25 * th1 * as_ * cf2 * uu)", 1: "fcs * (-0.5 * th1 * as_ * cf2 * u)",
+      2: "fcs * (-0.5 * th1 * as_ * cf2 * v)", 3: "fcs * (-0.5 * th1 * as_ * cf2 * w)",
+      5: "fcs * (-0.5 * th1 * af * bty * cf * rr * (cf2 - g21 * a2))",
+      6: "fcs * (-0.5 * th1 * af * btz * cf * rr * (cf2 - g21 * a2))",
+      7: "fcs * (0.5 * th1 * as_ * cf2)"},
+     {0: "fcs * (0.5 * th2 * (sb * as_ * ca * u + af * cf * vb))",
+      1: "fcs * (-(sb * 0.5 * th2 * as_ * ca))", 2: "fcs * (-0.5 * th2 * af * bty * cf)",
+      3: "fcs * (-0.5 * th2 * af * btz * cf)"},
+     {0: "fcs * as_", 1: "fcs * (as_ * u)", 2: "fcs * (as_ * v)", 3: "fcs * (as_ * w)",
+      5: "fcs * (-af * bty * a2 / (cf * rr))", 6: "fcs * (-af * btz * a2 / (cf * rr))",
+      7: "fcs * (0.5 * as_ * uu + as_ * cs2 / g1 + g21 * as_ * (cs2 - a2))"},
+     {1: "fcs * (-(as_ * cs))", 2: "fcs * (-(sb * af * bty * a))",
+      3: "fcs * (-(sb * af * btz * a))", 7: "fcs * (-(as_ * cs * u) - sb * af * a * vb)"}),
+    (1, 5,
+     {5: "0.5 * btz * rr", 6: "-0.5 * bty * rr"},
+     {0: "sb * (-0.5 * (btz * v - bty * w))", 2: "sb * (0.5 * btz)", 3: "sb * (-0.5 * bty)"},
+     {5: "btz / rr", 6: "-bty / rr"},
+     {2: "sb * btz", 3: "-(sb * bty)", 7: "sb * (btz * v - bty * w)"}),
+    (3, 3, L3, {}, R3, {}),
+]
+
+
+def check_pairs():
+    """The pair tables restate the rows: L_k = A + B, L_{6-k} = A - B, R likewise."""
+    import math
+    import random
+    rnd = random.Random(5)
+    for _ in range(20):
+        env = {n: rnd.uniform(0.3, 2.0) for n in MID_FIELDS + ["g21", "g1", "uu"]}
+        env.update({"sb": rnd.choice((-1.0, 1.0)), "fcf": rnd.choice((-1.0, 1.0)),
+                    "fcs": rnd.choice((-1.0, 1.0)), "sqrt": math.sqrt})
+        for k, k2, A, B, C, D in PAIRS:
+            for rows, P, Q in ((LROWS, A, B), (RROWS, C, D)):
+                for m in range(8):
+                    pa = eval(P[m], env) if m in P else 0.0
+                    pb = eval(Q[m], env) if m in Q else 0.0
+                    for kk, s in ((k, 1.0), (k2, -1.0)):
+                        if kk == k2 and s < 0 and k == k2:
+                            continue
+                        want = eval(rows[kk][m], env) if m in rows[kk] else 0.0
+                        got = pa + s * pb
+                        assert abs(got - want) <= 1e-12 * (1.0 + abs(want)), (k, kk, m, got, want)
+
 # --------------------------------------------------------------------------
 # Physical x flux of one cell (updateFluxes); q0..q7 the conserved state.
 
@@ -231,31 +294,43 @@ MID_NAMES.update({"g21": "G.g21", "g1": "G.g1"})
 CONSTS = ("gm", "gm1", "g21", "sb", "g1", "SMALL", "fcf", "fcs")
 
 
-def emit_rows():
+def emit_pairs():
     o = []
-    o.append("// Adds the adjoint of left row k (lb) and right row k (rb) to mb.")
-    o.append("__device__ __forceinline__ void row_adjoint(const Mid& e, const Gas& G, int k,")
-    o.append("                                            const double* lb, const double* rb,")
-    o.append("                                            MidBar& mb) {")
+    o.append("// Adds the adjoint of rows k and 6 - k of the pair pi (k = 0, 2, 1, 3 for")
+    o.append("// pi = 0..3) to mb: LS = lb_k + lb_{6-k}, LD = lb_k - lb_{6-k} (left rows,")
+    o.append("// columns 0-3, 5-7 in slots 0-6), and right-row seeds (fS +- fD) * lF.")
+    o.append("__device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,")
+    o.append("                                             const double* LS, const double* LD,")
+    o.append("                                             double fS, double fD,")
+    o.append("                                             const double* lF, MidBar& mb) {")
     o.append("  const double sb = (e.sbxm ? -1.0 : 1.0), fcf = (e.fcfm ? -1.0 : 1.0),")
     o.append("               fcs = (e.fcsm ? -1.0 : 1.0);")
     o.append("  (void)fcf; (void)fcs; (void)sb;")
-    o.append("  switch (k) {")
-    for k in range(7):
-        o.append(f"    case {k}: {{")
-        for rows, seedname in ((LROWS, "lb"), (RROWS, "rb")):
-            for m, expr in sorted(rows[k].items()):
+    o.append("  switch (pi) {")
+    for pi, (k, k2, A, B, C, D) in enumerate(PAIRS):
+        o.append(f"    case {pi}: {{  // rows {k} and {k2}")
+        for table, seed_of in ((A, lambda m: f"LS[{m if m < 4 else m - 1}]"),
+                               (B, lambda m: f"LD[{m if m < 4 else m - 1}]"),
+                               (C, lambda m: f"rs{m}"), (D, lambda m: f"rd{m}")):
+            for m, expr in sorted(table.items()):
+                seed = seed_of(m)
                 lines = []
-                for var, coef in reverse_of(expr, f"{seedname}[{m}]"):
+                for var, coef in reverse_of(expr, seed):
                     if var in CONSTS:
                         continue
                     assert var in MID_FIELDS, var
                     field = "as" if var == "as_" else var
                     lines.append(f"        mb.{field} += {c_expr(coef, MID_NAMES)};")
-                if lines:
-                    # a zero seed adds nothing (and must not meet an infinite
-                    # partial derivative: 0 * inf would be NaN)
-                    o.append(f"      if ({seedname}[{m}] != 0.0) {{")
+                if not lines:
+                    continue
+                if seed.startswith("rs") or seed.startswith("rd"):
+                    src = "fS" if seed.startswith("rs") else "fD"
+                    o.append(f"      {{ const double {seed} = {src} * lF[{m}];")
+                    o.append(f"      if ({seed} != 0.0) {{")
+                    o.extend(lines)
+                    o.append("      } }")
+                else:
+                    o.append(f"      if ({seed} != 0.0) {{")
                     o.extend(lines)
                     o.append("      }")
         o.append("      break;")
@@ -353,7 +428,8 @@ def main():
     o.append("  double " + ", ".join("as" if f == "as_" else f for f in MID_FIELDS) + ";")
     o.append("};")
     o.append("")
-    o.extend(emit_rows())
+    check_pairs()
+    o.extend(emit_pairs())
     o.append("")
     o.append("// Adds d(Mid)/d(U1, U2)^T mb to U1b, U2b (midpoint() of mhd_eigen.cuh).")
     o.extend(emit_mid())

@@ -148,6 +148,7 @@ __device__ __forceinline__ long long cell_at(const Grid& g, bool ydir, int k, in
 }
 
 constexpr int AIB = 64;  // threads per block of ka_adj_iface (37 KB of shared memory)
+constexpr int AIB_MIN = 6;  // resident blocks per SM: 168 registers, 6 x 37 KB shared
 
 // Adjoint of the numerical flux of every interface of one direction.  One
 // thread per interface; the interface's frame is the x frame (y interfaces
@@ -155,11 +156,15 @@ constexpr int AIB = 64;  // threads per block of ka_adj_iface (37 KB of shared m
 // words per interface: S[c][f][t] (x) or S[c][t][f] (y) with c = 7p +
 // slot(m) for the adjoint of the frame flux component m at stencil point p,
 // 28 + k for the adjoint of the frame state U1[k], 36 + k for U2[k].
+//
+// The characteristics are walked in pairs (0, 6), (2, 4), (1, 5), (3):
+// rows k and 6 - k share a symmetric part, so the adjoint of the pair's
+// eigenvector rows is one pass (pair_adjoint) over the summed and
+// differenced seeds.
 template <bool YDIR>
-__global__ void __launch_bounds__(AIB) ka_adj_iface(Grid g, Gas G, const double* __restrict__ X,
-                                                    const unsigned* __restrict__ mask,
-                                                    const double* __restrict__ lUL,
-                                                    double* __restrict__ S, double inv_d) {
+__global__ void __launch_bounds__(AIB, AIB_MIN)
+    ka_adj_iface(Grid g, Gas G, const double* __restrict__ X, const unsigned* __restrict__ mask,
+                 const double* __restrict__ lUL, double* __restrict__ S, double inv_d) {
   __shared__ double sF[28][AIB];   // frame fluxes of the 4 stencil points
   __shared__ double sFb[28][AIB];  // their adjoints
   __shared__ double sQ[16][AIB];   // U1, U2 (frame)
@@ -229,51 +234,77 @@ __global__ void __launch_bounds__(AIB) ka_adj_iface(Grid g, Gas G, const double*
   const unsigned mw = mask[YDIR ? (long long)t * g.NY + f : (long long)f * g.NY + t];
   MidBar mb{};
 #pragma unroll 1
-  for (int k = 0; k < 7; k++) {
-    double l[NF], r[NF];
+  for (int pi = 0; pi < 4; pi++) {
+    const int ka = pi == 0 ? 0 : pi == 1 ? 2 : pi == 2 ? 1 : 3;
+    // pair seeds: LS / LD = lb_k +- lb_{6-k} (slots 0..6), fS / fD likewise
+    double LS[7], LD[7], fS = 0.0, fD = 0.0;
 #pragma unroll
-    for (int m = 0; m < NF; m++) { l[m] = 0.0; r[m] = 0.0; }
-    lv_row(e0, G, k, l);
-    rv_row(e0, G, k, r);
-    const unsigned code = (mw >> (4 * k)) & 0xFu;
-    const int up = int(code >> 2);
-    // upwind choice "zero": the characteristic's flux is the constant 0 (its
-    // row may even be non-finite, as at a midpoint whose pressure was clamped)
-    if (up == 2) continue;
-    double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;  // frozen ENO combination of the 4 points
-    if (up == 0) {
-      if (code & 1u) { c0 = -0.5; c1 = 1.5; } else { c1 = 0.5; c2 = 0.5; }
-    } else {
-      if (code & 2u) { c1 = 0.5; c2 = 0.5; } else { c2 = 1.5; c3 = -0.5; }
-    }
-    double phi[NF], fw = 0.0, gk = 0.0;
+    for (int s = 0; s < 7; s++) { LS[s] = 0.0; LD[s] = 0.0; }
 #pragma unroll
-    for (int m = 0; m < NF; m++) {
-      if (m == 4) { phi[m] = 0.0; continue; }
-      const int s = slot_of(m);
-      phi[m] = c0 * sF[s][tid] + c1 * sF[7 + s][tid] + c2 * sF[14 + s][tid] + c3 * sF[21 + s][tid];
-      fw += l[m] * phi[m];
-    }
+    for (int h = 0; h < 2; h++) {
+      const int k = h == 0 ? ka : 6 - ka;
+      if (h == 1 && k == ka) break;
+      // keeps the row products inside the iteration (fewer live registers)
+      opaque(e0);
+      const unsigned code = (mw >> (4 * k)) & 0xFu;
+      const int up = int(code >> 2);
+      // upwind choice "zero": the characteristic's flux is the constant 0 (its
+      // row may even be non-finite, as at a midpoint whose pressure was clamped)
+      if (up == 2) continue;
+      double l[NF], r[NF];
 #pragma unroll
-    for (int m = 0; m < NF; m++) gk += lF[m] * r[m];
-    double lb[NF], rb[NF];
+      for (int m = 0; m < NF; m++) { l[m] = 0.0; r[m] = 0.0; }
+      lv_row(e0, G, k, l);
+      rv_row(e0, G, k, r);
+      double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;  // frozen ENO combination of the 4 points
+      if (up == 0) {
+        if (code & 1u) { c0 = -0.5; c1 = 1.5; } else { c1 = 0.5; c2 = 0.5; }
+      } else {
+        if (code & 2u) { c1 = 0.5; c2 = 0.5; } else { c2 = 1.5; c3 = -0.5; }
+      }
+      double phi[NF], fw = 0.0, gk = 0.0;
 #pragma unroll
-    for (int m = 0; m < NF; m++) {
-      lb[m] = gk * phi[m];
-      rb[m] = fw * lF[m];
-    }
-    row_adjoint(e0, G, k, lb, rb, mb);
-    if (gk != 0.0) {
+      for (int m = 0; m < NF; m++) {
+        if (m == 4) { phi[m] = 0.0; continue; }
+        const int s = slot_of(m);
+        phi[m] = c0 * sF[s][tid] + c1 * sF[7 + s][tid] + c2 * sF[14 + s][tid] + c3 * sF[21 + s][tid];
+        fw += l[m] * phi[m];
+      }
+#pragma unroll
+      for (int m = 0; m < NF; m++) gk += lF[m] * r[m];
+      const double sg = h == 0 ? 1.0 : -1.0;
 #pragma unroll
       for (int m = 0; m < NF; m++) {
         if (m == 4) continue;
         const int s = slot_of(m);
-        const double v = gk * l[m];
-        sFb[s][tid] += c0 * v;
-        sFb[7 + s][tid] += c1 * v;
-        sFb[14 + s][tid] += c2 * v;
-        sFb[21 + s][tid] += c3 * v;
+        LS[s] += gk * phi[m];
+        LD[s] += sg * (gk * phi[m]);
       }
+      fS += fw;
+      fD += sg * fw;
+      if (gk != 0.0) {
+#pragma unroll
+        for (int m = 0; m < NF; m++) {
+          if (m == 4) continue;
+          const int s = slot_of(m);
+          const double v = gk * l[m];
+          sFb[s][tid] += c0 * v;
+          sFb[7 + s][tid] += c1 * v;
+          sFb[14 + s][tid] += c2 * v;
+          sFb[21 + s][tid] += c3 * v;
+        }
+      }
+    }
+    opaque(e0);
+    pair_adjoint(e0, G, pi, LS, LD, fS, fD, lF, mb);
+  }
+  // U1, U2 again from shared memory (volatile: not kept live across the loop)
+  {
+    const volatile double* vq = &sQ[0][0];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      U1[k] = vq[k * AIB + tid];
+      U2[k] = vq[(8 + k) * AIB + tid];
     }
   }
   double U1b[NF], U2b[NF];

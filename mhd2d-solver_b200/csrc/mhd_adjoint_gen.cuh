@@ -17,644 +17,433 @@ struct MidBar {
   double u, v, w, uu, a2, a, ca2, ca, cs2, cs, cf2, cf, rr, af2, af, as2, as, bty, btz, th1, th2, vb;
 };
 
-// Adds the adjoint of left row k (lb) and right row k (rb) to mb.
-__device__ __forceinline__ void row_adjoint(const Mid& e, const Gas& G, int k,
-                                            const double* lb, const double* rb,
-                                            MidBar& mb) {
+// Adds the adjoint of rows k and 6 - k of the pair pi (k = 0, 2, 1, 3 for
+// pi = 0..3) to mb: LS = lb_k + lb_{6-k}, LD = lb_k - lb_{6-k} (left rows,
+// columns 0-3, 5-7 in slots 0-6), and right-row seeds (fS +- fD) * lF.
+__device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
+                                             const double* LS, const double* LD,
+                                             double fS, double fD,
+                                             const double* lF, MidBar& mb) {
   const double sb = (e.sbxm ? -1.0 : 1.0), fcf = (e.fcfm ? -1.0 : 1.0),
                fcs = (e.fcsm ? -1.0 : 1.0);
   (void)fcf; (void)fcs; (void)sb;
-  switch (k) {
-    case 0: {
-      if (lb[0] != 0.0) {
-        mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
-        mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
-        mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
-        mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
-        mb.th2 += lb[0] * fcf * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
-        mb.af += lb[0] * fcf * (0.5 * e.th2) * e.u * e.a * sb;
-        mb.a += lb[0] * fcf * (0.5 * e.th2) * e.u * (sb * e.af);
-        mb.u += lb[0] * fcf * (0.5 * e.th2) * (sb * e.af * e.a);
-        mb.as += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.cs;
-        mb.cs += -(lb[0] * fcf * (0.5 * e.th2)) * e.vb * e.as;
-        mb.vb += -(lb[0] * fcf * (0.5 * e.th2)) * (e.as * e.cs);
+  switch (pi) {
+    case 0: {  // rows 0 and 6
+      if (LS[0] != 0.0) {
+        mb.th1 += LS[0] * fcf * e.uu * e.a2 * e.af * 0.25;
+        mb.af += LS[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
+        mb.a2 += LS[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
+        mb.uu += LS[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
       }
-      if (lb[1] != 0.0) {
-        mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
-        mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
-        mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
-        mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-        mb.th2 += -(lb[1] * fcf) * e.a * e.af * (sb * 0.5);
-        mb.af += -(lb[1] * fcf) * e.a * (sb * 0.5 * e.th2);
-        mb.a += -(lb[1] * fcf) * (sb * 0.5 * e.th2 * e.af);
+      if (LS[1] != 0.0) {
+        mb.th1 += LS[1] * fcf * e.u * e.a2 * e.af * -0.5;
+        mb.af += LS[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
+        mb.a2 += LS[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
+        mb.u += LS[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
       }
-      if (lb[2] != 0.0) {
-        mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
-        mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
-        mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
-        mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-        mb.th2 += lb[2] * fcf * e.cs * e.bty * e.as * 0.5;
-        mb.as += lb[2] * fcf * e.cs * e.bty * (0.5 * e.th2);
-        mb.bty += lb[2] * fcf * e.cs * (0.5 * e.th2 * e.as);
-        mb.cs += lb[2] * fcf * (0.5 * e.th2 * e.as * e.bty);
+      if (LS[2] != 0.0) {
+        mb.th1 += LS[2] * fcf * e.v * e.a2 * e.af * -0.5;
+        mb.af += LS[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
+        mb.a2 += LS[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
+        mb.v += LS[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
       }
-      if (lb[3] != 0.0) {
-        mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
-        mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
-        mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
-        mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-        mb.th2 += lb[3] * fcf * e.cs * e.btz * e.as * 0.5;
-        mb.as += lb[3] * fcf * e.cs * e.btz * (0.5 * e.th2);
-        mb.btz += lb[3] * fcf * e.cs * (0.5 * e.th2 * e.as);
-        mb.cs += lb[3] * fcf * (0.5 * e.th2 * e.as * e.btz);
+      if (LS[3] != 0.0) {
+        mb.th1 += LS[3] * fcf * e.w * e.a2 * e.af * -0.5;
+        mb.af += LS[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
+        mb.a2 += LS[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
+        mb.w += LS[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
       }
-      if (lb[5] != 0.0) {
-        mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
-        mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
-        mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-        mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
-        mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
-        mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
-        mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
+      if (LS[4] != 0.0) {
+        mb.th1 += LS[4] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
+        mb.as += LS[4] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
+        mb.bty += LS[4] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+        mb.cf += LS[4] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
+        mb.rr += LS[4] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
+        mb.cs2 += LS[4] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
+        mb.a2 += -(LS[4] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
       }
-      if (lb[6] != 0.0) {
-        mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
-        mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
-        mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-        mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
-        mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
-        mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
-        mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
+      if (LS[5] != 0.0) {
+        mb.th1 += LS[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
+        mb.as += LS[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
+        mb.btz += LS[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
+        mb.cf += LS[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
+        mb.rr += LS[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
+        mb.cs2 += LS[5] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
+        mb.a2 += -(LS[5] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
       }
-      if (lb[7] != 0.0) {
-        mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
-        mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
-        mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
+      if (LS[6] != 0.0) {
+        mb.th1 += LS[6] * fcf * e.a2 * e.af * 0.5;
+        mb.af += LS[6] * fcf * e.a2 * (0.5 * e.th1);
+        mb.a2 += LS[6] * fcf * (0.5 * e.th1 * e.af);
       }
-      if (rb[0] != 0.0) {
-        mb.af += rb[0] * fcf;
+      if (LD[0] != 0.0) {
+        mb.th2 += LD[0] * fcf * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
+        mb.af += LD[0] * fcf * (0.5 * e.th2) * e.u * e.a * sb;
+        mb.a += LD[0] * fcf * (0.5 * e.th2) * e.u * (sb * e.af);
+        mb.u += LD[0] * fcf * (0.5 * e.th2) * (sb * e.af * e.a);
+        mb.as += -(LD[0] * fcf * (0.5 * e.th2)) * e.vb * e.cs;
+        mb.cs += -(LD[0] * fcf * (0.5 * e.th2)) * e.vb * e.as;
+        mb.vb += -(LD[0] * fcf * (0.5 * e.th2)) * (e.as * e.cs);
       }
-      if (rb[1] != 0.0) {
-        mb.af += rb[1] * fcf * (e.u - e.cf);
-        mb.u += rb[1] * fcf * e.af;
-        mb.cf += -(rb[1] * fcf * e.af);
+      if (LD[1] != 0.0) {
+        mb.th2 += -(LD[1] * fcf) * e.a * e.af * (sb * 0.5);
+        mb.af += -(LD[1] * fcf) * e.a * (sb * 0.5 * e.th2);
+        mb.a += -(LD[1] * fcf) * (sb * 0.5 * e.th2 * e.af);
       }
-      if (rb[2] != 0.0) {
-        mb.af += rb[2] * fcf * e.v;
-        mb.v += rb[2] * fcf * e.af;
-        mb.as += rb[2] * fcf * e.ca * e.bty * sb;
-        mb.bty += rb[2] * fcf * e.ca * (sb * e.as);
-        mb.ca += rb[2] * fcf * (sb * e.as * e.bty);
+      if (LD[2] != 0.0) {
+        mb.th2 += LD[2] * fcf * e.cs * e.bty * e.as * 0.5;
+        mb.as += LD[2] * fcf * e.cs * e.bty * (0.5 * e.th2);
+        mb.bty += LD[2] * fcf * e.cs * (0.5 * e.th2 * e.as);
+        mb.cs += LD[2] * fcf * (0.5 * e.th2 * e.as * e.bty);
       }
-      if (rb[3] != 0.0) {
-        mb.af += rb[3] * fcf * e.w;
-        mb.w += rb[3] * fcf * e.af;
-        mb.as += rb[3] * fcf * e.ca * e.btz * sb;
-        mb.btz += rb[3] * fcf * e.ca * (sb * e.as);
-        mb.ca += rb[3] * fcf * (sb * e.as * e.btz);
+      if (LD[3] != 0.0) {
+        mb.th2 += LD[3] * fcf * e.cs * e.btz * e.as * 0.5;
+        mb.as += LD[3] * fcf * e.cs * e.btz * (0.5 * e.th2);
+        mb.btz += LD[3] * fcf * e.cs * (0.5 * e.th2 * e.as);
+        mb.cs += LD[3] * fcf * (0.5 * e.th2 * e.as * e.btz);
       }
-      if (rb[5] != 0.0) {
-        mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
-        mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
-        mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
-        mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
-      }
-      if (rb[6] != 0.0) {
-        mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
-        mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
-        mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
-        mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
-      }
-      if (rb[7] != 0.0) {
-        mb.af += rb[7] * fcf * e.uu * 0.5;
-        mb.uu += rb[7] * fcf * (0.5 * e.af);
-        mb.af += rb[7] * fcf / G.g1 * e.cf2;
-        mb.cf2 += rb[7] * fcf / G.g1 * e.af;
-        mb.af += -(rb[7] * fcf) * e.u * e.cf;
-        mb.cf += -(rb[7] * fcf) * e.u * e.af;
-        mb.u += -(rb[7] * fcf) * (e.af * e.cf);
-        mb.as += rb[7] * fcf * e.vb * e.ca * sb;
-        mb.ca += rb[7] * fcf * e.vb * (sb * e.as);
-        mb.vb += rb[7] * fcf * (sb * e.as * e.ca);
-        mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
-        mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
-        mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
-      }
+      { const double rs0 = fS * lF[0];
+      if (rs0 != 0.0) {
+        mb.af += rs0 * fcf;
+      } }
+      { const double rs1 = fS * lF[1];
+      if (rs1 != 0.0) {
+        mb.af += rs1 * fcf * e.u;
+        mb.u += rs1 * fcf * e.af;
+      } }
+      { const double rs2 = fS * lF[2];
+      if (rs2 != 0.0) {
+        mb.af += rs2 * fcf * e.v;
+        mb.v += rs2 * fcf * e.af;
+      } }
+      { const double rs3 = fS * lF[3];
+      if (rs3 != 0.0) {
+        mb.af += rs3 * fcf * e.w;
+        mb.w += rs3 * fcf * e.af;
+      } }
+      { const double rs5 = fS * lF[5];
+      if (rs5 != 0.0) {
+        mb.as += rs5 * fcf / e.rr * e.cf * e.bty;
+        mb.bty += rs5 * fcf / e.rr * e.cf * e.as;
+        mb.cf += rs5 * fcf / e.rr * (e.as * e.bty);
+        mb.rr += -(rs5 * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
+      } }
+      { const double rs6 = fS * lF[6];
+      if (rs6 != 0.0) {
+        mb.as += rs6 * fcf / e.rr * e.cf * e.btz;
+        mb.btz += rs6 * fcf / e.rr * e.cf * e.as;
+        mb.cf += rs6 * fcf / e.rr * (e.as * e.btz);
+        mb.rr += -(rs6 * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
+      } }
+      { const double rs7 = fS * lF[7];
+      if (rs7 != 0.0) {
+        mb.af += rs7 * fcf * e.uu * 0.5;
+        mb.uu += rs7 * fcf * (0.5 * e.af);
+        mb.af += rs7 * fcf / G.g1 * e.cf2;
+        mb.cf2 += rs7 * fcf / G.g1 * e.af;
+        mb.af += rs7 * fcf * (e.cf2 - e.a2) * G.g21;
+        mb.cf2 += rs7 * fcf * (G.g21 * e.af);
+        mb.a2 += -(rs7 * fcf * (G.g21 * e.af));
+      } }
+      { const double rd1 = fD * lF[1];
+      if (rd1 != 0.0) {
+        mb.af += -(rd1 * fcf) * e.cf;
+        mb.cf += -(rd1 * fcf) * e.af;
+      } }
+      { const double rd2 = fD * lF[2];
+      if (rd2 != 0.0) {
+        mb.as += rd2 * fcf * e.ca * e.bty * sb;
+        mb.bty += rd2 * fcf * e.ca * (sb * e.as);
+        mb.ca += rd2 * fcf * (sb * e.as * e.bty);
+      } }
+      { const double rd3 = fD * lF[3];
+      if (rd3 != 0.0) {
+        mb.as += rd3 * fcf * e.ca * e.btz * sb;
+        mb.btz += rd3 * fcf * e.ca * (sb * e.as);
+        mb.ca += rd3 * fcf * (sb * e.as * e.btz);
+      } }
+      { const double rd7 = fD * lF[7];
+      if (rd7 != 0.0) {
+        mb.af += -(rd7 * fcf) * e.u * e.cf;
+        mb.cf += -(rd7 * fcf) * e.u * e.af;
+        mb.u += -(rd7 * fcf) * (e.af * e.cf);
+        mb.as += rd7 * fcf * e.vb * e.ca * sb;
+        mb.ca += rd7 * fcf * e.vb * (sb * e.as);
+        mb.vb += rd7 * fcf * (sb * e.as * e.ca);
+      } }
       break;
     }
-    case 1: {
-      if (lb[0] != 0.0) {
-        mb.btz += lb[0] * sb * -0.5 * e.v;
-        mb.v += lb[0] * sb * -0.5 * e.btz;
-        mb.bty += -(lb[0] * sb * -0.5) * e.w;
-        mb.w += -(lb[0] * sb * -0.5) * e.bty;
+    case 1: {  // rows 2 and 4
+      if (LS[0] != 0.0) {
+        mb.th1 += LS[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
+        mb.as += LS[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
+        mb.cf2 += LS[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
+        mb.uu += LS[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
       }
-      if (lb[2] != 0.0) {
-        mb.btz += lb[2] * sb * 0.5;
+      if (LS[1] != 0.0) {
+        mb.th1 += LS[1] * fcs * e.u * e.cf2 * e.as * -0.5;
+        mb.as += LS[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += LS[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
+        mb.u += LS[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
       }
-      if (lb[3] != 0.0) {
-        mb.bty += lb[3] * sb * -0.5;
+      if (LS[2] != 0.0) {
+        mb.th1 += LS[2] * fcs * e.v * e.cf2 * e.as * -0.5;
+        mb.as += LS[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += LS[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
+        mb.v += LS[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
       }
-      if (lb[5] != 0.0) {
-        mb.btz += lb[5] * e.rr * 0.5;
-        mb.rr += lb[5] * (0.5 * e.btz);
+      if (LS[3] != 0.0) {
+        mb.th1 += LS[3] * fcs * e.w * e.cf2 * e.as * -0.5;
+        mb.as += LS[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
+        mb.cf2 += LS[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
+        mb.w += LS[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
       }
-      if (lb[6] != 0.0) {
-        mb.bty += lb[6] * e.rr * -0.5;
-        mb.rr += lb[6] * (-0.5 * e.bty);
+      if (LS[4] != 0.0) {
+        mb.th1 += LS[4] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
+        mb.af += LS[4] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
+        mb.bty += LS[4] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+        mb.cf += LS[4] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
+        mb.rr += LS[4] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
+        mb.cf2 += LS[4] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
+        mb.a2 += -(LS[4] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
       }
-      if (rb[2] != 0.0) {
-        mb.btz += rb[2] * sb;
+      if (LS[5] != 0.0) {
+        mb.th1 += LS[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
+        mb.af += LS[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
+        mb.btz += LS[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
+        mb.cf += LS[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
+        mb.rr += LS[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
+        mb.cf2 += LS[5] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
+        mb.a2 += -(LS[5] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
       }
-      if (rb[3] != 0.0) {
-        mb.bty += -rb[3] * sb;
+      if (LS[6] != 0.0) {
+        mb.th1 += LS[6] * fcs * e.cf2 * e.as * 0.5;
+        mb.as += LS[6] * fcs * e.cf2 * (0.5 * e.th1);
+        mb.cf2 += LS[6] * fcs * (0.5 * e.th1 * e.as);
       }
-      if (rb[5] != 0.0) {
-        mb.btz += rb[5] / e.rr;
-        mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
+      if (LD[0] != 0.0) {
+        mb.th2 += LD[0] * fcs * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
+        mb.as += LD[0] * fcs * (0.5 * e.th2) * e.u * e.ca * sb;
+        mb.ca += LD[0] * fcs * (0.5 * e.th2) * e.u * (sb * e.as);
+        mb.u += LD[0] * fcs * (0.5 * e.th2) * (sb * e.as * e.ca);
+        mb.af += LD[0] * fcs * (0.5 * e.th2) * e.vb * e.cf;
+        mb.cf += LD[0] * fcs * (0.5 * e.th2) * e.vb * e.af;
+        mb.vb += LD[0] * fcs * (0.5 * e.th2) * (e.af * e.cf);
       }
-      if (rb[6] != 0.0) {
-        mb.bty += -(rb[6] / e.rr);
-        mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
+      if (LD[1] != 0.0) {
+        mb.th2 += -(LD[1] * fcs) * e.ca * e.as * (sb * 0.5);
+        mb.as += -(LD[1] * fcs) * e.ca * (sb * 0.5 * e.th2);
+        mb.ca += -(LD[1] * fcs) * (sb * 0.5 * e.th2 * e.as);
       }
-      if (rb[7] != 0.0) {
-        mb.btz += rb[7] * sb * e.v;
-        mb.v += rb[7] * sb * e.btz;
-        mb.bty += -(rb[7] * sb) * e.w;
-        mb.w += -(rb[7] * sb) * e.bty;
+      if (LD[2] != 0.0) {
+        mb.th2 += LD[2] * fcs * e.cf * e.bty * e.af * -0.5;
+        mb.af += LD[2] * fcs * e.cf * e.bty * (-0.5 * e.th2);
+        mb.bty += LD[2] * fcs * e.cf * (-0.5 * e.th2 * e.af);
+        mb.cf += LD[2] * fcs * (-0.5 * e.th2 * e.af * e.bty);
       }
+      if (LD[3] != 0.0) {
+        mb.th2 += LD[3] * fcs * e.cf * e.btz * e.af * -0.5;
+        mb.af += LD[3] * fcs * e.cf * e.btz * (-0.5 * e.th2);
+        mb.btz += LD[3] * fcs * e.cf * (-0.5 * e.th2 * e.af);
+        mb.cf += LD[3] * fcs * (-0.5 * e.th2 * e.af * e.btz);
+      }
+      { const double rs0 = fS * lF[0];
+      if (rs0 != 0.0) {
+        mb.as += rs0 * fcs;
+      } }
+      { const double rs1 = fS * lF[1];
+      if (rs1 != 0.0) {
+        mb.as += rs1 * fcs * e.u;
+        mb.u += rs1 * fcs * e.as;
+      } }
+      { const double rs2 = fS * lF[2];
+      if (rs2 != 0.0) {
+        mb.as += rs2 * fcs * e.v;
+        mb.v += rs2 * fcs * e.as;
+      } }
+      { const double rs3 = fS * lF[3];
+      if (rs3 != 0.0) {
+        mb.as += rs3 * fcs * e.w;
+        mb.w += rs3 * fcs * e.as;
+      } }
+      { const double rs5 = fS * lF[5];
+      if (rs5 != 0.0) {
+        mb.af += -(rs5 * fcs / (e.cf * e.rr) * e.a2 * e.bty);
+        mb.bty += rs5 * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+        mb.a2 += rs5 * fcs / (e.cf * e.rr) * (-e.af * e.bty);
+        mb.cf += -(rs5 * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+        mb.rr += -(rs5 * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      } }
+      { const double rs6 = fS * lF[6];
+      if (rs6 != 0.0) {
+        mb.af += -(rs6 * fcs / (e.cf * e.rr) * e.a2 * e.btz);
+        mb.btz += rs6 * fcs / (e.cf * e.rr) * e.a2 * -e.af;
+        mb.a2 += rs6 * fcs / (e.cf * e.rr) * (-e.af * e.btz);
+        mb.cf += -(rs6 * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
+        mb.rr += -(rs6 * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+      } }
+      { const double rs7 = fS * lF[7];
+      if (rs7 != 0.0) {
+        mb.as += rs7 * fcs * e.uu * 0.5;
+        mb.uu += rs7 * fcs * (0.5 * e.as);
+        mb.as += rs7 * fcs / G.g1 * e.cs2;
+        mb.cs2 += rs7 * fcs / G.g1 * e.as;
+        mb.as += rs7 * fcs * (e.cs2 - e.a2) * G.g21;
+        mb.cs2 += rs7 * fcs * (G.g21 * e.as);
+        mb.a2 += -(rs7 * fcs * (G.g21 * e.as));
+      } }
+      { const double rd1 = fD * lF[1];
+      if (rd1 != 0.0) {
+        mb.as += -(rd1 * fcs) * e.cs;
+        mb.cs += -(rd1 * fcs) * e.as;
+      } }
+      { const double rd2 = fD * lF[2];
+      if (rd2 != 0.0) {
+        mb.af += -(rd2 * fcs) * e.a * e.bty * sb;
+        mb.bty += -(rd2 * fcs) * e.a * (sb * e.af);
+        mb.a += -(rd2 * fcs) * (sb * e.af * e.bty);
+      } }
+      { const double rd3 = fD * lF[3];
+      if (rd3 != 0.0) {
+        mb.af += -(rd3 * fcs) * e.a * e.btz * sb;
+        mb.btz += -(rd3 * fcs) * e.a * (sb * e.af);
+        mb.a += -(rd3 * fcs) * (sb * e.af * e.btz);
+      } }
+      { const double rd7 = fD * lF[7];
+      if (rd7 != 0.0) {
+        mb.as += -(rd7 * fcs) * e.u * e.cs;
+        mb.cs += -(rd7 * fcs) * e.u * e.as;
+        mb.u += -(rd7 * fcs) * (e.as * e.cs);
+        mb.af += -(rd7 * fcs) * e.vb * e.a * sb;
+        mb.a += -(rd7 * fcs) * e.vb * (sb * e.af);
+        mb.vb += -(rd7 * fcs) * (sb * e.af * e.a);
+      } }
       break;
     }
-    case 2: {
-      if (lb[0] != 0.0) {
-        mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
-        mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
-        mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
-        mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
-        mb.th2 += lb[0] * fcs * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
-        mb.as += lb[0] * fcs * (0.5 * e.th2) * e.u * e.ca * sb;
-        mb.ca += lb[0] * fcs * (0.5 * e.th2) * e.u * (sb * e.as);
-        mb.u += lb[0] * fcs * (0.5 * e.th2) * (sb * e.as * e.ca);
-        mb.af += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.cf;
-        mb.cf += lb[0] * fcs * (0.5 * e.th2) * e.vb * e.af;
-        mb.vb += lb[0] * fcs * (0.5 * e.th2) * (e.af * e.cf);
+    case 2: {  // rows 1 and 5
+      if (LS[4] != 0.0) {
+        mb.btz += LS[4] * e.rr * 0.5;
+        mb.rr += LS[4] * (0.5 * e.btz);
       }
-      if (lb[1] != 0.0) {
-        mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
-        mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
-        mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
-        mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-        mb.th2 += -(lb[1] * fcs) * e.ca * e.as * (sb * 0.5);
-        mb.as += -(lb[1] * fcs) * e.ca * (sb * 0.5 * e.th2);
-        mb.ca += -(lb[1] * fcs) * (sb * 0.5 * e.th2 * e.as);
+      if (LS[5] != 0.0) {
+        mb.bty += LS[5] * e.rr * -0.5;
+        mb.rr += LS[5] * (-0.5 * e.bty);
       }
-      if (lb[2] != 0.0) {
-        mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
-        mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
-        mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
-        mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-        mb.th2 += -(lb[2] * fcs) * e.cf * e.bty * e.af * 0.5;
-        mb.af += -(lb[2] * fcs) * e.cf * e.bty * (0.5 * e.th2);
-        mb.bty += -(lb[2] * fcs) * e.cf * (0.5 * e.th2 * e.af);
-        mb.cf += -(lb[2] * fcs) * (0.5 * e.th2 * e.af * e.bty);
+      if (LD[0] != 0.0) {
+        mb.btz += LD[0] * sb * -0.5 * e.v;
+        mb.v += LD[0] * sb * -0.5 * e.btz;
+        mb.bty += -(LD[0] * sb * -0.5) * e.w;
+        mb.w += -(LD[0] * sb * -0.5) * e.bty;
       }
-      if (lb[3] != 0.0) {
-        mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
-        mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
-        mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
-        mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-        mb.th2 += -(lb[3] * fcs) * e.cf * e.btz * e.af * 0.5;
-        mb.af += -(lb[3] * fcs) * e.cf * e.btz * (0.5 * e.th2);
-        mb.btz += -(lb[3] * fcs) * e.cf * (0.5 * e.th2 * e.af);
-        mb.cf += -(lb[3] * fcs) * (0.5 * e.th2 * e.af * e.btz);
+      if (LD[2] != 0.0) {
+        mb.btz += LD[2] * sb * 0.5;
       }
-      if (lb[5] != 0.0) {
-        mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
-        mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
-        mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-        mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
-        mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
-        mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
-        mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
+      if (LD[3] != 0.0) {
+        mb.bty += LD[3] * sb * -0.5;
       }
-      if (lb[6] != 0.0) {
-        mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
-        mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
-        mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-        mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
-        mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
-        mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
-        mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
-      }
-      if (lb[7] != 0.0) {
-        mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
-        mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
-        mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
-      }
-      if (rb[0] != 0.0) {
-        mb.as += rb[0] * fcs;
-      }
-      if (rb[1] != 0.0) {
-        mb.as += rb[1] * fcs * (e.u - e.cs);
-        mb.u += rb[1] * fcs * e.as;
-        mb.cs += -(rb[1] * fcs * e.as);
-      }
-      if (rb[2] != 0.0) {
-        mb.as += rb[2] * fcs * e.v;
-        mb.v += rb[2] * fcs * e.as;
-        mb.af += -(rb[2] * fcs) * e.a * e.bty * sb;
-        mb.bty += -(rb[2] * fcs) * e.a * (sb * e.af);
-        mb.a += -(rb[2] * fcs) * (sb * e.af * e.bty);
-      }
-      if (rb[3] != 0.0) {
-        mb.as += rb[3] * fcs * e.w;
-        mb.w += rb[3] * fcs * e.as;
-        mb.af += -(rb[3] * fcs) * e.a * e.btz * sb;
-        mb.btz += -(rb[3] * fcs) * e.a * (sb * e.af);
-        mb.a += -(rb[3] * fcs) * (sb * e.af * e.btz);
-      }
-      if (rb[5] != 0.0) {
-        mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
-        mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-        mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
-        mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-        mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      }
-      if (rb[6] != 0.0) {
-        mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
-        mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-        mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
-        mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-        mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      }
-      if (rb[7] != 0.0) {
-        mb.as += rb[7] * fcs * e.uu * 0.5;
-        mb.uu += rb[7] * fcs * (0.5 * e.as);
-        mb.as += rb[7] * fcs / G.g1 * e.cs2;
-        mb.cs2 += rb[7] * fcs / G.g1 * e.as;
-        mb.as += -(rb[7] * fcs) * e.u * e.cs;
-        mb.cs += -(rb[7] * fcs) * e.u * e.as;
-        mb.u += -(rb[7] * fcs) * (e.as * e.cs);
-        mb.af += -(rb[7] * fcs) * e.vb * e.a * sb;
-        mb.a += -(rb[7] * fcs) * e.vb * (sb * e.af);
-        mb.vb += -(rb[7] * fcs) * (sb * e.af * e.a);
-        mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
-        mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
-        mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
-      }
+      { const double rs5 = fS * lF[5];
+      if (rs5 != 0.0) {
+        mb.btz += rs5 / e.rr;
+        mb.rr += -rs5 * e.btz / (e.rr * e.rr);
+      } }
+      { const double rs6 = fS * lF[6];
+      if (rs6 != 0.0) {
+        mb.bty += -(rs6 / e.rr);
+        mb.rr += -rs6 * -e.bty / (e.rr * e.rr);
+      } }
+      { const double rd2 = fD * lF[2];
+      if (rd2 != 0.0) {
+        mb.btz += rd2 * sb;
+      } }
+      { const double rd3 = fD * lF[3];
+      if (rd3 != 0.0) {
+        mb.bty += -rd3 * sb;
+      } }
+      { const double rd7 = fD * lF[7];
+      if (rd7 != 0.0) {
+        mb.btz += rd7 * sb * e.v;
+        mb.v += rd7 * sb * e.btz;
+        mb.bty += -(rd7 * sb) * e.w;
+        mb.w += -(rd7 * sb) * e.bty;
+      } }
       break;
     }
-    case 3: {
-      if (lb[0] != 0.0) {
-        mb.th1 += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * e.uu * 0.5;
-        mb.uu += -lb[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * (0.5 * e.th1);
-        mb.af2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.a2;
-        mb.a2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.af2;
-        mb.as2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.cf2;
-        mb.cf2 += -lb[0] * (0.5 * e.th1 * e.uu) * e.as2;
+    case 3: {  // rows 3 and 3
+      if (LS[0] != 0.0) {
+        mb.th1 += -LS[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * e.uu * 0.5;
+        mb.uu += -LS[0] * (e.af2 * e.a2 + e.as2 * e.cf2) * (0.5 * e.th1);
+        mb.af2 += -LS[0] * (0.5 * e.th1 * e.uu) * e.a2;
+        mb.a2 += -LS[0] * (0.5 * e.th1 * e.uu) * e.af2;
+        mb.as2 += -LS[0] * (0.5 * e.th1 * e.uu) * e.cf2;
+        mb.cf2 += -LS[0] * (0.5 * e.th1 * e.uu) * e.as2;
       }
-      if (lb[1] != 0.0) {
-        mb.th1 += lb[1] * e.u * (e.af2 * e.a2 + e.as2 * e.cf2);
-        mb.af2 += lb[1] * e.u * e.th1 * e.a2;
-        mb.a2 += lb[1] * e.u * e.th1 * e.af2;
-        mb.as2 += lb[1] * e.u * e.th1 * e.cf2;
-        mb.cf2 += lb[1] * e.u * e.th1 * e.as2;
-        mb.u += lb[1] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      if (LS[1] != 0.0) {
+        mb.th1 += LS[1] * e.u * (e.af2 * e.a2 + e.as2 * e.cf2);
+        mb.af2 += LS[1] * e.u * e.th1 * e.a2;
+        mb.a2 += LS[1] * e.u * e.th1 * e.af2;
+        mb.as2 += LS[1] * e.u * e.th1 * e.cf2;
+        mb.cf2 += LS[1] * e.u * e.th1 * e.as2;
+        mb.u += LS[1] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
       }
-      if (lb[2] != 0.0) {
-        mb.th1 += lb[2] * e.v * (e.af2 * e.a2 + e.as2 * e.cf2);
-        mb.af2 += lb[2] * e.v * e.th1 * e.a2;
-        mb.a2 += lb[2] * e.v * e.th1 * e.af2;
-        mb.as2 += lb[2] * e.v * e.th1 * e.cf2;
-        mb.cf2 += lb[2] * e.v * e.th1 * e.as2;
-        mb.v += lb[2] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      if (LS[2] != 0.0) {
+        mb.th1 += LS[2] * e.v * (e.af2 * e.a2 + e.as2 * e.cf2);
+        mb.af2 += LS[2] * e.v * e.th1 * e.a2;
+        mb.a2 += LS[2] * e.v * e.th1 * e.af2;
+        mb.as2 += LS[2] * e.v * e.th1 * e.cf2;
+        mb.cf2 += LS[2] * e.v * e.th1 * e.as2;
+        mb.v += LS[2] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
       }
-      if (lb[3] != 0.0) {
-        mb.th1 += lb[3] * e.w * (e.af2 * e.a2 + e.as2 * e.cf2);
-        mb.af2 += lb[3] * e.w * e.th1 * e.a2;
-        mb.a2 += lb[3] * e.w * e.th1 * e.af2;
-        mb.as2 += lb[3] * e.w * e.th1 * e.cf2;
-        mb.cf2 += lb[3] * e.w * e.th1 * e.as2;
-        mb.w += lb[3] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
+      if (LS[3] != 0.0) {
+        mb.th1 += LS[3] * e.w * (e.af2 * e.a2 + e.as2 * e.cf2);
+        mb.af2 += LS[3] * e.w * e.th1 * e.a2;
+        mb.a2 += LS[3] * e.w * e.th1 * e.af2;
+        mb.as2 += LS[3] * e.w * e.th1 * e.cf2;
+        mb.cf2 += LS[3] * e.w * e.th1 * e.as2;
+        mb.w += LS[3] * (e.th1 * (e.af2 * e.a2 + e.as2 * e.cf2));
       }
-      if (lb[5] != 0.0) {
-        mb.th1 += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.af;
-        mb.af += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.th1;
-        mb.as += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * (e.th1 * e.af);
-        mb.bty += lb[5] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
-        mb.cf += lb[5] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.bty);
-        mb.rr += lb[5] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.bty * e.cf);
-        mb.cf2 += lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr);
-        mb.cs2 += -(lb[5] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr));
+      if (LS[4] != 0.0) {
+        mb.th1 += LS[4] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.af;
+        mb.af += LS[4] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * e.as * e.th1;
+        mb.as += LS[4] * (e.cf2 - e.cs2) * e.rr * e.cf * e.bty * (e.th1 * e.af);
+        mb.bty += LS[4] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
+        mb.cf += LS[4] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.bty);
+        mb.rr += LS[4] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.bty * e.cf);
+        mb.cf2 += LS[4] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr);
+        mb.cs2 += -(LS[4] * (e.th1 * e.af * e.as * e.bty * e.cf * e.rr));
       }
-      if (lb[6] != 0.0) {
-        mb.th1 += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.af;
-        mb.af += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.th1;
-        mb.as += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * (e.th1 * e.af);
-        mb.btz += lb[6] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
-        mb.cf += lb[6] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.btz);
-        mb.rr += lb[6] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.btz * e.cf);
-        mb.cf2 += lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr);
-        mb.cs2 += -(lb[6] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr));
+      if (LS[5] != 0.0) {
+        mb.th1 += LS[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.af;
+        mb.af += LS[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * e.as * e.th1;
+        mb.as += LS[5] * (e.cf2 - e.cs2) * e.rr * e.cf * e.btz * (e.th1 * e.af);
+        mb.btz += LS[5] * (e.cf2 - e.cs2) * e.rr * e.cf * (e.th1 * e.af * e.as);
+        mb.cf += LS[5] * (e.cf2 - e.cs2) * e.rr * (e.th1 * e.af * e.as * e.btz);
+        mb.rr += LS[5] * (e.cf2 - e.cs2) * (e.th1 * e.af * e.as * e.btz * e.cf);
+        mb.cf2 += LS[5] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr);
+        mb.cs2 += -(LS[5] * (e.th1 * e.af * e.as * e.btz * e.cf * e.rr));
       }
-      if (lb[7] != 0.0) {
-        mb.th1 += -(lb[7] * (e.af2 * e.a2 + e.as2 * e.cf2));
-        mb.af2 += lb[7] * -e.th1 * e.a2;
-        mb.a2 += lb[7] * -e.th1 * e.af2;
-        mb.as2 += lb[7] * -e.th1 * e.cf2;
-        mb.cf2 += lb[7] * -e.th1 * e.as2;
+      if (LS[6] != 0.0) {
+        mb.th1 += -(LS[6] * (e.af2 * e.a2 + e.as2 * e.cf2));
+        mb.af2 += LS[6] * -e.th1 * e.a2;
+        mb.a2 += LS[6] * -e.th1 * e.af2;
+        mb.as2 += LS[6] * -e.th1 * e.cf2;
+        mb.cf2 += LS[6] * -e.th1 * e.as2;
       }
-      if (rb[1] != 0.0) {
-        mb.u += rb[1];
-      }
-      if (rb[2] != 0.0) {
-        mb.v += rb[2];
-      }
-      if (rb[3] != 0.0) {
-        mb.w += rb[3];
-      }
-      if (rb[7] != 0.0) {
-        mb.uu += rb[7] * 0.5;
-      }
-      break;
-    }
-    case 4: {
-      if (lb[0] != 0.0) {
-        mb.th1 += lb[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
-        mb.as += lb[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
-        mb.cf2 += lb[0] * fcs * e.uu * (0.25 * e.th1 * e.as);
-        mb.uu += lb[0] * fcs * (0.25 * e.th1 * e.as * e.cf2);
-        mb.th2 += -(lb[0] * fcs) * (sb * e.as * e.ca * e.u + e.af * e.cf * e.vb) * 0.5;
-        mb.as += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * e.ca * sb;
-        mb.ca += -(lb[0] * fcs) * (0.5 * e.th2) * e.u * (sb * e.as);
-        mb.u += -(lb[0] * fcs) * (0.5 * e.th2) * (sb * e.as * e.ca);
-        mb.af += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.cf;
-        mb.cf += -(lb[0] * fcs) * (0.5 * e.th2) * e.vb * e.af;
-        mb.vb += -(lb[0] * fcs) * (0.5 * e.th2) * (e.af * e.cf);
-      }
-      if (lb[1] != 0.0) {
-        mb.th1 += lb[1] * fcs * e.u * e.cf2 * e.as * -0.5;
-        mb.as += lb[1] * fcs * e.u * e.cf2 * (-0.5 * e.th1);
-        mb.cf2 += lb[1] * fcs * e.u * (-0.5 * e.th1 * e.as);
-        mb.u += lb[1] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-        mb.th2 += lb[1] * fcs * e.ca * e.as * (sb * 0.5);
-        mb.as += lb[1] * fcs * e.ca * (sb * 0.5 * e.th2);
-        mb.ca += lb[1] * fcs * (sb * 0.5 * e.th2 * e.as);
-      }
-      if (lb[2] != 0.0) {
-        mb.th1 += lb[2] * fcs * e.v * e.cf2 * e.as * -0.5;
-        mb.as += lb[2] * fcs * e.v * e.cf2 * (-0.5 * e.th1);
-        mb.cf2 += lb[2] * fcs * e.v * (-0.5 * e.th1 * e.as);
-        mb.v += lb[2] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-        mb.th2 += lb[2] * fcs * e.cf * e.bty * e.af * 0.5;
-        mb.af += lb[2] * fcs * e.cf * e.bty * (0.5 * e.th2);
-        mb.bty += lb[2] * fcs * e.cf * (0.5 * e.th2 * e.af);
-        mb.cf += lb[2] * fcs * (0.5 * e.th2 * e.af * e.bty);
-      }
-      if (lb[3] != 0.0) {
-        mb.th1 += lb[3] * fcs * e.w * e.cf2 * e.as * -0.5;
-        mb.as += lb[3] * fcs * e.w * e.cf2 * (-0.5 * e.th1);
-        mb.cf2 += lb[3] * fcs * e.w * (-0.5 * e.th1 * e.as);
-        mb.w += lb[3] * fcs * (-0.5 * e.th1 * e.as * e.cf2);
-        mb.th2 += lb[3] * fcs * e.cf * e.btz * e.af * 0.5;
-        mb.af += lb[3] * fcs * e.cf * e.btz * (0.5 * e.th2);
-        mb.btz += lb[3] * fcs * e.cf * (0.5 * e.th2 * e.af);
-        mb.cf += lb[3] * fcs * (0.5 * e.th2 * e.af * e.btz);
-      }
-      if (lb[5] != 0.0) {
-        mb.th1 += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.af * -0.5;
-        mb.af += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (-0.5 * e.th1);
-        mb.bty += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-        mb.cf += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.bty);
-        mb.rr += lb[5] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.bty * e.cf);
-        mb.cf2 += lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr);
-        mb.a2 += -(lb[5] * fcs * (-0.5 * e.th1 * e.af * e.bty * e.cf * e.rr)) * G.g21;
-      }
-      if (lb[6] != 0.0) {
-        mb.th1 += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.af * -0.5;
-        mb.af += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (-0.5 * e.th1);
-        mb.btz += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * e.cf * (-0.5 * e.th1 * e.af);
-        mb.cf += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * e.rr * (-0.5 * e.th1 * e.af * e.btz);
-        mb.rr += lb[6] * fcs * (e.cf2 - G.g21 * e.a2) * (-0.5 * e.th1 * e.af * e.btz * e.cf);
-        mb.cf2 += lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr);
-        mb.a2 += -(lb[6] * fcs * (-0.5 * e.th1 * e.af * e.btz * e.cf * e.rr)) * G.g21;
-      }
-      if (lb[7] != 0.0) {
-        mb.th1 += lb[7] * fcs * e.cf2 * e.as * 0.5;
-        mb.as += lb[7] * fcs * e.cf2 * (0.5 * e.th1);
-        mb.cf2 += lb[7] * fcs * (0.5 * e.th1 * e.as);
-      }
-      if (rb[0] != 0.0) {
-        mb.as += rb[0] * fcs;
-      }
-      if (rb[1] != 0.0) {
-        mb.as += rb[1] * fcs * (e.u + e.cs);
-        mb.u += rb[1] * fcs * e.as;
-        mb.cs += rb[1] * fcs * e.as;
-      }
-      if (rb[2] != 0.0) {
-        mb.as += rb[2] * fcs * e.v;
-        mb.v += rb[2] * fcs * e.as;
-        mb.af += rb[2] * fcs * e.a * e.bty * sb;
-        mb.bty += rb[2] * fcs * e.a * (sb * e.af);
-        mb.a += rb[2] * fcs * (sb * e.af * e.bty);
-      }
-      if (rb[3] != 0.0) {
-        mb.as += rb[3] * fcs * e.w;
-        mb.w += rb[3] * fcs * e.as;
-        mb.af += rb[3] * fcs * e.a * e.btz * sb;
-        mb.btz += rb[3] * fcs * e.a * (sb * e.af);
-        mb.a += rb[3] * fcs * (sb * e.af * e.btz);
-      }
-      if (rb[5] != 0.0) {
-        mb.af += -(rb[5] * fcs / (e.cf * e.rr) * e.a2 * e.bty);
-        mb.bty += rb[5] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-        mb.a2 += rb[5] * fcs / (e.cf * e.rr) * (-e.af * e.bty);
-        mb.cf += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-        mb.rr += -(rb[5] * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      }
-      if (rb[6] != 0.0) {
-        mb.af += -(rb[6] * fcs / (e.cf * e.rr) * e.a2 * e.btz);
-        mb.btz += rb[6] * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-        mb.a2 += rb[6] * fcs / (e.cf * e.rr) * (-e.af * e.btz);
-        mb.cf += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-        mb.rr += -(rb[6] * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
-      }
-      if (rb[7] != 0.0) {
-        mb.as += rb[7] * fcs * e.uu * 0.5;
-        mb.uu += rb[7] * fcs * (0.5 * e.as);
-        mb.as += rb[7] * fcs / G.g1 * e.cs2;
-        mb.cs2 += rb[7] * fcs / G.g1 * e.as;
-        mb.as += rb[7] * fcs * e.u * e.cs;
-        mb.cs += rb[7] * fcs * e.u * e.as;
-        mb.u += rb[7] * fcs * (e.as * e.cs);
-        mb.af += rb[7] * fcs * e.vb * e.a * sb;
-        mb.a += rb[7] * fcs * e.vb * (sb * e.af);
-        mb.vb += rb[7] * fcs * (sb * e.af * e.a);
-        mb.as += rb[7] * fcs * (e.cs2 - e.a2) * G.g21;
-        mb.cs2 += rb[7] * fcs * (G.g21 * e.as);
-        mb.a2 += -(rb[7] * fcs * (G.g21 * e.as));
-      }
-      break;
-    }
-    case 5: {
-      if (lb[0] != 0.0) {
-        mb.btz += lb[0] * sb * 0.5 * e.v;
-        mb.v += lb[0] * sb * 0.5 * e.btz;
-        mb.bty += -(lb[0] * sb * 0.5) * e.w;
-        mb.w += -(lb[0] * sb * 0.5) * e.bty;
-      }
-      if (lb[2] != 0.0) {
-        mb.btz += lb[2] * sb * -0.5;
-      }
-      if (lb[3] != 0.0) {
-        mb.bty += lb[3] * sb * 0.5;
-      }
-      if (lb[5] != 0.0) {
-        mb.btz += lb[5] * e.rr * 0.5;
-        mb.rr += lb[5] * (0.5 * e.btz);
-      }
-      if (lb[6] != 0.0) {
-        mb.bty += lb[6] * e.rr * -0.5;
-        mb.rr += lb[6] * (-0.5 * e.bty);
-      }
-      if (rb[2] != 0.0) {
-        mb.btz += -rb[2] * sb;
-      }
-      if (rb[3] != 0.0) {
-        mb.bty += rb[3] * sb;
-      }
-      if (rb[5] != 0.0) {
-        mb.btz += rb[5] / e.rr;
-        mb.rr += -rb[5] * e.btz / (e.rr * e.rr);
-      }
-      if (rb[6] != 0.0) {
-        mb.bty += -(rb[6] / e.rr);
-        mb.rr += -rb[6] * -e.bty / (e.rr * e.rr);
-      }
-      if (rb[7] != 0.0) {
-        mb.btz += -rb[7] * sb * e.v;
-        mb.v += -rb[7] * sb * e.btz;
-        mb.bty += -(-rb[7] * sb) * e.w;
-        mb.w += -(-rb[7] * sb) * e.bty;
-      }
-      break;
-    }
-    case 6: {
-      if (lb[0] != 0.0) {
-        mb.th1 += lb[0] * fcf * e.uu * e.a2 * e.af * 0.25;
-        mb.af += lb[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
-        mb.a2 += lb[0] * fcf * e.uu * (0.25 * e.th1 * e.af);
-        mb.uu += lb[0] * fcf * (0.25 * e.th1 * e.af * e.a2);
-        mb.th2 += -(lb[0] * fcf) * (sb * e.af * e.a * e.u - e.as * e.cs * e.vb) * 0.5;
-        mb.af += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * e.a * sb;
-        mb.a += -(lb[0] * fcf) * (0.5 * e.th2) * e.u * (sb * e.af);
-        mb.u += -(lb[0] * fcf) * (0.5 * e.th2) * (sb * e.af * e.a);
-        mb.as += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.cs;
-        mb.cs += -(-(lb[0] * fcf) * (0.5 * e.th2)) * e.vb * e.as;
-        mb.vb += -(-(lb[0] * fcf) * (0.5 * e.th2)) * (e.as * e.cs);
-      }
-      if (lb[1] != 0.0) {
-        mb.th1 += lb[1] * fcf * e.u * e.a2 * e.af * -0.5;
-        mb.af += lb[1] * fcf * e.u * e.a2 * (-0.5 * e.th1);
-        mb.a2 += lb[1] * fcf * e.u * (-0.5 * e.th1 * e.af);
-        mb.u += lb[1] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-        mb.th2 += lb[1] * fcf * e.a * e.af * (sb * 0.5);
-        mb.af += lb[1] * fcf * e.a * (sb * 0.5 * e.th2);
-        mb.a += lb[1] * fcf * (sb * 0.5 * e.th2 * e.af);
-      }
-      if (lb[2] != 0.0) {
-        mb.th1 += lb[2] * fcf * e.v * e.a2 * e.af * -0.5;
-        mb.af += lb[2] * fcf * e.v * e.a2 * (-0.5 * e.th1);
-        mb.a2 += lb[2] * fcf * e.v * (-0.5 * e.th1 * e.af);
-        mb.v += lb[2] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-        mb.th2 += -(lb[2] * fcf) * e.cs * e.bty * e.as * 0.5;
-        mb.as += -(lb[2] * fcf) * e.cs * e.bty * (0.5 * e.th2);
-        mb.bty += -(lb[2] * fcf) * e.cs * (0.5 * e.th2 * e.as);
-        mb.cs += -(lb[2] * fcf) * (0.5 * e.th2 * e.as * e.bty);
-      }
-      if (lb[3] != 0.0) {
-        mb.th1 += lb[3] * fcf * e.w * e.a2 * e.af * -0.5;
-        mb.af += lb[3] * fcf * e.w * e.a2 * (-0.5 * e.th1);
-        mb.a2 += lb[3] * fcf * e.w * (-0.5 * e.th1 * e.af);
-        mb.w += lb[3] * fcf * (-0.5 * e.th1 * e.af * e.a2);
-        mb.th2 += -(lb[3] * fcf) * e.cs * e.btz * e.as * 0.5;
-        mb.as += -(lb[3] * fcf) * e.cs * e.btz * (0.5 * e.th2);
-        mb.btz += -(lb[3] * fcf) * e.cs * (0.5 * e.th2 * e.as);
-        mb.cs += -(lb[3] * fcf) * (0.5 * e.th2 * e.as * e.btz);
-      }
-      if (lb[5] != 0.0) {
-        mb.th1 += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * e.as * 0.5;
-        mb.as += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.bty * (0.5 * e.th1);
-        mb.bty += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-        mb.cf += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.bty);
-        mb.rr += lb[5] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.bty * e.cf);
-        mb.cs2 += lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr);
-        mb.a2 += -(lb[5] * fcf * (0.5 * e.th1 * e.as * e.bty * e.cf * e.rr)) * G.g21;
-      }
-      if (lb[6] != 0.0) {
-        mb.th1 += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * e.as * 0.5;
-        mb.as += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * e.btz * (0.5 * e.th1);
-        mb.btz += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * e.cf * (0.5 * e.th1 * e.as);
-        mb.cf += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * e.rr * (0.5 * e.th1 * e.as * e.btz);
-        mb.rr += lb[6] * fcf * (e.cs2 - G.g21 * e.a2) * (0.5 * e.th1 * e.as * e.btz * e.cf);
-        mb.cs2 += lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr);
-        mb.a2 += -(lb[6] * fcf * (0.5 * e.th1 * e.as * e.btz * e.cf * e.rr)) * G.g21;
-      }
-      if (lb[7] != 0.0) {
-        mb.th1 += lb[7] * fcf * e.a2 * e.af * 0.5;
-        mb.af += lb[7] * fcf * e.a2 * (0.5 * e.th1);
-        mb.a2 += lb[7] * fcf * (0.5 * e.th1 * e.af);
-      }
-      if (rb[0] != 0.0) {
-        mb.af += rb[0] * fcf;
-      }
-      if (rb[1] != 0.0) {
-        mb.af += rb[1] * fcf * (e.u + e.cf);
-        mb.u += rb[1] * fcf * e.af;
-        mb.cf += rb[1] * fcf * e.af;
-      }
-      if (rb[2] != 0.0) {
-        mb.af += rb[2] * fcf * e.v;
-        mb.v += rb[2] * fcf * e.af;
-        mb.as += -(rb[2] * fcf) * e.ca * e.bty * sb;
-        mb.bty += -(rb[2] * fcf) * e.ca * (sb * e.as);
-        mb.ca += -(rb[2] * fcf) * (sb * e.as * e.bty);
-      }
-      if (rb[3] != 0.0) {
-        mb.af += rb[3] * fcf * e.w;
-        mb.w += rb[3] * fcf * e.af;
-        mb.as += -(rb[3] * fcf) * e.ca * e.btz * sb;
-        mb.btz += -(rb[3] * fcf) * e.ca * (sb * e.as);
-        mb.ca += -(rb[3] * fcf) * (sb * e.as * e.btz);
-      }
-      if (rb[5] != 0.0) {
-        mb.as += rb[5] * fcf / e.rr * e.cf * e.bty;
-        mb.bty += rb[5] * fcf / e.rr * e.cf * e.as;
-        mb.cf += rb[5] * fcf / e.rr * (e.as * e.bty);
-        mb.rr += -(rb[5] * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
-      }
-      if (rb[6] != 0.0) {
-        mb.as += rb[6] * fcf / e.rr * e.cf * e.btz;
-        mb.btz += rb[6] * fcf / e.rr * e.cf * e.as;
-        mb.cf += rb[6] * fcf / e.rr * (e.as * e.btz);
-        mb.rr += -(rb[6] * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
-      }
-      if (rb[7] != 0.0) {
-        mb.af += rb[7] * fcf * e.uu * 0.5;
-        mb.uu += rb[7] * fcf * (0.5 * e.af);
-        mb.af += rb[7] * fcf / G.g1 * e.cf2;
-        mb.cf2 += rb[7] * fcf / G.g1 * e.af;
-        mb.af += rb[7] * fcf * e.u * e.cf;
-        mb.cf += rb[7] * fcf * e.u * e.af;
-        mb.u += rb[7] * fcf * (e.af * e.cf);
-        mb.as += -(rb[7] * fcf) * e.vb * e.ca * sb;
-        mb.ca += -(rb[7] * fcf) * e.vb * (sb * e.as);
-        mb.vb += -(rb[7] * fcf) * (sb * e.as * e.ca);
-        mb.af += rb[7] * fcf * (e.cf2 - e.a2) * G.g21;
-        mb.cf2 += rb[7] * fcf * (G.g21 * e.af);
-        mb.a2 += -(rb[7] * fcf * (G.g21 * e.af));
-      }
+      { const double rs1 = fS * lF[1];
+      if (rs1 != 0.0) {
+        mb.u += rs1;
+      } }
+      { const double rs2 = fS * lF[2];
+      if (rs2 != 0.0) {
+        mb.v += rs2;
+      } }
+      { const double rs3 = fS * lF[3];
+      if (rs3 != 0.0) {
+        mb.w += rs3;
+      } }
+      { const double rs7 = fS * lF[7];
+      if (rs7 != 0.0) {
+        mb.uu += rs7 * 0.5;
+      } }
       break;
     }
     default:
