@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=2000,
                     help="steps of the plasma-sheet adjoint measurement (0: skip it)")
     ap.add_argument("--adjoint-grid", default="1024x512")
+    ap.add_argument("--adjoint-store", type=int, default=-1,
+                    help="bytes of device memory for kept stage inputs (-1 automatic, 0 none)")
     return ap.parse_args()
 
 
@@ -280,13 +282,14 @@ def batched_measure(dev, n_runs, steps, seed=0):
                         "log-uniform 64..1024, eno-roe/eno-lf, rk3, generated on the device"}
 
 
-def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1):
+def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1, store=-1):
     """Cost of the discrete adjoint on the plasma sheet (1024 x 512 on
     [-2, 2] x [-1, 1], Neumann in x, periodic in y, By = tanh(x/0.1), 16
     velocity amplitudes a_k ~ N(0, 1e-3), ENO-Roe RK3, `steps` steps,
     checkpoints every K steps): a plain forward run (mhd_steps), the
     recording forward, the backward sweep (segment replays included), and
-    central differences of J in two amplitudes through the frozen replay."""
+    central differences of J in two amplitudes through the frozen replay.
+    `store` bounds the device memory of kept stage inputs (-1 automatic)."""
     import numpy as np
     import torch
 
@@ -314,6 +317,7 @@ def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1):
     ms_plain = e0.elapsed_time(e1)
     ctx.close()
     a = Adjoint(nx, ny, p.dx, p.dy, p.gamma, p.bc, checkpoint_every=K, device=dev, **kw)
+    a.set_store(store)
     a.init_plasma_sheet(amps)
     J = a.forward(steps, dt0)
     a.backward()
@@ -347,8 +351,11 @@ def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1):
             "forward_plus_adjoint_over_forward": (info["ms_forward"] + info["ms_backward"]) / ms_plain,
             "forward_cell_updates_per_s": cell_updates / (ms_plain * 1e-3),
             "stages": info["stages"], "checkpoints": info["checkpoints"],
+            "stage_store": {"limit_bytes": store, "stored_stages": info["stored_stages"],
+                            "replayed_segments": info["replayed_segments"]},
             "central_differences": {"steps": fd_steps, "J": J_short, "checks": fd},
-            "note": "backward = segment replays from checkpoints + reverse sweep.  The "
+            "note": "backward = reverse sweep + replays of the checkpoint segments whose stage "
+                    "inputs the recording could not keep in device memory.  The "
                     "frozen-stencil linearisation of the sheet is unstable over the full "
                     "window (dJ/da grows to ~1e6 and perturbed frozen replays diverge by "
                     "t ~ 1), so central differences check the gradient on the first "
@@ -481,7 +488,7 @@ def run_ours(args):
             line["batched"] = bm
     if args.adjoint_steps > 0:
         anx, any_ = (int(v) for v in args.adjoint_grid.split("x"))
-        am = adjoint_measure(dev, args.adjoint_steps, nx=anx, ny=any_)
+        am = adjoint_measure(dev, args.adjoint_steps, nx=anx, ny=any_, store=args.adjoint_store)
         if rank == 0:
             line["adjoint"] = am
     if rank == 0:

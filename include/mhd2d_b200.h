@@ -281,6 +281,8 @@ int mhd_batch_launches( mhd_batch* b, long long* launches );
  * mhd_adj_backward computes dJ/dU0 of that discrete map with the recorded
  * choices and dt frozen: per checkpoint segment, last first, the segment is
  * replayed from its checkpoint and its stages are differentiated in reverse.
+ * Segments whose stage inputs the recording kept in device memory (the
+ * stage store, mhd_adj_set_store) are not replayed.
  * mhd_adj_replay runs the same frozen map from another initial state (the
  * frozen-stencil, frozen-dt forward that central finite differences of J
  * need). */
@@ -293,6 +295,8 @@ typedef struct {
    double    ms_backward;        /* device time of the last backward (replays included) */
    double    ms_replay;          /* device time of the last full replay */
    long long launches;
+   int       stored_stages;      /* stage inputs the recording kept (stage store) */
+   int       replayed_segments;  /* segments the last backward replayed */
 } mhd_adj_stats;
 
 int mhd_adj_create( int nx, int ny, double dx, double dy, double gamma, const int bc[4],
@@ -300,6 +304,12 @@ int mhd_adj_create( int nx, int ny, double dx, double dy, double gamma, const in
                     int checkpoint_every, int device, mhd_adj** out );
 int mhd_adj_destroy( mhd_adj* a );
 int mhd_adj_last_error( mhd_adj* a, char* buf, size_t len, int* is_error );
+/* Device memory the recording may fill with stage inputs, in bytes: the last
+   checkpoint segments that fit are kept whole and the backward uses them
+   instead of replaying.  -1 (the default): all free memory but a reserve for
+   the backward; 0: none, every segment is replayed from its checkpoint.
+   Results are bit-identical either way. */
+int mhd_adj_set_store( mhd_adj* a, long long max_bytes );
 /* Initial state from the host (Dirichlet sides take their edges from it). */
 int mhd_adj_upload( mhd_adj* a, const double* U0 );
 /* Initial state generated on the device (kinds of mhd_batch_init_problem). */

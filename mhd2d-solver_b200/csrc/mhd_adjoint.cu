@@ -21,11 +21,15 @@
 //   1. ka_adj_iface: per x / y interface, recompute the midpoint
 //      eigen-system and the frozen ENO combination, and form the adjoints
 //      of the 4 stencil fluxes and of the two midpoint states
-//      (mhd_adjoint_gen.cuh, generated reverse-mode code);
+//      (mhd_adjoint_gen.cuh, generated reverse-mode code); it reads the
+//      adjoint of UL as a multiple of the stage output's adjoint;
 //   2. ka_adj_gather: per cell, sum the contributions of every interface
-//      that used it and apply the transposed flux Jacobians;
-//   3. ka_adj_bc: transpose of the boundary fill (ghost -> interior; the
-//      Dirichlet edges, snapshots of U0, collect their own adjoints).
+//      that used it and apply the transposed flux Jacobians; interior cells
+//      also apply the rest of the stage update's adjoint and add the result
+//      to the stage input's adjoint, ghost cells go to T;
+//   3. ka_adj_bc: transpose of the boundary fill (ghost adjoints in T ->
+//      interior; the Dirichlet edges, snapshots of U0, collect their own
+//      adjoints).
 // The result is dJ/dU0 for J = sum of the kinetic energy |m|^2 / (2 rho)
 // dx dy over the final interior.
 #include <cuda_runtime.h>
@@ -102,30 +106,23 @@ __global__ void ka_combine(Grid g, int mode, double dt, double* __restrict__ U,
   combine_at(mode, dt, g.at(k, i, j), U, U1, U2, UL);
 }
 
-// Adjoint of one stage update (interior, elementwise); lUL receives the
-// adjoint of UL.
-__global__ void ka_combine_adj(Grid g, int mode, double dt, double* __restrict__ lU,
-                               double* __restrict__ lU1, double* __restrict__ lU2,
-                               double* __restrict__ lUL) {
-  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = 2 + blockIdx.y;
-  const int k = blockIdx.z;
-  if (j >= g.ny + 2) return;
-  const long long a = g.at(k, i, j);
+// Adjoint of one stage update at element a, except its UL term: the adjoint
+// of UL is ul_coef(mode, dt) times the adjoint of the update's output
+// (stage_out), which ka_adj_iface reads directly.
+__device__ __forceinline__ void combine_adj_at(int mode, long long a, double* __restrict__ lU,
+                                               double* __restrict__ lU1,
+                                               double* __restrict__ lU2) {
   switch (mode) {
     case 0:  // U = U + dt*UL
-      lUL[a] = dt * lU[a];
       break;
     case 1: {  // U1 = U + dt*UL
       const double b = lU1[a];
-      lUL[a] = dt * b;
       lU[a] += b;
       lU1[a] = 0.0;
       break;
     }
     case 2: {  // U2 = (3/4)U + (1/4)U1 + (1/4)dt*UL
       const double b = lU2[a];
-      lUL[a] = (1.0 / 4.0) * dt * b;
       lU[a] += (3.0 / 4.0) * b;
       lU1[a] += (1.0 / 4.0) * b;
       lU2[a] = 0.0;
@@ -133,12 +130,18 @@ __global__ void ka_combine_adj(Grid g, int mode, double dt, double* __restrict__
     }
     default: {  // U = (1/3)U + (2/3)U2 + (2/3)dt*UL
       const double b = lU[a];
-      lUL[a] = (2.0 / 3.0) * dt * b;
       lU2[a] += (2.0 / 3.0) * b;
       lU[a] = (1.0 / 3.0) * b;
       break;
     }
   }
+}
+
+// Which buffer a stage update writes (0 U, 1 U1, 2 U2) and the coefficient
+// of its UL term.
+__host__ __device__ inline int stage_out(int mode) { return mode == 1 ? 1 : (mode == 2 ? 2 : 0); }
+__host__ __device__ inline double ul_coef(int mode, double dt) {
+  return mode == 2 ? (1.0 / 4.0) * dt : (mode == 3 ? (2.0 / 3.0) * dt : dt);
 }
 
 // Stencil of interface f (between cells f and f+1 along the direction) at
@@ -164,7 +167,8 @@ constexpr int AIB_MIN = 6;  // resident blocks per SM: 168 registers, 6 x 37 KB 
 template <bool YDIR>
 __global__ void __launch_bounds__(AIB, AIB_MIN)
     ka_adj_iface(Grid g, Gas G, const double* __restrict__ X, const unsigned* __restrict__ mask,
-                 const double* __restrict__ lUL, double* __restrict__ S, double inv_d) {
+                 const double* __restrict__ lB, double cL, double* __restrict__ S,
+                 double inv_d) {
   __shared__ double sF[28][AIB];   // frame fluxes of the 4 stencil points
   __shared__ double sFb[28][AIB];  // their adjoints
   __shared__ double sQ[16][AIB];   // U1, U2 (frame)
@@ -206,7 +210,8 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
       for (int k = 0; k < NF; k++) sQ[8 + k][tid] = q[k];
     }
   }
-  // adjoint of the frame numerical flux: UL = -(F_f - F_{f-1}) / d - ...
+  // adjoint of the frame numerical flux: UL = -(F_f - F_{f-1}) / d - ...;
+  // the adjoint of UL is cL times the adjoint lB of the stage update's output
   double lF[NF];
   const int cell_lo = f, cell_hi = f + 1;  // the two cells sharing the face
 #pragma unroll
@@ -214,9 +219,9 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
     const int kk = YDIR ? swap_xy(m) : m;
     double v = 0.0;
     if (cell_lo >= 2 && cell_lo <= ncell + 1)
-      v -= inv_d * lUL[YDIR ? g.at(kk, t, cell_lo) : g.at(kk, cell_lo, t)];
+      v -= inv_d * (cL * lB[YDIR ? g.at(kk, t, cell_lo) : g.at(kk, cell_lo, t)]);
     if (cell_hi >= 2 && cell_hi <= ncell + 1)
-      v += inv_d * lUL[YDIR ? g.at(kk, t, cell_hi) : g.at(kk, cell_hi, t)];
+      v += inv_d * (cL * lB[YDIR ? g.at(kk, t, cell_hi) : g.at(kk, cell_hi, t)]);
     lF[m] = v;
   }
   double U1[NF], U2[NF];
@@ -319,13 +324,18 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
   }
 }
 
-// Per cell: sum the interface contributions of both directions, apply the
-// transposed flux Jacobians; T gets the adjoint of the stage input incl.
-// ghost cells (before the boundary-fill transpose).
+// Per cell: sum the interface contributions of both directions and apply the
+// transposed flux Jacobians.  Interior cells first take the adjoint of the
+// stage update (combine_adj_at, mode) and then add the result to the
+// stage input's adjoint lbuf (one of lU, lU1, lU2, selected by in_buf); ghost
+// cells write it to T for the boundary-fill transpose.
 __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double* __restrict__ X,
                                                      const double* __restrict__ SX,
                                                      const double* __restrict__ SY,
-                                                     double* __restrict__ T) {
+                                                     double* __restrict__ T, int mode,
+                                                     int in_buf, double* __restrict__ lU,
+                                                     double* __restrict__ lU1,
+                                                     double* __restrict__ lU2) {
   const long long NXY = (long long)g.NX * g.NY;
   const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (e >= NXY) return;
@@ -372,19 +382,29 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
 #pragma unroll
     for (int k = 0; k < NF; k++) lu[yd ? swap_xy(k) : k] += qb[k];
   }
+  if (i >= 2 && i <= g.nx + 1 && j >= 2 && j <= g.ny + 1) {
+    double* lbuf = in_buf == 0 ? lU : (in_buf == 1 ? lU1 : lU2);
 #pragma unroll
-  for (int k = 0; k < NF; k++) T[g.at(k, i, j)] = lu[k];
+    for (int k = 0; k < NF; k++) {
+      const long long a = g.at(k, i, j);
+      combine_adj_at(mode, a, lU, lU1, lU2);
+      lbuf[a] += lu[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NF; k++) T[g.at(k, i, j)] = lu[k];
+  }
 }
 
 // Transpose of the boundary fill (k_bc / bc_elem) for one side: adds the
-// adjoints of the side's two ghost layers to the interior cells they were
-// copied from.  pass 0: the copies (one thread per field and boundary cell,
+// adjoints of the side's two ghost layers (in T) to the interior cells of D
+// they were copied from.  pass 0: the copies (one thread per field and boundary cell,
 // both layers); Dirichlet ghosts hold the edge snapshot of the initial
 // state, so their adjoints go to lsnap (the side's [8][NY] or [8][NX]
 // array).  pass 1: the div B terms of Neumann Bx / By ghosts, gathered per
 // target cell so no two threads add to the same cell.
-__global__ void ka_adj_bc(Grid g, int side, int pass, double* __restrict__ T,
-                          double* __restrict__ lsnap) {
+__global__ void ka_adj_bc(Grid g, int side, int pass, const double* __restrict__ T,
+                          double* __restrict__ D, double* __restrict__ lsnap) {
   const bool xs = side == LEFT || side == RIGHT;
   const int nb = xs ? g.ny : g.nx;  // boundary cells along the side
   const int b = g.bc[side];
@@ -424,7 +444,7 @@ __global__ void ka_adj_bc(Grid g, int side, int pass, double* __restrict__ T,
         sj = b == PERIODIC ? 1 + gl : g.ny + 1 - gl;
         if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj - 2;
       }
-      T[g.at(k, si, sj)] += T[g.at(k, gi, gj)];
+      D[g.at(k, si, sj)] += T[g.at(k, gi, gj)];
     }
     return;
   }
@@ -450,7 +470,7 @@ __global__ void ka_adj_bc(Grid g, int side, int pass, double* __restrict__ T,
       double acc = 0.0;
       if (c + 1 >= 3 && c + 1 < g.ny + 1) acc += cm * T[g.at(4, gi, c + 1)];
       if (c - 1 >= 3 && c - 1 < g.ny + 1) acc += cp * T[g.at(4, gi, c - 1)];
-      T[g.at(5, s5, c)] += acc;
+      D[g.at(5, s5, c)] += acc;
     } else {
       int gj, s4;
       double cm, cp;
@@ -466,7 +486,7 @@ __global__ void ka_adj_bc(Grid g, int side, int pass, double* __restrict__ T,
       double acc = 0.0;
       if (c + 1 >= 3 && c + 1 < g.nx + 1) acc += cm * T[g.at(5, c + 1, gj)];
       if (c - 1 >= 3 && c - 1 < g.nx + 1) acc += cp * T[g.at(5, c - 1, gj)];
-      T[g.at(4, c, s4)] += acc;
+      D[g.at(4, c, s4)] += acc;
     }
   }
 }
@@ -485,16 +505,6 @@ __global__ void ka_snap_adj(Grid g, int side, const double* __restrict__ lsnap,
   else if (side == RIGHT) lU[g.at(k, g.nx + 1, c)] += v;
   else if (side == BOTTOM) lU[g.at(k, c, 2)] += v;
   else lU[g.at(k, c, g.ny + 1)] += v;
-}
-
-// dst[interior] += T[interior]
-__global__ void ka_accum(Grid g, const double* __restrict__ T, double* __restrict__ dst) {
-  const int j = 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = 2 + blockIdx.y;
-  const int k = blockIdx.z;
-  if (j >= g.ny + 2) return;
-  const long long a = g.at(k, i, j);
-  dst[a] += T[a];
 }
 
 // J = sum over the interior of |m|^2 / (2 rho): per-block partial sums in a
@@ -600,9 +610,18 @@ struct mhd_adj {
   std::vector<double*> ckpt;      // U at steps 0, K, 2K, ...
   std::vector<unsigned*> chunks;  // mask slots (2 x NX x NY words per stage)
   size_t slot_words = 0;
-  double *lU = nullptr, *lU1 = nullptr, *lU2 = nullptr, *lUL = nullptr, *T = nullptr;
+  double *lU = nullptr, *lU1 = nullptr, *lU2 = nullptr, *T = nullptr;
   double *SX = nullptr, *SY = nullptr;
-  std::vector<double*> seg;  // stage inputs of one segment
+  std::vector<double*> seg;  // stage inputs of one replayed segment
+  int nseg = 0;              // checkpoint segments of the recording
+  // Stage store: the recording keeps the inputs of every stage of segments
+  // q >= store_seg0, stage s at store + (s - store_first) * blk while
+  // s - store_first < store_slots; the backward skips their replays.
+  long long store_limit = -1;  // bytes; -1 automatic, 0 none
+  double* store = nullptr;
+  size_t store_slots = 0;
+  int store_seg0 = 0, store_first = -1;
+  int replayed_segments = 0;
   double *partial = nullptr, *hpartial = nullptr;
   bool recorded = false, have_grad = false;
   int steps = 0;
@@ -716,6 +735,16 @@ int read_ctl(mhd_adj* a) {
   return MHD_OK;
 }
 
+// Stage store: keeps the input of stage s (after its boundary fill) when s
+// falls into the store.
+void keep_input(mhd_adj* a, int s, const double* X) {
+  if (a->store_first < 0 || s < a->store_first) return;
+  const size_t slot = size_t(s - a->store_first);
+  if (slot >= a->store_slots) return;
+  cudaMemcpyAsync(a->store + slot * a->blk, X, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                  a->stream);
+}
+
 // One recorded time step from U (TimeIntegrationRK3::step /
 // TimeIntegrationEuler::step, as a context runs it).  The i-th flux launched
 // since the last synchronisation, if it runs, is logged as stage base + i,
@@ -725,6 +754,7 @@ int record_step(mhd_adj* a, double* dt_inout) {
   if ((st = ensure_slots(a, base + 3))) return st;
   launch_control(a, PH_RESET_STEP, *dt_inout);
   launch_bc(a, a->U);
+  keep_input(a, base, a->U);
   launch_flux<1>(a, a->U, mask_slot(a, base));
   if (a->time_method == 1) {
     launch_control(a, PH_EULER);
@@ -737,10 +767,12 @@ int record_step(mhd_adj* a, double* dt_inout) {
     for (;;) {
       launch_combine_ctl(a, 1);
       launch_bc(a, a->U1);
+      keep_input(a, base + 1, a->U1);
       launch_flux<1>(a, a->U1, mask_slot(a, base + 1));
       launch_control(a, PH_RK_SECOND);
       launch_combine_ctl(a, 2);
       launch_bc(a, a->U2);
+      keep_input(a, base + 2, a->U2);
       launch_flux<1>(a, a->U2, mask_slot(a, base + 2));
       launch_control(a, PH_RK_FINAL);
       launch_combine_ctl(a, 3);
@@ -808,27 +840,35 @@ void snapshot_into(mhd_adj* a, const double* U, double* const* dst) {
   a->launches++;
 }
 
-// Adjoint of the spatial operator of stage s at its stored input X:
-// lbuf += L'(X)^T lUL.
-void adjoint_L(mhd_adj* a, int s, const double* X, double* lbuf) {
+// Adjoint of stage s (its update r.mode, then the spatial operator at its
+// stored input X): the adjoint of the stage input, lU / lU1 / lU2 by
+// r.in_buf, gets L'(X)^T applied to the adjoint of UL.
+void adjoint_stage(mhd_adj* a, int s, const StageRec& r, const double* X) {
   const Grid& g = a->g;
   unsigned* mx = mask_slot(a, s);
   unsigned* my = mx + (size_t)g.NX * g.NY;
+  double* lb[3] = {a->lU, a->lU1, a->lU2};
+  const double* lB = lb[stage_out(r.mode)];
+  const double cL = ul_coef(r.mode, r.dt);
   const long long nx_faces = (long long)(g.nx + 1) * g.ny, ny_faces = (long long)(g.ny + 1) * g.nx;
   ka_adj_iface<false><<<int((nx_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
-      g, a->G, X, mx, a->lUL, a->SX, 1.0 / g.dx);
+      g, a->G, X, mx, lB, cL, a->SX, 1.0 / g.dx);
   ka_adj_iface<true><<<int((ny_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
-      g, a->G, X, my, a->lUL, a->SY, 1.0 / g.dy);
+      g, a->G, X, my, lB, cL, a->SY, 1.0 / g.dy);
   const long long ncell = (long long)g.NX * g.NY;
-  ka_adj_gather<<<int((ncell + 127) / 128), 128, 0, a->stream>>>(g, a->G, X, a->SX, a->SY, a->T);
+  ka_adj_gather<<<int((ncell + 127) / 128), 128, 0, a->stream>>>(
+      g, a->G, X, a->SX, a->SY, a->T, r.mode, r.in_buf, a->lU, a->lU1, a->lU2);
+  a->launches += 3;
+  double* dst = lb[r.in_buf];
   for (int side = 0; side < 4; side++) {
     const int nb = (side < 2) ? g.ny : g.nx;
-    ka_adj_bc<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, 0, a->T, a->lsnap[side]);
-    ka_adj_bc<<<(nb + 127) / 128, 128, 0, a->stream>>>(g, side, 1, a->T, a->lsnap[side]);
+    ka_adj_bc<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, 0, a->T, dst,
+                                                              a->lsnap[side]);
+    a->launches++;
+    if (g.bc[side] != NEUMANN) continue;  // pass 1 is the Neumann div B term
+    ka_adj_bc<<<(nb + 127) / 128, 128, 0, a->stream>>>(g, side, 1, a->T, dst, a->lsnap[side]);
+    a->launches++;
   }
-  dim3 cgrid((g.ny + 255) / 256, g.nx, NF);
-  ka_accum<<<cgrid, 256, 0, a->stream>>>(g, a->T, lbuf);
-  a->launches += 12;
 }
 
 int check_ready(mhd_adj* a) {
@@ -880,7 +920,7 @@ int mhd_adj_create(int nx, int ny, double dx, double dy, double gamma, const int
   a->blk = size_t(NF) * g.fstride + 16;
   a->slot_words = 2 * (size_t)g.NX * g.NY;
   for (double** p : {&a->U, &a->U1, &a->U2, &a->UL, &a->U0, &a->Ufinal, &a->lU, &a->lU1, &a->lU2,
-                     &a->lUL, &a->T})
+                     &a->T})
     AK(alloc_block(a, p));
   const size_t sn = sizeof(double) * NF * std::max(g.NX, g.NY);
   for (int s = 0; s < 4; s++) {
@@ -911,8 +951,8 @@ int mhd_adj_destroy(mhd_adj* a) {
   if (!a) return MHD_OK;
   cudaSetDevice(a->device);
   if (a->stream) cudaStreamSynchronize(a->stream);
-  for (double* p : {a->U, a->U1, a->U2, a->UL, a->U0, a->Ufinal, a->lU, a->lU1, a->lU2, a->lUL,
-                    a->T, a->SX, a->SY, a->aF, a->aG, a->partial})
+  for (double* p : {a->U, a->U1, a->U2, a->UL, a->U0, a->Ufinal, a->lU, a->lU1, a->lU2, a->T,
+                    a->SX, a->SY, a->aF, a->aG, a->partial})
     cudaFree(p);
   for (int s = 0; s < 4; s++) {
     cudaFree(a->snap[s]);
@@ -920,6 +960,7 @@ int mhd_adj_destroy(mhd_adj* a) {
     cudaFree(a->lsnap[s]);
   }
   for (double* p : a->ckpt) cudaFree(p);
+  cudaFree(a->store);
   for (double* p : a->seg) cudaFree(p);
   for (unsigned* p : a->chunks) cudaFree(p);
   cudaFree(a->dlog);
@@ -977,17 +1018,81 @@ int mhd_adj_init_problem(mhd_adj* a, int kind, const double* p, int np) {
   return aset(a, MHD_OK, false, "");
 }
 
+// Sizes the stage store for a recording of nsteps steps in nseg segments:
+// the last m segments whose stages fit (with room for RK3 retries) in the
+// memory left after a reserve for the backward's replay buffers.
+int plan_store(mhd_adj* a, int nsteps, int nseg, int per_step) {
+  a->store_seg0 = nseg;
+  a->store_first = -1;
+  if (a->store_limit == 0) return MHD_OK;
+  const size_t bb = a->blk * sizeof(double);
+  auto slots_for = [&](int m) -> size_t {
+    const long long kept_steps = (long long)nsteps - (long long)(nseg - m) * a->K;
+    return size_t(per_step * kept_steps + 3 * m + 8);
+  };
+  size_t have = a->store ? a->store_slots * bb : 0;
+  size_t free_b = 0, total_b = 0;
+  AK(cudaMemGetInfo(&free_b, &total_b));
+  const size_t seg_need = size_t(per_step) * a->K + 2;
+  const size_t seg_missing = seg_need > a->seg.size() ? seg_need - a->seg.size() : 0;
+  const size_t reserve = seg_missing * bb + (size_t(2) << 30);
+  size_t avail = free_b + have > reserve ? free_b + have - reserve : 0;
+  if (a->store_limit > 0) avail = std::min(avail, size_t(a->store_limit));
+  int m = nseg;
+  while (m > 0 && slots_for(m) * bb > avail) m--;
+  if (m == 0) return MHD_OK;
+  const size_t want = slots_for(m);
+  if (!a->store || a->store_slots < want || a->store_slots > want + want / 4) {
+    cudaFree(a->store);
+    a->store = nullptr;
+    a->store_slots = 0;
+    while (m > 0 && cudaMalloc(&a->store, slots_for(m) * bb) != cudaSuccess) {
+      cudaGetLastError();
+      m--;
+    }
+    if (m == 0) return MHD_OK;
+    a->store_slots = slots_for(m);
+  }
+  a->store_seg0 = nseg - m;
+  return MHD_OK;
+}
+
+int mhd_adj_set_store(mhd_adj* a, long long max_bytes) {
+  if (!a || max_bytes < -1) return MHD_ERR_WRONG_PARAMETER;
+  a->store_limit = max_bytes;
+  if (max_bytes == 0 && a->store) {
+    AK(cudaSetDevice(a->device));
+    AK(cudaStreamSynchronize(a->stream));
+    cudaFree(a->store);
+    a->store = nullptr;
+    a->store_slots = 0;
+  }
+  a->store_seg0 = a->nseg;
+  a->store_first = -1;
+  return aset(a, MHD_OK, false, "");
+}
+
 int mhd_adj_forward(mhd_adj* a, int nsteps, double dt0, double* J) {
   if (!a || nsteps < 1) return MHD_ERR_WRONG_PARAMETER;
   AK(cudaSetDevice(a->device));
-  for (double* p : a->ckpt) cudaFree(p);
-  a->ckpt.clear();
   a->log.clear();
   a->step_stage.clear();
   a->recorded = false;
   a->have_grad = false;
   a->cur_snap = a->snap;
   int st;
+  // everything the recording needs is allocated before it starts: the
+  // checkpoints, the mask slots of the expected stages and the stage store
+  const int nseg = (nsteps + a->K - 1) / a->K;
+  const int per_step = a->time_method == 2 ? 3 : 1;
+  while ((int)a->ckpt.size() < nseg) {
+    double* c = nullptr;
+    AK(cudaMalloc(&c, a->blk * sizeof(double)));
+    a->ckpt.push_back(c);
+  }
+  a->nseg = nseg;
+  if ((st = ensure_slots(a, per_step * nsteps + 8))) return st;
+  if ((st = plan_store(a, nsteps, nseg, per_step))) return st;
   if ((st = reset_ctl(a))) return st;
   AK(cudaMemsetAsync(a->dnlog, 0, sizeof(int), a->stream));
   *a->hnlog = 0;
@@ -1000,10 +1105,9 @@ int mhd_adj_forward(mhd_adj* a, int nsteps, double dt0, double* J) {
   int done = 0;
   for (int s = 0; s < nsteps; s++) {
     if (s % a->K == 0) {
-      double* c = nullptr;
-      AK(cudaMalloc(&c, a->blk * sizeof(double)));
-      AK(cudaMemcpyAsync(c, a->U, a->blk * sizeof(double), cudaMemcpyDeviceToDevice, a->stream));
-      a->ckpt.push_back(c);
+      AK(cudaMemcpyAsync(a->ckpt[s / a->K], a->U, a->blk * sizeof(double),
+                         cudaMemcpyDeviceToDevice, a->stream));
+      if (s / a->K == a->store_seg0) a->store_first = *a->hnlog;
     }
     a->step_stage.push_back(*a->hnlog);
     if ((st = record_step(a, &dt))) break;
@@ -1092,13 +1196,17 @@ int mhd_adj_backward(mhd_adj* a) {
   AK(cudaSetDevice(a->device));
   const Grid& g = a->g;
   a->cur_snap = a->snap;
-  // the largest segment sizes the stage-input store
-  const int nseg = int(a->ckpt.size());
+  // the largest replayed segment sizes the replay buffers
+  const int nseg = a->nseg;
+  auto kept = [&](int q, int s0, int s1) {
+    return q >= a->store_seg0 && a->store_first >= 0 && s0 >= a->store_first &&
+           size_t(s1 - a->store_first) <= a->store_slots;
+  };
   int maxst = 0;
   for (int q = 0; q < nseg; q++) {
     const int s0 = a->step_stage[q * a->K];
     const int s1 = a->step_stage[std::min((q + 1) * a->K, a->steps)];
-    maxst = std::max(maxst, s1 - s0);
+    if (!kept(q, s0, s1)) maxst = std::max(maxst, s1 - s0);
   }
   while ((int)a->seg.size() < maxst) {
     double* p = nullptr;
@@ -1109,28 +1217,30 @@ int mhd_adj_backward(mhd_adj* a) {
   AK(cudaEventCreate(&e0));
   AK(cudaEventCreate(&e1));
   AK(cudaEventRecord(e0, a->stream));
-  for (double* p : {a->lU, a->lU1, a->lU2, a->lUL, a->T})
+  for (double* p : {a->lU, a->lU1, a->lU2, a->T})
     AK(cudaMemsetAsync(p, 0, a->blk * sizeof(double), a->stream));
   for (int side = 0; side < 4; side++)
     AK(cudaMemsetAsync(a->lsnap[side], 0, sizeof(double) * NF * std::max(g.NX, g.NY), a->stream));
-  dim3 cgrid((g.ny + 255) / 256, g.nx, NF);
   dim3 sgrid((g.ny + 255) / 256, g.nx);
   ka_seed<<<sgrid, 256, 0, a->stream>>>(g, a->Ufinal, a->lU, g.dx * g.dy);
   a->launches++;
-  double* lb[3] = {a->lU, a->lU1, a->lU2};
+  a->replayed_segments = 0;
   for (int q = nseg - 1; q >= 0; q--) {
     const int s0 = a->step_stage[q * a->K];
     const int s1 = a->step_stage[std::min((q + 1) * a->K, a->steps)];
-    AK(cudaMemcpyAsync(a->U, a->ckpt[q], a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
-                       a->stream));
-    if ((st = reset_ctl(a))) return st;
-    replay_stages(a, s0, s1, true);
+    const bool from_store = kept(q, s0, s1);
+    if (!from_store) {
+      AK(cudaMemcpyAsync(a->U, a->ckpt[q], a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                         a->stream));
+      if ((st = reset_ctl(a))) return st;
+      replay_stages(a, s0, s1, true);
+      a->replayed_segments++;
+    }
     for (int s = s1 - 1; s >= s0; s--) {
       const StageRec& r = a->log[s];
-      ka_combine_adj<<<cgrid, 256, 0, a->stream>>>(g, r.mode, r.dt, a->lU, a->lU1, a->lU2,
-                                                   a->lUL);
-      a->launches++;
-      adjoint_L(a, s, a->seg[s - s0], lb[r.in_buf]);
+      const double* X = from_store ? a->store + size_t(s - a->store_first) * a->blk
+                                   : a->seg[s - s0];
+      adjoint_stage(a, s, r, X);
     }
   }
   for (int side = 0; side < 4; side++) {
@@ -1195,7 +1305,7 @@ int mhd_adj_info(mhd_adj* a, mhd_adj_stats* out) {
   if (!a || !out) return MHD_ERR_WRONG_PARAMETER;
   out->steps = a->steps;
   out->stages = int(a->log.size());
-  out->checkpoints = int(a->ckpt.size());
+  out->checkpoints = a->nseg;
   int retries = 0;
   for (size_t s = 0; s < a->log.size(); s++)
     if (a->log[s].mode == 1 && a->log[s].in_buf != 0) retries++;
@@ -1206,6 +1316,11 @@ int mhd_adj_info(mhd_adj* a, mhd_adj_stats* out) {
   out->ms_backward = a->ms_backward;
   out->ms_replay = a->ms_replay;
   out->launches = a->launches;
+  out->stored_stages = 0;
+  if (a->store_first >= 0 && a->log.size() > size_t(a->store_first))
+    out->stored_stages =
+        int(std::min(a->log.size() - size_t(a->store_first), a->store_slots));
+  out->replayed_segments = a->replayed_segments;
   return MHD_OK;
 }
 

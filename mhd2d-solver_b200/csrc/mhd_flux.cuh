@@ -166,7 +166,28 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
     lv_row(e, G, k, l);
     const unsigned lm = DENSE ? 0xFFu : lv_mask(k);
     double fw;
-    if (SCHEME == 2) {  // ENO-Roe: project F and its undivided differences
+    if constexpr (SCHEME == 2 && MASK == 2 && !DENSE) {
+      // frozen replay: only the upwind side's two stencil points are
+      // projected (the same sums, in the same order, as the recording's)
+      const unsigned c = (*mw >> (4 * k)) & 0xFu;
+      const int up = int(c >> 2);
+      fw = 0.0;
+      if (up != 2) {
+        // points pa, pa + 1; pa = 0: -(1/2) wa + (3/2) wb, 1: (1/2) wa + (1/2) wb,
+        // 2: (3/2) wa - (1/2) wb
+        const int pa = up == 0 ? ((c & 1u) ? 0 : 1) : ((c & 2u) ? 1 : 2);
+        double wa = 0.0, wb = 0.0;
+#pragma unroll
+        for (int m = 0; m < NF; m++) {
+          if (!(lm & (1u << m))) continue;
+          wa += l[m] * L.F(m, pa);
+          wb += l[m] * L.F(m, pa + 1);
+        }
+        fw = pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
+           : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
+                        : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
+      }
+    } else if (SCHEME == 2) {  // ENO-Roe: project F and its undivided differences
       // w = lv.F at the 4 points, Vw = lv.(F[p+1] - F[p]) at 3 points; each
       // sum runs over m in ascending order, like the reference's loops
       double w[4] = {0.0, 0.0, 0.0, 0.0}, vw[3] = {0.0, 0.0, 0.0};

@@ -53,7 +53,8 @@ class AdjStats(C.Structure):
     _fields_ = [("steps", C.c_int), ("stages", C.c_int), ("checkpoints", C.c_int),
                 ("retries", C.c_int), ("t", C.c_double), ("dt", C.c_double),
                 ("ms_forward", C.c_double), ("ms_backward", C.c_double),
-                ("ms_replay", C.c_double), ("launches", C.c_longlong)]
+                ("ms_replay", C.c_double), ("launches", C.c_longlong),
+                ("stored_stages", C.c_int), ("replayed_segments", C.c_int)]
 
 
 class BatchDesc(C.Structure):
@@ -140,6 +141,7 @@ def library():
         "mhd_adj_create": [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _ip, C.c_int,
                            C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(vp)],
         "mhd_adj_destroy": [vp],
+        "mhd_adj_set_store": [vp, C.c_longlong],
         "mhd_adj_last_error": [vp, C.c_char_p, C.c_size_t, _ip],
         "mhd_adj_upload": [vp, _dp],
         "mhd_adj_init_problem": [vp, C.c_int, _dp, C.c_int],

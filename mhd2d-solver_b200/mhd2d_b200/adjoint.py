@@ -54,6 +54,10 @@ class Adjoint:
     def __exit__(self, *a):
         self.close()
 
+    def set_store(self, max_bytes=-1):
+        """Device memory for kept stage inputs (-1 automatic, 0 none: replay every segment)."""
+        self._check(self.lib.mhd_adj_set_store(self.h, int(max_bytes)), "set_store")
+
     # -- initial state ---------------------------------------------------------------
     def upload(self, U0):
         self._check(self.lib.mhd_adj_upload(self.h, _p(np.ascontiguousarray(U0))), "upload")

@@ -23,9 +23,10 @@ def _interior_dirs(shape, n, seed):
     return d
 
 
-def _adjoint(p, nsteps, dt0=1e-3, dt_max=0.01, tm=M.RK3, K=4, cfl=0.4, dt_min=1e-9):
+def _adjoint(p, nsteps, dt0=1e-3, dt_max=0.01, tm=M.RK3, K=4, cfl=0.4, dt_min=1e-9, store=-1):
     a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, time_method=tm, dt_min=dt_min,
                 dt_max=dt_max, cfl=cfl, checkpoint_every=K)
+    a.set_store(store)
     a.upload(p.U)
     J = a.forward(nsteps, dt0)
     return a, J
@@ -132,10 +133,30 @@ def test_checkpoint_interval_does_not_change_the_gradient():
     p = P.random_blocky(24, 16, seed=8, bc=(M.PERIODIC, M.PERIODIC, M.NEUMANN, M.NEUMANN))
     grads = []
     for K in (1, 3, 100):
-        a, _ = _adjoint(p, 7, K=K)
+        for store in (0, -1):  # replayed segments / stage inputs kept by the recording
+            a, _ = _adjoint(p, 7, K=K, store=store)
+            a.backward()
+            grads.append(a.gradient())
+            info = a.info()
+            assert info["checkpoints"] == -(-7 // K)
+            assert info["replayed_segments"] == (info["checkpoints"] if store == 0 else 0)
+    for g in grads[1:]:
+        assert same(grads[0], g)
+
+
+def test_stage_store_keeps_the_last_segments():
+    p = P.random_blocky(24, 16, seed=8, bc=(M.PERIODIC, M.PERIODIC, M.NEUMANN, M.NEUMANN))
+    grads, infos = [], []
+    # a 2 MB store holds the stage inputs (86 KB each here) of the last segment only
+    for store in (0, 2 << 20, -1):
+        a, _ = _adjoint(p, 7, K=3, store=store)
         a.backward()
         grads.append(a.gradient())
-        assert a.info()["checkpoints"] == -(-7 // K)
+        infos.append(a.info())
+    assert infos[0]["stored_stages"] == 0 and infos[0]["replayed_segments"] == 3
+    assert 0 < infos[1]["stored_stages"] < infos[1]["stages"]
+    assert 0 < infos[1]["replayed_segments"] < 3
+    assert infos[2]["stored_stages"] == infos[2]["stages"] and infos[2]["replayed_segments"] == 0
     assert same(grads[0], grads[1]) and same(grads[0], grads[2])
 
 
@@ -155,6 +176,9 @@ def test_retry_steps_and_euler_match_tangent_linear():
                 dt_min=kw["dt_min"], dt_max=kw["dt_max"], cfl=kw["cfl"])
     for q in range(3):
         assert abs(_dot(g, dirs[q]) - r["dJ"][q]) <= 1e-9 * abs(r["dJ"][q])
+    a0, _ = _adjoint(p, n, store=0, **kw)  # the retried stages replayed from checkpoints
+    a0.backward()
+    assert same(a0.gradient(), g)
     pe = P.random_smooth(20, 20, seed=13)
     a, J = _adjoint(pe, 5, tm=M.EULER)
     a.backward()
