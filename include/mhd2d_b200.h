@@ -310,6 +310,12 @@ int mhd_adj_last_error( mhd_adj* a, char* buf, size_t len, int* is_error );
    the backward; 0: none, every segment is replayed from its checkpoint.
    Results are bit-identical either way. */
 int mhd_adj_set_store( mhd_adj* a, long long max_bytes );
+/* keep_all 1 (the default): the recording keeps the ENO codes of every stage
+   (mhd_adj_replay needs them).  0: only those of stored stages; the backward
+   records the others again while it replays their segments, so a recording
+   needs mask memory for its stored stages only.  Changing it discards the
+   recording. */
+int mhd_adj_set_masks( mhd_adj* a, int keep_all );
 /* Initial state from the host (Dirichlet sides take their edges from it). */
 int mhd_adj_upload( mhd_adj* a, const double* U0 );
 /* Initial state generated on the device (kinds of mhd_batch_init_problem). */
@@ -331,6 +337,17 @@ int mhd_adj_sheet_gradient( mhd_adj* a, double x0, double y0, int K, double* dJd
 /* which: 0 initial state, 1 final state of the recording, 2 working state. */
 int mhd_adj_download( mhd_adj* a, int which, double* U );
 int mhd_adj_info( mhd_adj* a, mhd_adj_stats* out );
+/* Several recordings or reverse sweeps at once on one device (batched
+   gradients): each object keeps its own stream; the host issues their steps
+   in lockstep (forward) and their stages round robin (backward), so small
+   grids share the GPU.  The stage stores share the free memory in proportion
+   to each recording's stage inputs.  Results are bit-identical to separate
+   mhd_adj_forward / mhd_adj_backward calls.  J (n values) and ms (device
+   time of the whole group) may be NULL; the first failing member's status
+   is returned and its message is in its own mhd_adj_last_error. */
+int mhd_adj_forward_group( int n, mhd_adj* const* a, const int* nsteps, const double* dt0,
+                           double* J, double* ms );
+int mhd_adj_backward_group( int n, mhd_adj* const* a, double* ms );
 
 #ifdef __cplusplus
 }

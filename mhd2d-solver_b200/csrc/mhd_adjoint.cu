@@ -622,6 +622,15 @@ struct mhd_adj {
   size_t store_slots = 0;
   int store_seg0 = 0, store_first = -1;
   int replayed_segments = 0;
+  // Masks: keep_masks 1 keeps the ENO codes of every stage (the frozen replay
+  // of the whole run needs them); 0 keeps those of stored stages only, the
+  // recording writes the others to a scratch slot and the backward's segment
+  // replays record them again (bit-identical runs) into seg_masks.
+  int keep_masks = 1;
+  unsigned* scratch_mask = nullptr;
+  unsigned* seg_masks = nullptr;
+  int seg_mask_slots = 0;
+  int replay_s0 = -1;  // first stage of the segment whose masks are in seg_masks
   double *partial = nullptr, *hpartial = nullptr;
   bool recorded = false, have_grad = false;
   int steps = 0;
@@ -659,17 +668,36 @@ cudaError_t alloc_block(mhd_adj* a, double** p) {
   return e;
 }
 
-unsigned* mask_slot(mhd_adj* a, int s) {
-  return a->chunks[s / kSlotsPerChunk] + (size_t)(s % kSlotsPerChunk) * a->slot_words;
+unsigned* chunk_slot(mhd_adj* a, int i) {
+  return a->chunks[i / kSlotsPerChunk] + (size_t)(i % kSlotsPerChunk) * a->slot_words;
 }
 
-// Room for stages [0, n): mask slots and the device stage log.
-int ensure_slots(mhd_adj* a, int n) {
-  while ((int)a->chunks.size() * kSlotsPerChunk < n) {
+// Mask slot of stage s (see keep_masks).
+unsigned* mask_slot(mhd_adj* a, int s) {
+  if (a->replay_s0 >= 0 && s >= a->replay_s0 && s - a->replay_s0 < a->seg_mask_slots)
+    return a->seg_masks + (size_t)(s - a->replay_s0) * a->slot_words;
+  if (a->keep_masks) return chunk_slot(a, s);
+  if (a->store_first >= 0 && s >= a->store_first) return chunk_slot(a, s - a->store_first);
+  return a->scratch_mask;
+}
+
+// Room for nm kept mask slots.
+int ensure_mask_chunks(mhd_adj* a, int nm) {
+  while ((int)a->chunks.size() * kSlotsPerChunk < nm) {
     unsigned* p = nullptr;
     AK(cudaMalloc(&p, (size_t)kSlotsPerChunk * a->slot_words * sizeof(unsigned)));
     a->chunks.push_back(p);
   }
+  if (!a->scratch_mask) AK(cudaMalloc(&a->scratch_mask, a->slot_words * sizeof(unsigned)));
+  return MHD_OK;
+}
+
+// Room for stages [0, n): mask slots and the device stage log.
+int ensure_slots(mhd_adj* a, int n) {
+  int nm = n;  // kept mask slots
+  if (!a->keep_masks) nm = a->store_first >= 0 ? std::max(0, n - a->store_first) : 0;
+  int st = ensure_mask_chunks(a, nm);
+  if (st) return st;
   if (n > a->log_cap) {
     const int cap = std::max(n, 2 * a->log_cap + 64);
     StageRec* d = nullptr;
@@ -748,11 +776,36 @@ void keep_input(mhd_adj* a, int s, const double* X) {
 // One recorded time step from U (TimeIntegrationRK3::step /
 // TimeIntegrationEuler::step, as a context runs it).  The i-th flux launched
 // since the last synchronisation, if it runs, is logged as stage base + i,
-// so its choices go to that mask slot.
-int record_step(mhd_adj* a, double* dt_inout) {
-  int base = *a->hnlog, st;
+// so its choices go to that mask slot.  record_issue enqueues the step and
+// the read-back of the control block; record_finish waits for it, runs the
+// RK3 retry tails (each synchronously) and returns the step's status.
+
+void ctl_readback(mhd_adj* a) {
+  cudaMemcpyAsync(a->hctl, a->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, a->stream);
+  cudaMemcpyAsync(a->hnlog, a->dnlog, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
+}
+
+// The RK3 stages after the first (U1 and U2 fluxes, stage updates, dt control).
+void record_rk_tail(mhd_adj* a, int base) {
+  launch_combine_ctl(a, 1);
+  launch_bc(a, a->U1);
+  keep_input(a, base + 1, a->U1);
+  launch_flux<1>(a, a->U1, mask_slot(a, base + 1));
+  launch_control(a, PH_RK_SECOND);
+  launch_combine_ctl(a, 2);
+  launch_bc(a, a->U2);
+  keep_input(a, base + 2, a->U2);
+  launch_flux<1>(a, a->U2, mask_slot(a, base + 2));
+  launch_control(a, PH_RK_FINAL);
+  launch_combine_ctl(a, 3);
+  launch_control(a, PH_DONE);
+}
+
+int record_issue(mhd_adj* a, double dt) {
+  const int base = *a->hnlog;
+  int st;
   if ((st = ensure_slots(a, base + 3))) return st;
-  launch_control(a, PH_RESET_STEP, *dt_inout);
+  launch_control(a, PH_RESET_STEP, dt);
   launch_bc(a, a->U);
   keep_input(a, base, a->U);
   launch_flux<1>(a, a->U, mask_slot(a, base));
@@ -760,30 +813,28 @@ int record_step(mhd_adj* a, double* dt_inout) {
     launch_control(a, PH_EULER);
     launch_combine_ctl(a, 0);
     launch_control(a, PH_DONE);
-    if ((st = read_ctl(a))) return st;
   } else {
     launch_control(a, PH_RK_FIRST);
+    record_rk_tail(a, base);
+  }
+  ctl_readback(a);
+  return MHD_OK;
+}
+
+int record_finish(mhd_adj* a, double* dt_inout) {
+  int st;
+  AK(cudaStreamSynchronize(a->stream));
+  AK(cudaGetLastError());
+  if (a->time_method != 1) {
     int guard = 0;
-    for (;;) {
-      launch_combine_ctl(a, 1);
-      launch_bc(a, a->U1);
-      keep_input(a, base + 1, a->U1);
-      launch_flux<1>(a, a->U1, mask_slot(a, base + 1));
-      launch_control(a, PH_RK_SECOND);
-      launch_combine_ctl(a, 2);
-      launch_bc(a, a->U2);
-      keep_input(a, base + 2, a->U2);
-      launch_flux<1>(a, a->U2, mask_slot(a, base + 2));
-      launch_control(a, PH_RK_FINAL);
-      launch_combine_ctl(a, 3);
-      launch_control(a, PH_DONE);
-      if ((st = read_ctl(a))) return st;
-      if (!a->hctl->retry || a->hctl->error) break;
+    while (a->hctl->retry && !a->hctl->error) {
       if (++guard > 64)
         return aset(a, MHD_ERR_WRONG_PARAMETER, true, "RK3 retry loop did not settle");
-      base = *a->hnlog - 1;  // the retry tail's first flux takes the next slot
+      const int base = *a->hnlog - 1;  // the retry tail's first flux takes the next slot
       if ((st = ensure_slots(a, base + 3))) return st;
       launch_control(a, PH_RK_RETRY);
+      record_rk_tail(a, base);
+      if ((st = read_ctl(a))) return st;
     }
   }
   const Ctl& h = *a->hctl;
@@ -810,22 +861,28 @@ int objective(mhd_adj* a, const double* U, double* J) {
   return MHD_OK;
 }
 
-// Replays stages [s0, s1) on the working buffers; with keep, the input of
-// stage s (after its boundary fill) is copied to a->seg[s - s0].
-void replay_stages(mhd_adj* a, int s0, int s1, bool keep) {
+// Replays stage s on the working buffers; keep (if not null) receives its
+// input after the boundary fill.  While replay_s0 is set (masks not kept)
+// the stage records its masks again instead of reading them.
+void replay_stage(mhd_adj* a, int s, double* keep) {
   const Grid& g = a->g;
   dim3 cgrid((g.ny + 255) / 256, g.nx, NF);
-  for (int s = s0; s < s1; s++) {
-    const StageRec& r = a->log[s];
-    double* X = buf(a, r.in_buf);
-    launch_bc(a, X);
-    if (keep)
-      cudaMemcpyAsync(a->seg[s - s0], X, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
-                      a->stream);
+  const StageRec& r = a->log[s];
+  double* X = buf(a, r.in_buf);
+  launch_bc(a, X);
+  if (keep)
+    cudaMemcpyAsync(keep, X, a->blk * sizeof(double), cudaMemcpyDeviceToDevice, a->stream);
+  if (a->replay_s0 >= 0)
+    launch_flux<1>(a, X, mask_slot(a, s));  // the masks again, into seg_masks
+  else
     launch_flux<2>(a, X, mask_slot(a, s));
-    ka_combine<<<cgrid, 256, 0, a->stream>>>(g, r.mode, r.dt, a->U, a->U1, a->U2, a->UL);
-    a->launches++;
-  }
+  ka_combine<<<cgrid, 256, 0, a->stream>>>(g, r.mode, r.dt, a->U, a->U1, a->U2, a->UL);
+  a->launches++;
+}
+
+// Replays stages [s0, s1); with keep, stage s's input goes to a->seg[s - s0].
+void replay_stages(mhd_adj* a, int s0, int s1, bool keep) {
+  for (int s = s0; s < s1; s++) replay_stage(a, s, keep ? a->seg[s - s0] : nullptr);
 }
 
 int reset_ctl(mhd_adj* a) {
@@ -877,6 +934,16 @@ int check_ready(mhd_adj* a) {
   return MHD_OK;
 }
 
+int check_replay(mhd_adj* a) {
+  int st = check_ready(a);
+  if (st) return st;
+  if (!a->keep_masks)
+    return aset(a, MHD_ERR_WRONG_PARAMETER, true,
+                "the recording kept the masks of its stored stages only (mhd_adj_set_masks)");
+  return MHD_OK;
+}
+
+// Elapsed time between e0 and e1; destroys both events.
 int timed_ms(cudaEvent_t e0, cudaEvent_t e1, double* out) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
@@ -887,6 +954,309 @@ int timed_ms(cudaEvent_t e0, cudaEvent_t e1, double* out) {
 }
 
 }  // namespace
+
+// Sizes the stage store for a recording of nsteps steps in nseg segments:
+// the last m segments whose stages fit (with room for RK3 retries) in the
+// memory left after a reserve for the backward's replay buffers, and in
+// budget bytes when budget >= 0.
+int plan_store(mhd_adj* a, int nsteps, int nseg, int per_step, long long budget) {
+  a->store_seg0 = nseg;
+  a->store_first = -1;
+  if (a->store_limit == 0) return MHD_OK;
+  const size_t mask_b = a->slot_words * sizeof(unsigned);
+  // a kept stage holds its input and, without kept masks, its mask slot
+  const size_t bb = a->blk * sizeof(double) + (a->keep_masks ? 0 : mask_b);
+  auto slots_for = [&](int m) -> size_t {
+    const long long kept_steps = (long long)nsteps - (long long)(nseg - m) * a->K;
+    return size_t(per_step * kept_steps + 3 * m + 8);
+  };
+  size_t have = a->store ? a->store_slots * a->blk * sizeof(double) : 0;
+  size_t free_b = 0, total_b = 0;
+  AK(cudaMemGetInfo(&free_b, &total_b));
+  const size_t seg_need = size_t(per_step) * a->K + 2;
+  const size_t seg_missing = seg_need > a->seg.size() ? seg_need - a->seg.size() : 0;
+  const size_t reserve = seg_missing * (a->blk * sizeof(double) + mask_b) + (size_t(2) << 30);
+  size_t avail = free_b + have > reserve ? free_b + have - reserve : 0;
+  if (a->store_limit > 0) avail = std::min(avail, size_t(a->store_limit));
+  if (budget >= 0) avail = std::min(avail, size_t(budget));
+  int m = nseg;
+  while (m > 0 && slots_for(m) * bb > avail) m--;
+  if (m == 0) return MHD_OK;
+  const size_t want = slots_for(m);
+  if (!a->store || a->store_slots < want || a->store_slots > want + want / 4) {
+    cudaFree(a->store);
+    a->store = nullptr;
+    a->store_slots = 0;
+    while (m > 0 &&
+           cudaMalloc(&a->store, slots_for(m) * a->blk * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      m--;
+    }
+    if (m == 0) return MHD_OK;
+    a->store_slots = slots_for(m);
+  }
+  a->store_seg0 = nseg - m;
+  return MHD_OK;
+}
+
+// Recording state between forward_start and forward_end.
+struct FwState {
+  int nsteps = 0, done = 0, status = MHD_OK;
+  double dt = 0.0, t = 0.0;
+  bool active = false;
+};
+
+// Allocations of a recording of nsteps steps that do not depend on the
+// stage store: checkpoints and, with kept masks, every mask slot.
+int forward_prepare(mhd_adj* a, int nsteps) {
+  AK(cudaSetDevice(a->device));
+  a->log.clear();
+  a->step_stage.clear();
+  a->recorded = false;
+  a->have_grad = false;
+  a->cur_snap = a->snap;
+  a->nseg = (nsteps + a->K - 1) / a->K;
+  while ((int)a->ckpt.size() < a->nseg) {
+    double* c = nullptr;
+    AK(cudaMalloc(&c, a->blk * sizeof(double)));
+    a->ckpt.push_back(c);
+  }
+  if (a->keep_masks) return ensure_slots(a, (a->time_method == 2 ? 3 : 1) * nsteps + 8);
+  return MHD_OK;
+}
+
+// The stage store (and, without kept masks, the mask slots of its stages).
+int forward_store(mhd_adj* a, int nsteps, long long budget) {
+  const int per_step = a->time_method == 2 ? 3 : 1;
+  int st = plan_store(a, nsteps, a->nseg, per_step, budget);
+  if (st) return st;
+  if (!a->keep_masks) {
+    if ((st = ensure_mask_chunks(a, int(a->store_slots)))) return st;
+    if ((st = ensure_slots(a, per_step * nsteps + 8))) return st;
+  }
+  return MHD_OK;
+}
+
+int forward_start(mhd_adj* a, FwState& f, int nsteps, double dt0) {
+  int st;
+  if ((st = reset_ctl(a))) return st;
+  AK(cudaMemsetAsync(a->dnlog, 0, sizeof(int), a->stream));
+  *a->hnlog = 0;
+  AK(cudaMemcpyAsync(a->U, a->U0, a->blk * sizeof(double), cudaMemcpyDeviceToDevice, a->stream));
+  f = FwState{};
+  f.nsteps = nsteps;
+  f.dt = dt0;
+  f.active = true;
+  return MHD_OK;
+}
+
+// Enqueues step f.done (its checkpoint first when it starts a segment).
+int forward_issue(mhd_adj* a, FwState& f) {
+  const int s = f.done;
+  if (s % a->K == 0) {
+    AK(cudaMemcpyAsync(a->ckpt[s / a->K], a->U, a->blk * sizeof(double),
+                       cudaMemcpyDeviceToDevice, a->stream));
+    if (s / a->K == a->store_seg0) a->store_first = *a->hnlog;
+  }
+  a->step_stage.push_back(*a->hnlog);
+  return record_issue(a, f.dt);
+}
+
+// Completes the issued step; ends the recording on an error or after the
+// last step.
+void forward_finish(mhd_adj* a, FwState& f) {
+  const int st = record_finish(a, &f.dt);
+  if (st) {
+    f.status = st;
+    f.active = false;
+    return;
+  }
+  f.t += f.dt;
+  if (++f.done >= f.nsteps) f.active = false;
+}
+
+int forward_end(mhd_adj* a, const FwState& f, double* J) {
+  int st;
+  if (f.status) return f.status;
+  a->step_stage.push_back(*a->hnlog);
+  a->log.resize(*a->hnlog);
+  AK(cudaMemcpy(a->log.data(), a->dlog, sizeof(StageRec) * a->log.size(),
+                cudaMemcpyDeviceToHost));
+  AK(cudaMemcpyAsync(a->Ufinal, a->U, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
+                     a->stream));
+  a->steps = f.done;
+  a->t = f.t;
+  a->dt = f.dt;
+  a->recorded = true;
+  if (J && (st = objective(a, a->U, J))) return st;
+  return aset(a, MHD_OK, false, "");
+}
+
+// Segment q of the recording kept in the stage store (no replay needed).
+bool seg_kept(const mhd_adj* a, int q, int s0, int s1) {
+  return q >= a->store_seg0 && a->store_first >= 0 && s0 >= a->store_first &&
+         size_t(s1 - a->store_first) <= a->store_slots;
+}
+int seg_first(const mhd_adj* a, int q) { return a->step_stage[q * a->K]; }
+int seg_end(const mhd_adj* a, int q) { return a->step_stage[std::min((q + 1) * a->K, a->steps)]; }
+
+// Replay buffers (stage inputs, and masks when not kept) of the largest
+// replayed segment.
+int backward_prepare(mhd_adj* a) {
+  AK(cudaSetDevice(a->device));
+  a->cur_snap = a->snap;
+  int maxst = 0;
+  for (int q = 0; q < a->nseg; q++) {
+    const int s0 = seg_first(a, q), s1 = seg_end(a, q);
+    if (!seg_kept(a, q, s0, s1)) maxst = std::max(maxst, s1 - s0);
+  }
+  if (!a->keep_masks && a->seg_mask_slots < maxst) {
+    cudaFree(a->seg_masks);
+    a->seg_masks = nullptr;
+    a->seg_mask_slots = 0;
+    AK(cudaMalloc(&a->seg_masks, (size_t)maxst * a->slot_words * sizeof(unsigned)));
+    a->seg_mask_slots = maxst;
+  }
+  while ((int)a->seg.size() < maxst) {
+    double* p = nullptr;
+    AK(cudaMalloc(&p, a->blk * sizeof(double)));
+    a->seg.push_back(p);
+  }
+  return MHD_OK;
+}
+
+// Progress of a reverse sweep: segments last first; in each, a replay of
+// its stages (unless kept) and then their adjoints in reverse.
+struct BwState {
+  enum Phase { SEGMENT, REPLAY, ADJOINT, FINISH, DONE };
+  Phase phase = SEGMENT;
+  int q = 0, s0 = 0, s1 = 0, s = 0;
+  bool kept = false;
+};
+
+int backward_start(mhd_adj* a, BwState& b) {
+  const Grid& g = a->g;
+  for (double* p : {a->lU, a->lU1, a->lU2, a->T})
+    AK(cudaMemsetAsync(p, 0, a->blk * sizeof(double), a->stream));
+  for (int side = 0; side < 4; side++)
+    AK(cudaMemsetAsync(a->lsnap[side], 0, sizeof(double) * NF * std::max(g.NX, g.NY), a->stream));
+  dim3 sgrid((g.ny + 255) / 256, g.nx);
+  ka_seed<<<sgrid, 256, 0, a->stream>>>(g, a->Ufinal, a->lU, g.dx * g.dy);
+  a->launches++;
+  a->replayed_segments = 0;
+  a->replay_s0 = -1;
+  b = BwState{};
+  b.q = a->nseg - 1;
+  b.phase = b.q >= 0 ? BwState::SEGMENT : BwState::FINISH;
+  return MHD_OK;
+}
+
+// Enqueues the next unit of the reverse sweep: one replayed stage, one
+// stage adjoint, or the closing snapshot adjoints.
+int backward_issue(mhd_adj* a, BwState& b) {
+  const Grid& g = a->g;
+  int st;
+  switch (b.phase) {
+    case BwState::SEGMENT:
+      b.s0 = seg_first(a, b.q);
+      b.s1 = seg_end(a, b.q);
+      b.kept = seg_kept(a, b.q, b.s0, b.s1);
+      if (!b.kept) {
+        AK(cudaMemcpyAsync(a->U, a->ckpt[b.q], a->blk * sizeof(double),
+                           cudaMemcpyDeviceToDevice, a->stream));
+        if ((st = reset_ctl(a))) return st;
+        if (!a->keep_masks) a->replay_s0 = b.s0;
+        a->replayed_segments++;
+        b.s = b.s0;
+        b.phase = b.s < b.s1 ? BwState::REPLAY : BwState::ADJOINT;
+      } else {
+        b.phase = BwState::ADJOINT;
+      }
+      if (b.phase == BwState::ADJOINT) b.s = b.s1 - 1;
+      return MHD_OK;
+    case BwState::REPLAY:
+      replay_stage(a, b.s, a->seg[b.s - b.s0]);
+      if (++b.s == b.s1) {
+        b.phase = BwState::ADJOINT;
+        b.s = b.s1 - 1;
+      }
+      return MHD_OK;
+    case BwState::ADJOINT:
+      if (b.s >= b.s0) {
+        const double* X = b.kept ? a->store + size_t(b.s - a->store_first) * a->blk
+                                 : a->seg[b.s - b.s0];
+        adjoint_stage(a, b.s, a->log[b.s], X);
+        b.s--;
+      }
+      if (b.s < b.s0) {
+        a->replay_s0 = -1;
+        b.phase = --b.q >= 0 ? BwState::SEGMENT : BwState::FINISH;
+      }
+      return MHD_OK;
+    case BwState::FINISH:
+      for (int side = 0; side < 4; side++) {
+        if (g.bc[side] != DIRICHLET) continue;
+        const int nb = (side < 2) ? g.ny : g.nx;
+        ka_snap_adj<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, a->lsnap[side],
+                                                                  a->lU);
+        a->launches++;
+      }
+      b.phase = BwState::DONE;
+      return MHD_OK;
+    default:
+      return MHD_OK;
+  }
+}
+
+// Group timing: a stream that waits for every member's work.
+struct GroupClock {
+  cudaStream_t gs = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<cudaEvent_t> ends;
+};
+
+cudaError_t group_begin(GroupClock& c, int n, mhd_adj* const* as) {
+  cudaError_t e = cudaStreamCreateWithFlags(&c.gs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c.e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c.e1);
+  if (e == cudaSuccess) e = cudaEventRecord(c.e0, c.gs);
+  for (int i = 0; i < n && e == cudaSuccess; i++) e = cudaStreamWaitEvent(as[i]->stream, c.e0, 0);
+  return e;
+}
+
+cudaError_t group_end(GroupClock& c, int n, mhd_adj* const* as, double* ms) {
+  cudaError_t e = cudaSuccess;
+  c.ends.assign(n, nullptr);
+  for (int i = 0; i < n && e == cudaSuccess; i++) {
+    e = cudaEventCreateWithFlags(&c.ends[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(c.ends[i], as[i]->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c.gs, c.ends[i], 0);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(c.e1, c.gs);
+  if (e == cudaSuccess) e = cudaEventSynchronize(c.e1);
+  float f = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&f, c.e0, c.e1);
+  if (ms) *ms = f;
+  return e;
+}
+
+void group_free(GroupClock& c) {
+  for (cudaEvent_t ev : c.ends)
+    if (ev) cudaEventDestroy(ev);
+  if (c.e0) cudaEventDestroy(c.e0);
+  if (c.e1) cudaEventDestroy(c.e1);
+  if (c.gs) cudaStreamDestroy(c.gs);
+}
+
+int group_check(int n, mhd_adj* const* as) {
+  if (n < 1 || !as) return MHD_ERR_WRONG_PARAMETER;
+  for (int i = 0; i < n; i++) {
+    if (!as[i] || as[i]->device != as[0]->device) return MHD_ERR_WRONG_PARAMETER;
+    for (int j = 0; j < i; j++)
+      if (as[j] == as[i]) return MHD_ERR_WRONG_PARAMETER;
+  }
+  return MHD_OK;
+}
 
 extern "C" {
 
@@ -963,6 +1333,8 @@ int mhd_adj_destroy(mhd_adj* a) {
   cudaFree(a->store);
   for (double* p : a->seg) cudaFree(p);
   for (unsigned* p : a->chunks) cudaFree(p);
+  cudaFree(a->scratch_mask);
+  cudaFree(a->seg_masks);
   cudaFree(a->dlog);
   cudaFree(a->dnlog);
   cudaFree(a->ctl);
@@ -1018,45 +1390,6 @@ int mhd_adj_init_problem(mhd_adj* a, int kind, const double* p, int np) {
   return aset(a, MHD_OK, false, "");
 }
 
-// Sizes the stage store for a recording of nsteps steps in nseg segments:
-// the last m segments whose stages fit (with room for RK3 retries) in the
-// memory left after a reserve for the backward's replay buffers.
-int plan_store(mhd_adj* a, int nsteps, int nseg, int per_step) {
-  a->store_seg0 = nseg;
-  a->store_first = -1;
-  if (a->store_limit == 0) return MHD_OK;
-  const size_t bb = a->blk * sizeof(double);
-  auto slots_for = [&](int m) -> size_t {
-    const long long kept_steps = (long long)nsteps - (long long)(nseg - m) * a->K;
-    return size_t(per_step * kept_steps + 3 * m + 8);
-  };
-  size_t have = a->store ? a->store_slots * bb : 0;
-  size_t free_b = 0, total_b = 0;
-  AK(cudaMemGetInfo(&free_b, &total_b));
-  const size_t seg_need = size_t(per_step) * a->K + 2;
-  const size_t seg_missing = seg_need > a->seg.size() ? seg_need - a->seg.size() : 0;
-  const size_t reserve = seg_missing * bb + (size_t(2) << 30);
-  size_t avail = free_b + have > reserve ? free_b + have - reserve : 0;
-  if (a->store_limit > 0) avail = std::min(avail, size_t(a->store_limit));
-  int m = nseg;
-  while (m > 0 && slots_for(m) * bb > avail) m--;
-  if (m == 0) return MHD_OK;
-  const size_t want = slots_for(m);
-  if (!a->store || a->store_slots < want || a->store_slots > want + want / 4) {
-    cudaFree(a->store);
-    a->store = nullptr;
-    a->store_slots = 0;
-    while (m > 0 && cudaMalloc(&a->store, slots_for(m) * bb) != cudaSuccess) {
-      cudaGetLastError();
-      m--;
-    }
-    if (m == 0) return MHD_OK;
-    a->store_slots = slots_for(m);
-  }
-  a->store_seg0 = nseg - m;
-  return MHD_OK;
-}
-
 int mhd_adj_set_store(mhd_adj* a, long long max_bytes) {
   if (!a || max_bytes < -1) return MHD_ERR_WRONG_PARAMETER;
   a->store_limit = max_bytes;
@@ -1072,69 +1405,153 @@ int mhd_adj_set_store(mhd_adj* a, long long max_bytes) {
   return aset(a, MHD_OK, false, "");
 }
 
+int mhd_adj_set_masks(mhd_adj* a, int keep_all) {
+  if (!a || (keep_all != 0 && keep_all != 1)) return MHD_ERR_WRONG_PARAMETER;
+  if (a->keep_masks != keep_all) {
+    // the mask slots of a recording follow the policy it ran with
+    a->keep_masks = keep_all;
+    a->recorded = false;
+    a->have_grad = false;
+  }
+  return aset(a, MHD_OK, false, "");
+}
+
 int mhd_adj_forward(mhd_adj* a, int nsteps, double dt0, double* J) {
   if (!a || nsteps < 1) return MHD_ERR_WRONG_PARAMETER;
-  AK(cudaSetDevice(a->device));
-  a->log.clear();
-  a->step_stage.clear();
-  a->recorded = false;
-  a->have_grad = false;
-  a->cur_snap = a->snap;
+  // everything the recording needs is allocated before it starts
   int st;
-  // everything the recording needs is allocated before it starts: the
-  // checkpoints, the mask slots of the expected stages and the stage store
-  const int nseg = (nsteps + a->K - 1) / a->K;
-  const int per_step = a->time_method == 2 ? 3 : 1;
-  while ((int)a->ckpt.size() < nseg) {
-    double* c = nullptr;
-    AK(cudaMalloc(&c, a->blk * sizeof(double)));
-    a->ckpt.push_back(c);
-  }
-  a->nseg = nseg;
-  if ((st = ensure_slots(a, per_step * nsteps + 8))) return st;
-  if ((st = plan_store(a, nsteps, nseg, per_step))) return st;
-  if ((st = reset_ctl(a))) return st;
-  AK(cudaMemsetAsync(a->dnlog, 0, sizeof(int), a->stream));
-  *a->hnlog = 0;
-  AK(cudaMemcpyAsync(a->U, a->U0, a->blk * sizeof(double), cudaMemcpyDeviceToDevice, a->stream));
+  if ((st = forward_prepare(a, nsteps))) return st;
+  if ((st = forward_store(a, nsteps, -1))) return st;
+  FwState f;
+  if ((st = forward_start(a, f, nsteps, dt0))) return st;
   cudaEvent_t e0, e1;
   AK(cudaEventCreate(&e0));
   AK(cudaEventCreate(&e1));
   AK(cudaEventRecord(e0, a->stream));
-  double dt = dt0, t = 0.0;
-  int done = 0;
-  for (int s = 0; s < nsteps; s++) {
-    if (s % a->K == 0) {
-      AK(cudaMemcpyAsync(a->ckpt[s / a->K], a->U, a->blk * sizeof(double),
-                         cudaMemcpyDeviceToDevice, a->stream));
-      if (s / a->K == a->store_seg0) a->store_first = *a->hnlog;
+  while (f.active) {
+    if ((st = forward_issue(a, f))) {
+      f.status = st;
+      break;
     }
-    a->step_stage.push_back(*a->hnlog);
-    if ((st = record_step(a, &dt))) break;
-    t += dt;
-    done++;
+    forward_finish(a, f);
   }
   AK(cudaEventRecord(e1, a->stream));
   AK(cudaEventSynchronize(e1));
-  timed_ms(e0, e1, &a->ms_forward);
+  timed_ms(e0, e1, &a->ms_forward);  // destroys e0, e1
+  return forward_end(a, f, J);
+}
+
+int mhd_adj_forward_group(int n, mhd_adj* const* as, const int* nsteps, const double* dt0,
+                          double* J, double* ms) {
+  int st = group_check(n, as);
   if (st) return st;
-  a->step_stage.push_back(*a->hnlog);
-  a->log.resize(*a->hnlog);
-  AK(cudaMemcpy(a->log.data(), a->dlog, sizeof(StageRec) * a->log.size(),
-                cudaMemcpyDeviceToHost));
-  AK(cudaMemcpyAsync(a->Ufinal, a->U, a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
-                     a->stream));
-  a->steps = done;
-  a->t = t;
-  a->dt = dt;
-  a->recorded = true;
-  if (J && (st = objective(a, a->U, J))) return st;
-  return aset(a, MHD_OK, false, "");
+  if (!nsteps || !dt0) return MHD_ERR_WRONG_PARAMETER;
+  for (int i = 0; i < n; i++)
+    if (nsteps[i] < 1) return MHD_ERR_WRONG_PARAMETER;
+  if (cudaSetDevice(as[0]->device) != cudaSuccess) return MHD_ERR_CUDA;
+  for (int i = 0; i < n; i++)
+    if ((st = forward_prepare(as[i], nsteps[i]))) return st;
+  // the stage stores share the free memory in proportion to the stage
+  // inputs each recording has, after every member's backward reserve
+  size_t reserve = size_t(2) << 30, want_total = 0;
+  std::vector<size_t> want(n, 0);
+  for (int i = 0; i < n; i++) {
+    mhd_adj* a = as[i];
+    const int per_step = a->time_method == 2 ? 3 : 1;
+    const size_t slot_b =
+        a->blk * sizeof(double) + (a->keep_masks ? 0 : a->slot_words * sizeof(unsigned));
+    const size_t seg_need = size_t(per_step) * a->K + 2;
+    if (seg_need > a->seg.size()) reserve += (seg_need - a->seg.size()) * slot_b;
+    if (a->store_limit != 0) {
+      cudaFree(a->store);
+      a->store = nullptr;
+      a->store_slots = 0;
+      want[i] = size_t(per_step) * nsteps[i] * slot_b;
+      want_total += want[i];
+    }
+  }
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return MHD_ERR_CUDA;
+  const double avail = free_b > reserve ? double(free_b - reserve) : 0.0;
+  for (int i = 0; i < n; i++) {
+    const long long budget =
+        want_total ? (long long)(avail * (double(want[i]) / double(want_total))) : 0;
+    if ((st = forward_store(as[i], nsteps[i], budget))) return st;
+  }
+  std::vector<FwState> f(n);
+  for (int i = 0; i < n; i++)
+    if ((st = forward_start(as[i], f[i], nsteps[i], dt0[i]))) return st;
+  GroupClock clk;
+  cudaError_t ce = group_begin(clk, n, as);
+  std::vector<char> issued(n, 0);
+  for (bool any = ce == cudaSuccess; any;) {
+    any = false;
+    for (int i = 0; i < n; i++) {
+      issued[i] = 0;
+      if (!f[i].active) continue;
+      if ((st = forward_issue(as[i], f[i]))) {
+        f[i].status = st;
+        f[i].active = false;
+        continue;
+      }
+      issued[i] = 1;
+    }
+    for (int i = 0; i < n; i++) {
+      if (!issued[i]) continue;
+      forward_finish(as[i], f[i]);
+      any = any || f[i].active;
+    }
+  }
+  if (ce == cudaSuccess) ce = group_end(clk, n, as, ms);
+  group_free(clk);
+  if (ce != cudaSuccess) return afail(as[0], ce, "mhd_adj_forward_group");
+  int first = MHD_OK;
+  for (int i = 0; i < n; i++) {
+    as[i]->ms_forward = ms ? *ms : 0.0;
+    st = forward_end(as[i], f[i], J ? &J[i] : nullptr);
+    if (st && first == MHD_OK) first = st;
+  }
+  return first;
+}
+
+int mhd_adj_backward_group(int n, mhd_adj* const* as, double* ms) {
+  int st = group_check(n, as);
+  if (st) return st;
+  for (int i = 0; i < n; i++)
+    if ((st = check_ready(as[i]))) return st;
+  for (int i = 0; i < n; i++)
+    if ((st = backward_prepare(as[i]))) return st;
+  GroupClock clk;
+  cudaError_t ce = group_begin(clk, n, as);
+  std::vector<BwState> b(n);
+  for (int i = 0; i < n && ce == cudaSuccess; i++)
+    if ((st = backward_start(as[i], b[i]))) return st;
+  // one unit (a replayed stage or a stage adjoint) per member per round
+  for (bool any = ce == cudaSuccess; any;) {
+    any = false;
+    for (int i = 0; i < n; i++) {
+      if (b[i].phase == BwState::DONE) continue;
+      if ((st = backward_issue(as[i], b[i]))) return st;
+      any = true;
+    }
+  }
+  double gms = 0.0;
+  if (ce == cudaSuccess) ce = group_end(clk, n, as, &gms);
+  group_free(clk);
+  if (ce != cudaSuccess) return afail(as[0], ce, "mhd_adj_backward_group");
+  if ((ce = cudaGetLastError()) != cudaSuccess) return afail(as[0], ce, "mhd_adj_backward_group");
+  for (int i = 0; i < n; i++) {
+    as[i]->ms_backward = gms;
+    as[i]->have_grad = true;
+    aset(as[i], MHD_OK, false, "");
+  }
+  if (ms) *ms = gms;
+  return MHD_OK;
 }
 
 int mhd_adj_replay(mhd_adj* a, const double* U0, double* J) {
   if (!a) return MHD_ERR_WRONG_PARAMETER;
-  int st = check_ready(a);
+  int st = check_replay(a);
   if (st) return st;
   AK(cudaSetDevice(a->device));
   const Grid& g = a->g;
@@ -1167,7 +1584,7 @@ int mhd_adj_replay(mhd_adj* a, const double* U0, double* J) {
 
 int mhd_adj_replay_problem(mhd_adj* a, int kind, const double* p, int np, double* J) {
   if (!a) return MHD_ERR_WRONG_PARAMETER;
-  int st = check_ready(a);
+  int st = check_replay(a);
   if (st) return st;
   AK(cudaSetDevice(a->device));
   ProblemArgs pa{};
@@ -1193,66 +1610,19 @@ int mhd_adj_backward(mhd_adj* a) {
   if (!a) return MHD_ERR_WRONG_PARAMETER;
   int st = check_ready(a);
   if (st) return st;
-  AK(cudaSetDevice(a->device));
-  const Grid& g = a->g;
-  a->cur_snap = a->snap;
-  // the largest replayed segment sizes the replay buffers
-  const int nseg = a->nseg;
-  auto kept = [&](int q, int s0, int s1) {
-    return q >= a->store_seg0 && a->store_first >= 0 && s0 >= a->store_first &&
-           size_t(s1 - a->store_first) <= a->store_slots;
-  };
-  int maxst = 0;
-  for (int q = 0; q < nseg; q++) {
-    const int s0 = a->step_stage[q * a->K];
-    const int s1 = a->step_stage[std::min((q + 1) * a->K, a->steps)];
-    if (!kept(q, s0, s1)) maxst = std::max(maxst, s1 - s0);
-  }
-  while ((int)a->seg.size() < maxst) {
-    double* p = nullptr;
-    AK(cudaMalloc(&p, a->blk * sizeof(double)));
-    a->seg.push_back(p);
-  }
+  if ((st = backward_prepare(a))) return st;
   cudaEvent_t e0, e1;
   AK(cudaEventCreate(&e0));
   AK(cudaEventCreate(&e1));
   AK(cudaEventRecord(e0, a->stream));
-  for (double* p : {a->lU, a->lU1, a->lU2, a->T})
-    AK(cudaMemsetAsync(p, 0, a->blk * sizeof(double), a->stream));
-  for (int side = 0; side < 4; side++)
-    AK(cudaMemsetAsync(a->lsnap[side], 0, sizeof(double) * NF * std::max(g.NX, g.NY), a->stream));
-  dim3 sgrid((g.ny + 255) / 256, g.nx);
-  ka_seed<<<sgrid, 256, 0, a->stream>>>(g, a->Ufinal, a->lU, g.dx * g.dy);
-  a->launches++;
-  a->replayed_segments = 0;
-  for (int q = nseg - 1; q >= 0; q--) {
-    const int s0 = a->step_stage[q * a->K];
-    const int s1 = a->step_stage[std::min((q + 1) * a->K, a->steps)];
-    const bool from_store = kept(q, s0, s1);
-    if (!from_store) {
-      AK(cudaMemcpyAsync(a->U, a->ckpt[q], a->blk * sizeof(double), cudaMemcpyDeviceToDevice,
-                         a->stream));
-      if ((st = reset_ctl(a))) return st;
-      replay_stages(a, s0, s1, true);
-      a->replayed_segments++;
-    }
-    for (int s = s1 - 1; s >= s0; s--) {
-      const StageRec& r = a->log[s];
-      const double* X = from_store ? a->store + size_t(s - a->store_first) * a->blk
-                                   : a->seg[s - s0];
-      adjoint_stage(a, s, r, X);
-    }
-  }
-  for (int side = 0; side < 4; side++) {
-    if (g.bc[side] != DIRICHLET) continue;
-    const int nb = (side < 2) ? g.ny : g.nx;
-    ka_snap_adj<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, a->lsnap[side], a->lU);
-    a->launches++;
-  }
+  BwState b;
+  if ((st = backward_start(a, b))) return st;
+  while (b.phase != BwState::DONE)
+    if ((st = backward_issue(a, b))) return st;
   AK(cudaEventRecord(e1, a->stream));
   AK(cudaEventSynchronize(e1));
   AK(cudaGetLastError());
-  timed_ms(e0, e1, &a->ms_backward);
+  timed_ms(e0, e1, &a->ms_backward);  // destroys e0, e1
   a->have_grad = true;
   return aset(a, MHD_OK, false, "");
 }

@@ -142,6 +142,7 @@ def library():
                            C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(vp)],
         "mhd_adj_destroy": [vp],
         "mhd_adj_set_store": [vp, C.c_longlong],
+        "mhd_adj_set_masks": [vp, C.c_int],
         "mhd_adj_last_error": [vp, C.c_char_p, C.c_size_t, _ip],
         "mhd_adj_upload": [vp, _dp],
         "mhd_adj_init_problem": [vp, C.c_int, _dp, C.c_int],
@@ -153,6 +154,10 @@ def library():
         "mhd_adj_sheet_gradient": [vp, C.c_double, C.c_double, C.c_int, _dp],
         "mhd_adj_download": [vp, C.c_int, _dp],
         "mhd_adj_info": [vp, C.POINTER(AdjStats)],
+        "mhd_adj_forward_group": [C.c_int, C.POINTER(vp), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)],
+        "mhd_adj_backward_group": [C.c_int, C.POINTER(vp), C.POINTER(C.c_double)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -58,6 +58,10 @@ class Adjoint:
         """Device memory for kept stage inputs (-1 automatic, 0 none: replay every segment)."""
         self._check(self.lib.mhd_adj_set_store(self.h, int(max_bytes)), "set_store")
 
+    def set_masks(self, keep_all=True):
+        """Keep the ENO codes of every stage (True) or of stored stages only."""
+        self._check(self.lib.mhd_adj_set_masks(self.h, 1 if keep_all else 0), "set_masks")
+
     # -- initial state ---------------------------------------------------------------
     def upload(self, U0):
         self._check(self.lib.mhd_adj_upload(self.h, _p(np.ascontiguousarray(U0))), "upload")
@@ -120,3 +124,44 @@ class Adjoint:
         s = AdjStats()
         self._check(self.lib.mhd_adj_info(self.h, C.byref(s)), "info")
         return {f: getattr(s, f) for f, _ in AdjStats._fields_}
+
+
+def _group_handles(adjs):
+    hs = (C.c_void_p * len(adjs))(*[a.h for a in adjs])
+    return hs
+
+
+def _group_error(adjs, st, what):
+    for a in adjs:
+        buf = C.create_string_buffer(1024)
+        e = C.c_int(0)
+        a.lib.mhd_adj_last_error(a.h, buf, 1024, C.byref(e))
+        if e.value:
+            raise MhdError(f"{what}: {STATUS_NAMES.get(st, st)} {buf.value.decode()}")
+    raise MhdError(f"{what}: {STATUS_NAMES.get(st, st)}")
+
+
+def forward_group(adjs, nsteps, dt0):
+    """Recording forwards of several Adjoint objects at once (mhd_adj_forward_group).
+    nsteps, dt0: one value or one per object.  Returns (list of J, device ms)."""
+    n = len(adjs)
+    lib = library()
+    ns = np.broadcast_to(np.asarray(nsteps, dtype=np.int32), (n,)).copy()
+    d0 = np.broadcast_to(np.asarray(dt0, dtype=np.float64), (n,)).copy()
+    J = np.zeros(n)
+    ms = C.c_double(0.0)
+    st = lib.mhd_adj_forward_group(n, _group_handles(adjs), ns.ctypes.data_as(C.POINTER(C.c_int)),
+                                   _p(d0), _p(J), C.byref(ms))
+    if st != OK:
+        _group_error(adjs, st, "forward_group")
+    return [float(x) for x in J], ms.value
+
+
+def backward_group(adjs):
+    """Reverse sweeps of several recorded Adjoint objects at once.  Returns device ms."""
+    lib = library()
+    ms = C.c_double(0.0)
+    st = lib.mhd_adj_backward_group(len(adjs), _group_handles(adjs), C.byref(ms))
+    if st != OK:
+        _group_error(adjs, st, "backward_group")
+    return ms.value

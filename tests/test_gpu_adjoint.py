@@ -147,17 +147,30 @@ def test_checkpoint_interval_does_not_change_the_gradient():
 def test_stage_store_keeps_the_last_segments():
     p = P.random_blocky(24, 16, seed=8, bc=(M.PERIODIC, M.PERIODIC, M.NEUMANN, M.NEUMANN))
     grads, infos = [], []
-    # a 2 MB store holds the stage inputs (86 KB each here) of the last segment only
-    for store in (0, 2 << 20, -1):
-        a, _ = _adjoint(p, 7, K=3, store=store)
-        a.backward()
-        grads.append(a.gradient())
-        infos.append(a.info())
-    assert infos[0]["stored_stages"] == 0 and infos[0]["replayed_segments"] == 3
-    assert 0 < infos[1]["stored_stages"] < infos[1]["stages"]
-    assert 0 < infos[1]["replayed_segments"] < 3
-    assert infos[2]["stored_stages"] == infos[2]["stages"] and infos[2]["replayed_segments"] == 0
-    assert same(grads[0], grads[1]) and same(grads[0], grads[2])
+    # a 2 MB store holds the stage inputs (86 KB each here) of the last segment only;
+    # without kept masks the replayed segments record their ENO codes again
+    for keep_masks in (True, False):
+        for store in (0, 2 << 20, -1):
+            a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-9, dt_max=0.01,
+                        checkpoint_every=3)
+            a.set_masks(keep_masks)
+            a.set_store(store)
+            a.upload(p.U)
+            a.forward(7, 1e-3)
+            a.backward()
+            grads.append(a.gradient())
+            infos.append(a.info())
+            if not keep_masks:
+                with pytest.raises(M.MhdError):
+                    a.replay()
+    for off in (0, 3):
+        assert infos[off]["stored_stages"] == 0 and infos[off]["replayed_segments"] == 3
+        assert 0 < infos[off + 1]["stored_stages"] < infos[off + 1]["stages"]
+        assert 0 < infos[off + 1]["replayed_segments"] < 3
+        assert infos[off + 2]["stored_stages"] == infos[off + 2]["stages"]
+        assert infos[off + 2]["replayed_segments"] == 0
+    for g in grads[1:]:
+        assert same(grads[0], g)
 
 
 def test_retry_steps_and_euler_match_tangent_linear():
@@ -179,6 +192,14 @@ def test_retry_steps_and_euler_match_tangent_linear():
     a0, _ = _adjoint(p, n, store=0, **kw)  # the retried stages replayed from checkpoints
     a0.backward()
     assert same(a0.gradient(), g)
+    a1 = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=kw["dt_min"], dt_max=kw["dt_max"],
+                 cfl=kw["cfl"], checkpoint_every=4)
+    a1.set_masks(False)  # ... with their masks recorded again by the replays
+    a1.set_store(0)
+    a1.upload(p.U)
+    a1.forward(n, kw["dt0"])
+    a1.backward()
+    assert same(a1.gradient(), g)
     pe = P.random_smooth(20, 20, seed=13)
     a, J = _adjoint(pe, 5, tm=M.EULER)
     a.backward()
@@ -234,3 +255,38 @@ def test_autograd_function_wrapper():
     fd = (a.replay(p.U + h * d) - a.replay(p.U - h * d)) / (2 * h)
     adj = float((U0.grad.numpy() * d).sum())
     assert abs(fd - adj) <= 1e-6 * abs(adj)
+
+
+def test_group_forward_and_backward_match_separate_runs():
+    from mhd2d_b200.adjoint import backward_group, forward_group
+    probs = [P.plasma_sheet(32, 16, np.random.default_rng(3).normal(0, 1e-2, 6)),
+             P.random_smooth(24, 20, seed=2),
+             P.random_blocky(20, 20, seed=6, bc=(M.NEUMANN,) * 4),
+             P.random_smooth(22, 18, seed=4, bc=(M.DIRICHLET, M.NEUMANN, M.NEUMANN, M.OPEN))]
+    nsteps = [7, 5, 6, 4]
+    setups = [(True, -1), (False, 0), (False, 2 << 20), (True, 0)]  # (keep masks, store)
+
+    def make(i):
+        p = probs[i]
+        a = Adjoint(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, dt_min=1e-9, dt_max=0.01,
+                    checkpoint_every=3)
+        a.set_masks(setups[i][0])
+        a.set_store(setups[i][1])
+        a.upload(p.U)
+        return a
+
+    solo = []
+    for i in range(len(probs)):
+        a = make(i)
+        J = a.forward(nsteps[i], 1e-3)
+        a.backward()
+        solo.append((J, a.gradient(), a.download(1)))
+    group = [make(i) for i in range(len(probs))]
+    Js, ms_f = forward_group(group, nsteps, 1e-3)
+    ms_b = backward_group(group)
+    assert ms_f > 0 and ms_b > 0
+    for i, a in enumerate(group):
+        assert Js[i] == solo[i][0]
+        assert same(a.download(1), solo[i][2])
+        assert same(a.gradient(), solo[i][1])
+        assert a.info()["steps"] == nsteps[i]
