@@ -261,18 +261,17 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
       for (int m = 0; m < NF; m++) { l[m] = 0.0; r[m] = 0.0; }
       lv_row(e0, G, k, l);
       rv_row(e0, G, k, r);
-      double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;  // frozen ENO combination of the 4 points
-      if (up == 0) {
-        if (code & 1u) { c0 = -0.5; c1 = 1.5; } else { c1 = 0.5; c2 = 0.5; }
-      } else {
-        if (code & 2u) { c1 = 0.5; c2 = 0.5; } else { c2 = 1.5; c3 = -0.5; }
-      }
+      // frozen ENO combination: ca * F[pa] + cb * F[pa + 1] (the other two points have
+      // weight 0)
+      const int pa = up == 0 ? ((code & 1u) ? 0 : 1) : ((code & 2u) ? 1 : 2);
+      const double ca = pa == 0 ? -0.5 : (pa == 1 ? 0.5 : 1.5);
+      const double cb = pa == 0 ? 1.5 : (pa == 1 ? 0.5 : -0.5);
       double phi[NF], fw = 0.0, gk = 0.0;
 #pragma unroll
       for (int m = 0; m < NF; m++) {
         if (m == 4) { phi[m] = 0.0; continue; }
         const int s = slot_of(m);
-        phi[m] = c0 * sF[s][tid] + c1 * sF[7 + s][tid] + c2 * sF[14 + s][tid] + c3 * sF[21 + s][tid];
+        phi[m] = ca * sF[7 * pa + s][tid] + cb * sF[7 * pa + 7 + s][tid];
         fw += l[m] * phi[m];
       }
 #pragma unroll
@@ -293,10 +292,8 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
           if (m == 4) continue;
           const int s = slot_of(m);
           const double v = gk * l[m];
-          sFb[s][tid] += c0 * v;
-          sFb[7 + s][tid] += c1 * v;
-          sFb[14 + s][tid] += c2 * v;
-          sFb[21 + s][tid] += c3 * v;
+          sFb[7 * pa + s][tid] += ca * v;
+          sFb[7 * pa + 7 + s][tid] += cb * v;
         }
       }
     }
@@ -975,7 +972,10 @@ int plan_store(mhd_adj* a, int nsteps, int nseg, int per_step, long long budget)
   AK(cudaMemGetInfo(&free_b, &total_b));
   const size_t seg_need = size_t(per_step) * a->K + 2;
   const size_t seg_missing = seg_need > a->seg.size() ? seg_need - a->seg.size() : 0;
-  const size_t reserve = seg_missing * (a->blk * sizeof(double) + mask_b) + (size_t(2) << 30);
+  const size_t seg_masks_missing =
+      !a->keep_masks && seg_need > size_t(a->seg_mask_slots) ? seg_need - a->seg_mask_slots : 0;
+  const size_t reserve =
+      seg_missing * a->blk * sizeof(double) + seg_masks_missing * mask_b + (size_t(2) << 30);
   size_t avail = free_b + have > reserve ? free_b + have - reserve : 0;
   if (a->store_limit > 0) avail = std::min(avail, size_t(a->store_limit));
   if (budget >= 0) avail = std::min(avail, size_t(budget));
@@ -1016,12 +1016,22 @@ int forward_prepare(mhd_adj* a, int nsteps) {
   a->have_grad = false;
   a->cur_snap = a->snap;
   a->nseg = (nsteps + a->K - 1) / a->K;
+  const int per_step = a->time_method == 2 ? 3 : 1;
+  const int chunks_needed =
+      a->keep_masks ? (per_step * nsteps + 8 + kSlotsPerChunk - 1) / kSlotsPerChunk : 0;
+  if (a->store && ((int)a->ckpt.size() < a->nseg || (int)a->chunks.size() < chunks_needed)) {
+    // the store is sized last, from what is left: give its memory back first
+    AK(cudaStreamSynchronize(a->stream));
+    cudaFree(a->store);
+    a->store = nullptr;
+    a->store_slots = 0;
+  }
   while ((int)a->ckpt.size() < a->nseg) {
     double* c = nullptr;
     AK(cudaMalloc(&c, a->blk * sizeof(double)));
     a->ckpt.push_back(c);
   }
-  if (a->keep_masks) return ensure_slots(a, (a->time_method == 2 ? 3 : 1) * nsteps + 8);
+  if (a->keep_masks) return ensure_slots(a, per_step * nsteps + 8);
   return MHD_OK;
 }
 
@@ -1461,7 +1471,9 @@ int mhd_adj_forward_group(int n, mhd_adj* const* as, const int* nsteps, const do
     const size_t slot_b =
         a->blk * sizeof(double) + (a->keep_masks ? 0 : a->slot_words * sizeof(unsigned));
     const size_t seg_need = size_t(per_step) * a->K + 2;
-    if (seg_need > a->seg.size()) reserve += (seg_need - a->seg.size()) * slot_b;
+    if (seg_need > a->seg.size()) reserve += (seg_need - a->seg.size()) * a->blk * sizeof(double);
+    if (!a->keep_masks && seg_need > size_t(a->seg_mask_slots))
+      reserve += (seg_need - a->seg_mask_slots) * a->slot_words * sizeof(unsigned);
     if (a->store_limit != 0) {
       cudaFree(a->store);
       a->store = nullptr;
