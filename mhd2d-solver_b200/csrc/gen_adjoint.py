@@ -20,6 +20,7 @@ taken as 0 at v = 0, the one-sided convention of a frozen branch (it only
 arises where the forward value is exactly zero, e.g. B_x = 0).
 """
 import ast
+import re
 import sys
 
 # --------------------------------------------------------------------------
@@ -30,7 +31,32 @@ def _src(node):
     return ast.unparse(node)
 
 
-def _rev(node, seed, out):
+class Rcp:
+    """Reciprocals of the denominators met in one reverse sweep: each distinct
+    denominator is divided once (rcpN = 1 / d) and the adjoints multiply."""
+
+    def __init__(self, prefix="rcp"):
+        self.map = {}
+        self.known = set()  # names that already hold the reciprocal
+        self.prefix = prefix
+
+    def name(self, src):
+        if src not in self.map:
+            self.map[src] = f"{self.prefix}{len(self.map)}"
+        return self.map[src]
+
+    def alias(self, src, name):
+        """`name` is 1 / src already (a statement t = 1.0 / (src))."""
+        self.map[src] = name
+        self.known.add(name)
+
+    def defs(self, indent, names=None):
+        return [f"{indent}[[maybe_unused]] const double {n} = "
+                f"1.0 / ({c_expr(src, names) if names else src});"
+                for src, n in self.map.items() if n not in self.known]
+
+
+def _rev(node, seed, out, rcp=None):
     """Append (variable, coefficient * seed) pairs for the leaves of `node`."""
     if isinstance(node, ast.Name):
         out.append((node.id, seed))
@@ -38,36 +64,41 @@ def _rev(node, seed, out):
         pass
     elif isinstance(node, ast.UnaryOp):
         if isinstance(node.op, ast.USub):
-            _rev(node.operand, f"-({seed})", out)
+            _rev(node.operand, f"-({seed})", out, rcp)
         elif isinstance(node.op, ast.UAdd):
-            _rev(node.operand, seed, out)
+            _rev(node.operand, seed, out, rcp)
         else:
             raise ValueError(ast.dump(node))
     elif isinstance(node, ast.BinOp):
         a, b = node.left, node.right
         if isinstance(node.op, ast.Add):
-            _rev(a, seed, out)
-            _rev(b, seed, out)
+            _rev(a, seed, out, rcp)
+            _rev(b, seed, out, rcp)
         elif isinstance(node.op, ast.Sub):
-            _rev(a, seed, out)
-            _rev(b, f"-({seed})", out)
+            _rev(a, seed, out, rcp)
+            _rev(b, f"-({seed})", out, rcp)
         elif isinstance(node.op, ast.Mult):
-            _rev(a, f"({seed}) * ({_src(b)})", out)
-            _rev(b, f"({seed}) * ({_src(a)})", out)
+            _rev(a, f"({seed}) * ({_src(b)})", out, rcp)
+            _rev(b, f"({seed}) * ({_src(a)})", out, rcp)
         elif isinstance(node.op, ast.Div):
-            _rev(a, f"({seed}) / ({_src(b)})", out)
-            _rev(b, f"-({seed}) * ({_src(a)}) / (({_src(b)}) * ({_src(b)}))", out)
+            if rcp is None:
+                _rev(a, f"({seed}) / ({_src(b)})", out, rcp)
+                _rev(b, f"-({seed}) * ({_src(a)}) / (({_src(b)}) * ({_src(b)}))", out, rcp)
+            else:
+                r = rcp.name(_src(b))
+                _rev(a, f"({seed}) * {r}", out, rcp)
+                _rev(b, f"-({seed}) * ({_src(a)}) * {r} * {r}", out, rcp)
         else:
             raise ValueError(ast.dump(node))
     elif isinstance(node, ast.Call) and node.func.id == "sqrt":
-        _rev(node.args[0], f"({seed}) * inv2sqrt({_src(node.args[0])})", out)
+        _rev(node.args[0], f"({seed}) * inv2sqrt({_src(node.args[0])})", out, rcp)
     else:
         raise ValueError(ast.dump(node))
 
 
-def reverse_of(expr, seed):
+def reverse_of(expr, seed, rcp=None):
     out = []
-    _rev(ast.parse(expr, mode="eval").body, seed, out)
+    _rev(ast.parse(expr, mode="eval").body, seed, out, rcp)
     return out
 
 
@@ -309,13 +340,15 @@ def emit_pairs():
     o.append("  switch (pi) {")
     for pi, (k, k2, A, B, C, D) in enumerate(PAIRS):
         o.append(f"    case {pi}: {{  // rows {k} and {k2}")
+        rcp = Rcp()
+        body = []
         for table, seed_of in ((A, lambda m: f"LS[{m if m < 4 else m - 1}]"),
                                (B, lambda m: f"LD[{m if m < 4 else m - 1}]"),
                                (C, lambda m: f"rs{m}"), (D, lambda m: f"rd{m}")):
             for m, expr in sorted(table.items()):
                 seed = seed_of(m)
                 lines = []
-                for var, coef in reverse_of(expr, seed):
+                for var, coef in reverse_of(expr, seed, rcp):
                     if var in CONSTS:
                         continue
                     assert var in MID_FIELDS, var
@@ -325,14 +358,16 @@ def emit_pairs():
                     continue
                 if seed.startswith("rs") or seed.startswith("rd"):
                     src = "fS" if seed.startswith("rs") else "fD"
-                    o.append(f"      {{ const double {seed} = {src} * lF[{m}];")
-                    o.append(f"      if ({seed} != 0.0) {{")
-                    o.extend(lines)
-                    o.append("      } }")
+                    body.append(f"      {{ const double {seed} = {src} * lF[{m}];")
+                    body.append(f"      if ({seed} != 0.0) {{")
+                    body.extend(lines)
+                    body.append("      } }")
                 else:
-                    o.append(f"      if ({seed} != 0.0) {{")
-                    o.extend(lines)
-                    o.append("      }")
+                    body.append(f"      if ({seed} != 0.0) {{")
+                    body.extend(lines)
+                    body.append("      }")
+        o.extend(rcp.defs("      ", MID_NAMES))
+        o.extend(body)
         o.append("      break;")
         o.append("    }")
     o.append("    default:")
@@ -342,8 +377,11 @@ def emit_pairs():
     return o
 
 
-def emit_program(name, decl, stmts, inputs, prologue, seeds, epilogue):
-    """Forward sweep (values, frozen-branch flags) then reverse sweep."""
+def emit_program(name, decl, stmts, inputs, prologue, seeds, epilogue, subst=None):
+    """Forward sweep (values, frozen-branch flags) then reverse sweep.  subst
+    maps a target to an expression that already holds its (final) value; its
+    frozen flag, if any, must not depend on the target itself."""
+    subst = subst or {}
     o = [f"__device__ __forceinline__ void {name}({', '.join(decl)}) {{"]
     o.extend(prologue)
     targets = []
@@ -353,28 +391,45 @@ def emit_program(name, decl, stmts, inputs, prologue, seeds, epilogue):
             continue
         t, expr = st[0], st[1]
         targets.append(t)
+        if t in subst:
+            o.append(f"  [[maybe_unused]] double {t} = {subst[t]};")
+            if len(st) > 2:
+                assert not re.search(r"\b" + t + r"\b", st[2]), t
+                o.append(f"  const bool {t}_fz = {st[2]};")
+            continue
         o.append(f"  [[maybe_unused]] double {t} = {expr};")
         if len(st) > 2:
             o.append(f"  const bool {t}_fz = {st[2]};")
             o.append(f"  if ({t}_fz) {t} = {st[3]};")
-    o.append("  // reverse sweep")
-    for v in targets + inputs:
-        o.append(f"  double {v}_b = 0.0;")
-    o.extend(seeds)
+    rcp = Rcp()
+    for st in stmts:
+        if st[0] == "#":
+            continue
+        node = ast.parse(st[1], mode="eval").body
+        if (isinstance(node, ast.BinOp) and isinstance(node.op, ast.Div)
+                and isinstance(node.left, ast.Constant) and node.left.value == 1.0):
+            rcp.alias(_src(node.right), st[0])
+    rev = []
     for st in reversed(stmts):
         if st[0] == "#":
             continue
         t, expr = st[0], st[1]
         lines = []
-        for var, coef in reverse_of(expr, f"{t}_b"):
+        for var, coef in reverse_of(expr, f"{t}_b", rcp):
             if var in CONSTS:
                 continue
             lines.append(f"    {var}_b += {coef};")
         if not lines:
             continue
-        o.append(f"  if (!{t}_fz && {t}_b != 0.0) {{" if len(st) > 2 else f"  if ({t}_b != 0.0) {{")
-        o.extend(lines)
-        o.append("  }")
+        rev.append(f"  if (!{t}_fz && {t}_b != 0.0) {{" if len(st) > 2 else f"  if ({t}_b != 0.0) {{")
+        rev.extend(lines)
+        rev.append("  }")
+    o.append("  // reverse sweep (one division per distinct denominator)")
+    o.extend(rcp.defs("  "))
+    for v in targets + inputs:
+        o.append(f"  double {v}_b = 0.0;")
+    o.extend(seeds)
+    o.extend(rev)
     o.extend(epilogue)
     o.append("}")
     return o
@@ -393,7 +448,13 @@ def emit_mid():
         seeds.append(f"  {f}_b += mb.{field};")
     epi = ["  " + " ".join(f"U1b[{k}] += {MID_INPUTS[k]}_b;" for k in range(8)),
            "  " + " ".join(f"U2b[{k}] += {MID_INPUTS[8 + k]}_b;" for k in range(8))]
-    return emit_program("midpoint_adjoint", decl, MID, MID_INPUTS, pro, seeds, epi)
+    # the midpoint scalars the forward already holds in e (bit-identical
+    # arithmetic); frozen statements whose flag needs their raw value are
+    # recomputed
+    subst = {f: f"e.{'as' if f == 'as_' else f}" for f in
+             ("u", "v", "w", "uu", "a", "ca2", "ca", "cs", "cf", "rr", "af", "as_", "bty", "btz",
+              "th1", "th2", "vb")}
+    return emit_program("midpoint_adjoint", decl, MID, MID_INPUTS, pro, seeds, epi, subst)
 
 
 def emit_flux():
@@ -420,7 +481,7 @@ def main():
     o.append("")
     o.append("// d sqrt(v) / dv, 0 at v = 0 (frozen one-sided branch)")
     o.append("__device__ __forceinline__ double inv2sqrt(double v) {")
-    o.append("  return v > 0.0 ? 0.5 / sqrt(v) : 0.0;")
+    o.append("  return v > 0.0 ? 0.5 * rsqrt(v) : 0.0;")
     o.append("}")
     o.append("")
     o.append("// Adjoints of the Mid scalars.")

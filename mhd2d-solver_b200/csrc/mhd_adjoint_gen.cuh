@@ -9,7 +9,7 @@ namespace MHD_KNS {
 
 // d sqrt(v) / dv, 0 at v = 0 (frozen one-sided branch)
 __device__ __forceinline__ double inv2sqrt(double v) {
-  return v > 0.0 ? 0.5 / sqrt(v) : 0.0;
+  return v > 0.0 ? 0.5 * rsqrt(v) : 0.0;
 }
 
 // Adjoints of the Mid scalars.
@@ -29,6 +29,8 @@ __device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
   (void)fcf; (void)fcs; (void)sb;
   switch (pi) {
     case 0: {  // rows 0 and 6
+      [[maybe_unused]] const double rcp0 = 1.0 / (e.rr);
+      [[maybe_unused]] const double rcp1 = 1.0 / (G.g1);
       if (LS[0] != 0.0) {
         mb.th1 += LS[0] * fcf * e.uu * e.a2 * e.af * 0.25;
         mb.af += LS[0] * fcf * e.uu * e.a2 * (0.25 * e.th1);
@@ -123,24 +125,24 @@ __device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
       } }
       { const double rs5 = fS * lF[5];
       if (rs5 != 0.0) {
-        mb.as += rs5 * fcf / e.rr * e.cf * e.bty;
-        mb.bty += rs5 * fcf / e.rr * e.cf * e.as;
-        mb.cf += rs5 * fcf / e.rr * (e.as * e.bty);
-        mb.rr += -(rs5 * fcf) * (e.as * e.bty * e.cf) / (e.rr * e.rr);
+        mb.as += rs5 * fcf * rcp0 * e.cf * e.bty;
+        mb.bty += rs5 * fcf * rcp0 * e.cf * e.as;
+        mb.cf += rs5 * fcf * rcp0 * (e.as * e.bty);
+        mb.rr += -(rs5 * fcf) * (e.as * e.bty * e.cf) * rcp0 * rcp0;
       } }
       { const double rs6 = fS * lF[6];
       if (rs6 != 0.0) {
-        mb.as += rs6 * fcf / e.rr * e.cf * e.btz;
-        mb.btz += rs6 * fcf / e.rr * e.cf * e.as;
-        mb.cf += rs6 * fcf / e.rr * (e.as * e.btz);
-        mb.rr += -(rs6 * fcf) * (e.as * e.btz * e.cf) / (e.rr * e.rr);
+        mb.as += rs6 * fcf * rcp0 * e.cf * e.btz;
+        mb.btz += rs6 * fcf * rcp0 * e.cf * e.as;
+        mb.cf += rs6 * fcf * rcp0 * (e.as * e.btz);
+        mb.rr += -(rs6 * fcf) * (e.as * e.btz * e.cf) * rcp0 * rcp0;
       } }
       { const double rs7 = fS * lF[7];
       if (rs7 != 0.0) {
         mb.af += rs7 * fcf * e.uu * 0.5;
         mb.uu += rs7 * fcf * (0.5 * e.af);
-        mb.af += rs7 * fcf / G.g1 * e.cf2;
-        mb.cf2 += rs7 * fcf / G.g1 * e.af;
+        mb.af += rs7 * fcf * rcp1 * e.cf2;
+        mb.cf2 += rs7 * fcf * rcp1 * e.af;
         mb.af += rs7 * fcf * (e.cf2 - e.a2) * G.g21;
         mb.cf2 += rs7 * fcf * (G.g21 * e.af);
         mb.a2 += -(rs7 * fcf * (G.g21 * e.af));
@@ -174,6 +176,8 @@ __device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
       break;
     }
     case 1: {  // rows 2 and 4
+      [[maybe_unused]] const double rcp0 = 1.0 / (e.cf * e.rr);
+      [[maybe_unused]] const double rcp1 = 1.0 / (G.g1);
       if (LS[0] != 0.0) {
         mb.th1 += LS[0] * fcs * e.uu * e.cf2 * e.as * 0.25;
         mb.as += LS[0] * fcs * e.uu * e.cf2 * (0.25 * e.th1);
@@ -268,26 +272,26 @@ __device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
       } }
       { const double rs5 = fS * lF[5];
       if (rs5 != 0.0) {
-        mb.af += -(rs5 * fcs / (e.cf * e.rr) * e.a2 * e.bty);
-        mb.bty += rs5 * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-        mb.a2 += rs5 * fcs / (e.cf * e.rr) * (-e.af * e.bty);
-        mb.cf += -(rs5 * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-        mb.rr += -(rs5 * fcs) * (-e.af * e.bty * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+        mb.af += -(rs5 * fcs * rcp0 * e.a2 * e.bty);
+        mb.bty += rs5 * fcs * rcp0 * e.a2 * -e.af;
+        mb.a2 += rs5 * fcs * rcp0 * (-e.af * e.bty);
+        mb.cf += -(rs5 * fcs) * (-e.af * e.bty * e.a2) * rcp0 * rcp0 * e.rr;
+        mb.rr += -(rs5 * fcs) * (-e.af * e.bty * e.a2) * rcp0 * rcp0 * e.cf;
       } }
       { const double rs6 = fS * lF[6];
       if (rs6 != 0.0) {
-        mb.af += -(rs6 * fcs / (e.cf * e.rr) * e.a2 * e.btz);
-        mb.btz += rs6 * fcs / (e.cf * e.rr) * e.a2 * -e.af;
-        mb.a2 += rs6 * fcs / (e.cf * e.rr) * (-e.af * e.btz);
-        mb.cf += -(rs6 * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.rr;
-        mb.rr += -(rs6 * fcs) * (-e.af * e.btz * e.a2) / (e.cf * e.rr * (e.cf * e.rr)) * e.cf;
+        mb.af += -(rs6 * fcs * rcp0 * e.a2 * e.btz);
+        mb.btz += rs6 * fcs * rcp0 * e.a2 * -e.af;
+        mb.a2 += rs6 * fcs * rcp0 * (-e.af * e.btz);
+        mb.cf += -(rs6 * fcs) * (-e.af * e.btz * e.a2) * rcp0 * rcp0 * e.rr;
+        mb.rr += -(rs6 * fcs) * (-e.af * e.btz * e.a2) * rcp0 * rcp0 * e.cf;
       } }
       { const double rs7 = fS * lF[7];
       if (rs7 != 0.0) {
         mb.as += rs7 * fcs * e.uu * 0.5;
         mb.uu += rs7 * fcs * (0.5 * e.as);
-        mb.as += rs7 * fcs / G.g1 * e.cs2;
-        mb.cs2 += rs7 * fcs / G.g1 * e.as;
+        mb.as += rs7 * fcs * rcp1 * e.cs2;
+        mb.cs2 += rs7 * fcs * rcp1 * e.as;
         mb.as += rs7 * fcs * (e.cs2 - e.a2) * G.g21;
         mb.cs2 += rs7 * fcs * (G.g21 * e.as);
         mb.a2 += -(rs7 * fcs * (G.g21 * e.as));
@@ -321,6 +325,7 @@ __device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
       break;
     }
     case 2: {  // rows 1 and 5
+      [[maybe_unused]] const double rcp0 = 1.0 / (e.rr);
       if (LS[4] != 0.0) {
         mb.btz += LS[4] * e.rr * 0.5;
         mb.rr += LS[4] * (0.5 * e.btz);
@@ -343,13 +348,13 @@ __device__ __forceinline__ void pair_adjoint(const Mid& e, const Gas& G, int pi,
       }
       { const double rs5 = fS * lF[5];
       if (rs5 != 0.0) {
-        mb.btz += rs5 / e.rr;
-        mb.rr += -rs5 * e.btz / (e.rr * e.rr);
+        mb.btz += rs5 * rcp0;
+        mb.rr += -rs5 * e.btz * rcp0 * rcp0;
       } }
       { const double rs6 = fS * lF[6];
       if (rs6 != 0.0) {
-        mb.bty += -(rs6 / e.rr);
-        mb.rr += -rs6 * -e.bty / (e.rr * e.rr);
+        mb.bty += -(rs6 * rcp0);
+        mb.rr += -rs6 * -e.bty * rcp0 * rcp0;
       } }
       { const double rd2 = fD * lF[2];
       if (rd2 != 0.0) {
@@ -472,13 +477,13 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
   const double gm = G.gm, gm1 = gm - 1.0, g21 = G.g21;
   const double sb = (e.sbxm ? -1.0 : 1.0);
   [[maybe_unused]] double r = 0.5 * (a0 + b0);
-  [[maybe_unused]] double u = 0.5 * (a1 / a0 + b1 / b0);
-  [[maybe_unused]] double v = 0.5 * (a2_ / a0 + b2 / b0);
-  [[maybe_unused]] double w = 0.5 * (a3 / a0 + b3 / b0);
+  [[maybe_unused]] double u = e.u;
+  [[maybe_unused]] double v = e.v;
+  [[maybe_unused]] double w = e.w;
   [[maybe_unused]] double bx = 0.5 * (a4 + b4);
   [[maybe_unused]] double by = 0.5 * (a5 + b5);
   [[maybe_unused]] double bz = 0.5 * (a6 + b6);
-  [[maybe_unused]] double uu = u * u + v * v + w * w;
+  [[maybe_unused]] double uu = e.uu;
   [[maybe_unused]] double bb = bx * bx + by * by + bz * bz;
   [[maybe_unused]] double mml = a1 * a1 + a2_ * a2_ + a3 * a3;
   [[maybe_unused]] double bbl = a4 * a4 + a5 * a5 + a6 * a6;
@@ -493,9 +498,9 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
   [[maybe_unused]] double a2 = gm * p / r;
   const bool a2_fz = a2 < 0.0;
   if (a2_fz) a2 = 0.0;
-  [[maybe_unused]] double a = sqrt(a2);
-  [[maybe_unused]] double ca2 = bx * bx / r;
-  [[maybe_unused]] double ca = sqrt(ca2);
+  [[maybe_unused]] double a = e.a;
+  [[maybe_unused]] double ca2 = e.ca2;
+  [[maybe_unused]] double ca = e.ca;
   [[maybe_unused]] double c2 = 0.5 * (bb / r + a2);
   [[maybe_unused]] double ct = c2 * c2 - a2 * ca2;
   const bool ct_fz = ct < 0.0;
@@ -507,9 +512,9 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
   [[maybe_unused]] double cf2 = c2 + sct;
   const bool cf2_fz = cf2 < 0.0;
   if (cf2_fz) cf2 = SMALL;
-  [[maybe_unused]] double cs = sqrt(cs2);
-  [[maybe_unused]] double cf = sqrt(cf2);
-  [[maybe_unused]] double rr = sqrt(r);
+  [[maybe_unused]] double cs = e.cs;
+  [[maybe_unused]] double cf = e.cf;
+  [[maybe_unused]] double rr = e.rr;
   [[maybe_unused]] double bp2 = by * by + bz * bz;
   const bool deg = (bp2 < SMALL) && (fabs(ca2 - a2) < SMALL);
   [[maybe_unused]] double af2 = (cf2 - ca2) / (cf2 - cs2);
@@ -518,21 +523,24 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
   [[maybe_unused]] double as2 = (cf2 - a2) / (cf2 - cs2);
   const bool as2_fz = deg || as2 < 0.0;
   if (as2_fz) as2 = deg ? 1.0 : 0.0;
-  [[maybe_unused]] double af = sqrt(af2);
-  [[maybe_unused]] double as_ = sqrt(as2);
+  [[maybe_unused]] double af = e.af;
+  [[maybe_unused]] double as_ = e.as;
   [[maybe_unused]] double sbp = sqrt(bp2);
   const bool sbp_fz = !(bp2 > SMALL);
   if (sbp_fz) sbp = 1.0;
-  [[maybe_unused]] double bty = by / sbp;
+  [[maybe_unused]] double bty = e.bty;
   const bool bty_fz = !(bp2 > SMALL);
-  if (bty_fz) bty = G.rs2;
-  [[maybe_unused]] double btz = bz / sbp;
+  [[maybe_unused]] double btz = e.btz;
   const bool btz_fz = !(bp2 > SMALL);
-  if (btz_fz) btz = G.rs2;
-  [[maybe_unused]] double th1 = 1.0 / (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2));
-  [[maybe_unused]] double th2 = 1.0 / (sb * af2 * cf * a + sb * as2 * cs * ca);
-  [[maybe_unused]] double vb = bty * v + btz * w;
-  // reverse sweep
+  [[maybe_unused]] double th1 = e.th1;
+  [[maybe_unused]] double th2 = e.th2;
+  [[maybe_unused]] double vb = e.vb;
+  // reverse sweep (one division per distinct denominator)
+  [[maybe_unused]] const double rcp2 = 1.0 / (sbp);
+  [[maybe_unused]] const double rcp3 = 1.0 / (cf2 - cs2);
+  [[maybe_unused]] const double rcp4 = 1.0 / (r);
+  [[maybe_unused]] const double rcp5 = 1.0 / (b0);
+  [[maybe_unused]] const double rcp6 = 1.0 / (a0);
   double r_b = 0.0;
   double u_b = 0.0;
   double v_b = 0.0;
@@ -618,30 +626,30 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     w_b += (vb_b) * (btz);
   }
   if (th2_b != 0.0) {
-    af2_b += (((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (a)) * (cf)) * (sb);
-    cf_b += ((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (a)) * (sb * af2);
-    a_b += (-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (sb * af2 * cf);
-    as2_b += (((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (ca)) * (cs)) * (sb);
-    cs_b += ((-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (ca)) * (sb * as2);
-    ca_b += (-(th2_b) * (1.0) / ((sb * af2 * cf * a + sb * as2 * cs * ca) * (sb * af2 * cf * a + sb * as2 * cs * ca))) * (sb * as2 * cs);
+    af2_b += (((-(th2_b) * (1.0) * th2 * th2) * (a)) * (cf)) * (sb);
+    cf_b += ((-(th2_b) * (1.0) * th2 * th2) * (a)) * (sb * af2);
+    a_b += (-(th2_b) * (1.0) * th2 * th2) * (sb * af2 * cf);
+    as2_b += (((-(th2_b) * (1.0) * th2 * th2) * (ca)) * (cs)) * (sb);
+    cs_b += ((-(th2_b) * (1.0) * th2 * th2) * (ca)) * (sb * as2);
+    ca_b += (-(th2_b) * (1.0) * th2 * th2) * (sb * as2 * cs);
   }
   if (th1_b != 0.0) {
-    af2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cf2 - g21 * a2)) * (a2);
-    a2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cf2 - g21 * a2)) * (af2);
-    cf2_b += (-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (af2 * a2);
-    a2_b += (-((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (af2 * a2))) * (g21);
-    as2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cs2 - g21 * a2)) * (cf2);
-    cf2_b += ((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (cs2 - g21 * a2)) * (as2);
-    cs2_b += (-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (as2 * cf2);
-    a2_b += (-((-(th1_b) * (1.0) / ((af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)) * (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2)))) * (as2 * cf2))) * (g21);
+    af2_b += ((-(th1_b) * (1.0) * th1 * th1) * (cf2 - g21 * a2)) * (a2);
+    a2_b += ((-(th1_b) * (1.0) * th1 * th1) * (cf2 - g21 * a2)) * (af2);
+    cf2_b += (-(th1_b) * (1.0) * th1 * th1) * (af2 * a2);
+    a2_b += (-((-(th1_b) * (1.0) * th1 * th1) * (af2 * a2))) * (g21);
+    as2_b += ((-(th1_b) * (1.0) * th1 * th1) * (cs2 - g21 * a2)) * (cf2);
+    cf2_b += ((-(th1_b) * (1.0) * th1 * th1) * (cs2 - g21 * a2)) * (as2);
+    cs2_b += (-(th1_b) * (1.0) * th1 * th1) * (as2 * cf2);
+    a2_b += (-((-(th1_b) * (1.0) * th1 * th1) * (as2 * cf2))) * (g21);
   }
   if (!btz_fz && btz_b != 0.0) {
-    bz_b += (btz_b) / (sbp);
-    sbp_b += -(btz_b) * (bz) / ((sbp) * (sbp));
+    bz_b += (btz_b) * rcp2;
+    sbp_b += -(btz_b) * (bz) * rcp2 * rcp2;
   }
   if (!bty_fz && bty_b != 0.0) {
-    by_b += (bty_b) / (sbp);
-    sbp_b += -(bty_b) * (by) / ((sbp) * (sbp));
+    by_b += (bty_b) * rcp2;
+    sbp_b += -(bty_b) * (by) * rcp2 * rcp2;
   }
   if (!sbp_fz && sbp_b != 0.0) {
     bp2_b += (sbp_b) * inv2sqrt(bp2);
@@ -653,16 +661,16 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     af2_b += (af_b) * inv2sqrt(af2);
   }
   if (!as2_fz && as2_b != 0.0) {
-    cf2_b += (as2_b) / (cf2 - cs2);
-    a2_b += -((as2_b) / (cf2 - cs2));
-    cf2_b += -(as2_b) * (cf2 - a2) / ((cf2 - cs2) * (cf2 - cs2));
-    cs2_b += -(-(as2_b) * (cf2 - a2) / ((cf2 - cs2) * (cf2 - cs2)));
+    cf2_b += (as2_b) * rcp3;
+    a2_b += -((as2_b) * rcp3);
+    cf2_b += -(as2_b) * (cf2 - a2) * rcp3 * rcp3;
+    cs2_b += -(-(as2_b) * (cf2 - a2) * rcp3 * rcp3);
   }
   if (!af2_fz && af2_b != 0.0) {
-    cf2_b += (af2_b) / (cf2 - cs2);
-    ca2_b += -((af2_b) / (cf2 - cs2));
-    cf2_b += -(af2_b) * (cf2 - ca2) / ((cf2 - cs2) * (cf2 - cs2));
-    cs2_b += -(-(af2_b) * (cf2 - ca2) / ((cf2 - cs2) * (cf2 - cs2)));
+    cf2_b += (af2_b) * rcp3;
+    ca2_b += -((af2_b) * rcp3);
+    cf2_b += -(af2_b) * (cf2 - ca2) * rcp3 * rcp3;
+    cs2_b += -(-(af2_b) * (cf2 - ca2) * rcp3 * rcp3);
   }
   if (bp2_b != 0.0) {
     by_b += (bp2_b) * (by);
@@ -697,24 +705,24 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     ca2_b += (-(ct_b)) * (a2);
   }
   if (c2_b != 0.0) {
-    bb_b += ((c2_b) * (0.5)) / (r);
-    r_b += -((c2_b) * (0.5)) * (bb) / ((r) * (r));
+    bb_b += ((c2_b) * (0.5)) * rcp4;
+    r_b += -((c2_b) * (0.5)) * (bb) * rcp4 * rcp4;
     a2_b += (c2_b) * (0.5);
   }
   if (ca_b != 0.0) {
     ca2_b += (ca_b) * inv2sqrt(ca2);
   }
   if (ca2_b != 0.0) {
-    bx_b += ((ca2_b) / (r)) * (bx);
-    bx_b += ((ca2_b) / (r)) * (bx);
-    r_b += -(ca2_b) * (bx * bx) / ((r) * (r));
+    bx_b += ((ca2_b) * rcp4) * (bx);
+    bx_b += ((ca2_b) * rcp4) * (bx);
+    r_b += -(ca2_b) * (bx * bx) * rcp4 * rcp4;
   }
   if (a_b != 0.0) {
     a2_b += (a_b) * inv2sqrt(a2);
   }
   if (!a2_fz && a2_b != 0.0) {
-    p_b += ((a2_b) / (r)) * (gm);
-    r_b += -(a2_b) * (gm * p) / ((r) * (r));
+    p_b += ((a2_b) * rcp4) * (gm);
+    r_b += -(a2_b) * (gm * p) * rcp4 * rcp4;
   }
   if (!p_fz && p_b != 0.0) {
     pt_b += p_b;
@@ -726,15 +734,15 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
   }
   if (ptr_b != 0.0) {
     b7_b += (ptr_b) * (gm1);
-    mmr_b += ((-((ptr_b) * (gm1))) / (b0)) * (0.5);
-    b0_b += -(-((ptr_b) * (gm1))) * (0.5 * mmr) / ((b0) * (b0));
+    mmr_b += ((-((ptr_b) * (gm1))) * rcp5) * (0.5);
+    b0_b += -(-((ptr_b) * (gm1))) * (0.5 * mmr) * rcp5 * rcp5;
     bbr_b += (-((ptr_b) * (gm1))) * (0.5);
     bbr_b += (ptr_b) * (0.5);
   }
   if (ptl_b != 0.0) {
     a7_b += (ptl_b) * (gm1);
-    mml_b += ((-((ptl_b) * (gm1))) / (a0)) * (0.5);
-    a0_b += -(-((ptl_b) * (gm1))) * (0.5 * mml) / ((a0) * (a0));
+    mml_b += ((-((ptl_b) * (gm1))) * rcp6) * (0.5);
+    a0_b += -(-((ptl_b) * (gm1))) * (0.5 * mml) * rcp6 * rcp6;
     bbl_b += (-((ptl_b) * (gm1))) * (0.5);
     bbl_b += (ptl_b) * (0.5);
   }
@@ -799,22 +807,22 @@ __device__ __forceinline__ void midpoint_adjoint(const Gas& G, const Mid& e, con
     b4_b += (bx_b) * (0.5);
   }
   if (w_b != 0.0) {
-    a3_b += ((w_b) * (0.5)) / (a0);
-    a0_b += -((w_b) * (0.5)) * (a3) / ((a0) * (a0));
-    b3_b += ((w_b) * (0.5)) / (b0);
-    b0_b += -((w_b) * (0.5)) * (b3) / ((b0) * (b0));
+    a3_b += ((w_b) * (0.5)) * rcp6;
+    a0_b += -((w_b) * (0.5)) * (a3) * rcp6 * rcp6;
+    b3_b += ((w_b) * (0.5)) * rcp5;
+    b0_b += -((w_b) * (0.5)) * (b3) * rcp5 * rcp5;
   }
   if (v_b != 0.0) {
-    a2__b += ((v_b) * (0.5)) / (a0);
-    a0_b += -((v_b) * (0.5)) * (a2_) / ((a0) * (a0));
-    b2_b += ((v_b) * (0.5)) / (b0);
-    b0_b += -((v_b) * (0.5)) * (b2) / ((b0) * (b0));
+    a2__b += ((v_b) * (0.5)) * rcp6;
+    a0_b += -((v_b) * (0.5)) * (a2_) * rcp6 * rcp6;
+    b2_b += ((v_b) * (0.5)) * rcp5;
+    b0_b += -((v_b) * (0.5)) * (b2) * rcp5 * rcp5;
   }
   if (u_b != 0.0) {
-    a1_b += ((u_b) * (0.5)) / (a0);
-    a0_b += -((u_b) * (0.5)) * (a1) / ((a0) * (a0));
-    b1_b += ((u_b) * (0.5)) / (b0);
-    b0_b += -((u_b) * (0.5)) * (b1) / ((b0) * (b0));
+    a1_b += ((u_b) * (0.5)) * rcp6;
+    a0_b += -((u_b) * (0.5)) * (a1) * rcp6 * rcp6;
+    b1_b += ((u_b) * (0.5)) * rcp5;
+    b0_b += -((u_b) * (0.5)) * (b1) * rcp5 * rcp5;
   }
   if (r_b != 0.0) {
     a0_b += (r_b) * (0.5);
@@ -850,7 +858,8 @@ __device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const
   [[maybe_unused]] double fo5 = q5 * fu - q4 * fv;
   [[maybe_unused]] double fo6 = q6 * fu - q4 * fw;
   [[maybe_unused]] double fo7 = (q7 + fpt) * fu - q4 * fub;
-  // reverse sweep
+  // reverse sweep (one division per distinct denominator)
+  [[maybe_unused]] const double rcp0 = 1.0 / (q0);
   double fu_b = 0.0;
   double fv_b = 0.0;
   double fw_b = 0.0;
@@ -957,16 +966,16 @@ __device__ __forceinline__ void flux_x_adjoint(double gm, const double* q, const
     fw_b += (fuu_b) * (fw);
   }
   if (fw_b != 0.0) {
-    q3_b += (fw_b) / (q0);
-    q0_b += -(fw_b) * (q3) / ((q0) * (q0));
+    q3_b += (fw_b) * rcp0;
+    q0_b += -(fw_b) * (q3) * rcp0 * rcp0;
   }
   if (fv_b != 0.0) {
-    q2_b += (fv_b) / (q0);
-    q0_b += -(fv_b) * (q2) / ((q0) * (q0));
+    q2_b += (fv_b) * rcp0;
+    q0_b += -(fv_b) * (q2) * rcp0 * rcp0;
   }
   if (fu_b != 0.0) {
-    q1_b += (fu_b) / (q0);
-    q0_b += -(fu_b) * (q1) / ((q0) * (q0));
+    q1_b += (fu_b) * rcp0;
+    q0_b += -(fu_b) * (q1) * rcp0 * rcp0;
   }
   qb[0] += q0_b;
   qb[1] += q1_b;
