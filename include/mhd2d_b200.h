@@ -128,6 +128,14 @@ int mhd_get_characteristics( mhd_ctx* ctx, double* cx, double* cy, double* LUx, 
 /* Replaces divBCalculation (div_b_fix.cpp:4-126) on the device state. */
 int mhd_divb_calc( mhd_ctx* ctx, double* maxdivb, double* totdivb );
 
+/* The numbers of the reference's non-grid output record (outputNonGridData,
+   file_access.cpp:1680-1736) for the context's state: out[0] u_max, out[1]
+   |div B|_max, out[2] sum |div B| dx dy, out[3] total mass, out[4] total
+   momentum (rho |u|), out[5] total energy, out[6] total entropy
+   (log(p rho^-gamma)), each sum times dx dy.  Computed on the device; like the
+   reference it fills periodic B ghosts on the way (divBCalculation). */
+int mhd_nongrid_data( mhd_ctx* ctx, double out[7] );
+
 /* Replaces divBCorrectionSOR (div_b_fix.cpp:129-403): one solve with the
    sublattice red-black ordering, warm-started from the context's
    potential, followed by the B correction.  *sweeps gets the sweep count. */
@@ -136,6 +144,43 @@ int mhd_divb_sor( mhd_ctx* ctx, const mhd_sor_params* p, int* sweeps );
 /* The cleaning loop of main.cpp:207-242 (up to sor_steps solves until
    max|div B| < sor_divbmax), final max|div B| in *maxdivb. */
 int mhd_divb_clean( mhd_ctx* ctx, const mhd_sor_params* p, double* maxdivb, int* total_sweeps );
+
+/* The reference main loop (main.cpp:174-344) on the device, without files:
+   step (mhd_step rules), the [divb corrector] cleaning loop every
+   divb_skip_steps steps, t += dt, stop at `steps` (time_mode 1, constant) or
+   at t >= t_max (time_mode 2, variable), on ErrorTimeUnderflow, on a fatal
+   status or on a NaN at U[0][2][2].  The non-grid output records
+   (mhd_nongrid_data) are taken at step 0 and then every nongrid_steps steps
+   (nongrid_mode 1) or every nongrid_t of simulated time (nongrid_mode 2),
+   as main.cpp:284-310 schedules them; up to max_records are stored. */
+typedef struct {
+   int    time_mode;        /* 1 constant (`steps` steps), 2 variable (until t_max) */
+   int    steps;
+   double t_max;
+   double dt0;              /* initial time step */
+   mhd_sor_params sor;      /* sor.sor_steps <= 0: no cleaning */
+   int    nongrid_mode;     /* 0 none, 1 by steps, 2 by simulated time */
+   int    nongrid_steps;
+   double nongrid_t;
+} mhd_run_params;
+
+typedef struct {
+   int    step;
+   double t, dt;
+   double values[7];        /* as mhd_nongrid_data */
+} mhd_nongrid_record;
+
+typedef struct {
+   int    steps;            /* completed steps */
+   double t, dt;            /* simulated time and the current dt at the end */
+   int    status, is_error; /* of the last step */
+   int    nan_stop;         /* stopped on a NaN */
+   int    records;          /* records taken (may exceed max_records) */
+   long long sor_sweeps;
+} mhd_run_result;
+
+int mhd_run( mhd_ctx* ctx, const mhd_run_params* p, mhd_nongrid_record* records,
+             int max_records, mhd_run_result* result );
 
 /* Counters of the last integrate / step: clamped midpoint pressures
    (the reference's "negative pressure" warning count) and kernel launches. */

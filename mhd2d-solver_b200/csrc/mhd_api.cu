@@ -9,6 +9,7 @@
 #include <limits>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/mhd2d_b200.h"
 #include "mhd_launch.h"
@@ -50,6 +51,7 @@ struct mhd_ctx {
   int npartial = 0;
   Ctl* ctl = nullptr;
   Ctl* hctl = nullptr;  // pinned mirror
+  double* hnan = nullptr;  // pinned: U[0][2][2] for the run loop's NaN stop
   std::string msg;
   bool is_error = false;
   long long launches = 0, neg_pressure = 0;
@@ -272,6 +274,37 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
 
 }  // namespace
 
+int do_nongrid(mhd_ctx* c, double out[7]) {
+  double mx = 0.0, tot = 0.0;
+  int st = do_divb_calc(c, &mx, &tot);
+  if (st) return st;
+  const int nb = c->ks->totals(c->g, c->U, c->partial, c->npartial / 5, c->stream);
+  c->launches++;
+  std::vector<double> h(5 * (size_t)nb);
+  CK(cudaMemcpyAsync(h.data(), c->partial, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  double ent = 0.0, en = 0.0, mass = 0.0, mom = 0.0, uumax = 0.0;
+  for (int b = 0; b < nb; b++) {
+    ent += h[5 * b];
+    en += h[5 * b + 1];
+    mass += h[5 * b + 2];
+    mom += h[5 * b + 3];
+    if (h[5 * b + 4] > uumax) uumax = h[5 * b + 4];
+  }
+  const double dxdy = c->g.dx * c->g.dy;
+  // the columns u_max .. total_entropy of the record line (file_access.cpp:1713-1733)
+  out[0] = std::sqrt(uumax);
+  out[1] = mx;
+  out[2] = tot;
+  out[3] = mass * dxdy;
+  out[4] = mom * dxdy;
+  out[5] = en * dxdy;
+  out[6] = ent * dxdy;
+  return MHD_OK;
+}
+
 extern "C" {
 
 int mhd_ctx_create(int nx, int ny, int halo, double dx, double dy, double gamma, const int bc[4],
@@ -327,6 +360,7 @@ int mhd_ctx_create(int nx, int ny, int halo, double dx, double dy, double gamma,
   if (e == cudaSuccess) e = cudaMalloc(&c->ctl, sizeof(Ctl));
   if (e == cudaSuccess) e = cudaMemsetAsync(c->ctl, 0, sizeof(Ctl), c->stream);
   if (e == cudaSuccess) e = cudaMallocHost(&c->hctl, sizeof(Ctl));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hnan, sizeof(double));
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     cuda_fail(nullptr, e, "mhd_ctx_create");
@@ -349,6 +383,7 @@ int mhd_ctx_destroy(mhd_ctx* c) {
     if (b) cudaFree(b);
   if (c->ctl) cudaFree(c->ctl);
   if (c->hctl) cudaFreeHost(c->hctl);
+  if (c->hnan) cudaFreeHost(c->hnan);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return MHD_OK;
@@ -504,6 +539,86 @@ int mhd_divb_calc(mhd_ctx* c, double* maxdivb, double* totdivb) {
   if (!c || !maxdivb || !totdivb) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   return do_divb_calc(c, maxdivb, totdivb);
+}
+
+int mhd_nongrid_data(mhd_ctx* c, double out[7]) {
+  if (!c || !out) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  int st = do_nongrid(c, out);
+  if (st) return st;
+  return set_status(c, MHD_OK, false, "");
+}
+
+int mhd_run(mhd_ctx* c, const mhd_run_params* p, mhd_nongrid_record* records, int max_records,
+            mhd_run_result* res) {
+  if (!c || !p || !res || (p->time_mode != 1 && p->time_mode != 2) ||
+      (p->time_mode == 1 && p->steps < 1) || (p->nongrid_mode == 1 && p->nongrid_steps < 1) ||
+      (p->nongrid_mode == 2 && !(p->nongrid_t > 0.0)) ||
+      (p->sor.sor_steps > 0 && p->sor.divb_skip_steps < 1))
+    return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  *res = mhd_run_result{};
+  int st = MHD_OK, step = 1, nrec = 0;
+  double t = 0.0, dt = p->dt0, next_t = p->nongrid_t;
+  auto record = [&](int s) -> int {
+    if (records && nrec < max_records) {
+      mhd_nongrid_record& r = records[nrec];
+      r.step = s;
+      r.t = t;
+      r.dt = dt;
+      const int e = do_nongrid(c, r.values);
+      if (e) return e;
+    }
+    nrec++;
+    return MHD_OK;
+  };
+  if (p->nongrid_mode && (st = record(0))) return st;
+  for (bool done = false; !done;) {
+    st = do_step(c, &dt);
+    res->status = st;
+    res->is_error = c->is_error ? 1 : 0;
+    if (st == MHD_ERR_TIME_UNDERFLOW || c->is_error) break;
+    if (p->sor.sor_steps > 0 && step % p->sor.divb_skip_steps == 0) {  // main.cpp:207-242
+      double mx = 0.0, tot = 0.0;
+      for (int it = 0; it < p->sor.sor_steps; it++) {
+        int e = do_divb_calc(c, &mx, &tot);
+        if (e) return e;
+        if (mx < p->sor.sor_divbmax) break;
+        int sw = 0;
+        e = do_sor(c, &p->sor, &sw);
+        res->sor_sweeps += sw;
+        if (e == MHD_ERR_NOT_CONVERGED) break;
+        if (e) return e;
+      }
+      int e = do_divb_calc(c, &mx, &tot);
+      if (e) return e;
+    }
+    t += dt;
+    done = p->time_mode == 1 ? step == p->steps : t >= p->t_max;
+    bool out = false;
+    if (p->nongrid_mode == 1) {
+      out = step % p->nongrid_steps == 0;
+    } else if (p->nongrid_mode == 2) {
+      out = t >= next_t;
+      while (out && next_t <= t) next_t += p->nongrid_t;
+    }
+    if (out && (st = record(step))) return st;
+    double u00 = 0.0;  // the NaN stop of main.cpp:335-341
+    CK(cudaMemcpyAsync(c->hnan, c->U + c->g.at(0, 2, 2), sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    u00 = *c->hnan;
+    if (std::isnan(u00)) {
+      res->nan_stop = 1;
+      done = true;
+    }
+    res->steps = step;
+    step++;
+  }
+  res->t = t;
+  res->dt = dt;
+  res->records = nrec;
+  return res->status;
 }
 
 int mhd_divb_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {

@@ -141,6 +141,13 @@ void l_sor_correct(const Grid& g, double* U, const double* phi, const int range[
   k_sor_correct<<<grid1d(n, 256), 256, 0, s>>>(g, U, phi, R, bxf, byf);
 }
 
+int l_totals(const Grid& g, const double* U, double* partial, int max_blocks, cudaStream_t s) {
+  int nb = grid1d((long long)g.nx * g.ny, TOT_THREADS);
+  if (nb > max_blocks) nb = max_blocks;
+  k_totals<<<nb, TOT_THREADS, 0, s>>>(g, U, partial);
+  return nb;
+}
+
 int l_smem() { return int(Geom::BYTES); }
 int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
 
@@ -149,6 +156,6 @@ int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
 using namespace MHD_KNS;
 extern const KernelSet MHD_KSET = {MHD_KSET_NAME, l_bc, l_snapshot, l_lf_alpha, l_flux,
                                    l_combine, l_control, l_divb, l_sor_rhs, l_sor_sweep,
-                                   l_sor_correct, l_smem, l_launches};
+                                   l_sor_correct, l_totals, l_smem, l_launches};
 
 }  // namespace mhd

@@ -45,6 +45,9 @@ struct KernelSet {
                     Ctl* ctl, cudaStream_t s);
   void (*sor_correct)(const Grid& g, double* U, const double* phi, const int range[4],
                       double bxf, double byf, cudaStream_t s);
+  // non-grid output totals: 5 partials per block (entropy, energy, mass,
+  // momentum sums, max |u|^2); returns the number of blocks used
+  int (*totals)(const Grid& g, const double* U, double* partial, int max_blocks, cudaStream_t s);
   int (*flux_smem_bytes)();
   int (*launches_per_integrate)(int scheme);
 };

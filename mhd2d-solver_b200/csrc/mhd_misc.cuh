@@ -335,6 +335,56 @@ __global__ void k_divb_finish(double* partial, int nb, double dxdy, Ctl* c) {
   c->divb_sum = s * dxdy;
 }
 
+// Totals of the reference's non-grid output (outputNonGridData,
+// file_access.cpp:1680-1712, on the primitives of toNaturalData,
+// conversions.cpp:37-57): per block of the interior, the sums of entropy
+// log(p rho^-gamma), energy, mass and rho |u|, and the max of |u|^2, as 5
+// partials per block (partial[5 b + q]); the host adds the blocks in order.
+constexpr int TOT_THREADS = 256;
+__global__ void __launch_bounds__(TOT_THREADS) k_totals(Grid g, const double* __restrict__ U,
+                                                         double* __restrict__ partial) {
+  const long long n = (long long)g.nx * g.ny;
+  const double gm = g.gamma;
+  double s_ent = 0.0, s_en = 0.0, s_mass = 0.0, s_mom = 0.0, uumax = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = 2 + int(e / g.ny), j = 2 + int(e % g.ny);
+    const double r = U[g.at(0, i, j)], mx = U[g.at(1, i, j)], my = U[g.at(2, i, j)];
+    const double mz = U[g.at(3, i, j)], bx = U[g.at(4, i, j)], by = U[g.at(5, i, j)];
+    const double bz = U[g.at(6, i, j)], en = U[g.at(7, i, j)];
+    const double u0 = mx / r, u1 = my / r, u2 = mz / r;
+    const double mm = mx * mx + my * my + mz * mz;
+    const double bb = bx * bx + by * by + bz * bz;
+    const double p = (gm - 1.0) * (en - 0.5 * mm / r - 0.5 * bb);
+    const double uu = u0 * u0 + u1 * u1 + u2 * u2;
+    uumax = take_max(uumax, uu);
+    s_ent += log(p * pow(r, -gm));
+    s_en += en;
+    s_mass += r;
+    s_mom += r * sqrt(uu);
+  }
+  double v[5] = {s_ent, s_en, s_mass, s_mom, uumax};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    v[4] = take_max(v[4], __shfl_xor_sync(0xffffffffu, v[4], o));
+  }
+  __shared__ double sm[5][TOT_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int q = 0; q < 5; q++) sm[q][wid] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < TOT_THREADS / 32; w++) {
+      for (int q = 0; q < 4; q++) t[q] += sm[q][w];
+      t[4] = take_max(t[4], sm[4][w]);
+    }
+    for (int q = 0; q < 5; q++) partial[5 * blockIdx.x + q] = t[q];
+  }
+}
+
 // One colour of a red-black sweep of the reference's SOR update
 // (div_b_fix.cpp:262-280).  The stride-2 Laplacian couples (i, j) only to
 // (i+-2, j) and (i, j+-2), so colour ((i>>1) + (j>>1)) & 1 makes every

@@ -84,6 +84,29 @@ class SorParams(C.Structure):
                 ("omega", C.c_double)]
 
 
+class RunParams(C.Structure):
+    """mhd_run_params: the main loop's stop rule, cleaning and non-grid output cadence."""
+
+    _fields_ = [("time_mode", C.c_int), ("steps", C.c_int), ("t_max", C.c_double),
+                ("dt0", C.c_double), ("sor", SorParams), ("nongrid_mode", C.c_int),
+                ("nongrid_steps", C.c_int), ("nongrid_t", C.c_double)]
+
+
+class NongridRecord(C.Structure):
+    """mhd_nongrid_record: step, t, dt and the 7 numbers of mhd_nongrid_data."""
+
+    _fields_ = [("step", C.c_int), ("t", C.c_double), ("dt", C.c_double),
+                ("values", C.c_double * 7)]
+
+
+class RunResult(C.Structure):
+    """mhd_run_result."""
+
+    _fields_ = [("steps", C.c_int), ("t", C.c_double), ("dt", C.c_double), ("status", C.c_int),
+                ("is_error", C.c_int), ("nan_stop", C.c_int), ("records", C.c_int),
+                ("sor_sweeps", C.c_longlong)]
+
+
 def sor_params(skip=1, steps=10, rsteps=100000, rmax=1e-10, divbmax=1e-10, use_static=True,
                omega=1.7):
     return SorParams(skip, steps, float(rsteps), rmax, divbmax, int(use_static), omega)
@@ -117,6 +140,9 @@ def library():
         "mhd_steps": [vp, C.c_int, _dp, _dp],
         "mhd_get_characteristics": [vp, _dp, _dp, _dp, _dp],
         "mhd_divb_calc": [vp, _dp, _dp],
+        "mhd_nongrid_data": [vp, _dp],
+        "mhd_run": [vp, C.POINTER(RunParams), C.POINTER(NongridRecord), C.c_int,
+                    C.POINTER(RunResult)],
         "mhd_divb_sor": [vp, C.POINTER(SorParams), _ip],
         "mhd_divb_clean": [vp, C.POINTER(SorParams), _dp, _ip],
         "mhd_get_counters": [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
@@ -300,10 +326,34 @@ class Context:
         self._check(self.lib.mhd_divb_calc(self.h, C.byref(m), C.byref(t)), "divb_calc")
         return m.value, t.value
 
+    def nongrid_data(self):
+        """(u_max, divb_max, divb_sum, mass, momentum, energy, entropy) of the state."""
+        out = np.zeros(7)
+        self._check(self.lib.mhd_nongrid_data(self.h, _p(out)), "nongrid_data")
+        return tuple(float(x) for x in out)
+
     def divb_sor(self, params):
         sw = C.c_int(0)
         st = self._check(self.lib.mhd_divb_sor(self.h, C.byref(params), C.byref(sw)), "divb_sor")
         return self.last_status(st), sw.value
+
+    def run(self, dt0, steps=0, t_max=0.0, sor=None, nongrid_steps=0, nongrid_t=0.0,
+            max_records=1024):
+        """The reference main loop on the device (mhd_run): `steps` steps (constant time
+        mode) or until t_max.  Returns (RunResult as a dict, list of record dicts)."""
+        p = RunParams()
+        p.time_mode = 1 if steps > 0 else 2
+        p.steps, p.t_max, p.dt0 = int(steps), float(t_max), float(dt0)
+        p.sor = sor if sor is not None else sor_params(steps=0)
+        p.nongrid_mode = 1 if nongrid_steps > 0 else (2 if nongrid_t > 0.0 else 0)
+        p.nongrid_steps, p.nongrid_t = int(nongrid_steps), float(nongrid_t)
+        recs = (NongridRecord * max(1, max_records))()
+        r = RunResult()
+        self._check(self.lib.mhd_run(self.h, C.byref(p), recs, max_records, C.byref(r)), "run")
+        res = {f: getattr(r, f) for f, _ in RunResult._fields_}
+        out = [dict(step=q.step, t=q.t, dt=q.dt, values=tuple(q.values))
+               for q in recs[:min(r.records, max_records)]]
+        return res, out
 
     def divb_clean(self, params):
         m, sw = C.c_double(0), C.c_int(0)

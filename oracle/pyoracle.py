@@ -136,6 +136,9 @@ def load_reference(fresh=False):
                                   C.c_char_p, C.c_int]
     lib.ref_update_dt.argtypes = [C.c_double, C.c_double, C.c_double, _dp, C.c_double, _ip]
     lib.ref_divb_calc.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _ip, _dp, _dp, _dp]
+    lib.ref_nongrid_data.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _ip,
+                                     _dp, _dp]
+    lib.ref_nongrid_data.restype = None
     lib.ref_divb_sor.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _ip,
                                  C.POINTER(SorParams), _dp, _ip]
     lib.ref_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -252,6 +255,14 @@ class Reference:
         m, t = C.c_double(0), C.c_double(0)
         self.lib.ref_divb_calc(NX - 4, NY - 4, dx, dy, _bc(bc), _p(U), C.byref(m), C.byref(t))
         return m.value, t.value
+
+    def nongrid_data(self, U, dx, dy, gamma, bc):
+        """(u_max, divb_max, divb_sum, mass, momentum, energy, entropy) of the reference's
+        non-grid output record (fills periodic B ghosts of U, as divBCalculation does)."""
+        _, NX, NY = U.shape
+        out = np.zeros(7)
+        self.lib.ref_nongrid_data(NX - 4, NY - 4, dx, dy, gamma, _bc(bc), _p(U), _p(out))
+        return tuple(float(x) for x in out)
 
     def divb_sor(self, U, dx, dy, bc, sp):
         _, NX, NY = U.shape

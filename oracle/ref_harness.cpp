@@ -167,6 +167,52 @@ void ref_divb_calc( int nx, int ny, double dx, double dy, const int* bc, double*
    divBCalculation( vU.m(), p, *maxdivb, *totdivb );
 }
 
+/* The numbers of one non-grid output record for state U: the reference's
+   own toNaturalData (conversions.cpp:37-57) and divBCalculation
+   (div_b_fix.cpp:4-126), and the sums of outputNonGridData
+   (file_access.cpp:1680-1716; that file needs the INI parser and is not
+   compiled here, so its loop is restated).  out: u_max, |div B|_max,
+   sum |div B|, total mass, momentum, energy, entropy. */
+void ref_nongrid_data( int nx, int ny, double dx, double dy, double gamma, const int* bc,
+                       double* U, double* out )
+{
+   t_params params; fillParams( params, nx, ny, dx, dy, bc );
+   params.gamma = gamma;
+   const int NXt = nx+4, NYt = ny+4;
+   std::vector<double> ubuf( size_t(VEL_DIM)*NXt*NYt ), pbuf( size_t(NXt)*NYt );
+   MatView vU( U, PRB_DIM, NXt, NYt ), vu( ubuf.data(), VEL_DIM, NXt, NYt ),
+           vp( pbuf.data(), 1, NXt, NYt );
+   t_data data{};
+   data.U = vU.m();
+   data.u = vu.m();
+   data.p = vp.m()[0];
+   toNaturalData( params, data );
+   double totenergy = 0.0, entropy, totentropy = 0.0, totmass = 0.0, totmomentum = 0.0;
+   double uu, uumax = 0.0;
+   for( int i = NXFIRST; i < NXLAST; i++ ){
+      for( int j = NYFIRST; j < NYLAST; j++ ){
+         uu = data.u[0][i][j]*data.u[0][i][j] + data.u[1][i][j]*data.u[1][i][j]
+            + data.u[2][i][j]*data.u[2][i][j];
+         if( uu > uumax ) uumax = uu;
+         entropy = log( data.p[i][j]*pow( data.U[0][i][j], -params.gamma ) );
+         totentropy  += entropy;
+         totenergy   += data.U[7][i][j];
+         totmass     += data.U[0][i][j];
+         totmomentum += data.U[0][i][j]*sqrt(uu);
+      }
+   }
+   double maxdivb = 0.0, totdivb = 0.0;
+   divBCalculation( data.U, params, maxdivb, totdivb );
+   const double dxdy = params.dx*params.dy;
+   out[0] = sqrt( uumax );
+   out[1] = maxdivb;
+   out[2] = totdivb;
+   out[3] = totmass*dxdy;
+   out[4] = totmomentum*dxdy;
+   out[5] = totenergy*dxdy;
+   out[6] = totentropy*dxdy;
+}
+
 /* One divBCorrectionSOR call.  The potential is a function-static buffer of
    the reference, kept across calls within one loaded copy of this library. */
 int ref_divb_sor( int nx, int ny, double dx, double dy, const int* bc,

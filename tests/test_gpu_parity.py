@@ -210,6 +210,22 @@ def test_divb_calc_vs_oracle():
     assert same(ctx.download(), U)  # periodic B ghosts filled the same way
 
 
+@pytest.mark.parametrize("bc", [(1, 1, 1, 1), (3, 3, 4, 4), (2, 1, 3, 1)])
+def test_nongrid_record_vs_reference(bc):
+    from pyoracle import Reference, reference_available
+    if not reference_available():
+        pytest.skip("oracle/_ref not built")
+    p = P.random_smooth(61, 47, seed=9, bc=bc)
+    ctx = make_ctx(p, flags=0)
+    got = ctx.nongrid_data()
+    U = p.U.copy()
+    want = Reference().nongrid_data(U, p.dx, p.dy, p.gamma, bc)
+    assert got[0] == want[0] and got[1] == want[1]  # maxima: same arithmetic, any order
+    for k in (2, 3, 4, 5, 6):  # sums in another order; log / pow of another library
+        assert abs(got[k] - want[k]) <= 1e-12 * abs(want[k]), (k, got[k], want[k])
+    assert same(ctx.download(), U)  # periodic B ghosts filled the same way
+
+
 def test_error_paths():
     d = np.load(os.path.join(GOLD, "integrate_negdensity_2.npz"))
     p = _problem(d)
