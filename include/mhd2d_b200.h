@@ -190,6 +190,13 @@ int mhd_get_counters( mhd_ctx* ctx, long long* neg_pressure, long long* launches
    sits at k*NX*pitch + i*pitch + row_offset + j doubles from its base. */
 int mhd_layout( const mhd_ctx* ctx, int* pitch, int* row_offset );
 
+/* Process-wide: stage the flux kernels' state tiles with TMA box copies (1,
+   the default where the driver offers tensor maps) or with per-element
+   asynchronous copies (0); -1 leaves the setting.  *tma_launches (optional)
+   gets the number of flux launches so far whose tiles were staged by TMA.
+   Results are bit-identical either way. */
+int mhd_set_tile_tma( int enable, long long* tma_launches );
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record
    events or order their own work against the context's kernels. */
 int mhd_stream( const mhd_ctx* ctx, void** stream );

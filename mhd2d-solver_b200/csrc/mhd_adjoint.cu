@@ -728,15 +728,19 @@ void launch_flux(mhd_adj* a, const double* X, unsigned* slot) {
   auto kern = k_flux<2, false, ATI, ATJ, ANW, MASK>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(AGeom::BYTES));
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(AGeom::TMA_BYTES));
     attr = true;
   }
   const Grid& g = a->g;
   dim3 grid((g.ny + ATJ - 1) / ATJ, (g.nx + ATI - 1) / ATI);
   const CharOut co{nullptr, nullptr, nullptr, nullptr};
-  kern<<<grid, ANW * 32, AGeom::BYTES, a->stream>>>(g, X, a->UL, a->aF, a->aG, 1.0 / g.dx,
+  CUtensorMap tm{};
+  const int use_tma =
+      tile_tma_enabled() && make_box_map(g, X, AGeom::CU, AGeom::RU, &tm) ? 1 : 0;
+  tile_tma_launches() += use_tma;
+  kern<<<grid, ANW * 32, AGeom::TMA_BYTES, a->stream>>>(g, X, a->UL, a->aF, a->aG, 1.0 / g.dx,
                                                      1.0 / g.dy, a->G, a->ctl, co, slot,
-                                                     slot + (size_t)g.NX * g.NY);
+                                                     slot + (size_t)g.NX * g.NY, tm, use_tma);
   a->launches++;
 }
 
@@ -839,6 +843,8 @@ int record_finish(mhd_adj* a, double* dt_inout) {
     return aset(a, MHD_ERR_NEGATIVE_DENSITY, true, "negative density encountered\n! getEigens_F");
   if (h.error == 4)
     return aset(a, MHD_ERR_TIME_UNDERFLOW, true, "CFL condition violated!\n! updateDt");
+  if (h.error == kErrTileCopyTimeout)
+    return aset(a, MHD_ERR_CUDA, true, "flux tile copy did not complete");
   if (h.error)
     return aset(a, MHD_ERR_WRONG_PARAMETER, true, "updateDt: no power-of-two time step fits");
   *dt_inout = h.dt;

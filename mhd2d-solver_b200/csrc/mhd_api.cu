@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/mhd2d_b200.h"
+#include "mhd_tma.cuh"
 #include "mhd_launch.h"
 
 using namespace mhd;
@@ -161,6 +162,8 @@ int step_status(mhd_ctx* c) {
   if (h.error == 10)
     return set_status(c, MHD_ERR_WRONG_PARAMETER, true,
                       "updateDt: no power-of-two time step satisfies the CFL window\n! mhd_step");
+  if (h.error == kErrTileCopyTimeout)
+    return set_status(c, MHD_ERR_CUDA, true, "flux tile copy did not complete\n! mhd_step");
   return MHD_OK;
 }
 
@@ -691,6 +694,13 @@ int mhd_fp64_peak(int device, double* tflops) {
   cudaFree(out);
   CK(cudaGetLastError());
   *tflops = 2.0 * 8.0 * double(iters) * blocks * threads / (double(ms) * 1e-3) / 1e12;
+  return MHD_OK;
+}
+
+int mhd_set_tile_tma(int enable, long long* tma_launches) {
+  if (enable != 0 && enable != 1 && enable != -1) return MHD_ERR_WRONG_PARAMETER;
+  if (enable >= 0) tile_tma_flag() = enable != 0;
+  if (tma_launches) *tma_launches = tile_tma_launches();
   return MHD_OK;
 }
 

@@ -22,6 +22,7 @@
 #pragma once
 
 #include "mhd_eigen.cuh"
+#include "mhd_tma.cuh"
 
 #ifndef MHD_MINB
 #define MHD_MINB 2
@@ -56,6 +57,7 @@ struct TileGeom {
   static constexpr int OFF_GY = OFF_FX + 8 * (TI + 1) * TJ;  // sGy[8][TI][TJ+1], y frame order
   static constexpr int TOTAL = OFF_GY + 8 * TI * (TJ + 1);
   static constexpr size_t BYTES = size_t(TOTAL) * sizeof(double);
+  static constexpr size_t TMA_BYTES = BYTES + 128;  // k_flux: room to align the box to 128 B
 };
 
 // Physical x / y fluxes of one cell, same arithmetic as updateFluxes.
@@ -309,10 +311,12 @@ __global__ void __launch_bounds__(NW * 32, MHD_MINB)
 k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
        const double* __restrict__ alphaF, const double* __restrict__ alphaG,
        double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co, unsigned* maskX,
-       unsigned* maskY) {
+       unsigned* maskY, const __grid_constant__ CUtensorMap tmU, int use_tma) {
   if (ctl->skip) return;
   const int tj = blockIdx.x, ti = blockIdx.y;
+#define MHD_TILE_TMA 1
 #include "mhd_flux_tile.inc"
+#undef MHD_TILE_TMA
 }
 
 // ENO-LF dissipation coefficients (spatialmethodenolf.cpp:66-125):

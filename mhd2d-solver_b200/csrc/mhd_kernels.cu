@@ -60,15 +60,18 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
   auto kern = k_flux<SCHEME, CHARS, TI, TJ, NW>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Geom::BYTES));
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Geom::TMA_BYTES));
     attr = true;
   }
   dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + TI - 1) / TI);
   CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
              ch ? ch[3] : nullptr};
   const Gas G{g.gamma, g.gamma - 1.0, (g.gamma - 2.0) / (g.gamma - 1.0), 1.0 / std::sqrt(2.0)};
-  kern<<<grid, NW * 32, Geom::BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co,
-                                          nullptr, nullptr);
+  CUtensorMap tm{};
+  const int use_tma = tile_tma_enabled() && make_box_map(g, U, Geom::CU, Geom::RU, &tm) ? 1 : 0;
+  tile_tma_launches() += use_tma;
+  kern<<<grid, NW * 32, Geom::TMA_BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co,
+                                          nullptr, nullptr, tm, use_tma);
 }
 
 void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
@@ -148,7 +151,7 @@ int l_totals(const Grid& g, const double* U, double* partial, int max_blocks, cu
   return nb;
 }
 
-int l_smem() { return int(Geom::BYTES); }
+int l_smem() { return int(Geom::TMA_BYTES); }
 int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
 
 }  // namespace MHD_KNS

@@ -107,6 +107,16 @@ class RunResult(C.Structure):
                 ("sor_sweeps", C.c_longlong)]
 
 
+def set_tile_tma(enable=None):
+    """Stage flux tiles by TMA (True) or per-element async copies (False); None keeps the
+    setting.  Returns the number of TMA-staged flux launches so far."""
+    n = C.c_longlong(0)
+    st = library().mhd_set_tile_tma(-1 if enable is None else int(bool(enable)), C.byref(n))
+    if st != OK:
+        raise MhdError(f"mhd_set_tile_tma: {STATUS_NAMES.get(st, st)}")
+    return n.value
+
+
 def sor_params(skip=1, steps=10, rsteps=100000, rmax=1e-10, divbmax=1e-10, use_static=True,
                omega=1.7):
     return SorParams(skip, steps, float(rsteps), rmax, divbmax, int(use_static), omega)
@@ -141,6 +151,7 @@ def library():
         "mhd_get_characteristics": [vp, _dp, _dp, _dp, _dp],
         "mhd_divb_calc": [vp, _dp, _dp],
         "mhd_nongrid_data": [vp, _dp],
+        "mhd_set_tile_tma": [C.c_int, C.POINTER(C.c_longlong)],
         "mhd_run": [vp, C.POINTER(RunParams), C.POINTER(NongridRecord), C.c_int,
                     C.POINTER(RunResult)],
         "mhd_divb_sor": [vp, C.POINTER(SorParams), _ip],

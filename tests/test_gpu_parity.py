@@ -226,6 +226,29 @@ def test_nongrid_record_vs_reference(bc):
     assert same(ctx.download(), U)  # periodic B ghosts filled the same way
 
 
+@pytest.mark.parametrize("scheme", [M.ENO_ROE, M.ENO_LF])
+@pytest.mark.parametrize("shape,bc", [((45, 70), (3, 4, 1, 2)), ((33, 29), (1, 1, 1, 1)),
+                                      ((8, 256), (3, 3, 3, 3))])
+def test_tile_staging_tma_matches_element_copies(scheme, shape, bc):
+    """The flux kernel's TMA box copy and its per-element async copies stage the
+    same tile (zeros past the grid included): integrate results are identical."""
+    p = P.random_blocky(shape[0], shape[1], seed=11, bc=bc)
+    out = []
+    for tma in (True, False):
+        before = M.set_tile_tma(tma)
+        ctx = make_ctx(p, scheme=scheme)
+        U = p.U.copy()
+        st, UL, ideal = ctx.integrate_host(U)
+        used = M.set_tile_tma(None) - before
+        assert (used > 0) == tma
+        out.append((st.status, U, UL, ideal) + tuple(ctx.characteristics()))
+    M.set_tile_tma(True)
+    a, b = out
+    assert a[0] == b[0] and a[3] == b[3]
+    for x, y in zip(a[1:3] + a[4:], b[1:3] + b[4:]):
+        assert same(x, y)
+
+
 def test_error_paths():
     d = np.load(os.path.join(GOLD, "integrate_negdensity_2.npz"))
     p = _problem(d)
