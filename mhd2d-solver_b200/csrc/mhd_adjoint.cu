@@ -322,10 +322,13 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
 }
 
 // Per cell: sum the interface contributions of both directions and apply the
-// transposed flux Jacobians.  Interior cells first take the adjoint of the
-// stage update (combine_adj_at, mode) and then add the result to the
-// stage input's adjoint lbuf (one of lU, lU1, lU2, selected by in_buf); ghost
-// cells write it to T for the boundary-fill transpose.
+// transposed flux Jacobians.  Two lanes per cell (an even / odd lane pair):
+// the even lane takes the x direction, the odd lane the y direction; the
+// pair then adds the two parts in the order x, y.  Interior cells first take
+// the adjoint of the stage update (combine_adj_at, mode) and then add the
+// result to the stage input's adjoint lbuf (one of lU, lU1, lU2, selected by
+// in_buf); ghost cells write it to T for the boundary-fill transpose.  The
+// even lane writes fields 0-3, the odd lane fields 4-7.
 __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double* __restrict__ X,
                                                      const double* __restrict__ SX,
                                                      const double* __restrict__ SY,
@@ -334,18 +337,18 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
                                                      double* __restrict__ lU1,
                                                      double* __restrict__ lU2) {
   const long long NXY = (long long)g.NX * g.NY;
-  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (e >= NXY) return;
-  const int i = int(e / g.NY), j = int(e % g.NY);
-  double lu[NF];
+  const long long e2 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long e = e2 >> 1;
+  const bool yd = (e2 & 1) != 0;
+  const bool valid = e < NXY;
+  const int i = valid ? int(e / g.NY) : 0, j = valid ? int(e % g.NY) : 0;
+  double part[NF];  // this lane's direction, in the cell's (x) frame
 #pragma unroll
-  for (int k = 0; k < NF; k++) lu[k] = 0.0;
-  for (int dir = 0; dir < 2; dir++) {
-    const bool yd = dir == 1;
-    const int a = yd ? j : i;  // position along the direction
-    const int t = yd ? i : j;  // transverse position
-    const int ncell = yd ? g.ny : g.nx, ntr = yd ? g.nx : g.ny;
-    if (t < 2 || t > ntr + 1) continue;
+  for (int k = 0; k < NF; k++) part[k] = 0.0;
+  const int a = yd ? j : i;  // position along the direction
+  const int t = yd ? i : j;  // transverse position
+  const int ncell = yd ? g.ny : g.nx, ntr = yd ? g.nx : g.ny;
+  if (valid && t >= 2 && t <= ntr + 1) {
     const double* S = yd ? SY : SX;
     const int lo_bc = yd ? BOTTOM : LEFT, hi_bc = yd ? TOP : RIGHT;
     double fb[NF], qb[NF];
@@ -371,25 +374,37 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
         for (int k = 0; k < NF; k++) qb[k] += S[(36 + k) * NXY + off];
       }
     }
-    if (!any) continue;
-    double q[NF];
+    if (any) {
+      double q[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) q[k] = X[g.at(yd ? swap_xy(k) : k, i, j)];
-    flux_x_adjoint(G.gm, q, fb, qb);
+      for (int k = 0; k < NF; k++) q[k] = X[g.at(yd ? swap_xy(k) : k, i, j)];
+      flux_x_adjoint(G.gm, q, fb, qb);
 #pragma unroll
-    for (int k = 0; k < NF; k++) lu[yd ? swap_xy(k) : k] += qb[k];
+      for (int k = 0; k < NF; k++) part[yd ? swap_xy(k) : k] = qb[k];
+    }
   }
+  // lu = (0 + x part) + y part on both lanes of the pair
+  double lu[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    const double other = __shfl_xor_sync(0xffffffffu, part[k], 1);
+    const double px = yd ? other : part[k], py = yd ? part[k] : other;
+    lu[k] = (0.0 + px) + py;
+  }
+  if (!valid) return;
+  const int k0 = yd ? 4 : 0;
   if (i >= 2 && i <= g.nx + 1 && j >= 2 && j <= g.ny + 1) {
     double* lbuf = in_buf == 0 ? lU : (in_buf == 1 ? lU1 : lU2);
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const long long a = g.at(k, i, j);
-      combine_adj_at(mode, a, lU, lU1, lU2);
-      lbuf[a] += lu[k];
+    for (int kk = 0; kk < 4; kk++) {
+      const int k = k0 + kk;
+      const long long ad = g.at(k, i, j);
+      combine_adj_at(mode, ad, lU, lU1, lU2);
+      lbuf[ad] += yd ? lu[4 + kk] : lu[kk];
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < NF; k++) T[g.at(k, i, j)] = lu[k];
+    for (int kk = 0; kk < 4; kk++) T[g.at(k0 + kk, i, j)] = yd ? lu[4 + kk] : lu[kk];
   }
 }
 
@@ -916,7 +931,7 @@ void adjoint_stage(mhd_adj* a, int s, const StageRec& r, const double* X) {
   ka_adj_iface<true><<<int((ny_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
       g, a->G, X, my, lB, cL, a->SY, 1.0 / g.dy);
   const long long ncell = (long long)g.NX * g.NY;
-  ka_adj_gather<<<int((ncell + 127) / 128), 128, 0, a->stream>>>(
+  ka_adj_gather<<<int((2 * ncell + 127) / 128), 128, 0, a->stream>>>(
       g, a->G, X, a->SX, a->SY, a->T, r.mode, r.in_buf, a->lU, a->lU1, a->lU2);
   a->launches += 3;
   double* dst = lb[r.in_buf];
