@@ -44,6 +44,10 @@ struct mhd_ctx {
   const KernelSet* ks = &kExact;
   size_t block_elems = 0;  // doubles per state block
   double *U = nullptr, *U1 = nullptr, *U2 = nullptr, *UL = nullptr;
+  // input of the last spatial integration (0 U, 1 U1, 2 U2) while it is
+  // unchanged, else -1: the characteristics of that integration can be
+  // recomputed on request (mhd_get_characteristics without the flag)
+  int chars_buf = -1;
   double *ch[4] = {nullptr, nullptr, nullptr, nullptr};  // cx, cy, LUx, LUy
   double *aF = nullptr, *aG = nullptr;
   double *snap[4] = {nullptr, nullptr, nullptr, nullptr};  // left, right, bottom, top
@@ -90,6 +94,7 @@ cudaError_t alloc_block(mhd_ctx* c, double** p) {
 // copy a host [8][NX][NY] block into / out of the pitched device block
 cudaError_t h2d(mhd_ctx* c, double* dst, const double* src) {
   const Grid& g = c->g;
+  if (dst == c->U && c->chars_buf == 0) c->chars_buf = -1;  // new interior for U
   return cudaMemcpy2DAsync(dst + g.off, g.pitch * sizeof(double), src, g.NY * sizeof(double),
                            g.NY * sizeof(double), size_t(NF) * g.NX, cudaMemcpyHostToDevice,
                            c->stream);
@@ -122,6 +127,12 @@ void enqueue_integrate(mhd_ctx* c, double* X, bool chars) {
   if (c->scheme == 3) c->ks->lf_alpha(g, X, c->aF, c->aG, c->ctl, c->stream);
   c->ks->flux(c->scheme, g, X, c->UL, c->aF, c->aG, c->ctl, chars ? c->ch : nullptr, c->stream);
   c->launches += c->ks->launches_per_integrate(c->scheme);
+  c->chars_buf = X == c->U ? 0 : (X == c->U1 ? 1 : (X == c->U2 ? 2 : -1));
+}
+
+// The interior of buffer b (0 U, 1 U1, 2 U2) is about to change.
+void touch_buf(mhd_ctx* c, int b) {
+  if (c->chars_buf == b) c->chars_buf = -1;
 }
 
 void enqueue_control(mhd_ctx* c, int phase, double arg = 0.0) {
@@ -130,6 +141,7 @@ void enqueue_control(mhd_ctx* c, int phase, double arg = 0.0) {
 }
 
 void enqueue_combine(mhd_ctx* c, int mode) {
+  touch_buf(c, mode == 1 ? 1 : (mode == 2 ? 2 : 0));
   c->ks->combine(c->g, mode, c->U, c->U1, c->U2, c->UL, c->ctl, c->stream);
   c->launches += 1;
 }
@@ -221,6 +233,7 @@ int do_divb_calc(mhd_ctx* c, double* mx, double* tot) {
 }
 
 int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
+  touch_buf(c, 0);  // the B correction changes U's interior
   int r[4];
   divb_range(c, r);
   const Grid& g = c->g;
@@ -445,6 +458,7 @@ int mhd_init_dirichlet(mhd_ctx* c) {
   if (!c) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   c->ks->snapshot(c->g, c->U, c->snap, c->stream);
+  c->chars_buf = -1;  // another Dirichlet snapshot, other boundary values
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
   c->dirichlet_ready = true;
@@ -462,6 +476,7 @@ int mhd_set_dirichlet(mhd_ctx* c, const double* left, const double* right, const
   CK(cudaMemcpyAsync(c->snap[3], top, nx, cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->dirichlet_ready = true;
+  c->chars_buf = -1;  // other boundary values
   return set_status(c, MHD_OK, false, "");
 }
 
@@ -527,10 +542,23 @@ int mhd_steps(mhd_ctx* c, int nsteps, double* dt_inout, double* dts) {
 
 int mhd_get_characteristics(mhd_ctx* c, double* cx, double* cy, double* LUx, double* LUy) {
   if (!c) return MHD_ERR_WRONG_PARAMETER;
-  if (!(c->flags & MHD_FLAG_CHARACTERISTICS))
-    return set_status(c, MHD_ERR_WRONG_PARAMETER, true,
-                      "characteristics were not requested at context creation");
   CK(cudaSetDevice(c->device));
+  if (!(c->flags & MHD_FLAG_CHARACTERISTICS)) {
+    // on request: the last spatial integration again, on its unchanged input,
+    // with the characteristics kernel (the same values the flag would keep)
+    if (c->chars_buf < 0)
+      return set_status(c, MHD_ERR_WRONG_PARAMETER, true,
+                        "characteristics not available: the input of the last spatial "
+                        "integration has changed since (or none ran); create the context with "
+                        "MHD_FLAG_CHARACTERISTICS to keep them every time");
+    for (int q = 0; q < 4; q++)
+      if (!c->ch[q]) CK(alloc_block(c, &c->ch[q]));
+    double* X = c->chars_buf == 0 ? c->U : (c->chars_buf == 1 ? c->U1 : c->U2);
+    enqueue_control(c, PH_RESET_INTEGRATE);
+    enqueue_integrate(c, X, true);
+    int st = read_ctl(c);
+    if (st) return st;
+  }
   double* dst[4] = {cx, cy, LUx, LUy};
   for (int q = 0; q < 4; q++)
     if (dst[q]) CK(d2h(c, dst[q], c->ch[q]));

@@ -249,6 +249,40 @@ def test_tile_staging_tma_matches_element_copies(scheme, shape, bc):
         assert same(x, y)
 
 
+@pytest.mark.parametrize("scheme", [M.ENO_ROE, M.ENO_LF])
+def test_characteristics_on_request_match_the_flag(scheme):
+    """Without MHD_FLAG_CHARACTERISTICS the characteristics of the last spatial
+    integration are recomputed on request from its unchanged input (the
+    reference writes them only at output steps): the same values as the flag
+    keeps, and the run itself is not disturbed."""
+    p = P.random_smooth(37, 29, seed=21, bc=(M.NEUMANN, M.NEUMANN, M.PERIODIC, M.PERIODIC))
+    kw = dict(scheme=scheme, dt_min=1e-9, dt_max=0.01)
+    a = make_ctx(p, flags=M.FLAG_CHARACTERISTICS, **kw)
+    b = make_ctx(p, flags=0, **kw)
+    dta = dtb = 1e-3
+    for _ in range(3):
+        _, dta = a.step(dta)
+        _, dtb = b.step(dtb)
+    for x, y in zip(a.characteristics(), b.characteristics()):
+        assert same(x, y)
+    _, dta = a.step(dta)
+    _, dtb = b.step(dtb)
+    assert dta == dtb and same(a.download(), b.download())
+    for x, y in zip(a.characteristics(), b.characteristics()):
+        assert same(x, y)
+    # after a single integration of U
+    U = p.U.copy()
+    a.integrate_host(U.copy())
+    b.integrate_host(U.copy())
+    for x, y in zip(a.characteristics(), b.characteristics()):
+        assert same(x, y)
+    # Euler: the last integration's input is U, which the step then changed
+    e = make_ctx(p, time_method=M.EULER, flags=0, **kw)
+    e.step(1e-3)
+    with pytest.raises(M.MhdError):
+        e.characteristics()
+
+
 def test_error_paths():
     d = np.load(os.path.join(GOLD, "integrate_negdensity_2.npz"))
     p = _problem(d)
