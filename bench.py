@@ -43,9 +43,10 @@ REF_SAMPLE = 512
 FLOPS_PER_CELL_INTEGRATE = {2: 3011.9, 3: 3514.0}
 FLOPS_PER_CELL_STEP = {2: 9147.6, 3: 10653.9}
 # DRAM bytes (read + write) of one k_flux launch per interior cell, from one
-# ncu capture of the 2048^2 ENO-Roe case (545.2 MB; profiles/
-# k_flux_eno_roe_ot2048_ncu.md), scaled to a launch by its cell count.
-DRAM_BYTES_PER_CELL_FLUX = 545.17e6 / 2048 ** 2
+# ncu capture of the 2048^2 ENO-Roe case with TMA-staged tiles (273.5 MB read
+# + 264.4 MB written; profiles/k_flux_eno_roe_ot2048_ncu.md), scaled to a
+# launch by its cell count.
+DRAM_BYTES_PER_CELL_FLUX = (273.486e6 + 264.385e6) / 2048 ** 2
 
 
 def parse():
