@@ -213,9 +213,10 @@ int mhd_time_integrate( mhd_ctx* ctx, int n, double* avg_ms );
 int mhd_fp64_peak( int device, double* tflops );
 
 /* No counterpart in the reference.  The div B diagnostic of mhd_divb_calc
-   for callers that cannot allocate device memory (code running under CUDA
-   graph capture, plug-ins inside an application that owns all device
-   memory, runtimes that forbid allocation after start-up).  It allocates
+   for callers that cannot allocate device memory (plug-ins inside an
+   application that owns all device memory through its own pool, runtimes
+   that forbid allocation once running, since cudaMalloc can synchronise
+   the device and stall every other stream).  It allocates
    nothing: its scratch (one partial max and sum per grid row) is a fixed
    file-scope device array of 2 x 16384 doubles that every GPU loading the
    library keeps until exit, so nx may not exceed 16384

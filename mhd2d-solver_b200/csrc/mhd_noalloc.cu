@@ -1,10 +1,11 @@
 // mhd_divb_calc_noalloc: the div B diagnostic (divBCalculation,
 // div_b_fix.cpp:4-126) for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is
-// being captured, plug-ins living inside a host application that owns all
-// device memory through its own pool, and runtimes that forbid allocation
-// after start-up.  This entry point works on buffers the caller already
+// Some callers cannot call cudaMalloc: plug-ins living inside a host
+// application that owns all device memory through its own pool, and
+// runtimes that forbid allocation once they are running (cudaMalloc can
+// synchronise the device and stall every other stream, which a solver
+// stepping in a time-critical loop cannot afford).  This entry point works on buffers the caller already
 // owns (the state and a 2-double result) and keeps its own scratch - one
 // partial maximum and one partial sum per grid row - in the file-scope
 // device array below, which every GPU that loads the library holds until

@@ -1,6 +1,7 @@
 """mhd_divb_calc_noalloc: the div B diagnostic for callers that cannot
-allocate device memory (graph capture, plug-ins inside applications that own
-all device memory, runtimes that forbid allocation after start-up).
+allocate device memory (plug-ins inside applications that own all device
+memory through their own pool, runtimes that forbid allocation once running,
+because cudaMalloc can synchronise the device and stall other streams).
 
 The caller owns the state and the 2-double result on the device; the entry
 point's own scratch is a fixed device array inside the library.  Checked
