@@ -197,6 +197,14 @@ int mhd_layout( const mhd_ctx* ctx, int* pitch, int* row_offset );
    Results are bit-identical either way. */
 int mhd_set_tile_tma( int enable, long long* tma_launches );
 
+/* SOR sweeps of this context (divBCorrectionSOR, div_b_fix.cpp:129-403):
+   1 (the default) runs a sweep as two launches, one per colour, where the
+   grid allows it (every periodic side's extent a multiple of 4): periodic
+   ghosts are read at their source points and the convergence test runs in
+   the second launch; 0 always refreshes the ghosts after each colour and
+   tests in a launch of its own (five launches).  Results are identical. */
+int mhd_set_sor_fused( mhd_ctx* ctx, int enable );
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record
    events or order their own work against the context's kernels. */
 int mhd_stream( const mhd_ctx* ctx, void** stream );

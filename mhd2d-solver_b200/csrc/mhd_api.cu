@@ -53,6 +53,7 @@ struct mhd_ctx {
   double *snap[4] = {nullptr, nullptr, nullptr, nullptr};  // left, right, bottom, top
   double *phi = nullptr, *partial = nullptr, *ratio = nullptr;
   double* sor_xy = nullptr;  // source terms of the current SOR solve (allocated on first use)
+  int sor_fused = 1;         // fused SOR sweeps where the grid allows them (mhd_set_sor_fused)
   int npartial = 0;
   Ctl* ctl = nullptr;
   Ctl* hctl = nullptr;  // pinned mirror
@@ -257,21 +258,32 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
   c->ks->sor_rhs(g, c->U, r, coef, c->sor_xy, c->stream);
   c->launches += 1;
   CK(cudaMemsetAsync(&c->ctl->rmax, 0, 2 * sizeof(unsigned long long), c->stream));
-  CK(cudaMemsetAsync(&c->ctl->sor_done, 0, 2 * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(&c->ctl->sor_done, 0, 3 * sizeof(int), c->stream));  // + sor_ticket
   CK(cudaMemcpyAsync(c->ratio, &nan_ratio, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   long long issued = 0;
   const int chunk = 16;
+  // fused sweeps: 2 launches per sweep instead of 5 (same arithmetic, same
+  // values; see sor_fused_ok), with the ghosts refreshed around the solve
+  const int fused = sor_fused_ok(g) && c->sor_fused ? 1 : 0;
   if (p->sor_rsteps > 0) {
+    if (fused) {
+      c->ks->phi_bc(g, c->phi, c->ctl, c->stream);
+      c->launches += 1;
+    }
     for (;;) {
       for (int s = 0; s < chunk; s++) {
         c->ks->sor_sweep(g, c->phi, c->sor_xy, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio,
-                         c->ctl, c->stream);
-        c->launches += 5;
+                         c->ctl, fused, c->stream);
+        c->launches += fused ? 2 : 5;
       }
       issued += chunk;
       int st = read_ctl(c);
       if (st) return st;
       if (c->hctl->sor_done) break;
+    }
+    if (fused) {
+      c->ks->phi_bc(g, c->phi, c->ctl, c->stream);
+      c->launches += 1;
     }
   }
   double last = 0.0;
@@ -729,6 +741,12 @@ int mhd_set_tile_tma(int enable, long long* tma_launches) {
   if (enable != 0 && enable != 1 && enable != -1) return MHD_ERR_WRONG_PARAMETER;
   if (enable >= 0) tile_tma_flag() = enable != 0;
   if (tma_launches) *tma_launches = tile_tma_launches();
+  return MHD_OK;
+}
+
+int mhd_set_sor_fused(mhd_ctx* c, int enable) {
+  if (!c || (enable != 0 && enable != 1)) return MHD_ERR_WRONG_PARAMETER;
+  c->sor_fused = enable;
   return MHD_OK;
 }
 

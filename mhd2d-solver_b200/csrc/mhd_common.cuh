@@ -32,6 +32,20 @@ struct Grid {
   }
 };
 
+// Fused SOR sweeps: a periodic side's ghost rows / columns are copies of
+// interior points (k_phi_bc).  When every periodic side's grid extent is a
+// multiple of 4, a copied point lies an odd number of 2-cell blocks away
+// from the points that read its ghost, so it has the other colour: during a
+// half sweep it does not change, and reading it in place gives the value
+// its ghost would hold.  Open sides copy a point that no sweep updates (row / column 2 or
+// n+1), so their ghosts need refreshing only once per solve.  A fused sweep
+// is then two launches with no ghost refresh in between.
+__host__ __device__ inline bool sor_fused_ok(const Grid& g) {
+  const bool px = g.bc[LEFT] == PERIODIC || g.bc[RIGHT] == PERIODIC;
+  const bool py = g.bc[BOTTOM] == PERIODIC || g.bc[TOP] == PERIODIC;
+  return (!px || g.nx % 4 == 0) && (!py || g.ny % 4 == 0);
+}
+
 // Device control block of one context: reductions, dt bookkeeping and the
 // status words the host reads back once per call.
 struct Ctl {
@@ -51,7 +65,8 @@ struct Ctl {
   unsigned long long divb_max;    // bit pattern of max |div B|
   double divb_sum;
   int sor_done, sor_sweeps;
-  int pad[2];
+  unsigned sor_ticket;  // blocks of a fused SOR colour launch that have finished
+  int pad;
 };
 
 // Phases of the one-thread time-step controller (k_control).

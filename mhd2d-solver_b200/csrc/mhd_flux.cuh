@@ -28,6 +28,22 @@
 #define MHD_MINB 2
 #endif
 
+// How pair_flux forms the characteristics of the fast (finite, structural
+// zeros skipped) interface flux, per scheme: bit 0 pairs the left rows of
+// the mirror waves k and 6 - k, bit 1 pairs their right rows; 0 forms one
+// row at a time.  -1 keeps the streamed one-pass loop of interface_flux.
+#ifndef MHD_PAIRS_ROE
+#define MHD_PAIRS_ROE -1
+#endif
+#ifndef MHD_PAIRS_LF
+#define MHD_PAIRS_LF 3
+#endif
+// ENO-Roe, streamed loop: 1 projects only the upwind side's stencil (see
+// roe_side_flux), 0 all four points and three differences.
+#ifndef MHD_ROE_SIDE
+#define MHD_ROE_SIDE 1
+#endif
+
 #ifndef MHD_KNS
 #define MHD_KNS exact
 #endif
@@ -113,6 +129,246 @@ struct Lane {
   }
 };
 
+// Upwind choice of the ENO-Roe flux of one characteristic from its
+// projections w (4 points) and undivided differences vw (3 points)
+// (spatialmethodenoroe.cpp:240-264).
+__device__ __forceinline__ double roe_upwind(const double* w, const double* vw, double ak) {
+  const double wm = eno_minus(w[0], w[1], w[2], vw[0], vw[1]);
+  const double wp = eno_plus(w[1], w[2], w[3], vw[1], vw[2]);
+  return (ak >= 0 && wm < 1.0e10) ? wm : ((ak <= 0 && wp < 1.0e10) ? wp : 0.0);
+}
+
+// ENO-Roe flux of characteristic k with left row l, projecting only what
+// the reference's choice keeps (spatialmethodenoroe.cpp:240-264).  The
+// reference projects the fluxes at all 4 stencil points and their 3
+// undivided differences, then keeps one ENO pair of the upwind side: for
+// lambda > 0 the ENO- pair, chosen by the differences 0 and 1, and for
+// lambda < 0 the ENO+ pair, chosen by the differences 1 and 2.  Here the two
+// differences of the upwind side decide the pair, and only its two points
+// are projected: 4 of the 7 dot products, each the same sum in the same
+// order, so fw carries the same bits.  lambda = 0 (both sides may be used)
+// and NaN take the full projection.
+__device__ __forceinline__ double roe_side_flux(const Lane& L, const double* l, unsigned lm,
+                                                double ak) {
+  if (ak > 0.0 || ak < 0.0) {
+    const int s0 = ak > 0.0 ? 0 : 1;
+    double va = 0.0, vb = 0.0;
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      if (!(lm & (1u << m))) continue;
+      const double fa = L.F(m, s0), fb = L.F(m, s0 + 1), fc = L.F(m, s0 + 2);
+      va += l[m] * (fb - fa);
+      vb += l[m] * (fc - fb);
+    }
+    // ENO-: |vw0| < |vw1| takes points 0, 1, else 1, 2; ENO+: |vw1| < |vw2|
+    // takes points 1, 2, else 2, 3
+    const int pa = s0 + (fabs(va) < fabs(vb) ? 0 : 1);
+    double wa = 0.0, wb = 0.0;
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      if (!(lm & (1u << m))) continue;
+      wa += l[m] * L.F(m, pa);
+      wb += l[m] * L.F(m, pa + 1);
+    }
+    const double v = pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
+                   : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
+                              : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
+    return v < 1.0e10 ? v : 0.0;
+  }
+  double w[4] = {0.0, 0.0, 0.0, 0.0}, vw[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    if (!(lm & (1u << m))) continue;
+    const double f0 = L.F(m, 0), f1 = L.F(m, 1), f2 = L.F(m, 2), f3 = L.F(m, 3);
+    w[0] += l[m] * f0;
+    w[1] += l[m] * f1;
+    w[2] += l[m] * f2;
+    w[3] += l[m] * f3;
+    vw[0] += l[m] * (f1 - f0);
+    vw[1] += l[m] * (f2 - f1);
+    vw[2] += l[m] * (f3 - f2);
+  }
+  return roe_upwind(w, vw, ak);
+}
+
+// ENO-LF flux of one characteristic from its projections of the state (ru)
+// and of the flux (rf) at the 4 stencil points and its dissipation
+// coefficient al (spatialmethodenolf.cpp:276-326).
+__device__ __forceinline__ double lf_split(const double* ru, const double* rf, double al) {
+  double w[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) w[p] = 0.5 * (rf[p] + al * ru[p]);
+  const double wm = eno_minus(w[0], w[1], w[2], w[1] - w[0], w[2] - w[1]);
+#pragma unroll
+  for (int p = 0; p < 4; p++) w[p] = 0.5 * (rf[p] - al * ru[p]);
+  const double wp = eno_plus(w[1], w[2], w[3], w[2] - w[1], w[3] - w[2]);
+  return wm + wp;
+}
+
+// Left row k of a characteristic projected on the stencil: the ENO-Roe
+// projections of the fluxes and their undivided differences, or the ENO-LF
+// projections of the state and the fluxes, reduced to the characteristic
+// flux fw; LU gets lv.U1 (Roe) or lv.U at point 1 (LF).  Two rows at once
+// (TWO) share the stencil reads and the differences.
+template <int SCHEME, bool CHARS, bool TWO>
+__device__ __forceinline__ void project_rows(const Mid& e, const Lane& L, const double* U1,
+                                             const double* alpha, int ka, int kb,
+                                             const double* la, const double* lb, double* fw,
+                                             double* LU) {
+  const unsigned lm = lv_mask(ka);  // == lv_mask(kb)
+  if constexpr (SCHEME == 2) {
+    double wa[4] = {0.0, 0.0, 0.0, 0.0}, va[3] = {0.0, 0.0, 0.0};
+    double wb[4] = {0.0, 0.0, 0.0, 0.0}, vb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      if (!(lm & (1u << m))) continue;
+      const double f0 = L.F(m, 0), f1 = L.F(m, 1), f2 = L.F(m, 2), f3 = L.F(m, 3);
+      const double d0 = f1 - f0, d1 = f2 - f1, d2 = f3 - f2;
+      wa[0] += la[m] * f0;
+      wa[1] += la[m] * f1;
+      wa[2] += la[m] * f2;
+      wa[3] += la[m] * f3;
+      va[0] += la[m] * d0;
+      va[1] += la[m] * d1;
+      va[2] += la[m] * d2;
+      if (TWO) {
+        wb[0] += lb[m] * f0;
+        wb[1] += lb[m] * f1;
+        wb[2] += lb[m] * f2;
+        wb[3] += lb[m] * f3;
+        vb[0] += lb[m] * d0;
+        vb[1] += lb[m] * d1;
+        vb[2] += lb[m] * d2;
+      }
+    }
+    fw[ka] = roe_upwind(wa, va, eigenvalue(e, ka));
+    if (TWO) fw[kb] = roe_upwind(wb, vb, eigenvalue(e, kb));
+    if (CHARS) {
+      double acc = 0.0, acb = 0.0;
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (lm & (1u << m)) {
+          acc += la[m] * U1[m];
+          if (TWO) acb += lb[m] * U1[m];
+        }
+      LU[ka] = acc;
+      if (TWO) LU[kb] = acb;
+    }
+  } else {
+    double rua[4], rfa[4], rub[4], rfb[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (lm & (1u << m)) {
+          const double q = L.Q(m, p), f = L.F(m, p);
+          a += la[m] * q;
+          b += la[m] * f;
+          if (TWO) {
+            c += lb[m] * q;
+            d += lb[m] * f;
+          }
+        }
+      rua[p] = a; rfa[p] = b; rub[p] = c; rfb[p] = d;
+    }
+    fw[ka] = lf_split(rua, rfa, alpha[ka]);
+    if (TWO) fw[kb] = lf_split(rub, rfb, alpha[kb]);
+    if (CHARS) {
+      LU[ka] = rua[1];
+      if (TWO) LU[kb] = rub[1];
+    }
+  }
+}
+
+// Characteristics 0..6 of one interface (SCHEME 2 ENO-Roe, 3 ENO-LF), fast
+// form (finite values, structural zeros skipped), in two passes: the left
+// rows give the 7 characteristic fluxes fw, the right rows project them
+// back.
+//
+// The rows of the mirror waves k and 6 - k are sums and differences of the
+// same products (spatialmethodeno.cpp:392-552).  LV_PAIRS forms both left
+// rows of a pair together, so the shared products are formed once and one
+// pass over the stencil serves both.  RV_PAIRS does the same for the right
+// rows; the back projection must still add the waves in the order 0..6
+// like the reference's loop, so the products of waves 6, 5, 4 (rounded on
+// their own, as the unfused build rounds every product) wait in registers
+// and are added after wave 3.  Every value is the reference's expression in
+// the reference's order, so all forms give the same bits.
+template <int SCHEME, bool CHARS, bool LV_PAIRS, bool RV_PAIRS>
+__device__ __forceinline__ void pair_flux(Mid& e, const Gas& G, const Lane& L, const double* U1,
+                                          const double* alpha, double* Fn, double* LU,
+                                          bool& nonfinite) {
+  double fw[7];
+  if constexpr (LV_PAIRS) {
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      opaque(e);
+      double la[NF], lb[NF];
+      lv_row(e, G, t, la);
+      if (t < 3) {
+        lv_row(e, G, 6 - t, lb);
+        project_rows<SCHEME, CHARS, true>(e, L, U1, alpha, t, 6 - t, la, lb, fw, LU);
+      } else {
+        project_rows<SCHEME, CHARS, false>(e, L, U1, alpha, t, t, la, la, fw, LU);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+      opaque(e);
+      double l[NF];
+      lv_row(e, G, k, l);
+      project_rows<SCHEME, CHARS, false>(e, L, U1, alpha, k, k, l, l, fw, LU);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 7; k++)
+    if (!isfinite(fw[k])) nonfinite = true;
+
+  if constexpr (RV_PAIRS) {
+    double h[3][NF];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      opaque(e);
+      const bool two = t < 3;
+      double qa[NF], qb[NF];
+      rv_row(e, G, t, qa);
+      if (two) rv_row(e, G, 6 - t, qb);
+      const unsigned rm = rv_mask(t);  // == rv_mask(6 - t)
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (rm & (1u << m)) {
+          Fn[m] += qa[m] * fw[t];
+          if (two) h[t][m] = qb[m] * fw[6 - t];
+        }
+    }
+#pragma unroll
+    for (int t = 2; t >= 0; t--) {  // waves 4, 5, 6
+      const unsigned rm = rv_mask(t);
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (rm & (1u << m)) Fn[m] += h[t][m];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+      opaque(e);
+      double q[NF];
+      rv_row(e, G, k, q);
+      const unsigned rm = rv_mask(k);
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (rm & (1u << m)) Fn[m] += q[m] * fw[k];
+    }
+  }
+  // the dummy wave 7 contributes +0 * +0 last in the reference's sums
+#pragma unroll
+  for (int m = 0; m < NF; m++)
+    if (m != 4) Fn[m] = Fn[m] + 0.0;
+  if (CHARS) LU[7] = 0.0;
+}
+
 // Numerical flux of one interface in the lane's frame: Fn[m], m = 0..7 (Fn[4]
 // is the structurally zero component), lam / LU the characteristic outputs.
 //
@@ -152,6 +408,13 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
 #pragma unroll
   for (int m = 0; m < NF; m++) Fn[m] = 0.0;
 
+  constexpr int PAIRS = SCHEME == 2 ? MHD_PAIRS_ROE : MHD_PAIRS_LF;
+  if constexpr (!DENSE && MASK == 0 && PAIRS >= 0) {
+    pair_flux<SCHEME, CHARS, (PAIRS & 1) != 0, (PAIRS & 2) != 0>(e, G, L, U1, alpha, Fn, LU,
+                                                                 nonfinite);
+    return true;
+  }
+
   constexpr int KN = DENSE ? 8 : 7;
 #ifndef MHD_K_UNROLL
 #define MHD_K_UNROLL 7
@@ -189,6 +452,8 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
            : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
                         : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
       }
+    } else if (SCHEME == 2 && MASK == 0 && !DENSE && MHD_ROE_SIDE) {
+      fw = roe_side_flux(L, l, lm, eigenvalue(e, k));
     } else if (SCHEME == 2) {  // ENO-Roe: project F and its undivided differences
       // w = lv.F at the 4 points, Vw = lv.(F[p+1] - F[p]) at 3 points; each
       // sum runs over m in ascending order, like the reference's loops

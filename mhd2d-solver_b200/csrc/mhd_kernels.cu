@@ -121,20 +121,34 @@ void l_sor_rhs(const Grid& g, const double* U, const int range[4], const double 
 
 void l_sor_sweep(const Grid& g, double* phi, const double* xy, const int range[4],
                  const double coef[6], double rtol, double max_sweeps, double* last_ratio,
-                 Ctl* ctl, cudaStream_t s) {
+                 Ctl* ctl, int fused, cudaStream_t s) {
   DivRange R{range[0], range[1], range[2], range[3]};
   SorCoef c{coef[0], coef[1], coef[2], coef[3], coef[4], coef[5]};
   dim3 grid((sor_pairs(R) + SOR_THREADS - 1) / SOR_THREADS,
             (R.x1 - R.x0 + SOR_ROWS - 1) / SOR_ROWS);
   const int m = g.nx > g.ny ? g.nx : g.ny;
   const double4* f = reinterpret_cast<const double4*>(xy);
+  if (fused) {
+    k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, 1, rtol, max_sweeps,
+                                            last_ratio);
+    k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, 1, rtol, max_sweeps,
+                                            last_ratio);
+    return;
+  }
   // ghosts are refreshed after each colour: with periodic sides they mirror
   // points of the other colour (see k_sor_half)
-  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl);
-  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl);
-  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl);
-  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl);
+  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, 0, rtol, max_sweeps,
+                                          last_ratio);
+  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 0);
+  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, 0, rtol, max_sweeps,
+                                          last_ratio);
+  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 0);
   k_sor_check<<<1, 32, 0, s>>>(ctl, rtol, max_sweeps, last_ratio);
+}
+
+void l_phi_bc(const Grid& g, double* phi, const Ctl* ctl, cudaStream_t s) {
+  const int m = g.nx > g.ny ? g.nx : g.ny;
+  k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 1);
 }
 
 void l_sor_correct(const Grid& g, double* U, const double* phi, const int range[4], double bxf,
@@ -159,6 +173,6 @@ int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
 using namespace MHD_KNS;
 extern const KernelSet MHD_KSET = {MHD_KSET_NAME, l_bc, l_snapshot, l_lf_alpha, l_flux,
                                    l_combine, l_control, l_divb, l_sor_rhs, l_sor_sweep,
-                                   l_sor_correct, l_totals, l_smem, l_launches};
+                                   l_phi_bc, l_sor_correct, l_totals, l_smem, l_launches};
 
 }  // namespace mhd

@@ -39,10 +39,16 @@ struct KernelSet {
   // column pair, sor_xy_doubles of them)
   void (*sor_rhs)(const Grid& g, const double* U, const int range[4], const double coef[6],
                   double* xy, cudaStream_t s);
-  // one SOR sweep (both colours, potential ghosts, convergence check)
+  // one SOR sweep (both colours, potential ghosts, convergence check).
+  // fused = 1: two launches that read periodic ghosts at their source and
+  // run the convergence check in the second one (sor_fused_ok must hold;
+  // the caller refreshes the ghosts with phi_bc before the first and after
+  // the last sweep of the solve)
   void (*sor_sweep)(const Grid& g, double* phi, const double* xy, const int range[4],
                     const double coef[6], double rtol, double max_sweeps, double* last_ratio,
-                    Ctl* ctl, cudaStream_t s);
+                    Ctl* ctl, int fused, cudaStream_t s);
+  // potential ghosts (div_b_fix.cpp:282-364), regardless of the stop flag
+  void (*phi_bc)(const Grid& g, double* phi, const Ctl* ctl, cudaStream_t s);
   void (*sor_correct)(const Grid& g, double* U, const double* phi, const int range[4],
                       double bxf, double byf, cudaStream_t s);
   // non-grid output totals: 5 partials per block (entropy, energy, mass,

@@ -432,12 +432,35 @@ __global__ void k_sor_rhs(Grid g, const double* __restrict__ U, DivRange R, SorC
   }
 }
 
+// Row read in place of periodic ghost row r (fused sweeps).
+__device__ __forceinline__ int sor_src_row(const Grid& g, int r) {
+  if (g.bc[LEFT] == PERIODIC && r < 2) return r + g.nx;
+  if (g.bc[RIGHT] == PERIODIC && r >= g.nx + 2) return r - g.nx;
+  return r;
+}
+
+// Convergence test after a sweep (div_b_fix.cpp:370-373): stop when
+// max|update| / max|phi| <= rmax.  The ratio of the last sweep is kept for
+// the final verdict, which the host evaluates as the reference does.
+__device__ __forceinline__ void sor_check(Ctl* c, double rtol, double max_sweeps,
+                                          double* last_ratio) {
+  const double ratio = bits_to_double(c->rmax) / bits_to_double(c->pmax);
+  *last_ratio = ratio;
+  c->rmax = 0ull; c->pmax = 0ull;
+  c->sor_sweeps += 1;
+  if (ratio <= rtol || c->sor_sweeps >= max_sweeps) c->sor_done = 1;
+}
+
 // One colour of a red-black sweep.  The potential pairs are read and written
-// as 16-byte items (jb is even, the padded row offset is even).
+// as 16-byte items (jb is even, the padded row offset is even).  fused = 1:
+// periodic ghosts are read at their source points, and the last block of the
+// colour-1 launch runs the convergence test.
 __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __restrict__ phi,
                                                           const double4* __restrict__ xy,
                                                           DivRange R, SorCoef s, int color,
-                                                          Ctl* c) {
+                                                          Ctl* c, int fused, double rtol,
+                                                          double max_sweeps,
+                                                          double* last_ratio) {
   if (c->sor_done) return;
   __shared__ double red[2][SOR_THREADS / 32];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -453,10 +476,19 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
       if (jb + 1 < R.y0 || jb >= R.y1) continue;
       double* prow = phi + (long long)i * P + g.off;
       const double4 f = xy[((long long)color * H + ir) * Q + q];
-      const double2 up = *reinterpret_cast<const double2*>(prow + jb + 2 * P);
-      const double2 dn = *reinterpret_cast<const double2*>(prow + jb - 2 * P);
-      const double2 lf = *reinterpret_cast<const double2*>(prow + jb - 2);
-      const double2 rt = *reinterpret_cast<const double2*>(prow + jb + 2);
+      const double* urow = prow + 2 * P;
+      const double* drow = prow - 2 * P;
+      int jl = jb - 2, jr = jb + 2;
+      if (fused) {
+        urow = phi + (long long)sor_src_row(g, i + 2) * P + g.off;
+        drow = phi + (long long)sor_src_row(g, i - 2) * P + g.off;
+        if (g.bc[BOTTOM] == PERIODIC && jl < 2) jl += g.ny;
+        if (g.bc[TOP] == PERIODIC && jr >= g.ny + 2) jr -= g.ny;
+      }
+      const double2 up = *reinterpret_cast<const double2*>(urow + jb);
+      const double2 dn = *reinterpret_cast<const double2*>(drow + jb);
+      const double2 lf = *reinterpret_cast<const double2*>(prow + jl);
+      const double2 rt = *reinterpret_cast<const double2*>(prow + jr);
       double2 me = *reinterpret_cast<const double2*>(prow + jb);
       const double ax[2] = {up.x, up.y}, bx[2] = {dn.x, dn.y};
       const double ay[2] = {rt.x, rt.y}, by[2] = {lf.x, lf.y};
@@ -497,12 +529,24 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
     }
     atomic_max_pos(&c->rmax, rmax);
     atomic_max_pos(&c->pmax, pmax);
+    if (fused && color == 1) {
+      // the last block to finish sees every block's maxima
+      __threadfence();
+      const unsigned nb = gridDim.x * gridDim.y;
+      if (atomicAdd(&c->sor_ticket, 1u) == nb - 1) {
+        __threadfence();
+        c->sor_ticket = 0u;
+        sor_check(c, rtol, max_sweeps, last_ratio);
+      }
+    }
   }
 }
 
-// Potential ghosts after each sweep (div_b_fix.cpp:282-364).
-__global__ void k_phi_bc(Grid g, double* __restrict__ phi, const Ctl* c) {
-  if (c->sor_done) return;
+// Potential ghosts after each sweep (div_b_fix.cpp:282-364).  force = 1
+// refreshes them whether or not the solve has stopped (fused sweeps: once
+// before the first and once after the last sweep).
+__global__ void k_phi_bc(Grid g, double* __restrict__ phi, const Ctl* c, int force) {
+  if (!force && c->sor_done) return;
   const int nx = g.nx, ny = g.ny, m = nx > ny ? nx : ny;
   const long long P = g.pitch;
   auto PH = [&](int i, int j) -> double& { return phi[(long long)i * P + g.off + j]; };
@@ -523,16 +567,10 @@ __global__ void k_phi_bc(Grid g, double* __restrict__ phi, const Ctl* c) {
   }
 }
 
-// Convergence test after a sweep (div_b_fix.cpp:370-373): stop when
-// max|update| / max|phi| <= rmax.  The ratio of the last sweep is kept for
-// the final verdict, which the host evaluates as the reference does.
+// The convergence test of the unfused sweep, as its own one-thread launch.
 __global__ void k_sor_check(Ctl* c, double rtol, double max_sweeps, double* last_ratio) {
   if (threadIdx.x != 0 || blockIdx.x != 0 || c->sor_done) return;
-  const double ratio = bits_to_double(c->rmax) / bits_to_double(c->pmax);
-  *last_ratio = ratio;
-  c->rmax = 0ull; c->pmax = 0ull;
-  c->sor_sweeps += 1;
-  if (ratio <= rtol || c->sor_sweeps >= max_sweeps) c->sor_done = 1;
+  sor_check(c, rtol, max_sweeps, last_ratio);
 }
 
 // B += central gradient of phi over [x0-1, x1+1) x [y0-1, y1+1)

@@ -152,6 +152,7 @@ def library():
         "mhd_divb_calc": [vp, _dp, _dp],
         "mhd_nongrid_data": [vp, _dp],
         "mhd_set_tile_tma": [C.c_int, C.POINTER(C.c_longlong)],
+        "mhd_set_sor_fused": [vp, C.c_int],
         "mhd_run": [vp, C.POINTER(RunParams), C.POINTER(NongridRecord), C.c_int,
                     C.POINTER(RunResult)],
         "mhd_divb_sor": [vp, C.POINTER(SorParams), _ip],
@@ -371,6 +372,10 @@ class Context:
         st = self._check(self.lib.mhd_divb_clean(self.h, C.byref(params), C.byref(m),
                                                  C.byref(sw)), "divb_clean")
         return self.last_status(st), m.value, sw.value
+
+    def set_sor_fused(self, enable):
+        """Two-launch SOR sweeps where the grid allows them (default on)."""
+        self._check(self.lib.mhd_set_sor_fused(self.h, int(bool(enable))), "set_sor_fused")
 
     def stream(self):
         """The context's cudaStream_t as an integer handle."""

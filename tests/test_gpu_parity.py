@@ -198,6 +198,33 @@ def test_sor_red_black_vs_oracle(bc):
         assert same(ctx.download(), Uo)
 
 
+@pytest.mark.parametrize("shape,bc,fusable", [
+    ((40, 36), (1, 1, 1, 1), True), ((42, 36), (1, 1, 1, 1), False),
+    ((44, 40), (1, 3, 4, 1), True), ((41, 37), (4, 4, 4, 4), True),
+    ((48, 38), (4, 1, 3, 1), False), ((36, 44), (2, 4, 1, 1), True)])
+def test_sor_fused_sweeps_match_unfused_and_oracle(shape, bc, fusable):
+    """Two-launch sweeps (periodic ghosts read at their source, convergence
+    test in the second launch) give the same potential, corrected field and
+    sweep counts as the five-launch sweeps and the oracle's red-black solve,
+    over two warm-started solves; grids whose periodic extent is not a
+    multiple of 4 keep the five-launch sweeps."""
+    p = P.random_smooth(*shape, seed=sum(bc) + shape[0], bc=bc)
+    sp = M.sor_params(1, 5, 20000, 1e-10, 1e-10, True, 1.7)
+    osp = SorParams(1, 5, 20000.0, 1e-10, 1e-10, 1, 1.7)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, bc)
+    Uo = p.U.copy()
+    ctxs = [make_ctx(p, flags=0), make_ctx(p, flags=0)]
+    ctxs[1].set_sor_fused(False)
+    for _ in range(2):
+        so, eo, swo = o.divb_sor(Uo, osp, red_black=1)
+        for ctx in ctxs:
+            st, sweeps = ctx.divb_sor(sp)
+            assert (st.status, int(st.isError), sweeps) == (so, eo, swo)
+            assert same(ctx.download(), Uo)
+    launches = [ctx.counters()["launches"] for ctx in ctxs]
+    assert (launches[0] < launches[1]) == fusable
+
+
 def test_divb_calc_vs_oracle():
     p = P.random_blocky(50, 41, seed=3, bc=(1, 1, 3, 4))
     ctx = make_ctx(p, flags=0)
