@@ -43,10 +43,10 @@ REF_SAMPLE = 512
 FLOPS_PER_CELL_INTEGRATE = {2: 3011.9, 3: 3514.0}
 FLOPS_PER_CELL_STEP = {2: 9147.6, 3: 10653.9}
 # DRAM bytes (read + write) of one k_flux launch per interior cell, from one
-# ncu capture of the 2048^2 ENO-Roe case with TMA-staged tiles (273.5 MB read
-# + 264.4 MB written; profiles/k_flux_eno_roe_ot2048_ncu.md), scaled to a
-# launch by its cell count.
-DRAM_BYTES_PER_CELL_FLUX = (273.486e6 + 264.385e6) / 2048 ** 2
+# ncu capture of the 2048^2 ENO-Roe case (273.4 MB read + 226.4 MB written
+# while the kernel ran; the rest of UL was still dirty in L2 when it ended;
+# profiles/k_flux_eno_roe_ot2048_ncu.md), scaled to a launch by its cell count.
+DRAM_BYTES_PER_CELL_FLUX = (273.373e6 + 226.401e6) / 2048 ** 2
 
 
 def parse():
@@ -551,7 +551,8 @@ def run_ours(args):
             "sor": {"ms_per_sweep": sor_ms, "sweeps": done, "status": st_sor.status,
                     "gbs_min_traffic": sor_bytes / (sor_ms * 1e-3) / 1e9,
                     "note": "red-black sweep (2 colours + ghost refresh + convergence test), "
-                            "32 B/cell minimum traffic; not part of the timed step"},
+                            "32 B/cell minimum traffic; two launches per sweep where every periodic extent is a "
+                            "multiple of 4; not part of the timed step"},
         }
     ctx.close()
     del ctx

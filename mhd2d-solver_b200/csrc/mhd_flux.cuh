@@ -33,7 +33,7 @@
 // the mirror waves k and 6 - k, bit 1 pairs their right rows; 0 forms one
 // row at a time.  -1 keeps the streamed one-pass loop of interface_flux.
 #ifndef MHD_PAIRS_ROE
-#define MHD_PAIRS_ROE -1
+#define MHD_PAIRS_ROE 3
 #endif
 #ifndef MHD_PAIRS_LF
 #define MHD_PAIRS_LF 3
@@ -216,7 +216,21 @@ __device__ __forceinline__ void project_rows(const Mid& e, const Lane& L, const 
                                              const double* la, const double* lb, double* fw,
                                              double* LU) {
   const unsigned lm = lv_mask(ka);  // == lv_mask(kb)
-  if constexpr (SCHEME == 2) {
+  if constexpr (SCHEME == 2 && MHD_ROE_SIDE) {
+    fw[ka] = roe_side_flux(L, la, lm, eigenvalue(e, ka));
+    if (TWO) fw[kb] = roe_side_flux(L, lb, lm, eigenvalue(e, kb));
+    if (CHARS) {
+      double acc = 0.0, acb = 0.0;
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (lm & (1u << m)) {
+          acc += la[m] * U1[m];
+          if (TWO) acb += lb[m] * U1[m];
+        }
+      LU[ka] = acc;
+      if (TWO) LU[kb] = acb;
+    }
+  } else if constexpr (SCHEME == 2) {
     double wa[4] = {0.0, 0.0, 0.0, 0.0}, va[3] = {0.0, 0.0, 0.0};
     double wb[4] = {0.0, 0.0, 0.0, 0.0}, vb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
