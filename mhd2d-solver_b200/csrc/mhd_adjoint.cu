@@ -600,6 +600,9 @@ constexpr int kSlotsPerChunk = 64;
 struct mhd_adj {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // the y-face interface adjoint runs beside the x-face one on this stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   Grid g{};
   Gas G{};
   StepParams sp{};
@@ -926,10 +929,16 @@ void adjoint_stage(mhd_adj* a, int s, const StageRec& r, const double* X) {
   const double* lB = lb[stage_out(r.mode)];
   const double cL = ul_coef(r.mode, r.dt);
   const long long nx_faces = (long long)(g.nx + 1) * g.ny, ny_faces = (long long)(g.ny + 1) * g.nx;
+  // the two directions read the same inputs and write their own scratch
+  // (SX, SY): the y faces run on the side stream, the gather waits for both
+  cudaEventRecord(a->fork, a->stream);
+  cudaStreamWaitEvent(a->side, a->fork, 0);
   ka_adj_iface<false><<<int((nx_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
       g, a->G, X, mx, lB, cL, a->SX, 1.0 / g.dx);
-  ka_adj_iface<true><<<int((ny_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
+  ka_adj_iface<true><<<int((ny_faces + AIB - 1) / AIB), AIB, 0, a->side>>>(
       g, a->G, X, my, lB, cL, a->SY, 1.0 / g.dy);
+  cudaEventRecord(a->join, a->side);
+  cudaStreamWaitEvent(a->stream, a->join, 0);
   const long long ncell = (long long)g.NX * g.NY;
   ka_adj_gather<<<int((2 * ncell + 127) / 128), 128, 0, a->stream>>>(
       g, a->G, X, a->SX, a->SY, a->T, r.mode, r.in_buf, a->lU, a->lU1, a->lU2);
@@ -1309,6 +1318,9 @@ int mhd_adj_create(int nx, int ny, double dx, double dy, double gamma, const int
   a->K = checkpoint_every;
   AK(cudaSetDevice(device));
   AK(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+  AK(cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking));
+  AK(cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming));
+  AK(cudaEventCreateWithFlags(&a->join, cudaEventDisableTiming));
   Grid& g = a->g;
   g.nx = nx; g.ny = ny; g.NX = nx + 4; g.NY = ny + 4;
   g.pitch = pitch_for(g.NY);
@@ -1372,6 +1384,12 @@ int mhd_adj_destroy(mhd_adj* a) {
   if (a->hctl) cudaFreeHost(a->hctl);
   if (a->hnlog) cudaFreeHost(a->hnlog);
   if (a->hpartial) cudaFreeHost(a->hpartial);
+  if (a->side) {
+    cudaStreamSynchronize(a->side);
+    cudaStreamDestroy(a->side);
+  }
+  if (a->fork) cudaEventDestroy(a->fork);
+  if (a->join) cudaEventDestroy(a->join);
   if (a->stream) cudaStreamDestroy(a->stream);
   delete a;
   return MHD_OK;

@@ -191,6 +191,30 @@ __device__ __forceinline__ double roe_side_flux(const Lane& L, const double* l, 
   return roe_upwind(w, vw, ak);
 }
 
+// ENO-Roe flux of a characteristic under a recorded choice code c (bits 0-1:
+// the ENO- / ENO+ stencil took the left pair, bits 2-3: upwind choice 0 wm,
+// 1 wp, 2 zero): the frozen-stencil replay projects only the two stencil
+// points of the recorded pair, the same sums in the same order as the
+// recording.
+__device__ __forceinline__ double roe_frozen_flux(const Lane& L, const double* l, unsigned lm,
+                                                  unsigned c) {
+  const int up = int(c >> 2);
+  if (up == 2) return 0.0;
+  // points pa, pa + 1; pa = 0: -(1/2) wa + (3/2) wb, 1: (1/2) wa + (1/2) wb,
+  // 2: (3/2) wa - (1/2) wb
+  const int pa = up == 0 ? ((c & 1u) ? 0 : 1) : ((c & 2u) ? 1 : 2);
+  double wa = 0.0, wb = 0.0;
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    if (!(lm & (1u << m))) continue;
+    wa += l[m] * L.F(m, pa);
+    wb += l[m] * L.F(m, pa + 1);
+  }
+  return pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
+       : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
+                  : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
+}
+
 // ENO-LF flux of one characteristic from its projections of the state (ru)
 // and of the flux (rf) at the 4 stencil points and its dissipation
 // coefficient al (spatialmethodenolf.cpp:276-326).
@@ -210,15 +234,20 @@ __device__ __forceinline__ double lf_split(const double* ru, const double* rf, d
 // projections of the state and the fluxes, reduced to the characteristic
 // flux fw; LU gets lv.U1 (Roe) or lv.U at point 1 (LF).  Two rows at once
 // (TWO) share the stencil reads and the differences.
-template <int SCHEME, bool CHARS, bool TWO>
+template <int SCHEME, bool CHARS, bool TWO, int MASK>
 __device__ __forceinline__ void project_rows(const Mid& e, const Lane& L, const double* U1,
                                              const double* alpha, int ka, int kb,
                                              const double* la, const double* lb, double* fw,
-                                             double* LU) {
+                                             double* LU, unsigned mw) {
   const unsigned lm = lv_mask(ka);  // == lv_mask(kb)
-  if constexpr (SCHEME == 2 && MHD_ROE_SIDE) {
-    fw[ka] = roe_side_flux(L, la, lm, eigenvalue(e, ka));
-    if (TWO) fw[kb] = roe_side_flux(L, lb, lm, eigenvalue(e, kb));
+  if constexpr (SCHEME == 2 && (MASK == 2 || MHD_ROE_SIDE)) {
+    if constexpr (MASK == 2) {
+      fw[ka] = roe_frozen_flux(L, la, lm, (mw >> (4 * ka)) & 0xFu);
+      if (TWO) fw[kb] = roe_frozen_flux(L, lb, lm, (mw >> (4 * kb)) & 0xFu);
+    } else {
+      fw[ka] = roe_side_flux(L, la, lm, eigenvalue(e, ka));
+      if (TWO) fw[kb] = roe_side_flux(L, lb, lm, eigenvalue(e, kb));
+    }
     if (CHARS) {
       double acc = 0.0, acb = 0.0;
 #pragma unroll
@@ -309,10 +338,10 @@ __device__ __forceinline__ void project_rows(const Mid& e, const Lane& L, const 
 // their own, as the unfused build rounds every product) wait in registers
 // and are added after wave 3.  Every value is the reference's expression in
 // the reference's order, so all forms give the same bits.
-template <int SCHEME, bool CHARS, bool LV_PAIRS, bool RV_PAIRS>
+template <int SCHEME, bool CHARS, bool LV_PAIRS, bool RV_PAIRS, int MASK>
 __device__ __forceinline__ void pair_flux(Mid& e, const Gas& G, const Lane& L, const double* U1,
                                           const double* alpha, double* Fn, double* LU,
-                                          bool& nonfinite) {
+                                          bool& nonfinite, unsigned mw) {
   double fw[7];
   if constexpr (LV_PAIRS) {
 #pragma unroll
@@ -322,9 +351,9 @@ __device__ __forceinline__ void pair_flux(Mid& e, const Gas& G, const Lane& L, c
       lv_row(e, G, t, la);
       if (t < 3) {
         lv_row(e, G, 6 - t, lb);
-        project_rows<SCHEME, CHARS, true>(e, L, U1, alpha, t, 6 - t, la, lb, fw, LU);
+        project_rows<SCHEME, CHARS, true, MASK>(e, L, U1, alpha, t, 6 - t, la, lb, fw, LU, mw);
       } else {
-        project_rows<SCHEME, CHARS, false>(e, L, U1, alpha, t, t, la, la, fw, LU);
+        project_rows<SCHEME, CHARS, false, MASK>(e, L, U1, alpha, t, t, la, la, fw, LU, mw);
       }
     }
   } else {
@@ -333,7 +362,7 @@ __device__ __forceinline__ void pair_flux(Mid& e, const Gas& G, const Lane& L, c
       opaque(e);
       double l[NF];
       lv_row(e, G, k, l);
-      project_rows<SCHEME, CHARS, false>(e, L, U1, alpha, k, k, l, l, fw, LU);
+      project_rows<SCHEME, CHARS, false, MASK>(e, L, U1, alpha, k, k, l, l, fw, LU, mw);
     }
   }
 #pragma unroll
@@ -423,9 +452,9 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
   for (int m = 0; m < NF; m++) Fn[m] = 0.0;
 
   constexpr int PAIRS = SCHEME == 2 ? MHD_PAIRS_ROE : MHD_PAIRS_LF;
-  if constexpr (!DENSE && MASK == 0 && PAIRS >= 0) {
-    pair_flux<SCHEME, CHARS, (PAIRS & 1) != 0, (PAIRS & 2) != 0>(e, G, L, U1, alpha, Fn, LU,
-                                                                 nonfinite);
+  if constexpr (!DENSE && (MASK == 0 || (MASK == 2 && SCHEME == 2)) && PAIRS >= 0) {
+    pair_flux<SCHEME, CHARS, (PAIRS & 1) != 0, (PAIRS & 2) != 0, MASK>(
+        e, G, L, U1, alpha, Fn, LU, nonfinite, MASK == 2 ? *mw : 0u);
     return true;
   }
 

@@ -129,19 +129,19 @@ void l_sor_sweep(const Grid& g, double* phi, const double* xy, const int range[4
   const int m = g.nx > g.ny ? g.nx : g.ny;
   const double4* f = reinterpret_cast<const double4*>(xy);
   if (fused) {
-    k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, 1, rtol, max_sweeps,
-                                            last_ratio);
-    k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, 1, rtol, max_sweeps,
-                                            last_ratio);
+    k_sor_half<true><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, rtol, max_sweeps,
+                                                  last_ratio);
+    k_sor_half<true><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, rtol, max_sweeps,
+                                                  last_ratio);
     return;
   }
   // ghosts are refreshed after each colour: with periodic sides they mirror
   // points of the other colour (see k_sor_half)
-  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, 0, rtol, max_sweeps,
-                                          last_ratio);
+  k_sor_half<false><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, rtol, max_sweeps,
+                                                 last_ratio);
   k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 0);
-  k_sor_half<<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, 0, rtol, max_sweeps,
-                                          last_ratio);
+  k_sor_half<false><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, rtol, max_sweeps,
+                                                 last_ratio);
   k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 0);
   k_sor_check<<<1, 32, 0, s>>>(ctl, rtol, max_sweeps, last_ratio);
 }

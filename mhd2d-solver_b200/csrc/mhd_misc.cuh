@@ -452,14 +452,14 @@ __device__ __forceinline__ void sor_check(Ctl* c, double rtol, double max_sweeps
 }
 
 // One colour of a red-black sweep.  The potential pairs are read and written
-// as 16-byte items (jb is even, the padded row offset is even).  fused = 1:
+// as 16-byte items (jb is even, the padded row offset is even).  FUSED:
 // periodic ghosts are read at their source points, and the last block of the
 // colour-1 launch runs the convergence test.
+template <bool FUSED>
 __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __restrict__ phi,
                                                           const double4* __restrict__ xy,
                                                           DivRange R, SorCoef s, int color,
-                                                          Ctl* c, int fused, double rtol,
-                                                          double max_sweeps,
+                                                          Ctl* c, double rtol, double max_sweeps,
                                                           double* last_ratio) {
   if (c->sor_done) return;
   __shared__ double red[2][SOR_THREADS / 32];
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
       const double* urow = prow + 2 * P;
       const double* drow = prow - 2 * P;
       int jl = jb - 2, jr = jb + 2;
-      if (fused) {
+      if (FUSED) {
         urow = phi + (long long)sor_src_row(g, i + 2) * P + g.off;
         drow = phi + (long long)sor_src_row(g, i - 2) * P + g.off;
         if (g.bc[BOTTOM] == PERIODIC && jl < 2) jl += g.ny;
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
     }
     atomic_max_pos(&c->rmax, rmax);
     atomic_max_pos(&c->pmax, pmax);
-    if (fused && color == 1) {
+    if (FUSED && color == 1) {
       // the last block to finish sees every block's maxima
       __threadfence();
       const unsigned nb = gridDim.x * gridDim.y;
