@@ -58,13 +58,17 @@ typedef struct {
 } mhd_sor_params;
 
 /* Context = the reference's method + stepper pair on one GPU.
-   Replaces: SpatialMethodEnoRoe / SpatialMethodEnoLF constructors
-   (spatialmethodenoroe.cpp:5-20, spatialmethodenolf.cpp:5-20) and
+   Replaces: SpatialMethodCentralFD2 / SpatialMethodEnoRoe /
+   SpatialMethodEnoLF constructors (spatialmethodcentralfd2.cpp:6-24,
+   spatialmethodenoroe.cpp:5-20, spatialmethodenolf.cpp:5-20) and
    TimeIntegrationRK3 / TimeIntegrationEuler constructors
    (timeintegrationrk3.cpp:4-27, timeintegrationeuler.cpp:4-15).
    halo must be 2 (bufferWidth = NXFIRST, main.cpp:117); a smaller halo is
    the reference's std::domain_error (spatialmethodeno.cpp:17-20) and
-   returns MHD_ERR_WRONG_PARAMETER. */
+   returns MHD_ERR_WRONG_PARAMETER.  scheme: 1 central FD2, 2 ENO-Roe,
+   3 ENO-LF (IntegrationMethod, enums.hpp:54-59).  Central FD2 statuses are
+   the reference's: a non-positive density (first cell in loop order) or
+   pressure (last cell) is fatal, the message names the cell. */
 int mhd_ctx_create( int nx, int ny, int halo, double dx, double dy, double gamma,
                     const int bc[4], int scheme, int time_method,
                     double dt_min, double dt_max, double cfl, int flags, int device,
@@ -122,7 +126,9 @@ int mhd_steps( mhd_ctx* ctx, int nsteps, double* dt_inout, double* dts );
 
 /* Replaces SpatialMethodEno::getCharacteristicsX/Y (spatialmethodeno.cpp:55-86)
    as called at timeintegrationrk3.cpp:151-152; requires
-   MHD_FLAG_CHARACTERISTICS.  Any pointer may be NULL. */
+   MHD_FLAG_CHARACTERISTICS.  Any pointer may be NULL.  Central FD2 keeps
+   no characteristics: MHD_NO_CHANGE, the arrays untouched (the base
+   class's getCharacteristicsX/Y return false, spatialintegrationmethod.cpp:69-82). */
 int mhd_get_characteristics( mhd_ctx* ctx, double* cx, double* cy, double* LUx, double* LUy );
 
 /* Replaces divBCalculation (div_b_fix.cpp:4-126) on the device state. */

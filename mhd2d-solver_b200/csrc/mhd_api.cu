@@ -159,9 +159,25 @@ void enqueue_rk3_tail(mhd_ctx* c, bool chars) {
   enqueue_control(c, PH_DONE);
 }
 
+// Fatal statuses of the central-FD integration, with the reference's
+// message (spatialmethodcentralfd2.cpp:71-77, 151-156) and a caller suffix.
+int cfd_status(mhd_ctx* c, const char* where) {
+  const Ctl& h = *c->hctl;
+  const bool dens = h.error == 6;
+  const unsigned long long lin = dens ? kCfdFirstBase - h.cfd_first : h.cfd_last - 1;
+  const int i = int(lin / c->g.NY) - 2, j = int(lin % c->g.NY) - 2;
+  char buf[256];
+  std::snprintf(buf, sizeof buf,
+                "Negative %s encountered at i = %d, j = %d\n! SpatialMethodCentralFD2::integrate%s",
+                dens ? "density" : "pressure", i, j, where);
+  return set_status(c, dens ? MHD_ERR_NEGATIVE_DENSITY : MHD_ERR_NEGATIVE_PRESSURE, true, buf);
+}
+
 int step_status(mhd_ctx* c) {
   const Ctl& h = *c->hctl;
   c->neg_pressure += (long long)h.neg_count;
+  if (c->scheme == 1 && (h.error == 6 || h.error == 7))
+    return cfd_status(c, "\n! mhd_step: spatial integration");
   if (h.error == 6)
     return set_status(c, MHD_ERR_NEGATIVE_DENSITY, true,
                       "negative density encountered\n! getEigens_F\n! mhd_step: spatial integration");
@@ -340,7 +356,7 @@ int mhd_ctx_create(int nx, int ny, int halo, double dx, double dy, double gamma,
                    int device, mhd_ctx** out) {
   if (!out) return MHD_ERR_WRONG_PARAMETER;
   *out = nullptr;
-  if (halo != 2 || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0) || (scheme != 2 && scheme != 3) ||
+  if (halo != 2 || nx < 2 || ny < 2 || !(dx > 0) || !(dy > 0) || scheme < 1 || scheme > 3 ||
       (time_method != 1 && time_method != 2) || !bc)
     return MHD_ERR_WRONG_PARAMETER;
   for (int s = 0; s < 4; s++)
@@ -503,6 +519,10 @@ int mhd_integrate(mhd_ctx* c, double* dtIdeal) {
   if ((st = read_ctl(c))) return st;
   const Ctl& h = *c->hctl;
   c->neg_pressure += (long long)h.neg_count;
+  if (c->scheme == 1 && (h.error == 6 || h.error == 7)) {
+    if (h.error == 7 && dtIdeal) *dtIdeal = h.dtIdeal;  // formed before the status
+    return cfd_status(c, "\n! mhd_integrate");
+  }
   if (h.error == 6)
     return set_status(c, MHD_ERR_NEGATIVE_DENSITY, true,
                       "negative density encountered\n! getEigens_F\n! mhd_integrate");
@@ -555,6 +575,9 @@ int mhd_steps(mhd_ctx* c, int nsteps, double* dt_inout, double* dts) {
 int mhd_get_characteristics(mhd_ctx* c, double* cx, double* cy, double* LUx, double* LUy) {
   if (!c) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
+  // central FD keeps no characteristics: the base class's getCharacteristicsX/Y
+  // return false and leave the arrays (spatialintegrationmethod.cpp:69-82)
+  if (c->scheme == 1) return set_status(c, MHD_NO_CHANGE, false, "no characteristics (central FD)");
   if (!(c->flags & MHD_FLAG_CHARACTERISTICS)) {
     // on request: the last spatial integration again, on its unchanged input,
     // with the characteristics kernel (the same values the flag would keep)

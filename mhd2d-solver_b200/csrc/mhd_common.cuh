@@ -67,7 +67,13 @@ struct Ctl {
   int sor_done, sor_sweeps;
   unsigned sor_ticket;  // blocks of a fused SOR colour launch that have finished
   int pad;
+  // central FD (k_cfd_check): kCfdFirstBase - (i*NY + j) of the first
+  // non-positive density, 1 + (i*NY + j) of the last non-positive pressure;
+  // 0 = none
+  unsigned long long cfd_first, cfd_last;
 };
+
+constexpr unsigned long long kCfdFirstBase = 1ull << 62;
 
 // Phases of the one-thread time-step controller (k_control).
 enum CtlPhase : int {

@@ -3,6 +3,7 @@
 //   MHD_KSET = kFast   with -fmad=true   (FMA contraction)
 #include <cmath>
 
+#include "mhd_cfd.cuh"
 #include "mhd_flux.cuh"
 #include "mhd_launch.h"
 #include "mhd_misc.cuh"
@@ -77,6 +78,12 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
 void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
             const double* aG, Ctl* ctl, double* const ch[4], cudaStream_t s) {
   const bool chars = ch && ch[0];
+  if (scheme == 1) {  // central FD: checks and maxima, then UL
+    dim3 ring((g.ny + 2 + 31) / 32, (g.nx + 2 + 7) / 8), inner((g.ny + 31) / 32, (g.nx + 7) / 8);
+    k_cfd_check<<<ring, 256, 0, s>>>(g, U, ctl);
+    k_cfd_ul<<<inner, 256, 0, s>>>(g, U, UL, 1.0 / (2.0 * g.dx), 1.0 / (2.0 * g.dy), ctl);
+    return;
+  }
   if (scheme == 3) {
     if (chars) flux_t<3, true>(g, U, UL, aF, aG, ctl, ch, s);
     else flux_t<3, false>(g, U, UL, aF, aG, ctl, ch, s);
@@ -166,7 +173,7 @@ int l_totals(const Grid& g, const double* U, double* partial, int max_blocks, cu
 }
 
 int l_smem() { return int(Geom::TMA_BYTES); }
-int l_launches(int scheme) { return scheme == 3 ? 3 : 2; }  // bc, [alpha], flux
+int l_launches(int scheme) { return scheme == 2 ? 2 : 3; }  // bc, [alpha], flux; bc, check, UL
 
 }  // namespace MHD_KNS
 

@@ -208,6 +208,7 @@ __device__ __forceinline__ void control_step(Ctl* c, const StepParams& p, int ph
     c->skip = 0; c->retry = 0; c->error = 0; c->neg_last = 0; c->step_done = 0;
     c->maxX = 0ull; c->maxY = 0ull;
     c->neg_count = 0ull; c->negd_count = 0ull;
+    c->cfd_first = 0ull; c->cfd_last = 0ull;
     if (phase == PH_RESET_STEP) {
       c->dt1 = arg; c->dt = arg; c->dt2 = p.dt_max; c->dt3 = p.dt_max;
     }
@@ -224,11 +225,16 @@ __device__ __forceinline__ void control_step(Ctl* c, const StepParams& p, int ph
     return;
   }
   if (c->skip) return;
-  if (c->error) { c->skip = 1; return; }
+  // central FD: a non-positive density (6) ends the integration before
+  // dtIdeal; a non-positive pressure (7) is fatal after dtIdeal and UL
+  // (spatialmethodcentralfd2.cpp:71-77, 139-159)
+  if (!c->error) c->error = c->cfd_first ? 6 : (c->cfd_last ? 7 : 0);
+  if (c->error && c->error != 7) { c->skip = 1; return; }
   const double ax = p.dx / bits_to_double(c->maxX), ay = p.dy / bits_to_double(c->maxY);
   const double ideal = (ay < ax) ? ay : ax;  // std::min(a, b)
   c->dtIdeal = ideal;
   c->maxX = 0ull; c->maxY = 0ull;
+  if (c->error) { c->skip = 1; return; }
   int st = 1;
   switch (phase) {
     case PH_RK_FIRST:

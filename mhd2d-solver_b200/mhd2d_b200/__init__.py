@@ -38,7 +38,7 @@ STATUS_NAMES = {0: "OK", 1: "NoChange", 2: "Updated", 3: "ErrorNotImplemented",
                 10: "ErrorWrongParameter", 100: "ErrorCuda"}
 
 PERIODIC, DIRICHLET, NEUMANN, OPEN = 1, 2, 3, 4
-ENO_ROE, ENO_LF = 2, 3
+CENTRAL_FD, ENO_ROE, ENO_LF = 1, 2, 3
 EULER, RK3 = 1, 2
 FLAG_CHARACTERISTICS, FLAG_FAST_MATH = 0x1, 0x2
 
@@ -329,6 +329,8 @@ class Context:
         out = [np.zeros(self.shape) for _ in range(4)]
         st = self._check(self.lib.mhd_get_characteristics(self.h, *[_p(a) for a in out]),
                          "characteristics")
+        if st == NO_CHANGE:  # central FD keeps none: the arrays stay as they are
+            return out
         if st != OK:
             raise MhdError(self.last_status(st).message)
         return out
@@ -402,11 +404,13 @@ class Context:
 
 class _SpatialMethod:
     scheme = ENO_ROE
+    min_buffer = 2
 
     def __init__(self, nx, ny, bufferWidth, dx, dy, boundary, gamma, characteristics=True,
                  fast_math=False, device=0):
-        if bufferWidth < 2:
-            raise ValueError("Buffer is too small for ENO; need at least 2 extra grids")
+        if bufferWidth < self.min_buffer:
+            raise ValueError("Buffer is too small for this method; need at least "
+                             f"{self.min_buffer} extra grids")
         flags = (FLAG_CHARACTERISTICS if characteristics else 0) | (FLAG_FAST_MATH if fast_math else 0)
         self.ctx = Context(nx, ny, dx, dy, gamma, boundary, scheme=self.scheme, time_method=RK3,
                            flags=flags, device=device)
@@ -422,12 +426,16 @@ class _SpatialMethod:
         return st, d
 
     def getCharacteristicsX(self, cx, LUx):
+        if self.scheme == CENTRAL_FD:
+            return False
         a = self.ctx.characteristics()
         cx[...] = a[0]
         LUx[...] = a[2]
         return True
 
     def getCharacteristicsY(self, cy, LUy):
+        if self.scheme == CENTRAL_FD:
+            return False
         a = self.ctx.characteristics()
         cy[...] = a[1]
         LUy[...] = a[3]
@@ -440,6 +448,13 @@ class SpatialMethodEnoRoe(_SpatialMethod):
 
 class SpatialMethodEnoLF(_SpatialMethod):
     scheme = ENO_LF
+
+
+class SpatialMethodCentralFD2(_SpatialMethod):
+    """SpatialMethodCentralFD2 (spatialmethodcentralfd2.cpp): second-order
+    central differences; keeps no characteristics."""
+    scheme = CENTRAL_FD
+    min_buffer = 1
 
 
 class _TimeMethod:

@@ -26,8 +26,10 @@ CudaSpatialMethod::CudaSpatialMethod(size_t nx, size_t ny, size_t bufferWidth, d
                                      bool characteristics)
     : SpatialIntegrationMethod{nx, ny, bufferWidth, dx, dy, boundary, gamma},
       characteristics_(characteristics) {
-  if (bufferWidth < 2)
-    throw std::domain_error("Buffer is too small for ENO; need at least 2 extra grids");
+  if (bufferWidth < (scheme == 1 ? 1u : 2u))
+    throw std::domain_error(scheme == 1 ? "Buffer is too small for second order central finite "
+                                          "difference; need at least 1 extra grid"
+                                        : "Buffer is too small for ENO; need at least 2 extra grids");
   if (bufferWidth != 2)
     throw std::domain_error("the device layout has exactly 2 ghost cells per side");
   const int bc[4] = {int(boundary.left), int(boundary.right), int(boundary.bottom),

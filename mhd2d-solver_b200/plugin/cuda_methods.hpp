@@ -1,7 +1,8 @@
 // Drop-in subclasses of the reference solver's plugin interfaces that run
 // the time-step hot path on a B200 through libmhd2d_b200.so.
 //
-//   CudaSpatialMethodEnoRoe / CudaSpatialMethodEnoLF : SpatialIntegrationMethod
+//   CudaSpatialMethodEnoRoe / CudaSpatialMethodEnoLF / CudaSpatialMethodCentralFD2
+//       : SpatialIntegrationMethod
 //       (spatialintegrationmethod.hpp:6-65) — integrate() uploads U, runs the
 //       boundary fill and the fused flux kernel, downloads U (ghosts filled)
 //       and UL, like SpatialMethodEnoRoe/EnoLF::integrate.
@@ -59,6 +60,15 @@ class CudaSpatialMethodEnoLF : public CudaSpatialMethod {
   CudaSpatialMethodEnoLF(size_t nx, size_t ny, size_t bufferWidth, double dx, double dy,
                          t_boundary boundary, double gamma)
       : CudaSpatialMethod(nx, ny, bufferWidth, dx, dy, boundary, gamma, 3) {}
+};
+
+// SpatialMethodCentralFD2 (spatialmethodcentralfd2.cpp): second-order
+// central differences; it keeps no characteristics.
+class CudaSpatialMethodCentralFD2 : public CudaSpatialMethod {
+ public:
+  CudaSpatialMethodCentralFD2(size_t nx, size_t ny, size_t bufferWidth, double dx, double dy,
+                              t_boundary boundary, double gamma)
+      : CudaSpatialMethod(nx, ny, bufferWidth, dx, dy, boundary, gamma, 1, false) {}
 };
 
 class CudaTimeIntegration : public TimeIntegrationMethod {

@@ -1,8 +1,8 @@
 // Drop-in check: the same run three ways, compared bit for bit.
-//   A  reference TimeIntegrationRK3 + reference SpatialMethodEnoRoe/EnoLF
-//   B  reference TimeIntegrationRK3 + CudaSpatialMethodEnoRoe/EnoLF
-//   C  CudaTimeIntegrationRK3      + CudaSpatialMethodEnoRoe/EnoLF
-// usage: plugin_check <scheme 2|3> <problem ot|bw|dir> <steps>
+//   A  reference TimeIntegrationRK3 + reference SpatialMethodEnoRoe/EnoLF/CentralFD2
+//   B  reference TimeIntegrationRK3 + CudaSpatialMethodEnoRoe/EnoLF/CentralFD2
+//   C  CudaTimeIntegrationRK3      + CudaSpatialMethodEnoRoe/EnoLF/CentralFD2
+// usage: plugin_check <scheme 1|2|3> <problem ot|bw|dir> <steps>
 // Prints one line per comparison and exits non-zero on any difference.
 #include <cmath>
 #include <cstdio>
@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "cuda_methods.hpp"
+#include "spatialmethodcentralfd2.hpp"
 #include "spatialmethodenolf.hpp"
 #include "spatialmethodenoroe.hpp"
 #include "timeintegrationrk3.hpp"
@@ -106,9 +107,12 @@ std::vector<double> run(const Problem& p, int scheme, Mode mode, int steps, doub
   std::unique_ptr<SpatialIntegrationMethod> m;
   if (mode == REF) {
     if (scheme == 3) m.reset(new SpatialMethodEnoLF(p.nx, p.ny, 2, p.dx, p.dy, p.b, p.gamma));
+    else if (scheme == 1) m.reset(new SpatialMethodCentralFD2(p.nx, p.ny, 2, p.dx, p.dy, p.b, p.gamma));
     else m.reset(new SpatialMethodEnoRoe(p.nx, p.ny, 2, p.dx, p.dy, p.b, p.gamma));
   } else {
     if (scheme == 3) m.reset(new CudaSpatialMethodEnoLF(p.nx, p.ny, 2, p.dx, p.dy, p.b, p.gamma));
+    else if (scheme == 1)
+      m.reset(new CudaSpatialMethodCentralFD2(p.nx, p.ny, 2, p.dx, p.dy, p.b, p.gamma));
     else m.reset(new CudaSpatialMethodEnoRoe(p.nx, p.ny, 2, p.dx, p.dy, p.b, p.gamma));
   }
   m->initializeDirichletBoundaries(U.m());
@@ -144,7 +148,7 @@ size_t differ(const std::vector<double>& a, const std::vector<double>& b) {
 
 int main(int argc, char** argv) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: %s scheme(2|3) problem(ot|bw|dir) steps\n", argv[0]);
+    std::fprintf(stderr, "usage: %s scheme(1|2|3) problem(ot|bw|dir) steps\n", argv[0]);
     return 2;
   }
   const int scheme = std::atoi(argv[1]), steps = std::atoi(argv[3]);

@@ -34,6 +34,7 @@ struct orc_ctx {
    double *U1, *U2, *UL;      /* time-stepper stages */
    double *phi;               /* SOR potential, persists across solves */
    long long retries;         /* RK3 stage restarts taken so far */
+   int cfd_i, cfd_j;          /* central FD: cell of the reported density / pressure error */
 };
 
 enum { L = 0, R = 1, B = 2, T = 3 };
@@ -481,12 +482,111 @@ static int lf_alpha( orc_ctx* c, const double* U, int* negp )
    The returned status follows the reference: the status of the last
    interface evaluated (so a clamped pressure there reports
    ErrorNegativePressure without isError). */
+/* std::max({ a, ... }) over the 8 signed wave speeds: the first largest,
+   so a NaN candidate never replaces the running value. */
+static double max_speeds( double m, double u, double cf, double ca, double cs )
+{
+   const double v[7] = { u - cf, u - ca, u - cs, u, u + cs, u + ca, u + cf };
+   int n;
+   for( n = 0; n < 7; n++ ) if( m < v[n] ) m = v[n];
+   return m;
+}
+
+/* SpatialMethodCentralFD2::integrate (spatialmethodcentralfd2.cpp:44-160):
+   physical fluxes on the interior and the ring of ghost cells around it,
+   the four ring corners skipped with nxFirst / nxLast for both indices
+   (lines 60-64); the maxima of the signed wave speeds (not |lambda|) for
+   dtIdeal; UL from central differences of F and G.  A non-positive density
+   returns at the first such cell in loop order before UL is formed; a
+   non-positive pressure is fatal too, reported at the last such cell, after
+   UL and dtIdeal.  F and G of skipped cells keep their initial zeros (the
+   reference leaves them unset). */
+static int cfd_integrate( orc_ctx* c, double* U, double* UL, double* dtIdeal, int* is_error )
+{
+   const int nx = c->nx, ny = c->ny, f0 = 2, l0 = nx + 2;
+   const double gm = c->gamma;
+   double cxm = 0.0, cym = 0.0;
+   int pok = 1, i, j, k, st;
+
+   st = orc_apply_bc( c, U, is_error );
+   if( *is_error ) return st;
+   for( i = f0-1; i < nx+3; i++ ) for( j = f0-1; j < ny+3; j++ ){
+      double r, mx, my, mz, bx, by, bz, e, u, v, w, uu, ub, bb, p, pt;
+      double c2, ca2, ca, ct2, ctemp, cs2, cs, cf2, cf;
+      if( ( i < f0 && j < f0 ) || ( i < f0 && j >= l0 ) || ( i >= l0 && j < f0 ) ||
+          ( i >= l0 && j >= l0 ) ) continue;
+      r = AT(U,0,i,j);
+      mx = AT(U,1,i,j); u = mx / r;
+      my = AT(U,2,i,j); v = my / r;
+      mz = AT(U,3,i,j); w = mz / r;
+      bx = AT(U,4,i,j); by = AT(U,5,i,j); bz = AT(U,6,i,j); e = AT(U,7,i,j);
+      uu = u*u + v*v + w*w;
+      ub = u*bx + v*by + w*bz;
+      bb = bx*bx + by*by + bz*bz;
+      p = (gm-1.0)*(e-0.5*r*uu-0.5*bb);
+      pt = p + 0.5*bb;
+      if( r <= 0.0 ){
+         c->cfd_i = i; c->cfd_j = j;
+         *is_error = 1;
+         return ORC_ERR_NEGATIVE_DENSITY;
+      }
+      if( p <= 0.0 ){ pok = 0; c->cfd_i = i; c->cfd_j = j; }
+      AT(c->F,0,i,j) = mx;
+      AT(c->F,1,i,j) = mx*u - bx*bx + pt;
+      AT(c->F,2,i,j) = my*u - bx*by;
+      AT(c->F,3,i,j) = mz*u - bx*bz;
+      AT(c->F,4,i,j) = 0;
+      AT(c->F,5,i,j) = by*u - bx*v;
+      AT(c->F,6,i,j) = bz*u - bx*w;
+      AT(c->F,7,i,j) = (e+pt)*u - bx*ub;
+      AT(c->G,0,i,j) = my;
+      AT(c->G,1,i,j) = mx*v - by*bx;
+      AT(c->G,2,i,j) = my*v - by*by + pt;
+      AT(c->G,3,i,j) = mz*v - by*bz;
+      AT(c->G,4,i,j) = bx*v - by*u;
+      AT(c->G,5,i,j) = 0;
+      AT(c->G,6,i,j) = bz*v - by*w;
+      AT(c->G,7,i,j) = (e+pt)*v - by*ub;
+      c2 = gm*p / r; if( c2 < 0.0 ) c2 = 0.0;
+      ca2 = bx*bx/r;
+      ca = sqrt(ca2);
+      ct2 = 0.5*(bb/r+c2);
+      ctemp = ct2*ct2-c2*ca2; if( ctemp < 0.0 ) ctemp = 0.0;
+      cs2 = ct2 - sqrt(ctemp); if( cs2 < 0.0 ) cs2 = 0.0;
+      cs = sqrt(cs2);
+      cf2 = ct2 + sqrt(ctemp); if( cf2 < 0.0 ) cf2 = 0.0;
+      cf = sqrt(cf2);
+      cxm = max_speeds( cxm, u, cf, ca, cs );
+      ca2 = by*by/r;
+      ca = sqrt(ca2);
+      ct2 = 0.5*(bb/r+c2);
+      ctemp = ct2*ct2-c2*ca2; if( ctemp < 0.0 ) ctemp = 0.0;
+      cs2 = ct2 - sqrt(ctemp); if( cs2 < 0.0 ) cs2 = 0.0;
+      cs = sqrt(cs2);
+      cf2 = ct2 + sqrt(ctemp); if( cf2 < 0.0 ) cf2 = 0.0;
+      cf = sqrt(cf2);
+      cym = max_speeds( cym, v, cf, ca, cs );
+   }
+   {  /* std::min( dx/cxmax, dy/cymax ) */
+      const double ax = c->dx/cxm, ay = c->dy/cym;
+      *dtIdeal = ( ay < ax ) ? ay : ax;
+   }
+   for( k = 0; k < NF; k++ ) for( i = 2; i < nx+2; i++ ) for( j = 2; j < ny+2; j++ )
+      AT(UL,k,i,j) = -(1.0/(2.0*c->dx)) * ( AT(c->F,k,i+1,j) - AT(c->F,k,i-1,j) )
+                     -(1.0/(2.0*c->dy)) * ( AT(c->G,k,i,j+1) - AT(c->G,k,i,j-1) );
+   if( !pok ){ *is_error = 1; return ORC_ERR_NEGATIVE_PRESSURE; }
+   *is_error = 0;
+   return ORC_OK;
+}
+
 int orc_integrate( orc_ctx* c, double* U, double* UL, double* dtIdeal, int* is_error )
 {
    const int nx = c->nx, ny = c->ny, lf = (c->scheme == 3);
    double U1[NF], U2[NF], Us[NF][4], Fs[NF][4], Vs[NF][3], Fn[NF], lam[NF], LU[NF], al[NF];
    double mX = 0.0, mY = 0.0, s;
    int i, j, k, l, st, negp = 0;
+
+   if( c->scheme == 1 ) return cfd_integrate( c, U, UL, dtIdeal, is_error );
 
    st = orc_apply_bc( c, U, is_error );
    if( *is_error ) return st;

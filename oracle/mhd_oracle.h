@@ -41,7 +41,7 @@ typedef struct {
    double omega;
 } orc_sor_params;
 
-/* scheme: 2 ENO-Roe, 3 ENO-LF.  time_method: 1 Euler, 2 RK3-TVD. */
+/* scheme: 1 central FD2, 2 ENO-Roe, 3 ENO-LF.  time_method: 1 Euler, 2 RK3-TVD. */
 orc_ctx* orc_create( int scheme, int time_method, int nx, int ny, double dx, double dy,
                      double gamma, const int* bc, double dt_min, double dt_max, double cfl );
 void     orc_destroy( orc_ctx* c );

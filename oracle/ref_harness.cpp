@@ -13,6 +13,7 @@
  *                                   spatialintegrationmethod.cpp:39-59
  *   SpatialMethodEnoRoe::integrate   spatialmethodenoroe.cpp:33-179
  *   SpatialMethodEnoLF::integrate    spatialmethodenolf.cpp:33-230
+ *   SpatialMethodCentralFD2::integrate  spatialmethodcentralfd2.cpp:44-160
  *   SpatialMethodEno::getCharacteristicsX/Y  spatialmethodeno.cpp:55-86
  *   TimeIntegrationMethod::updateDt  timeintegrationmethod.cpp:35-90
  *   TimeIntegrationRK3::step         timeintegrationrk3.cpp:48-156
@@ -24,6 +25,7 @@
 #include "mhd2d.hpp"
 #include "spatialmethodenoroe.hpp"
 #include "spatialmethodenolf.hpp"
+#include "spatialmethodcentralfd2.hpp"
 #include "timeintegrationrk3.hpp"
 #include "timeintegrationeuler.hpp"
 
@@ -89,6 +91,8 @@ void copyMsg( const std::string& s, char* msg, int msglen ){
 std::unique_ptr<SpatialIntegrationMethod> makeMethod( int scheme, int nx, int ny, double dx,
                                                       double dy, double gamma, const int* bc ){
    auto b = toBoundary( bc );
+   if( scheme == 1 )
+      return std::unique_ptr<SpatialIntegrationMethod>{ new SpatialMethodCentralFD2( nx, ny, 2, dx, dy, b, gamma ) };
    if( scheme == 3 )
       return std::unique_ptr<SpatialIntegrationMethod>{ new SpatialMethodEnoLF( nx, ny, 2, dx, dy, b, gamma ) };
    return std::unique_ptr<SpatialIntegrationMethod>{ new SpatialMethodEnoRoe( nx, ny, 2, dx, dy, b, gamma ) };

@@ -4,7 +4,7 @@ Runs the reference hot path (oracle/_ref/libmhdref.so, built by
 `make -C oracle ref` from the reference sources) on small seeded states and
 stores inputs and outputs as compressed .npz files:
 
-* integrate_*.npz — one SpatialMethodEnoRoe/EnoLF::integrate call: state in,
+* integrate_*.npz — one SpatialMethodEnoRoe/EnoLF/CentralFD2::integrate call: state in,
   state out (ghosts filled), UL, dtIdeal, status, characteristics;
 * run_*.npz       — the main loop for a few steps (RK3 / Euler, dt control
   with retries, optional SOR cleaning): final state, dt and div B history;
@@ -56,6 +56,40 @@ def integrate_cases():
     return cases
 
 
+def fill_corners(p):
+    """Ring corners of a central-FD state: the reference's corner test uses
+    the x bounds for j too, so with ny < nx it evaluates the ghost corners
+    (1, ny+2) and (nx+2, ny+2), which no boundary fill writes; give every
+    ghost corner the state of its nearest interior cell."""
+    U = p.U
+    nx, ny = p.nx, p.ny
+    for i in (0, 1, nx + 2, nx + 3):
+        for j in (0, 1, ny + 2, ny + 3):
+            U[:, i, j] = U[:, min(max(i, 2), nx + 1), min(max(j, 2), ny + 1)]
+    return p
+
+
+def cfd_integrate_cases():
+    """Central FD2 (scheme 1): smooth states with nx >= ny (with ny > nx the
+    reference reads flux entries it never wrote), its fatal negative
+    pressure and density, and an unfilled ring corner."""
+    cases = []
+    for n, bc in enumerate(BCS):
+        cases.append((f"cfd_smooth_bc{n}", fill_corners(P.random_smooth(12, 10, seed=60 + n, bc=bc))))
+    cases.append(("cfd_otvortex", P.ot_vortex(16)))
+    cases.append(("cfd_explosion", P.explosion(16)))
+    p = fill_corners(P.random_smooth(11, 9, seed=66, bc=(1, 1, 1, 1)))
+    p.U[7, 4, 5] = 0.0
+    p.U[7, 7, 3] = 0.0
+    cases.append(("cfd_negpressure", p))
+    p = fill_corners(P.random_smooth(11, 9, seed=67, bc=(3, 3, 3, 3)))
+    p.U[0, 6, 4] = -1.0
+    p.U[0, 3, 7] = -2.0
+    cases.append(("cfd_negdensity", p))
+    cases.append(("cfd_zerocorner", P.random_smooth(12, 10, seed=68, bc=(1, 1, 1, 1))))
+    return cases
+
+
 def run_cases():
     sp = sor_params(1, 5, 20000, 1e-9, 1e-9, True, 1.7)
     return [
@@ -72,6 +106,9 @@ def run_cases():
         ("ot_roe_sor", P.ot_vortex(16), 2, 2, 0.03125, 1e-6, 0.03125, 0.4, 3, 0.0, sp),
         ("smooth_lf_sor", P.random_smooth(16, 12, seed=42, bc=(3, 3, 1, 1)), 3, 2, 0.02, 1e-7,
          0.02, 0.4, 2, 0.0, sp),
+        ("cfd_ot_rk3", P.ot_vortex(16), 1, 2, 0.0078125, 1e-6, 0.0078125, 0.2, 6, 0.0, None),
+        ("cfd_smooth_euler", fill_corners(P.random_smooth(14, 12, seed=43, bc=(1, 1, 4, 4))), 1,
+         1, 0.002, 1e-9, 0.002, 0.2, 4, 0.0, None),
     ]
 
 
@@ -87,6 +124,15 @@ def main():
                 U_in=prob.U, U_out=U, UL=r["UL"], dtIdeal=r["dtIdeal"], status=r["status"],
                 is_error=r["is_error"], cx=r["cx"], cy=r["cy"], LUx=r["LUx"], LUy=r["LUy"],
                 dx=prob.dx, dy=prob.dy, gamma=prob.gamma, bc=np.array(prob.bc), scheme=scheme)
+    for name, prob in cfd_integrate_cases():
+        U = prob.U.copy()
+        r = ref.integrate(1, U, prob.dx, prob.dy, prob.gamma, prob.bc,
+                          U_dirichlet=prob.U.copy(), chars=True)
+        out[f"integrate_{name}_1"] = dict(
+            U_in=prob.U, U_out=U, UL=r["UL"], dtIdeal=r["dtIdeal"], status=r["status"],
+            is_error=r["is_error"], cx=r["cx"], cy=r["cy"], LUx=r["LUx"], LUy=r["LUy"],
+            dx=prob.dx, dy=prob.dy, gamma=prob.gamma, bc=np.array(prob.bc), scheme=1,
+            message=r.get("message", ""))
     for (name, prob, scheme, tm, dt0, dtmin, dtmax, cfl, nsteps, tmax, sp) in run_cases():
         ref = Reference(fresh=True)
         U = prob.U.copy()

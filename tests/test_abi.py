@@ -37,7 +37,7 @@ def test_python_binding_covers_header():
         assert getattr(lib, s).argtypes is not None, f"{s} has no ctypes signature"
 
 
-@pytest.mark.parametrize("kw,val", [("halo", 1), ("nx", 1), ("scheme", 1), ("scheme", 4),
+@pytest.mark.parametrize("kw,val", [("halo", 1), ("nx", 1), ("scheme", 0), ("scheme", 4),
                                     ("time_method", 3), ("bc", (1, 1, 0, 1)), ("bc", (5, 1, 1, 1)),
                                     ("dx", 0.0), ("dy", -1.0)])
 def test_ctx_create_rejects_bad_parameters(kw, val):

@@ -225,6 +225,53 @@ def test_sor_fused_sweeps_match_unfused_and_oracle(shape, bc, fusable):
     assert (launches[0] < launches[1]) == fusable
 
 
+def _fill_corners(p):
+    for i in (0, 1, p.nx + 2, p.nx + 3):
+        for j in (0, 1, p.ny + 2, p.ny + 3):
+            p.U[:, i, j] = p.U[:, min(max(i, 2), p.nx + 1), min(max(j, 2), p.ny + 1)]
+    return p
+
+
+@pytest.mark.parametrize("path", _gold("integrate_cfd_"), ids=os.path.basename)
+def test_central_fd_error_messages(path):
+    """Central FD's fatal statuses name the reference's cell: the first
+    non-positive density and the last non-positive pressure in loop order."""
+    d = np.load(path)
+    ctx = make_ctx(_problem(d), scheme=M.CENTRAL_FD)
+    st, _, _ = ctx.integrate_host(d["U_in"].copy())
+    assert st.status == int(d["status"])
+    if st.isError:
+        assert st.message.splitlines()[:2] == str(d["message"]).splitlines()[:2]
+
+
+@pytest.mark.parametrize("shape,bc", [((200, 130), (1, 1, 1, 1)), ((160, 97), (3, 4, 2, 1)),
+                                      ((77, 77), (4, 4, 3, 3)), ((70, 100), (1, 1, 1, 1))])
+def test_central_fd_vs_oracle(shape, bc):
+    """Central FD2 over many thread blocks and boundary mixes: one integrate
+    (UL, dtIdeal, ghosts) and 3 RK3 steps, bit for bit against the oracle.
+    The 70 x 100 grid has ny > nx, where the reference reads flux entries it
+    never wrote; the oracle and the device both take them as 0."""
+    p = _fill_corners(P.random_smooth(*shape, seed=shape[0] + shape[1], bc=bc, amp=0.05))
+    ctx = make_ctx(p, scheme=M.CENTRAL_FD, dt_min=1e-9, dt_max=0.01, cfl=0.2, flags=0)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, bc, scheme=1, dt_min=1e-9, dt_max=0.01, cfl=0.2)
+    o.init_dirichlet(p.U.copy())
+    U = p.U.copy()
+    st, UL, ideal = ctx.integrate_host(U)
+    Uo = p.U.copy()
+    so, eo, ULo, io = o.integrate(Uo)
+    assert (st.status, int(st.isError)) == (so, eo) == (0, 0)
+    assert same(U, Uo) and same(interior(UL), interior(ULo)) and ideal == io
+    ctx.upload(p.U)
+    Uo = p.U.copy()
+    dt = dto = 0.01
+    for _ in range(3):
+        st, dt = ctx.step(dt)
+        so, eo, dto = o.step(Uo, dto)
+        assert (st.status, int(st.isError), dt) == (so, eo, dto)
+    assert same(ctx.download(), Uo)
+    assert ctx.characteristics()[0].max() == 0.0  # central FD keeps none
+
+
 def test_divb_calc_vs_oracle():
     p = P.random_blocky(50, 41, seed=3, bc=(1, 1, 3, 4))
     ctx = make_ctx(p, flags=0)

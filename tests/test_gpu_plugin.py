@@ -17,8 +17,12 @@ EXE = os.path.join(ROOT, "mhd2d-solver_b200", "_build", "plugin_check")
 
 
 @pytest.mark.skipif(not os.path.exists(EXE), reason="plugin_check not built (needs the reference headers)")
-@pytest.mark.parametrize("scheme", [2, 3])
-@pytest.mark.parametrize("problem,steps", [("ot", 6), ("bw", 12), ("dir", 5)])
+@pytest.mark.parametrize("scheme,problem,steps",
+                         [(s, p, n) for s in (2, 3) for p, n in (("ot", 6), ("bw", 12), ("dir", 5))]
+                         # central FD2 on the square vortex only: with ny < nx the reference
+                         # evaluates ghost corners that this problem leaves at zero density,
+                         # and fails on them (in the reference's own stepper as well)
+                         + [(1, "ot", 6)])
 def test_plugin_subclasses_match_reference(scheme, problem, steps):
     r = subprocess.run([EXE, str(scheme), problem, str(steps)], capture_output=True, text=True,
                        timeout=600)

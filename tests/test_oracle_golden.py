@@ -144,3 +144,31 @@ def test_oracle_vs_reference_random(seed):
         assert st == r["status"] and err == r["is_error"]
         s = (slice(None), slice(2, nx + 2), slice(2, ny + 2))
         assert same(U1, U2) and same(UL[s], r["UL"][s]) and ideal == r["dtIdeal"]
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_central_fd_vs_reference_random(seed):
+    """Central FD2 on random square-or-wider grids (ny <= nx: the reference's
+    corner test reads flux entries it never wrote when ny > nx), corners
+    filled or left at zero, every boundary mix."""
+    rng = np.random.default_rng(50 + seed)
+    nx = int(rng.integers(6, 20))
+    ny = int(rng.integers(4, nx + 1))
+    bc = tuple(int(b) for b in rng.integers(1, 5, size=4))
+    p = (P.random_smooth if seed % 2 else P.random_blocky)(nx, ny, seed=200 + seed, bc=bc)
+    if seed % 3:  # ghost corners get their nearest interior state
+        for i in (0, 1, nx + 2, nx + 3):
+            for j in (0, 1, ny + 2, ny + 3):
+                p.U[:, i, j] = p.U[:, min(max(i, 2), nx + 1), min(max(j, 2), ny + 1)]
+    U1 = p.U.copy()
+    r = Reference().integrate(1, U1, p.dx, p.dy, p.gamma, bc, U_dirichlet=p.U.copy())
+    o = Oracle(nx, ny, p.dx, p.dy, p.gamma, bc, scheme=1)
+    o.init_dirichlet(p.U.copy())
+    U2 = p.U.copy()
+    st, err, UL, ideal = o.integrate(U2)
+    assert st == r["status"] and err == r["is_error"]
+    assert same(U1, U2)
+    if st != 6:
+        s = (slice(None), slice(2, nx + 2), slice(2, ny + 2))
+        assert same(UL[s], r["UL"][s]) and ideal == r["dtIdeal"]
