@@ -79,8 +79,8 @@ void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double
             const double* aG, Ctl* ctl, double* const ch[4], cudaStream_t s) {
   const bool chars = ch && ch[0];
   if (scheme == 1) {  // central FD: checks and maxima, then UL
-    dim3 ring((g.ny + 2 + 31) / 32, (g.nx + 2 + 7) / 8), inner((g.ny + 31) / 32, (g.nx + 7) / 8);
-    k_cfd_check<<<ring, 256, 0, s>>>(g, U, ctl);
+    dim3 inner((g.ny + CFD_TJ - 1) / CFD_TJ, (g.nx + CFD_TI - 1) / CFD_TI);
+    k_cfd_check<<<grid1d((long long)(g.nx + 2) * (g.ny + 2), 256), 256, 0, s>>>(g, U, ctl);
     k_cfd_ul<<<inner, 256, 0, s>>>(g, U, UL, 1.0 / (2.0 * g.dx), 1.0 / (2.0 * g.dy), ctl);
     return;
   }
