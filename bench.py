@@ -367,6 +367,29 @@ def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1, store=-1):
                     "derivative to 1e-9 at small sizes (tests/test_gpu_adjoint.py)"}
 
 
+def central_fd_measure(dev, n):
+    """The second-order central finite-difference method (scheme 1) on the
+    same Orszag-Tang state: one spatial operator (boundary fill, check pass,
+    UL pass) timed back to back with CUDA events on the library stream.  Its
+    algorithmic HBM traffic is three passes over the state (the check pass
+    reads U, the UL pass reads U and writes UL)."""
+    import mhd2d_b200 as M
+    from mhd2d_b200 import problems as P
+
+    p = P.ot_vortex(n)
+    ctx = M.Context(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=M.CENTRAL_FD, device=dev,
+                    dt_min=1e-6, dt_max=0.03125, cfl=0.4)
+    ctx.upload(p.U)
+    ctx.time_integrate(3)
+    ms = ctx.time_integrate(10)
+    ctx.close()
+    traffic = 3.0 * 8 * n * n * 8
+    return {"workload": f"orszag-tang {n}x{n}, central fd2, one spatial operator",
+            "ms_per_integrate": ms, "cell_updates_per_s": float(n) * n / (ms * 1e-3),
+            "gbs_min_traffic": traffic / (ms * 1e-3) / 1e9,
+            "note": "3 state passes of 64 B per cell each; HBM-bound"}
+
+
 def batched_adjoint_measure(dev, n=64, steps=500, seed=2, K=16, seq_steps=50):
     """Batched forward + adjoint on plasma sheets: n instances, sides nx
     uniform in [256, 1024] with ny = nx / 2, delta ~ U[0.05, 0.2] in
@@ -556,6 +579,9 @@ def run_ours(args):
         }
     ctx.close()
     del ctx
+    cfd = central_fd_measure(dev, n)
+    if rank == 0:
+        line["central_fd"] = cfd
     if args.batch_runs > 0:
         bm = batched_measure(dev, args.batch_runs, args.batch_steps)
         if rank == 0:
