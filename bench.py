@@ -568,6 +568,11 @@ def run_ours(args):
                                          "by cells; algorithmic 128 B/cell",
                          "kernel": "k_flux (fused spatial operator) + boundary fill",
                          "flops_per_launch": flops, "launch_ms": t_int,
+                         "peak_unfused": peak / 2.0, "frac_unfused": achieved / (peak / 2.0),
+                         "unfused_note": "the bit-exact build may not contract a product and a sum "
+                                         "into one FMA (the reference rounds each), so its adds "
+                                         "and multiplies issue one flop per FP64 lane and cycle: "
+                                         "half the FMA peak binds it",
                          "peak_source": "measured live: FP64 FMA-chain probe (mhd_fp64_peak); "
                                         "MEASURED_PEAKS.json has no FP64 figure"},
             "clocks": clocks,
