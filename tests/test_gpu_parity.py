@@ -225,6 +225,30 @@ def test_sor_fused_sweeps_match_unfused_and_oracle(shape, bc, fusable):
     assert (launches[0] < launches[1]) == fusable
 
 
+@pytest.mark.parametrize("shape,bc", [((200, 136), (1, 1, 1, 1)), ((150, 97), (3, 4, 2, 3)),
+                                      ((64, 256), (4, 4, 1, 1))])
+@pytest.mark.parametrize("rsteps", [7, 8, 20000])
+def test_sor_sweep_forms_on_larger_grids(shape, bc, rsteps):
+    """The default sweeps (two launches where every periodic extent is a
+    multiple of 4) against the five-launch sweeps and the oracle on grids of
+    many blocks: the same corrected field, sweep count and status, with odd
+    and even sweep limits (7, 8) and a solve left to converge (20000)."""
+    p = P.random_smooth(*shape, seed=shape[0] + rsteps, bc=bc)
+    sp = M.sor_params(1, 3, rsteps, 1e-10, 1e-10, True, 1.7)
+    osp = SorParams(1, 3, float(rsteps), 1e-10, 1e-10, 1, 1.7)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, bc)
+    o.init_dirichlet(p.U.copy())
+    Uo = p.U.copy()
+    ctxs = [make_ctx(p, flags=0), make_ctx(p, flags=0)]
+    ctxs[1].set_sor_fused(0)
+    for _ in range(2):  # the second solve warm-starts from the kept potential
+        so, eo, swo = o.divb_sor(Uo, osp, red_black=1)
+        for ctx in ctxs:
+            st, sweeps = ctx.divb_sor(sp)
+            assert (st.status, int(st.isError), sweeps) == (so, eo, swo)
+            assert same(ctx.download(), Uo)
+
+
 def _fill_corners(p):
     for i in (0, 1, p.nx + 2, p.nx + 3):
         for j in (0, 1, p.ny + 2, p.ny + 3):
