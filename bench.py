@@ -139,6 +139,18 @@ def dist_setup(n_gpus):
     return world, rank, local
 
 
+def allreduce_sum(world, x):
+    """Sum over ranks; NCCL on GPUs, gloo on CPU."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -224,7 +236,7 @@ def run_reference(args):
     return 0
 
 
-def batched_measure(dev, n_runs, steps, seed=0):
+def batched_measure(dev, n_runs, steps, seed=0, world=1, rank=0):
     """Batched vs one-run-at-a-time throughput of the same kernels.
 
     The mixed batch (mhd2d_b200.batch.mixed_runs: log-uniform sides 64..1024,
@@ -232,15 +244,21 @@ def batched_measure(dev, n_runs, steps, seed=0):
     tuned, warmed up and advanced `steps` RK3 steps (3*steps stages) in one
     timed call.  The sequential leg runs every run alone through a batch of
     one (same kernels, same graph replay), each warmed up with the same call
-    and then timed; its time is the sum over runs."""
+    and then timed; its time is the sum over runs.  With several ranks the
+    runs are sharded by cell count (batch.shard_runs, no exchange between
+    GPUs): each rank runs its share, and the job's time is the slowest
+    rank's, its cell-updates the sum over ranks."""
     import numpy as np
     import torch
 
     from mhd2d_b200 import batch as B
 
-    mix = B.mixed_runs(n_runs, seed=seed)
+    full = B.mixed_runs(n_runs, seed=seed)
+    all_cells = np.array([m.run.nx * m.run.ny for m in full], dtype=np.float64)
+    share = B.shard_runs(all_cells, world, rank)
+    mix = [full[i] for i in share]
     stages = 3 * steps
-    cells = np.array([m.run.nx * m.run.ny for m in mix], dtype=np.float64)
+    cells = all_cells
 
     def timed(b, nst):
         stream = torch.cuda.ExternalStream(b.stream(), device=dev)
@@ -257,14 +275,16 @@ def batched_measure(dev, n_runs, steps, seed=0):
     def cells_of(b):
         return b.cells().astype(np.float64)
 
-    with B.Batch([m.run for m in mix], device=dev) as b:
-        for i, m in enumerate(mix):
-            m.init(b, i)
-        tune = b.tune(reps=2)
-        b.advance(stages)  # warm-up: graph capture of this stage count, first steps
-        l0 = b.launches()
-        ms_b, cu_b = timed(b, stages)
-        launches_b = b.launches() - l0
+    ms_b, cu_b, launches_b, tune = 0.0, 0.0, 0, None
+    if mix:  # a rank without runs (more ranks than runs) only joins the reductions
+        with B.Batch([m.run for m in mix], device=dev) as b:
+            for i, m in enumerate(mix):
+                m.init(b, i)
+            tune = b.tune(reps=2)
+            b.advance(stages)  # warm-up: graph capture of this stage count, first steps
+            l0 = b.launches()
+            ms_b, cu_b = timed(b, stages)
+            launches_b = b.launches() - l0
     ms_s, cu_s = 0.0, 0.0
     for m in mix:
         with B.Batch([m.run], device=dev) as b1:
@@ -274,10 +294,14 @@ def batched_measure(dev, n_runs, steps, seed=0):
             t, c = timed(b1, stages)
             ms_s += t
             cu_s += c
+    ms_b, ms_s = allreduce_max(world, ms_b), allreduce_max(world, ms_s)
+    cu_b, cu_s = allreduce_sum(world, cu_b), allreduce_sum(world, cu_s)
     vb = cu_b / (ms_b * 1e-3)
     vs = cu_s / (ms_s * 1e-3)
     return {"runs": n_runs, "seed": seed, "cells": int(cells.sum()),
-            "roe_runs": int(sum(m.run.scheme == 2 for m in mix)),
+            "roe_runs": int(sum(m.run.scheme == 2 for m in full)),
+            "sharding": {"ranks": world, "runs_per_rank": [
+                len(B.shard_runs(all_cells, world, q)) for q in range(world)]},
             "steps": steps, "stages": stages,
             "batched": {"value": vb, "unit": UNIT, "ms": ms_b, "launches": int(launches_b)},
             "sequential": {"value": vs, "unit": UNIT, "ms": ms_s},
@@ -588,7 +612,7 @@ def run_ours(args):
     if rank == 0:
         line["central_fd"] = cfd
     if args.batch_runs > 0:
-        bm = batched_measure(dev, args.batch_runs, args.batch_steps)
+        bm = batched_measure(dev, args.batch_runs, args.batch_steps, world=world, rank=rank)
         if rank == 0:
             line["batched"] = bm
     if args.adjoint_steps > 0:

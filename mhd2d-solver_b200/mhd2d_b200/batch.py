@@ -199,6 +199,24 @@ class MixedRun:
             b.init_wave(i, self.wave, self.kx, self.ky, eps=1e-6)
 
 
+def shard_runs(costs, world, rank):
+    """Indices of the runs rank `rank` of `world` takes: the runs are
+    independent, so they are spread over the GPUs with no exchange at all.
+    Longest processing time first: runs in decreasing cost (ties by index),
+    each to the rank with the least cost so far (ties by rank).  Every rank
+    computes the same assignment from the same costs."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    load = [0.0] * world
+    mine = []
+    for i in sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += float(costs[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 def mixed_runs(n=512, seed=0, side_min=64, side_max=1024, gamma=5.0 / 3.0):
     """The mixed batch of independent runs (seeded):
 

@@ -30,8 +30,32 @@ def _rank_main(rank, world, port, out):
     bench.barrier(world)
     # each rank reports its own timing; the job takes the slowest
     out[rank] = bench.allreduce_max(world, 10.0 + rank)
+    out[10 + rank] = bench.allreduce_sum(world, 1.5 + rank)
     bench.barrier(world)
     dist.destroy_process_group()
+
+
+def test_batched_runs_shard_without_overlap_and_balanced():
+    """Instance sharding of the batched runs (no exchange between GPUs): the
+    shares of all ranks partition the runs, one rank takes all, and the
+    greedy assignment keeps every rank within one run's cost of the others."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "mhd2d-solver_b200"))
+    from mhd2d_b200 import batch as B
+
+    mix = B.mixed_runs(512, seed=0)
+    costs = np.array([m.run.nx * m.run.ny for m in mix], dtype=np.float64)
+    assert B.shard_runs(costs, 1, 0) == list(range(512))
+    for world in (2, 3, 4, 8):
+        shares = [B.shard_runs(costs, world, r) for r in range(world)]
+        flat = sorted(i for sh in shares for i in sh)
+        assert flat == list(range(512))
+        loads = [costs[sh].sum() for sh in shares]
+        assert max(loads) - min(loads) <= costs.max()
+        assert shares == [B.shard_runs(costs, world, r) for r in range(world)]  # deterministic
+    with pytest.raises(ValueError):
+        B.shard_runs(costs, 2, 2)
 
 
 def test_two_rank_max_over_ranks_gloo():
@@ -41,6 +65,7 @@ def test_two_rank_max_over_ranks_gloo():
         mp.start_processes(_rank_main, args=(world, port, out), nprocs=world, join=True,
                            start_method="spawn")
         assert out[0] == 11.0 and out[1] == 11.0
+        assert out[10] == 4.0 and out[11] == 4.0
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_bench")),
