@@ -615,7 +615,7 @@ __device__ __forceinline__ void flux_tile(const Grid& g, const double* __restric
 // maskX / maskY: ENO choice words of the x / y interfaces ([NX][NY] by the
 // interface's left / lower cell), written (MASK 1) or read (MASK 2).
 template <int SCHEME, bool CHARS, int TI, int TJ, int NW, int MASK = 0>
-__global__ void __launch_bounds__(NW * 32, MHD_MINB)
+__global__ void __launch_bounds__(NW * 32, NW * 32 > 256 ? 1 : MHD_MINB)
 k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
        const double* __restrict__ alphaF, const double* __restrict__ alphaG,
        double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co, unsigned* maskX,

@@ -16,18 +16,35 @@
 namespace mhd {
 namespace MHD_KNS {
 
-// 7 x 32 tiles, 8 warps: 16 warp tasks per tile = 2 rounds, 90 KB of shared
-// memory and at most 128 registers per thread, so 2 CTAs = 16 warps per SM
-// (measured best against 8x32/6 warps, 15x32 or 11x32/8 warps with one CTA,
-// and smaller tiles at 96 registers).
+// Tiles of the fused flux kernel, rows x 32 columns and warps per CTA, per
+// scheme.  ENO-Roe: 7 x 32, 8 warps: 16 warp tasks per tile = 2 rounds, 90 KB
+// of shared memory and at most 128 registers per thread, so 2 CTAs = 16 warps
+// per SM (measured best against 8x32/6 warps, 15x32/16 warps (5.43 against
+// 5.40 ms at 4096^2), 11x32/12 warps, and smaller tiles at 96 registers).
+// ENO-LF: 15 x 32, 16 warps: 32 tasks = 2 rounds, 172 KB, one CTA of 16
+// warps per SM, 16/15 x-interface rows per cell row instead of 8/7
+// (6.89 against 7.23 ms at 4096^2).
 #ifndef MHD_TI
 #define MHD_TI 7
 #endif
 #ifndef MHD_NW
 #define MHD_NW 8
 #endif
-// tile rows x columns and warps per CTA of the fused flux kernel
-constexpr int TI = MHD_TI, TJ = 32, NW = MHD_NW;
+#ifndef MHD_TI_LF
+#define MHD_TI_LF 15
+#endif
+#ifndef MHD_NW_LF
+#define MHD_NW_LF 16
+#endif
+constexpr int TI = MHD_TI, TJ = 32;  // the ENO-Roe tile (Geom: l_smem)
+template <int SCHEME>
+struct FluxShape {
+  static constexpr int TI = MHD_TI, NW = MHD_NW;
+};
+template <>
+struct FluxShape<3> {
+  static constexpr int TI = MHD_TI_LF, NW = MHD_NW_LF;
+};
 using Geom = TileGeom<TI, TJ>;
 
 int grid1d(long long n, int block) {
@@ -58,20 +75,22 @@ void l_lf_alpha(const Grid& g, const double* U, double* aF, double* aG, Ctl* ctl
 template <int SCHEME, bool CHARS>
 void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const double* aG,
             Ctl* ctl, double* const ch[4], cudaStream_t s) {
-  auto kern = k_flux<SCHEME, CHARS, TI, TJ, NW>;
+  constexpr int ti = FluxShape<SCHEME>::TI, nw = FluxShape<SCHEME>::NW;
+  using Gm = TileGeom<ti, TJ>;
+  auto kern = k_flux<SCHEME, CHARS, ti, TJ, nw>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Geom::TMA_BYTES));
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Gm::TMA_BYTES));
     attr = true;
   }
-  dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + TI - 1) / TI);
+  dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + ti - 1) / ti);
   CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
              ch ? ch[3] : nullptr};
   const Gas G{g.gamma, g.gamma - 1.0, (g.gamma - 2.0) / (g.gamma - 1.0), 1.0 / std::sqrt(2.0)};
   CUtensorMap tm{};
-  const int use_tma = tile_tma_enabled() && make_box_map(g, U, Geom::CU, Geom::RU, &tm) ? 1 : 0;
+  const int use_tma = tile_tma_enabled() && make_box_map(g, U, Gm::CU, Gm::RU, &tm) ? 1 : 0;
   tile_tma_launches() += use_tma;
-  kern<<<grid, NW * 32, Geom::TMA_BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co,
+  kern<<<grid, nw * 32, Gm::TMA_BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co,
                                           nullptr, nullptr, tm, use_tma);
 }
 
