@@ -138,57 +138,48 @@ __device__ __forceinline__ double roe_upwind(const double* w, const double* vw, 
   return (ak >= 0 && wm < 1.0e10) ? wm : ((ak <= 0 && wp < 1.0e10) ? wp : 0.0);
 }
 
-// ENO-Roe flux of characteristic k with left row l, projecting only what
-// the reference's choice keeps (spatialmethodenoroe.cpp:240-264).  The
-// reference projects the fluxes at all 4 stencil points and their 3
-// undivided differences, then keeps one ENO pair of the upwind side: for
-// lambda > 0 the ENO- pair, chosen by the differences 0 and 1, and for
-// lambda < 0 the ENO+ pair, chosen by the differences 1 and 2.  Here the two
-// differences of the upwind side decide the pair, and only its two points
-// are projected: 4 of the 7 dot products, each the same sum in the same
-// order, so fw carries the same bits.  lambda = 0 (both sides may be used)
-// and NaN take the full projection.
-__device__ __forceinline__ double roe_side_flux(const Lane& L, const double* l, unsigned lm,
-                                                double ak) {
-  if (ak > 0.0 || ak < 0.0) {
-    const int s0 = ak > 0.0 ? 0 : 1;
-    double va = 0.0, vb = 0.0;
-#pragma unroll
-    for (int m = 0; m < NF; m++) {
-      if (!(lm & (1u << m))) continue;
-      const double fa = L.F(m, s0), fb = L.F(m, s0 + 1), fc = L.F(m, s0 + 2);
-      va += l[m] * (fb - fa);
-      vb += l[m] * (fc - fb);
-    }
-    // ENO-: |vw0| < |vw1| takes points 0, 1, else 1, 2; ENO+: |vw1| < |vw2|
-    // takes points 1, 2, else 2, 3
-    const int pa = s0 + (fabs(va) < fabs(vb) ? 0 : 1);
-    double wa = 0.0, wb = 0.0;
-#pragma unroll
-    for (int m = 0; m < NF; m++) {
-      if (!(lm & (1u << m))) continue;
-      wa += l[m] * L.F(m, pa);
-      wb += l[m] * L.F(m, pa + 1);
-    }
-    const double v = pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
-                   : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
-                              : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
-    return v < 1.0e10 ? v : 0.0;
-  }
-  double w[4] = {0.0, 0.0, 0.0, 0.0}, vw[3] = {0.0, 0.0, 0.0};
+// ENO-Roe characteristic flux of one stencil side: s0 = 0 the ENO- side
+// (differences 0, 1 pick points 0, 1 or 1, 2), s0 = 1 the ENO+ side
+// (differences 1, 2 pick points 1, 2 or 2, 3); the same sums in the same
+// order as the full projection (spatialmethodenoroe.cpp:240-254).
+__device__ __forceinline__ double roe_side_value(const Lane& L, const double* l, unsigned lm,
+                                                 int s0) {
+  double va = 0.0, vb = 0.0;
 #pragma unroll
   for (int m = 0; m < NF; m++) {
     if (!(lm & (1u << m))) continue;
-    const double f0 = L.F(m, 0), f1 = L.F(m, 1), f2 = L.F(m, 2), f3 = L.F(m, 3);
-    w[0] += l[m] * f0;
-    w[1] += l[m] * f1;
-    w[2] += l[m] * f2;
-    w[3] += l[m] * f3;
-    vw[0] += l[m] * (f1 - f0);
-    vw[1] += l[m] * (f2 - f1);
-    vw[2] += l[m] * (f3 - f2);
+    const double fa = L.F(m, s0), fb = L.F(m, s0 + 1), fc = L.F(m, s0 + 2);
+    va += l[m] * (fb - fa);
+    vb += l[m] * (fc - fb);
   }
-  return roe_upwind(w, vw, ak);
+  const int pa = s0 + (fabs(va) < fabs(vb) ? 0 : 1);
+  double wa = 0.0, wb = 0.0;
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    if (!(lm & (1u << m))) continue;
+    wa += l[m] * L.F(m, pa);
+    wb += l[m] * L.F(m, pa + 1);
+  }
+  return pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
+       : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
+                  : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
+}
+
+// ENO-Roe flux of characteristic k with left row l, projecting only what
+// the reference's choice keeps (spatialmethodenoroe.cpp:240-264):
+// fw = (lambda >= 0 && wm < 1e10) ? wm : ((lambda <= 0 && wp < 1e10) ? wp : 0).
+// The reference projects the fluxes at all 4 stencil points and their 3
+// undivided differences; here the upwind side is projected alone (4 of the
+// 7 dot products): ENO- for lambda >= 0, ENO+ for lambda < 0.  Only lambda
+// = 0 with wm >= 1e10 (or NaN) needs ENO+ as well; a NaN lambda gives 0.
+__device__ __forceinline__ double roe_side_flux(const Lane& L, const double* l, unsigned lm,
+                                                double ak) {
+  if (ak != ak) return 0.0;
+  const double v = roe_side_value(L, l, lm, ak >= 0.0 ? 0 : 1);
+  if (v < 1.0e10) return v;
+  if (!(ak == 0.0)) return 0.0;
+  const double wp = roe_side_value(L, l, lm, 1);
+  return wp < 1.0e10 ? wp : 0.0;
 }
 
 // ENO-Roe flux of a characteristic under a recorded choice code c (bits 0-1:
