@@ -16,9 +16,10 @@ independent 4096^2 run (replicas; the single-run halo-exchange sharding is
 not built), so scaling is weak.
 
 --impl reference times the reference's own CPU code (the unmodified
-reference sources compiled by oracle/Makefile into oracle/_ref/ref_bench),
-one process per host core - the reference's own parallelisation - each
-advancing a 512^2 Orszag-Tang sample of the same workload.
+reference sources compiled by oracle/Makefile into oracle/_ref/ref_bench) on
+the same 4096^2 grid, one process per host core - the reference's own
+parallelisation - as many as host memory holds (one copy takes ~19 GB); the
+K timed steps are spread over the copies.
 """
 import argparse
 import json
@@ -35,7 +36,6 @@ sys.path.insert(0, os.path.join(ROOT, "mhd2d-solver_b200"))
 METRIC = "FP64 ENO-Roe cell-updates/s at 4096^2 (Orszag-Tang, RK3-TVD, CFL 0.4)"
 UNIT = "cell-updates/s"
 N_GRID = 4096
-REF_SAMPLE = 512
 
 # Floating-point operations per interior cell (+, -, *, /, sqrt = 1), counted
 # by oracle/opcount.cpp on a random state with structural zeros excluded,
@@ -44,8 +44,8 @@ FLOPS_PER_CELL_INTEGRATE = {2: 3011.9, 3: 3514.0}
 FLOPS_PER_CELL_STEP = {2: 9147.6, 3: 10653.9}
 # DRAM bytes (read + write) of one k_flux launch per interior cell, from one
 # ncu capture of the 2048^2 ENO-Roe case (273.4 MB read + 226.4 MB written
-# while the kernel ran; the rest of UL was still dirty in L2 when it ended;
-# profiles/k_flux_eno_roe_ot2048_ncu.md), scaled to a launch by its cell count.
+# while the kernel ran; the rest of UL was still dirty in L2 when it ended),
+# scaled to a launch by its cell count.
 DRAM_BYTES_PER_CELL_FLUX = (273.373e6 + 226.401e6) / 2048 ** 2
 
 
@@ -169,21 +169,76 @@ def allreduce_max(world, x):
     return float(t.item())
 
 
-def cpu_baseline_sample(scheme_code, steps=8):
-    """The reference (oracle/_ref) on one core, bounded sample: 512^2 OT."""
+# Host memory one copy of the reference takes per cell of its grid: every
+# t_matrices block it allocates (the stepper's U1, U2, UL, the method's
+# fluxes, differences and characteristic copies, the driver's U, cx, cy, LUx,
+# LUy): 19.4 GB resident for 4096^2 (measured peak RSS), ~1155 B per cell.
+REF_BYTES_PER_CELL = 1160.0
+
+
+def bench_config(n, scheme):
+    """The workload both arms report (identical dicts, so the two lines name
+    the same configuration)."""
+    state_gb = 8 * (n + 4) ** 2 * 8 / 1e9
+    l2 = (f"inputs larger than L2 ({state_gb:.2f} GB state), no flush" if state_gb > 0.126
+          else f"state of {state_gb * 1e3:.1f} MB fits in L2, no flush")
+    return {"workload": f"orszag-tang {n}x{n}, eno-{scheme}, rk3, cfl 0.4, fp64",
+            "grid": [n, n], "scheme": f"eno-{scheme}", "l2": l2}
+
+
+def _mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return float(ln.split()[1]) * 1024.0
+    except OSError:
+        pass
+    return None
+
+
+def ref_copies(n, want):
+    """How many concurrent copies of the reference fit: one per host core,
+    fewer when host memory does not hold that many (8 GB kept free)."""
+    avail = _mem_available()
+    per = REF_BYTES_PER_CELL * (n + 4) ** 2
+    fit = want if avail is None else int((avail - 8e9) // per)
+    return max(1, min(want, fit)), avail, per
+
+
+def _split(total, parts, c):
+    return total // parts + (1 if c < total % parts else 0)
+
+
+def _step_times(text):
+    return [float(ln.split()[2]) for ln in text.splitlines() if ln.startswith("step")]
+
+
+def cpu_baseline_start(n, scheme_code):
+    """The reference (oracle/_ref/ref_bench) on one core on the bench's own
+    grid, started in the background: one warm-up step (first touch of its
+    freshly allocated arrays) and one timed step.  Collected by
+    cpu_baseline_finish; it runs on a host core beside the GPU work."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
-    if not os.path.exists(exe):
+    if not os.path.exists(exe) or ref_copies(n, 1)[0] < 1:
         return None
-    out = subprocess.run([exe, str(REF_SAMPLE), str(steps), str(scheme_code)], capture_output=True,
-                         text=True, timeout=600)
-    times = [float(ln.split()[2]) for ln in out.stdout.splitlines() if ln.startswith("step")]
+    return subprocess.Popen([exe, str(n), "2", str(scheme_code)], stdout=subprocess.PIPE,
+                            stderr=subprocess.DEVNULL, text=True)
+
+
+def cpu_baseline_finish(proc, n):
+    if proc is None:
+        return None
+    out, _ = proc.communicate()
+    times = _step_times(out)
     if len(times) < 2:
         return None
     t = sum(times[1:])
-    return {"value": REF_SAMPLE * REF_SAMPLE * (len(times) - 1) / t, "unit": UNIT, "cores": 1,
+    return {"value": float(n) * n * (len(times) - 1) / t, "unit": UNIT, "cores": 1,
             "kind": "reference",
-            "sample": f"reference RK3+ENO on Orszag-Tang {REF_SAMPLE}^2, {len(times) - 1} timed "
-                      f"steps after 1 warm-up, 1 thread ({t:.1f} s)"}
+            "sample": f"the unmodified reference (RK3 + ENO, CFL 0.4) on the same Orszag-Tang "
+                      f"{n}^2 grid, {len(times) - 1} timed step after 1 warm-up step, 1 thread "
+                      f"({t:.1f} s), run on a host core while the GPU measurements ran"}
 
 
 def run_reference(args):
@@ -192,42 +247,56 @@ def run_reference(args):
         return 0
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
     scheme = 3 if args.scheme == "lf" else 2
-    config = {"workload": f"orszag-tang {args.n}x{args.n}, eno-{args.scheme}, rk3, cfl 0.4, fp64",
-              "grid": [args.n, args.n], "scheme": f"eno-{args.scheme}", "parallelism": "cpu",
-              "l2": "inputs larger than L2"}
+    n = args.n
+    config = bench_config(n, args.scheme)
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/ref_bench not built (the reference checkout was absent "
                           "when the oracle was compiled)"}))
         return 0
     cores = os.cpu_count() or 1
-    nsteps = args.warmup + args.steps
-    procs = [subprocess.Popen([exe, str(REF_SAMPLE), str(nsteps), str(scheme)],
-                              stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-             for _ in range(cores)]
+    want = min(cores, max(args.steps, 1))
+    copies, avail, per = ref_copies(n, want)
+    # The K timed steps (and the W warm-up steps) are spread over the copies;
+    # every copy's first step is untimed (first touch of its arrays).
+    plan = []
+    for c in range(copies):
+        k = _split(args.steps, copies, c)
+        w = max(1, _split(args.warmup, copies, c))
+        plan.append((w, k))
+    procs = [subprocess.Popen([exe, str(n), str(w + k), str(scheme)], stdout=subprocess.PIPE,
+                              stderr=subprocess.DEVNULL, text=True) for (w, k) in plan]
     t0 = time.time()
     outs = [p.communicate()[0] for p in procs]
     wall = time.time() - t0
-    rates, per_step = [], []
-    for o in outs:
-        ts = [float(ln.split()[2]) for ln in o.splitlines() if ln.startswith("step")]
-        if len(ts) == nsteps:
-            timed = ts[args.warmup:]
-            rates.append(REF_SAMPLE * REF_SAMPLE * len(timed) / sum(timed))
+    rates, per_step, timed_steps = [], [], 0
+    for (w, k), o in zip(plan, outs):
+        ts = _step_times(o)
+        if k > 0 and len(ts) == w + k:
+            timed = ts[w:]
+            rates.append(float(n) * n * len(timed) / sum(timed))
             per_step.append(sum(timed) / len(timed))
+            timed_steps += len(timed)
     if not rates:
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU run failed"}))
         return 0
     value = sum(rates)  # each copy's main-loop rate, summed (one copy per core)
     ms = 1000.0 * max(per_step)
-    sample = (f"{len(rates)} concurrent copies of the reference RK3+ENO-{args.scheme} on "
-              f"Orszag-Tang {REF_SAMPLE}^2 (one per host thread), {args.steps} timed steps after "
-              f"{args.warmup} warm-up; aggregate = sum of per-copy rates; wall {wall:.1f} s")
+    mem = (f"host memory {avail / 1e9:.0f} GB available, {per / 1e9:.1f} GB per copy"
+           if avail else "host memory unknown")
+    limit = ("host memory" if copies < want else
+             ("one per core" if want == cores else "one per timed step"))
+    sample = (f"{len(rates)} concurrent copies of the unmodified reference RK3+ENO-{args.scheme} "
+              f"on the Orszag-Tang {n}^2 grid ({cores} host cores; {mem}; copies limited by "
+              f"{limit}); {timed_steps} timed steps spread over the copies, each "
+              f"copy's first step untimed ({sum(w for w, _ in plan)} warm-up steps in all); "
+              f"aggregate = sum of per-copy rates; per-copy rates "
+              f"{min(rates):.3g}..{max(rates):.3g}; wall {wall:.0f} s")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (Orszag-Tang initial state, seeded by its formula)",
-            "config": config, "impl": "reference",
+            "data": "synthetic (Orszag-Tang initial state from its formula, no dataset)",
+            "config": config, "impl": "reference", "parallelism": f"{len(rates)} CPU processes",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(rates),
                              "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -546,6 +615,9 @@ def run_ours(args):
     e2e_ms = allreduce_max(world, e0.elapsed_time(e1))
     e2e_value = world * cells * e2e_steps / (e2e_ms / 1000.0)
     state_bytes = 8 * (n + 4) * (n + 4) * 8
+    # the reference on one host core, same grid, beside the GPU measurements
+    # below (started after the e2e leg, whose host copies it would disturb)
+    base_proc = cpu_baseline_start(n, scheme) if rank == 0 and world == 1 else None
 
     # roofline of the dominant kernel (the fused flux kernel; one spatial
     # operator = boundary fill + flux kernel, timed back to back on the
@@ -576,11 +648,9 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (Orszag-Tang initial state from its formula, no dataset)",
-            "config": {"workload": f"orszag-tang {n}x{n}, eno-{args.scheme}, rk3, cfl 0.4, fp64"
-                                   + (", fast-math" if args.fast_math else ", bit-exact build"),
-                       "grid": [n, n], "scheme": f"eno-{args.scheme}",
-                       "parallelism": "replicas" if world > 1 else "single-gpu",
-                       "l2": "inputs larger than L2 (1.08 GB state), no flush"},
+            "config": bench_config(n, args.scheme),
+            "build": "fast-math (FMA contraction)" if args.fast_math else "bit-exact",
+            "parallelism": f"replicas on {world} GPUs" if world > 1 else "single-gpu",
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
                     "call": "mhd_step_host (pinned host state)"},
@@ -626,7 +696,7 @@ def run_ours(args):
             line["batched_adjoint"] = bam
     if rank == 0:
         if world == 1:
-            line["cpu_baseline"] = cpu_baseline_sample(scheme)
+            line["cpu_baseline"] = cpu_baseline_finish(base_proc, n)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -845,10 +845,8 @@ int record_finish(mhd_adj* a, double* dt_inout) {
   AK(cudaStreamSynchronize(a->stream));
   AK(cudaGetLastError());
   if (a->time_method != 1) {
-    int guard = 0;
+    // no cap, as in TimeIntegrationRK3::step: every retry lowers dt strictly
     while (a->hctl->retry && !a->hctl->error) {
-      if (++guard > 64)
-        return aset(a, MHD_ERR_WRONG_PARAMETER, true, "RK3 retry loop did not settle");
       const int base = *a->hnlog - 1;  // the retry tail's first flux takes the next slot
       if ((st = ensure_slots(a, base + 3))) return st;
       launch_control(a, PH_RK_RETRY);

@@ -212,10 +212,11 @@ int do_step(mhd_ctx* c, double* dt_inout) {
     enqueue_control(c, PH_RK_FIRST);
     enqueue_rk3_tail(c, chars);
     if ((st = read_ctl(c))) return st;
-    int guard = 0;
+    // Like TimeIntegrationRK3::step (timeintegrationrk3.cpp:81-148) the
+    // retries have no cap: each one restarts from min(dt1, dt2, dt3), which
+    // is strictly below the dt it replaces, so the ladder runs out in
+    // underflow (ErrorTimeUnderflow) or in update_dt's bounded loops.
     while (c->hctl->retry && !c->hctl->error) {
-      if (++guard > 64)
-        return set_status(c, MHD_ERR_WRONG_PARAMETER, true, "RK3 retry loop did not settle");
       enqueue_control(c, PH_RK_RETRY);
       enqueue_rk3_tail(c, chars);
       if ((st = read_ctl(c))) return st;

@@ -158,6 +158,9 @@ extern "C" int mhd_divb_calc_noalloc(double* U, int nx, int ny, int pitch, int r
   if (nx > MHD_NOALLOC_MAX_ROWS) return MHD_ERR_WRONG_PARAMETER;  // scratch holds one slot per row
   for (int s = 0; s < 4; s++)
     if (bc[s] < 1 || bc[s] > 4) return MHD_ERR_WRONG_PARAMETER;
+  // An error left pending by the caller's earlier work is not ours to
+  // report or to clear: leave it in place and launch nothing.
+  if (cudaPeekAtLastError() != cudaSuccess) return MHD_ERR_CUDA;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return MHD_ERR_CUDA;
   double* scratch = nullptr;
@@ -170,8 +173,11 @@ extern "C" int mhd_divb_calc_noalloc(double* U, int nx, int ny, int pitch, int r
   // one cell in from every non-periodic side (div_b_fix.cpp:17-101)
   const int x0 = bc[0] == 1 ? 2 : 3, x1 = bc[1] == 1 ? nx + 2 : nx + 1;
   const int y0 = bc[2] == 1 ? 2 : 3, y1 = bc[3] == 1 ? ny + 2 : ny + 1;
-  const int rows = x1 - x0;
-  k_na_rows<<<rows, 256, 0, s>>>(U, L, x0, y0, y1, 2.0 * dx, 2.0 * dy, scratch);
+  // nx = 2 with both x sides non-periodic leaves no row: max and sum are 0
+  // (k_na_finish reads no slot then), as divBCalculation's empty loops give
+  const int rows = x1 > x0 ? x1 - x0 : 0;
+  if (rows > 0) k_na_rows<<<rows, 256, 0, s>>>(U, L, x0, y0, y1, 2.0 * dx, 2.0 * dy, scratch);
   k_na_finish<<<1, 256, 0, s>>>(scratch, rows, dx * dy, result);
+  // nothing was pending on entry, so an error here is one of these launches
   return cudaGetLastError() == cudaSuccess ? MHD_OK : MHD_ERR_CUDA;
 }

@@ -12,7 +12,7 @@ t_status status_from(mhd_ctx* ctx, int st, const char* where) {
   char msg[1024] = {0};
   int is_error = 0;
   mhd_last_error(ctx, msg, sizeof msg, &is_error);
-  t_status s{is_error != 0, static_cast<ReturnStatus>(st == MHD_ERR_CUDA ? int(ReturnStatus::ErrorNotImplemented) : st),
+  t_status s{is_error != 0, st == MHD_ERR_CUDA ? kCudaFailure : static_cast<ReturnStatus>(st),
              std::string(msg)};
   if (st == MHD_ERR_CUDA) s.isError = true;
   if (st != MHD_OK) s.message += std::string("\n! ") + where;

@@ -14,8 +14,10 @@
 //       Cuda spatial methods; the stepper takes over its device context.
 //
 // Built against the reference's own headers (mhd2d.hpp and the interface
-// headers); see INTEGRATION.md for the two lines of main.cpp that select
-// these classes.  Errors come back as the reference's t_status.
+// headers).  A caller selects these classes where main.cpp:124-151 builds
+// its method and stepper.  Errors come back as the reference's t_status;
+// a CUDA failure carries kCudaFailure, a status value outside the
+// reference's enumerators, with isError set and the CUDA error text.
 #ifndef MHD2D_B200_CUDA_METHODS_HPP
 #define MHD2D_B200_CUDA_METHODS_HPP
 
@@ -25,6 +27,12 @@
 #include "timeintegrationmethod.hpp"
 
 struct mhd_ctx;
+
+// Status of a failed CUDA call (an allocation, a launch, a copy).  The
+// reference's ReturnStatus has no such member and none of its members means
+// it, so the value is one past them; it compares unequal to every
+// reference status, and main.cpp's loop treats it as any other isError.
+constexpr ReturnStatus kCudaFailure = static_cast<ReturnStatus>(100);
 
 class CudaSpatialMethod : public SpatialIntegrationMethod {
  public:

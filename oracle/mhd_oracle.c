@@ -31,6 +31,7 @@ struct orc_ctx {
    double *FN, *GN;           /* numerical fluxes at interfaces */
    double *cx, *cy, *LUx, *LUy;
    double *aF, *aG;           /* ENO-LF dissipation [8][NY] / [8][NX] */
+   int alpha_fixed;           /* aF / aG set by orc_set_lf_alpha: integrate keeps them */
    double *U1, *U2, *UL;      /* time-stepper stages */
    double *phi;               /* SOR potential, persists across solves */
    long long retries;         /* RK3 stage restarts taken so far */
@@ -459,6 +460,7 @@ static int lf_alpha( orc_ctx* c, const double* U, int* negp )
 {
    int i, j, k, np;
    double s[NF], lam[NF];
+   if( c->alpha_fixed ) return 0;
    for( k = 0; k < NF; k++ ){
       for( i = 1; i < c->nx+2; i++ ) c->aG[(size_t)k*c->NX+i] = 0.0;
       for( j = 1; j < c->ny+2; j++ ) c->aF[(size_t)k*c->NY+j] = 0.0;
@@ -475,6 +477,30 @@ static int lf_alpha( orc_ctx* c, const double* U, int* negp )
       for( k = 0; k < NF; k++ ){ double a = fabs(lam[k]); if( a > c->aG[(size_t)k*c->NX+i] ) c->aG[(size_t)k*c->NX+i] = a; }
    }
    return 0;
+}
+
+/* Test hook: the dissipation coefficients of a whole grid (lf_alpha over a
+   grid of nx x ny cells whose ghost layers are already filled), computed
+   without a context, so that a window of a large grid can be integrated
+   with the coefficients of the whole grid (orc_set_lf_alpha). */
+int orc_lf_alpha_grid( double gamma, int nx, int ny, const double* U, double* aF, double* aG )
+{
+   orc_ctx c0;
+   int negp = 0;
+   memset( &c0, 0, sizeof c0 );
+   c0.nx = nx; c0.ny = ny; c0.NX = nx+4; c0.NY = ny+4; c0.gamma = gamma;
+   c0.aF = aF; c0.aG = aG;
+   return lf_alpha( &c0, U, &negp ) ? ORC_ERR_NEGATIVE_DENSITY : ORC_OK;
+}
+
+/* Test hook: fix aF [8][NY] and aG [8][NX] for the following ENO-LF
+   integrations of this context (NULL returns to computing them). */
+void orc_set_lf_alpha( orc_ctx* c, const double* aF, const double* aG )
+{
+   if( !aF || !aG ){ c->alpha_fixed = 0; return; }
+   memcpy( c->aF, aF, (size_t)NF*c->NY*sizeof(double) );
+   memcpy( c->aG, aG, (size_t)NF*c->NX*sizeof(double) );
+   c->alpha_fixed = 1;
 }
 
 /* SpatialMethodEnoRoe::integrate (spatialmethodenoroe.cpp:33-179) and

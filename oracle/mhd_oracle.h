@@ -57,6 +57,13 @@ int  orc_apply_bc( orc_ctx* c, double* U, int* is_error );
 int  orc_integrate( orc_ctx* c, double* U, double* UL, double* dtIdeal, int* is_error );
 void orc_get_characteristics( const orc_ctx* c, double* cx, double* cy, double* LUx, double* LUy );
 
+/* Test hooks for windows of large ENO-LF grids: the dissipation
+   coefficients aF [8][ny+4], aG [8][nx+4] of a whole grid (ghosts already
+   filled; spatialmethodenolf.cpp:66-125), and fixing them for the next
+   integrations of a context (NULL, NULL: computed again). */
+int  orc_lf_alpha_grid( double gamma, int nx, int ny, const double* U, double* aF, double* aG );
+void orc_set_lf_alpha( orc_ctx* c, const double* aF, const double* aG );
+
 /* Power-of-two CFL step control (updateDt). */
 int  orc_update_dt( double dt_min, double dt_max, double cfl, double* dt_inout, double dtIdeal,
                     int* is_error );

@@ -83,6 +83,9 @@ def load_oracle():
                             _dp, _dp, _dp, _ip, _dp, _dp, C.c_int, _ip]
     lib.orc_eigens_f.argtypes = [C.c_double, _dp, _dp, _dp, _dp, _dp, _ip]
     lib.orc_eigenvalues_at.argtypes = [C.c_double, _dp, _dp, _ip]
+    lib.orc_lf_alpha_grid.argtypes = [C.c_double, C.c_int, C.c_int, _dp, _dp, _dp]
+    lib.orc_set_lf_alpha.argtypes = [C.c_void_p, _dp, _dp]
+    lib.orc_set_lf_alpha.restype = None
     lib.orc_retries.argtypes = [C.c_void_p]
     lib.orc_retries.restype = C.c_longlong
     return lib
@@ -177,6 +180,15 @@ class Oracle:
     def retries(self):
         return int(self.lib.orc_retries(self.ctx))
 
+    def set_lf_alpha(self, aF=None, aG=None):
+        """Fix the ENO-LF dissipation coefficients (aF [8][ny+4], aG [8][nx+4])
+        for the following integrations; no arguments: computed again."""
+        if aF is None:
+            self.lib.orc_set_lf_alpha(self.ctx, None, None)
+        else:
+            self.lib.orc_set_lf_alpha(self.ctx, _p(np.ascontiguousarray(aF)),
+                                      _p(np.ascontiguousarray(aG)))
+
     def integrate(self, U, UL=None):
         UL = np.zeros(self.shape()) if UL is None else UL
         d = C.c_double(0.0)
@@ -216,6 +228,18 @@ class Oracle:
                               hist_len, C.byref(e))
         return dict(status=st, is_error=e.value, dt=d.value, t=t.value, steps=n.value,
                     dt_hist=dth[:min(n.value, hist_len)], divb_hist=dbh[:min(n.value, hist_len)])
+
+
+def lf_alpha_grid(U, gamma, lib=None):
+    """ENO-LF dissipation coefficients of a whole grid whose ghost layers
+    are filled: (aF [8][ny+4], aG [8][nx+4])."""
+    lib = lib or load_oracle()
+    _, NX, NY = U.shape
+    aF, aG = np.zeros((8, NY)), np.zeros((8, NX))
+    st = lib.orc_lf_alpha_grid(gamma, NX - 4, NY - 4, _p(U), _p(aF), _p(aG))
+    if st:
+        raise RuntimeError(f"lf_alpha_grid: status {st}")
+    return aF, aG
 
 
 def oracle_update_dt(dt_min, dt_max, cfl, dt, ideal, lib=None):

@@ -11,7 +11,9 @@ stores inputs and outputs as compressed .npz files:
 * sor_*.npz       — one divBCorrectionSOR call (lexicographic sweep);
 * update_dt.npz   — a table of TimeIntegrationMethod::updateDt cases.
 
-Usage:  python tests/golden/make_golden.py     (needs the reference checkout)
+Usage:  python tests/golden/make_golden.py [name-prefix ...]
+        (needs the reference build; with prefixes only the matching files are
+        written, so the others keep their bytes)
 """
 import os
 import sys
@@ -96,6 +98,11 @@ def run_cases():
         # name, problem, scheme, time method, dt0, dt_min, dt_max, cfl, nsteps, t_max, sor
         ("briowu_roe", P.brio_wu(32, 8), 2, 2, 0.0078125, 1e-6, 0.0078125, 0.4, 0, 0.04, None),
         ("briowu_lf", P.brio_wu(32, 8), 3, 2, 0.0078125, 1e-6, 0.0078125, 0.4, 0, 0.04, None),
+        # the Brio-Wu shock tube at its full size and end time (256 x 8, t = 0.2, ~410 steps)
+        ("briowu_full_roe", P.brio_wu(256, 8), 2, 2, 0.0078125, 1e-6, 0.0078125, 0.4, 0, 0.2,
+         None),
+        ("briowu_full_lf", P.brio_wu(256, 8), 3, 2, 0.0078125, 1e-6, 0.0078125, 0.4, 0, 0.2,
+         None),
         ("ot_roe", P.ot_vortex(16), 2, 2, 0.03125, 1e-6, 0.03125, 0.4, 5, 0.0, None),
         ("ot_lf", P.ot_vortex(16), 3, 2, 0.03125, 1e-6, 0.03125, 0.4, 5, 0.0, None),
         ("explosion_retry", P.explosion(16), 2, 2, 0.02, 1e-9, 0.02, 0.4, 4, 0.0, None),
@@ -169,9 +176,14 @@ def main():
         st, err, newdt = ref.update_dt(dtmin, dtmax, cfl, dt, ideal)
         rows.append([dtmin, dtmax, cfl, dt, ideal, st, err, newdt])
     out["update_dt"] = dict(table=np.array(rows))
+    only = sys.argv[1:]
+    n = 0
     for key, d in out.items():
+        if only and not any(key.startswith(p) for p in only):
+            continue
         np.savez_compressed(os.path.join(HERE, key + ".npz"), **d)
-    print(f"wrote {len(out)} golden files to {HERE}")
+        n += 1
+    print(f"wrote {n} golden files to {HERE}")
 
 
 if __name__ == "__main__":

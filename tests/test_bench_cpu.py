@@ -71,9 +71,12 @@ def test_two_rank_max_over_ranks_gloo():
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_bench")),
                     reason="oracle/_ref not built")
 def test_reference_arm_prints_one_json_line():
+    """The reference arm on a small grid (the bench's default is 4096^2, ~19
+    GB and ~35 s per step per copy): one JSON line naming the same config
+    as the GPU arm, the requested steps spread over the copies."""
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--steps", "1", "--warmup", "1"], capture_output=True, text=True,
-                       timeout=900, cwd=ROOT)
+                        "--n", "96", "--steps", "3", "--warmup", "2"], capture_output=True,
+                       text=True, timeout=900, cwd=ROOT)
     assert r.returncode == 0, r.stderr
     lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
     assert len(lines) == 1
@@ -81,3 +84,17 @@ def test_reference_arm_prints_one_json_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "cell-updates/s"
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["higher_is_better"] is True
+    assert d["steps"] == 3 and d["warmup"] == 2
+    assert d["config"] == _load_bench().bench_config(96, "roe")
+    assert "3 timed steps" in d["cpu_baseline"]["sample"]
+
+
+def test_reference_copies_bounded_by_host_memory():
+    bench = _load_bench()
+    copies, avail, per = bench.ref_copies(4096, 16)
+    assert 1 <= copies <= 16
+    if avail is not None:
+        assert copies == 1 or copies * per <= avail - 8e9
+    # the timed and warm-up steps are spread over the copies without loss
+    for total, parts in ((20, 9), (3, 8), (10, 10)):
+        assert sum(bench._split(total, parts, c) for c in range(parts)) == total

@@ -1,0 +1,260 @@
+"""Parity at the benchmark configurations' sizes, and the stated tolerance of
+the FMA-contracted build (MHD_FLAG_FAST_MATH).
+
+Parity build (the default; bit for bit):
+* the Orszag-Tang vortex at 512^2, 50 CFL-controlled RK3 steps, ENO-Roe and
+  ENO-LF, against the unmodified reference's own main loop (oracle/_ref);
+* one ENO-LF spatial operator at 4096^2 on random windows: the oracle
+  integrates each window with the dissipation coefficients of the whole
+  grid (they are row and column maxima over the full grid);
+* a 16-run slice of the seeded 512-run batched mix (the cheapest 10 waves
+  and 6 explosions), each run to its own end time, against the oracle;
+* the Brio-Wu shock tube at its full size (256 x 8, t = 0.2) is a golden run
+  file (tests/golden/run_briowu_full_*.npz) checked by test_run_golden.
+
+FMA build, against the same reference runs, with the tolerances stated for
+this path: relative L-infinity <= 1e-10 on smooth problems (the 512^2
+vortex at t ~ 0.1, linear waves over one period, where it must also give
+the same measured convergence order) and relative L1 <= 1e-8 on shocked
+problems (Brio-Wu 256 x 8 to t = 0.2, the vortex at 128^2 to t = 1, the
+explosion at 128^2 to t = 0.1).  Norms are taken field by field over the
+interior cells and the worst field is reported:
+    rel_linf = max_k max|a_k - b_k| / max|b_k|,
+    rel_l1   = max_k sum|a_k - b_k| / sum|b_k|,
+fields that are identically zero in the reference (w, Bz in these 2-D
+problems) must be zero on the device too.
+
+The reference and oracle runs take most of this file's time; they run in a
+`spawn` process pool while the device runs.
+"""
+import concurrent.futures as cf
+import math
+import multiprocessing as mp
+import os
+
+import numpy as np
+import pytest
+
+import mhd2d_b200 as M
+from mhd2d_b200 import batch as B
+from mhd2d_b200 import problems as P
+from gpu_helpers import gpu_run, linear_wave, make_ctx, same
+from pyoracle import Oracle, lf_alpha_grid, reference_available
+import ref_jobs
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+SMOOTH_LINF = 1e-10
+SHOCKED_L1 = 1e-8
+
+# name -> (problem, side, dt0, dt_min, dt_max, cfl, steps, t_max)
+REF_CASES = {
+    "ot512": ("ot", 512, 0.03125, 1e-6, 0.03125, 0.4, 50, 0.0),
+    "ot128_t1": ("ot", 128, 0.03125, 1e-6, 0.03125, 0.4, 0, 1.0),
+    "explosion128": ("explosion", 128, 0.0078125, 1e-9, 0.0078125, 0.4, 0, 0.1),
+}
+SCHEMES = {"roe": M.ENO_ROE, "lf": M.ENO_LF}
+
+
+def _interior(U):
+    return U[:, 2:-2, 2:-2]
+
+
+def rel_norms(a, b):
+    """(rel_linf, rel_l1) of a against b, field by field (see module doc)."""
+    a, b = _interior(a), _interior(b)
+    linf = l1 = 0.0
+    for k in range(a.shape[0]):
+        d = np.abs(a[k] - b[k])
+        mb = np.max(np.abs(b[k]))
+        if mb == 0.0:
+            assert np.max(d) == 0.0, f"field {k} is zero in the reference only"
+            continue
+        linf = max(linf, float(np.max(d) / mb))
+        l1 = max(l1, float(np.sum(d) / np.sum(np.abs(b[k]))))
+    return linf, l1
+
+
+@pytest.fixture(scope="module")
+def pool():
+    if not reference_available():
+        pytest.skip("oracle/_ref (the reference build) is not present")
+    ex = cf.ProcessPoolExecutor(max_workers=min(8, os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn"))
+    yield ex
+    ex.shutdown(wait=True, cancel_futures=True)
+
+
+@pytest.fixture(scope="module")
+def ref_runs(pool):
+    """Futures of the reference's runs, submitted once for the module."""
+    futs = {}
+    for name, (kind, n, dt0, dmin, dmax, cfl, steps, tmax) in REF_CASES.items():
+        for sname, scheme in SCHEMES.items():
+            futs[(name, sname)] = pool.submit(ref_jobs.reference_run, kind, n, scheme, dt0, dmin,
+                                              dmax, cfl, steps, tmax)
+    return futs
+
+
+def _device_run(case, scheme, flags):
+    kind, n, dt0, dmin, dmax, cfl, steps, tmax = REF_CASES[case]
+    p = ref_jobs.problem(kind, n)
+    ctx = make_ctx(p, scheme=scheme, dt_min=dmin, dt_max=dmax, cfl=cfl, flags=flags)
+    r = gpu_run(ctx, dt0, nsteps=steps, t_max=tmax)
+    U = ctx.download()
+    ctx.close()
+    return U, r
+
+
+@pytest.mark.parametrize("sname", ["roe", "lf"])
+def test_orszag_tang_512_multistep_bitwise(ref_runs, sname):
+    ref = ref_runs[("ot512", sname)].result()
+    assert ref["status"] == M.OK and ref["steps"] == 50
+    U, r = _device_run("ot512", SCHEMES[sname], 0)
+    assert r["steps"] == ref["steps"] and r["t"] == ref["t"] and r["dt"] == ref["dt"]
+    assert same(_interior(U), _interior(ref["U"]))
+
+
+@pytest.mark.parametrize("sname", ["roe", "lf"])
+def test_fast_math_smooth_orszag_tang_512(ref_runs, sname):
+    ref = ref_runs[("ot512", sname)].result()
+    U, r = _device_run("ot512", SCHEMES[sname], M.FLAG_FAST_MATH)
+    assert r["status"] == M.OK and r["steps"] == ref["steps"] and r["t"] == ref["t"]
+    linf, _ = rel_norms(U, ref["U"])
+    assert linf <= SMOOTH_LINF, linf
+
+
+@pytest.mark.parametrize("case", ["ot128_t1", "explosion128"])
+@pytest.mark.parametrize("sname", ["roe", "lf"])
+def test_fast_math_shocked_runs(ref_runs, case, sname):
+    ref = ref_runs[(case, sname)].result()
+    assert ref["status"] == M.OK
+    U, r = _device_run(case, SCHEMES[sname], M.FLAG_FAST_MATH)
+    assert r["status"] == M.OK and r["steps"] == ref["steps"] and r["t"] == ref["t"]
+    _, l1 = rel_norms(U, ref["U"])
+    assert l1 <= SHOCKED_L1, l1
+
+
+@pytest.mark.parametrize("sname", ["roe", "lf"])
+def test_fast_math_brio_wu_full(sname):
+    """Config-1 Brio-Wu (256 x 8, Neumann, gamma 2, t_end 0.2) against the
+    reference's golden run."""
+    d = np.load(os.path.join(GOLD, f"run_briowu_full_{sname}.npz"))
+    p = P.Problem(d["U_in"].copy(), float(d["dx"]), float(d["dy"]), float(d["gamma"]),
+                  tuple(int(b) for b in d["bc"]))
+    ctx = make_ctx(p, scheme=int(d["scheme"]), dt_min=float(d["dt_min"]),
+                   dt_max=float(d["dt_max"]), cfl=float(d["cfl"]), flags=M.FLAG_FAST_MATH)
+    r = gpu_run(ctx, float(d["dt0"]), t_max=float(d["t_max"]))
+    U = ctx.download()
+    assert r["status"] == int(d["status"]) and r["steps"] == int(d["steps"])
+    _, l1 = rel_norms(U, d["U_out"])
+    assert l1 <= SHOCKED_L1, l1
+
+
+@pytest.mark.parametrize("wave", [6, 5, 4], ids=["fast", "alfven", "slow"])
+def test_fast_math_linear_waves(wave):
+    """One period of a 1e-6 linear wave (the convergence deck) at N = 16, 32,
+    64: within the smooth tolerance of the parity build (itself bit-identical
+    to the reference, test_gpu_convergence), with the same measured order."""
+    errs = {0: [], M.FLAG_FAST_MATH: []}
+    for n in (16, 32, 64):
+        p, speed = linear_wave(n, wave)
+        period = 1.0 / speed
+        kw = dict(dt_min=1e-9, dt_max=period / 16.0, cfl=0.4)
+        out = {}
+        for flags in (0, M.FLAG_FAST_MATH):
+            ctx = make_ctx(p, flags=flags, **kw)
+            r = gpu_run(ctx, period / 64.0, t_max=period)
+            assert r["status"] == M.OK
+            out[flags] = (ctx.download(), r)
+            ctx.close()
+            U = out[flags][0]
+            errs[flags].append(np.abs(_interior(U) - _interior(p.U)).sum() * p.dx * p.dy)
+        (Ue, re), (Uf, rf) = out[0], out[M.FLAG_FAST_MATH]
+        assert rf["steps"] == re["steps"] and rf["t"] == re["t"]
+        linf, _ = rel_norms(Uf, Ue)
+        assert linf <= SMOOTH_LINF, (n, linf)
+    orders = {f: (math.log2(e[0] / e[1]), math.log2(e[1] / e[2])) for f, e in errs.items()}
+    assert abs(orders[M.FLAG_FAST_MATH][0] - orders[0][0]) < 0.01, orders
+    assert abs(orders[M.FLAG_FAST_MATH][1] - orders[0][1]) < 0.01, orders
+
+
+def _fill_periodic(U):
+    nx, ny = U.shape[1] - 4, U.shape[2] - 4
+    U[:, 0:2, 2:ny + 2] = U[:, nx:nx + 2, 2:ny + 2]
+    U[:, nx + 2:nx + 4, 2:ny + 2] = U[:, 2:4, 2:ny + 2]
+    U[:, 2:nx + 2, 0:2] = U[:, 2:nx + 2, ny:ny + 2]
+    U[:, 2:nx + 2, ny + 2:ny + 4] = U[:, 2:nx + 2, 2:4]
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_full_size_window_parity_lf(seed):
+    """4096^2 Orszag-Tang, one ENO-LF spatial operator on the device.  The
+    dissipation coefficients are maxima over whole grid rows and columns, so
+    the oracle takes them from the whole grid (its own lf_alpha on the
+    periodically filled state) and integrates random 96 x 96 windows with
+    them; UL agrees bit for bit on the cells at least 4 cells (2-cell
+    stencil reach + 1) from the window edge."""
+    n = 4096
+    p = P.ot_vortex(n)
+    ctx = make_ctx(p, scheme=M.ENO_LF, flags=0)
+    st, _ = ctx.integrate()
+    assert not st.isError
+    UL = ctx.download_ul()
+    ctx.close()
+    Ufull = p.U.copy()
+    _fill_periodic(Ufull)
+    aF, aG = lf_alpha_grid(Ufull, p.gamma)
+    rng = np.random.default_rng(seed)
+    w, m = 96, 4
+    for _ in range(3):
+        i0, j0 = (int(v) for v in rng.integers(0, n - w, size=2))
+        win = np.zeros((8, w + 4, w + 4))
+        win[:, 2:-2, 2:-2] = p.U[:, 2 + i0:2 + i0 + w, 2 + j0:2 + j0 + w]
+        o = Oracle(w, w, p.dx, p.dy, p.gamma, (3, 3, 3, 3), scheme=M.ENO_LF)
+        # window column jw is grid column j0 + jw (both with 2 ghost columns)
+        o.set_lf_alpha(aF[:, j0:j0 + w + 4], aG[:, i0:i0 + w + 4])
+        st_o, err, ULo, _ = o.integrate(win)
+        assert not err
+        a = ULo[:, 2 + m:2 + w - m, 2 + m:2 + w - m]
+        b = UL[:, 2 + i0 + m:2 + i0 + w - m, 2 + j0 + m:2 + j0 + w - m]
+        assert same(a, b)
+
+
+def _slice_indices(mix, waves=10, explosions=6):
+    """The cheapest runs of the mix by cells x estimated steps."""
+    def cost(i):
+        r = mix[i].run
+        speed = 6.0 if mix[i].kind == "explosion" else 2.1
+        dt = min(r.dt_max, r.cfl * min(r.dx, r.dy) / speed)
+        return r.nx * r.ny * r.t_end / dt
+
+    w = sorted((i for i, m in enumerate(mix) if m.kind == "wave"), key=cost)[:waves]
+    e = sorted((i for i, m in enumerate(mix) if m.kind == "explosion"), key=cost)[:explosions]
+    return sorted(w + e)
+
+
+def test_batched_mix_slice_matches_oracle(pool):
+    """16 runs of the seeded 512-run mix (mixed_runs(512, seed=0)), batched
+    and run to their own end times, each bit-identical to the oracle's main
+    loop from the same device-generated initial state."""
+    mix = B.mixed_runs(512, seed=0)
+    idx = _slice_indices(mix)
+    sel = [mix[i] for i in idx]
+    with B.Batch([m.run for m in sel]) as b:
+        for i, m in enumerate(sel):
+            m.init(b, i)
+        U0 = [b.download(i) for i in range(len(sel))]
+        futs = [pool.submit(ref_jobs.oracle_run, U0[i], m.run.nx, m.run.ny, m.run.dx, m.run.dy,
+                            m.run.gamma, tuple(m.run.bc), m.run.scheme, m.run.time_method,
+                            m.run.dt0, m.run.dt_min, m.run.dt_max, m.run.cfl, m.run.t_end)
+                for i, m in enumerate(sel)]
+        assert b.run(check_every=50) == 0
+        for i, (m, f) in enumerate(zip(sel, futs)):
+            ref = f.result()
+            st = b.state(i)
+            assert st["steps"] == ref["steps"] and st["t"] == ref["t"], (idx[i], st, ref["steps"])
+            assert st["dt"] == ref["dt"] and st["status"].status == ref["status"], idx[i]
+            assert st["retries"] == ref["retries"], idx[i]
+            assert same(_interior(b.download(i)), _interior(ref["U"])), idx[i]

@@ -4,7 +4,6 @@ the unmodified reference sources) with identical states.  The wave setup is
 the reference's wave test (file_access.cpp:922-1045): a 1e-6 right-eigenvector
 perturbation of the midpoint eigen-system of the background state, along x,
 run for one period."""
-import ctypes as C
 import math
 
 import numpy as np
@@ -12,37 +11,10 @@ import pytest
 
 import mhd2d_b200 as M
 from mhd2d_b200 import problems as P
-from gpu_helpers import gpu_run, make_ctx, same
-from pyoracle import Reference, load_oracle, reference_available
+from gpu_helpers import gpu_run, linear_wave as _wave, make_ctx, same
+from pyoracle import Reference, reference_available
 
 pytestmark = pytest.mark.gpu
-GAMMA = 5.0 / 3.0
-BACKGROUND = (1.0, 0.0, 0.0, 0.0, 1.0, math.sqrt(2.0), 0.5, 1.0 / GAMMA)  # rho u v w Bx By Bz p
-
-
-def _conserved(q):
-    rho, u, v, w, bx, by, bz, p = q
-    uu, bb = u * u + v * v + w * w, bx * bx + by * by + bz * bz
-    return np.array([rho, u * rho, v * rho, w * rho, bx, by, bz,
-                     p / (GAMMA - 1.0) + 0.5 * rho * uu + 0.5 * bb])
-
-
-def _wave(n, wave, eps=1e-6, ny=4):
-    avg = _conserved(BACKGROUND)
-    lam, lv, rv = np.zeros(8), np.zeros(64), np.zeros(64)
-    npr = C.c_int(0)
-    dp = C.POINTER(C.c_double)
-    st = load_oracle().orc_eigens_f(C.c_double(GAMMA), avg.ctypes.data_as(dp),
-                                    avg.ctypes.data_as(dp), lam.ctypes.data_as(dp),
-                                    lv.ctypes.data_as(dp), rv.ctypes.data_as(dp), C.byref(npr))
-    assert st == 0
-    dx = 1.0 / n
-    U = np.zeros((8, n + 4, ny + 4))
-    x = -0.5 + np.arange(n) * dx  # cell i at x0 + i dx
-    prof = np.cos(2.0 * math.pi * x)
-    for k in range(8):
-        U[k, 2:-2, 2:-2] = (avg[k] + eps * rv.reshape(8, 8)[wave][k] * prof)[:, None]
-    return P.Problem(U, dx, dx, GAMMA, (M.PERIODIC,) * 4), abs(lam[wave])
 
 
 @pytest.mark.parametrize("wave", [6, 5, 4], ids=["fast", "alfven", "slow"])

@@ -172,3 +172,24 @@ def test_oracle_central_fd_vs_reference_random(seed):
     if st != 6:
         s = (slice(None), slice(2, nx + 2), slice(2, ny + 2))
         assert same(UL[s], r["UL"][s]) and ideal == r["dtIdeal"]
+
+
+def test_fixed_lf_alpha_hook():
+    """The window hook of the oracle: integrating with the coefficients of
+    lf_alpha_grid (on the filled state) gives the ordinary ENO-LF result;
+    other coefficients change it."""
+    from pyoracle import Oracle, lf_alpha_grid
+    from mhd2d_b200 import problems as P
+
+    p = P.ot_vortex(40)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=3)
+    U = p.U.copy()
+    _, _, UL, ideal = o.integrate(U)
+    aF, aG = lf_alpha_grid(U, p.gamma)
+    o2 = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=3)
+    o2.set_lf_alpha(aF, aG)
+    _, _, UL2, ideal2 = o2.integrate(p.U.copy())
+    assert np.array_equal(UL, UL2) and ideal == ideal2
+    o2.set_lf_alpha(1.1 * aF, 1.1 * aG)
+    _, _, UL3, _ = o2.integrate(p.U.copy())
+    assert not np.array_equal(UL, UL3)
