@@ -34,12 +34,18 @@ namespace MHD_KNS {
 // (gamma - 1), rs2 = 1 / sqrt(2).
 struct Gas {
   double gm, g1, g21, rs2;
+#ifdef MHD_FAST
+  double ig1;  // 1 / (gamma - 1)
+#endif
 };
 
 struct Mid {
   double u, v, w, uu;
   double a2, a, ca2, ca, cs2, cs, cf2, cf;
   double rr, af2, af, as2, as, bty, btz, th1, th2, vb;
+#ifdef MHD_FAST
+  double irr, icfrr;  // 1 / sqrt(rho), 1 / (c_f sqrt(rho))
+#endif
   unsigned sbxm, fcfm, fcsm;  // sign-bit masks of sgn(Bx), cffactor, csfactor
   int negp;                   // midpoint pressure was negative and clamped
 };
@@ -122,6 +128,85 @@ __device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const d
   return true;
 }
 
+#ifdef MHD_FAST
+// Fast build (MHD_FLAG_FAST_MATH): the same midpoint state, from each
+// side's density and magnetic field (U1, U2) and its primitives P = (u, v,
+// w, total pressure), which phase 1 of the tile computes once per cell.  The
+// reference divides each side's momenta and 0.5*|m|^2 by its density per
+// interface and divides by the midpoint density, (c_f^2 - c_s^2), |B_perp|,
+// sqrt(rho) and c_f sqrt(rho) several times over; here every distinct
+// denominator is inverted once.  Not bit-identical to the reference (the
+// parity build is); agrees to the stated FP64 tolerance.
+__device__ __forceinline__ bool midpoint_fast(const Gas& G, const double* U1, const double* U2,
+                                              const double* P1, const double* P2, Mid& e) {
+  const double gm = G.gm;
+  const double r = 0.5 * (U1[0] + U2[0]);
+  e.u = 0.5 * (P1[0] + P2[0]);
+  e.v = 0.5 * (P1[1] + P2[1]);
+  e.w = 0.5 * (P1[2] + P2[2]);
+  const double bx = 0.5 * (U1[4] + U2[4]);
+  const double by = 0.5 * (U1[5] + U2[5]);
+  const double bz = 0.5 * (U1[6] + U2[6]);
+  if (r <= 0.0) return false;
+  const double u = e.u, v = e.v, w = e.w;
+  e.uu = u * u + v * v + w * w;
+  const double bb = bx * bx + by * by + bz * bz;
+  const double pt = 0.5 * (P1[3] + P2[3]);
+  double p = pt - 0.5 * bb;
+  e.negp = 0;
+  if (p < 0.0) { p = 0.0; e.negp = 1; }
+  const double ir = 1.0 / r;
+  double a2 = gm * p * ir;
+  if (a2 < 0.0) a2 = 0.0;
+  e.a2 = a2;
+  e.a = sqrt(a2);
+  e.ca2 = bx * bx * ir;
+  e.ca = sqrt(e.ca2);
+  const double c2 = 0.5 * (bb * ir + a2);
+  double ct = c2 * c2 - a2 * e.ca2;
+  if (ct < 0.0) ct = 0.0;
+  const double sct = sqrt(ct);
+  double cs2 = c2 - sct;
+  if (cs2 < 0.0) cs2 = SMALL;
+  double cf2 = c2 + sct;
+  if (cf2 < 0.0) cf2 = SMALL;
+  e.cs2 = cs2; e.cs = sqrt(cs2);
+  e.cf2 = cf2; e.cf = sqrt(cf2);
+  const double irr = rsqrt(r);
+  e.irr = irr;
+  e.rr = r * irr;
+  const double bp2 = by * by + bz * bz;
+  e.sbxm = (bx < 0.0) ? 0x80000000u : 0u;
+  const bool deg = (bp2 < SMALL) && (fabs(e.ca2 - a2) < SMALL);
+  const double idn = 1.0 / (cf2 - cs2);
+  double af2 = deg ? 1.0 : (cf2 - e.ca2) * idn;
+  if (af2 < 0.0) af2 = 0.0;
+  double as2 = deg ? 1.0 : (cf2 - a2) * idn;
+  if (as2 < 0.0) as2 = 0.0;
+  e.af2 = af2; e.af = sqrt(af2);
+  e.as2 = as2; e.as = sqrt(as2);
+  if (bp2 > SMALL) {
+    const double isb = rsqrt(bp2);
+    e.bty = by * isb;
+    e.btz = bz * isb;
+  } else {
+    e.bty = G.rs2;
+    e.btz = G.rs2;
+  }
+  const double g21 = G.g21;
+  e.th1 = 1.0 / (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2));
+  e.th2 = 1.0 / (flip(af2 * e.cf * e.a, e.sbxm) + flip(as2 * e.cs * e.ca, e.sbxm));
+  e.icfrr = irr / e.cf;
+  e.vb = e.bty * v + e.btz * w;
+
+  const bool sgnbt_pos = (by > 0.0) || (fabs(by) < SMALL && (bz > 0.0));
+  const unsigned bt = sgnbt_pos ? 0u : 0x80000000u;
+  e.fcsm = a2 > e.ca2 ? bt : 0u;
+  e.fcfm = a2 < e.ca2 ? bt : 0u;
+  return true;
+}
+#endif
+
 // Makes the midpoint scalars opaque to the optimiser at the top of each
 // characteristic iteration (an empty asm that "may modify" them, no
 // instruction emitted).  Without it the compiler hoists every row's
@@ -133,6 +218,9 @@ __device__ __forceinline__ void opaque(Mid& e) {
   asm volatile("" : "+d"(e.af), "+d"(e.as), "+d"(e.af2), "+d"(e.as2), "+d"(e.bty), "+d"(e.btz),
                     "+d"(e.th1), "+d"(e.th2), "+d"(e.vb), "+r"(e.sbxm), "+r"(e.fcfm),
                     "+r"(e.fcsm));
+#ifdef MHD_FAST
+  asm volatile("" : "+d"(e.irr), "+d"(e.icfrr));
+#endif
 }
 
 __device__ __forceinline__ double eigenvalue(const Mid& e, int k) {
@@ -237,12 +325,22 @@ __device__ __forceinline__ void lv_row(const Mid& e, const Gas& G, int k, double
 }
 
 // Right eigenvector row k (spatialmethodeno.cpp:392-471, sign flips 554-568).
+// FR (fast build only): divide by sqrt(rho), c_f sqrt(rho) and gamma - 1
+// through the midpoint's reciprocals.
+template <bool FR = false>
 __device__ __forceinline__ void rv_row(const Mid& e, const Gas& G, int k, double* q) {
   const double u = e.u, v = e.v, w = e.w, uu = e.uu, a2 = e.a2, a = e.a, ca = e.ca;
   const double cs = e.cs, cs2 = e.cs2, cf = e.cf, cf2 = e.cf2, rr = e.rr;
   const double af = e.af, as = e.as, bty = e.bty, btz = e.btz, g1 = G.g1, g21 = G.g21;
   const double vb = e.vb;
   const unsigned sb = e.sbxm;
+#ifdef MHD_FAST
+#define RV_DIV(x, d, inv) (FR ? (x) * (inv) : (x) / (d))
+#define DIV_G1(x) (FR ? (x) * G.ig1 : (x) / g1)
+#else
+#define RV_DIV(x, d, inv) ((x) / (d))
+#define DIV_G1(x) ((x) / g1)
+#endif
   switch (k) {
     case 0:
     case 6: {
@@ -251,16 +349,16 @@ __device__ __forceinline__ void rv_row(const Mid& e, const Gas& G, int k, double
         q[1] = af * (u - cf);
         q[2] = af * v + flip(as * bty * ca, sb);
         q[3] = af * w + flip(as * btz * ca, sb);
-        q[7] = 0.5 * af * uu + af * cf2 / g1 - af * cf * u + flip(as * ca, sb) * vb + g21 * af * (cf2 - a2);
+        q[7] = 0.5 * af * uu + DIV_G1(af * cf2) - af * cf * u + flip(as * ca, sb) * vb + g21 * af * (cf2 - a2);
       } else {
         q[0] = af;
         q[1] = af * (u + cf);
         q[2] = af * v - flip(as * bty * ca, sb);
         q[3] = af * w - flip(as * btz * ca, sb);
-        q[7] = 0.5 * af * uu + af * cf2 / g1 + af * cf * u - flip(as * ca, sb) * vb + g21 * af * (cf2 - a2);
+        q[7] = 0.5 * af * uu + DIV_G1(af * cf2) + af * cf * u - flip(as * ca, sb) * vb + g21 * af * (cf2 - a2);
       }
-      q[5] = as * bty * cf / rr;
-      q[6] = as * btz * cf / rr;
+      q[5] = RV_DIV(as * bty * cf, rr, e.irr);
+      q[6] = RV_DIV(as * btz * cf, rr, e.irr);
       const unsigned f = e.fcfm;
       q[0] = flip(q[0], f); q[1] = flip(q[1], f); q[2] = flip(q[2], f); q[3] = flip(q[3], f);
       q[5] = flip(q[5], f); q[6] = flip(q[6], f); q[7] = flip(q[7], f);
@@ -269,8 +367,8 @@ __device__ __forceinline__ void rv_row(const Mid& e, const Gas& G, int k, double
     case 1:
       q[2] = flip(btz, sb);
       q[3] = flip(-bty, sb);
-      q[5] = btz / rr;
-      q[6] = -bty / rr;
+      q[5] = RV_DIV(btz, rr, e.irr);
+      q[6] = RV_DIV(-bty, rr, e.irr);
       q[7] = flip(btz * v - bty * w, sb);
       break;
     case 2:
@@ -280,16 +378,16 @@ __device__ __forceinline__ void rv_row(const Mid& e, const Gas& G, int k, double
         q[1] = as * (u - cs);
         q[2] = as * v - flip(af * bty * a, sb);
         q[3] = as * w - flip(af * btz * a, sb);
-        q[7] = 0.5 * as * uu + as * cs2 / g1 - as * cs * u - flip(af * a, sb) * vb + g21 * as * (cs2 - a2);
+        q[7] = 0.5 * as * uu + DIV_G1(as * cs2) - as * cs * u - flip(af * a, sb) * vb + g21 * as * (cs2 - a2);
       } else {
         q[0] = as;
         q[1] = as * (u + cs);
         q[2] = as * v + flip(af * bty * a, sb);
         q[3] = as * w + flip(af * btz * a, sb);
-        q[7] = 0.5 * as * uu + as * cs2 / g1 + as * cs * u + flip(af * a, sb) * vb + g21 * as * (cs2 - a2);
+        q[7] = 0.5 * as * uu + DIV_G1(as * cs2) + as * cs * u + flip(af * a, sb) * vb + g21 * as * (cs2 - a2);
       }
-      q[5] = -af * bty * a2 / (cf * rr);
-      q[6] = -af * btz * a2 / (cf * rr);
+      q[5] = RV_DIV(-af * bty * a2, (cf * rr), e.icfrr);
+      q[6] = RV_DIV(-af * btz * a2, (cf * rr), e.icfrr);
       const unsigned f = e.fcsm;
       q[0] = flip(q[0], f); q[1] = flip(q[1], f); q[2] = flip(q[2], f); q[3] = flip(q[3], f);
       q[5] = flip(q[5], f); q[6] = flip(q[6], f); q[7] = flip(q[7], f);
@@ -305,13 +403,15 @@ __device__ __forceinline__ void rv_row(const Mid& e, const Gas& G, int k, double
     case 5:
       q[2] = flip(-btz, sb);
       q[3] = flip(+bty, sb);
-      q[5] = btz / rr;
-      q[6] = -bty / rr;
+      q[5] = RV_DIV(btz, rr, e.irr);
+      q[6] = RV_DIV(-bty, rr, e.irr);
       q[7] = flip(-(btz * v - bty * w), sb);
       break;
     default:
       break;
   }
+#undef DIV_G1
+#undef RV_DIV
 }
 
 // Cell-centred eigenvalues (SpatialMethodEno::getEigenvaluesAt,

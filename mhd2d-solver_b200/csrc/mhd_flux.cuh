@@ -71,7 +71,13 @@ struct TileGeom {
   static constexpr int OFF_G = OFF_F + 7 * RU * TJ;        // sG[7][TI][CU], slots in y frame order
   static constexpr int OFF_FX = OFF_G + 7 * TI * CU;       // sFx[8][TI+1][TJ]
   static constexpr int OFF_GY = OFF_FX + 8 * (TI + 1) * TJ;  // sGy[8][TI][TJ+1], y frame order
+#ifdef MHD_FAST
+  // fast build: per-cell primitives sP[4][RU][CU] (u, v, w, total pressure)
+  static constexpr int OFF_P = OFF_GY + 8 * TI * (TJ + 1);
+  static constexpr int TOTAL = OFF_P + 4 * RU * CU;
+#else
   static constexpr int TOTAL = OFF_GY + 8 * TI * (TJ + 1);
+#endif
   static constexpr size_t BYTES = size_t(TOTAL) * sizeof(double);
   static constexpr size_t TMA_BYTES = BYTES + 128;  // k_flux: room to align the box to 128 B
 };
@@ -102,6 +108,42 @@ __device__ __forceinline__ void phys_flux(double gm, const double* q, double* F,
   G[7] = (en + pt) * v - by * ub;
 }
 
+#ifdef MHD_FAST
+// Fast build: the physical fluxes with one reciprocal of the density, and
+// the cell's primitives P = (u, v, w, total pressure) for the midpoints of
+// its four interfaces (midpoint_fast).
+__device__ __forceinline__ void phys_flux_fast(double gm, const double* q, double* F, double* G,
+                                               double* P) {
+  const double r = q[0], mx = q[1], my = q[2], mz = q[3];
+  const double bx = q[4], by = q[5], bz = q[6], en = q[7];
+  const double ir = 1.0 / r;
+  const double u = mx * ir, v = my * ir, w = mz * ir;
+  const double uu = u * u + v * v + w * w;
+  const double ub = u * bx + v * by + w * bz;
+  const double bb = bx * bx + by * by + bz * bz;
+  const double p = (gm - 1.0) * (en - 0.5 * r * uu - 0.5 * bb);
+  const double pt = p + 0.5 * bb;
+  F[0] = mx;
+  F[1] = mx * u - bx * bx + pt;
+  F[2] = my * u - bx * by;
+  F[3] = mz * u - bx * bz;
+  F[5] = by * u - bx * v;
+  F[6] = bz * u - bx * w;
+  F[7] = (en + pt) * u - bx * ub;
+  G[0] = my;
+  G[1] = mx * v - by * bx;
+  G[2] = my * v - by * by + pt;
+  G[3] = mz * v - by * bz;
+  G[4] = bx * v - by * u;
+  G[6] = bz * v - by * w;
+  G[7] = (en + pt) * v - by * ub;
+  P[0] = u;
+  P[1] = v;
+  P[2] = w;
+  P[3] = pt;
+}
+#endif
+
 // ENO-2 stencil choice on one characteristic (spatialmethodenoroe.cpp:240-254).
 __device__ __forceinline__ double eno_minus(double w0, double w1, double w2, double v0, double v1) {
   return (fabs(v0) < fabs(v1)) ? (-(1.0 / 2.0) * w0 + (3.0 / 2.0) * w1)
@@ -120,6 +162,12 @@ struct Lane {
   int qplane, qstep;
   bool swp;          // y interface: x/y roles swapped
   int l1, l2;        // stencil points of U1 / U2 (1 / 2, or open-boundary substitutes)
+#ifdef MHD_FAST
+  const double* p;   // primitives (u, v, w, pt) of point l at p[k*qplane + l*qstep]
+  __device__ __forceinline__ double P(int k, int l) const {
+    return p[(swp && k < 2 ? 1 - k : k) * qplane + l * qstep];
+  }
+#endif
   // component 4 of a frame flux is identically zero (F[4], G[5]) and not stored
   __device__ __forceinline__ double F(int m, int l) const {
     return m == 4 ? 0.0 : f[slot_of(m) * fplane + l * fstep];
@@ -144,6 +192,25 @@ __device__ __forceinline__ double roe_upwind(const double* w, const double* vw, 
 // order as the full projection (spatialmethodenoroe.cpp:240-254).
 __device__ __forceinline__ double roe_side_value(const Lane& L, const double* l, unsigned lm,
                                                  int s0) {
+#if defined(MHD_FAST) && MHD_FAST_ENO3
+  // fast build: project the side's three stencil points once and take the
+  // undivided differences of the projections (the reference projects the
+  // differences of the fluxes, then two of the points again)
+  double w0 = 0.0, w1 = 0.0, w2 = 0.0;
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    if (!(lm & (1u << m))) continue;
+    w0 += l[m] * L.F(m, s0);
+    w1 += l[m] * L.F(m, s0 + 1);
+    w2 += l[m] * L.F(m, s0 + 2);
+  }
+  const bool left = fabs(w1 - w0) < fabs(w2 - w1);
+  const int pa = s0 + (left ? 0 : 1);
+  const double wa = left ? w0 : w1, wb = left ? w1 : w2;
+  return pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
+       : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
+                  : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
+#else
   double va = 0.0, vb = 0.0;
 #pragma unroll
   for (int m = 0; m < NF; m++) {
@@ -163,6 +230,7 @@ __device__ __forceinline__ double roe_side_value(const Lane& L, const double* l,
   return pa == 0 ? (-(1.0 / 2.0) * wa + (3.0 / 2.0) * wb)
        : (pa == 1 ? ((1.0 / 2.0) * wa + (1.0 / 2.0) * wb)
                   : ((3.0 / 2.0) * wa - (1.0 / 2.0) * wb));
+#endif
 }
 
 // ENO-Roe flux of characteristic k with left row l, projecting only what
@@ -361,6 +429,26 @@ __device__ __forceinline__ void pair_flux(Mid& e, const Gas& G, const Lane& L, c
     if (!isfinite(fw[k])) nonfinite = true;
 
   if constexpr (RV_PAIRS) {
+#ifdef MHD_FAST
+    // fast build: the pair's two products go into the sums at once (any
+    // order of the seven terms is within the tolerance), with the rows'
+    // divisions taken through the midpoint's reciprocals
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      opaque(e);
+      const bool two = t < 3;
+      double qa[NF], qb[NF];
+      rv_row<true>(e, G, t, qa);
+      if (two) rv_row<true>(e, G, 6 - t, qb);
+      const unsigned rm = rv_mask(t);  // == rv_mask(6 - t)
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (rm & (1u << m)) {
+          Fn[m] += qa[m] * fw[t];
+          if (two) Fn[m] += qb[m] * fw[6 - t];
+        }
+    }
+#else
     double h[3][NF];
 #pragma unroll
     for (int t = 0; t < 4; t++) {
@@ -384,6 +472,7 @@ __device__ __forceinline__ void pair_flux(Mid& e, const Gas& G, const Lane& L, c
       for (int m = 0; m < NF; m++)
         if (rm & (1u << m)) Fn[m] += h[t][m];
     }
+#endif
   } else {
 #pragma unroll
     for (int k = 0; k < 7; k++) {
@@ -430,7 +519,21 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
     U2[k] = L.Q(k, L.l2);
   }
   Mid e;
+#ifdef MHD_FAST
+  if (!DENSE) {
+    double P1[4], P2[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      P1[k] = L.P(k, L.l1);
+      P2[k] = L.P(k, L.l2);
+    }
+    if (!midpoint_fast(G, U1, U2, P1, P2, e)) return false;
+  } else if (!midpoint(G, U1, U2, e)) {
+    return false;
+  }
+#else
   if (!midpoint(G, U1, U2, e)) return false;
+#endif
   negp = e.negp;
   smax = 0.0;
 #pragma unroll

@@ -86,7 +86,12 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
   dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + ti - 1) / ti);
   CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
              ch ? ch[3] : nullptr};
+#ifdef MHD_FAST
+  const Gas G{g.gamma, g.gamma - 1.0, (g.gamma - 2.0) / (g.gamma - 1.0), 1.0 / std::sqrt(2.0),
+              1.0 / (g.gamma - 1.0)};
+#else
   const Gas G{g.gamma, g.gamma - 1.0, (g.gamma - 2.0) / (g.gamma - 1.0), 1.0 / std::sqrt(2.0)};
+#endif
   CUtensorMap tm{};
   const int use_tma = tile_tma_enabled() && make_box_map(g, U, Gm::CU, Gm::RU, &tm) ? 1 : 0;
   tile_tma_launches() += use_tma;
