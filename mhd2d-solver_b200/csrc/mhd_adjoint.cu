@@ -47,6 +47,7 @@
 #include "mhd_flux.cuh"
 #include "mhd_misc.cuh"
 #include "mhd_problems.cuh"
+#include "mhd_trace.h"
 
 namespace mhd {
 namespace MHD_KNS {
@@ -1464,6 +1465,7 @@ int mhd_adj_set_masks(mhd_adj* a, int keep_all) {
 }
 
 int mhd_adj_forward(mhd_adj* a, int nsteps, double dt0, double* J) {
+  MHD_TRACE("mhd_adj_forward");
   if (!a || nsteps < 1) return MHD_ERR_WRONG_PARAMETER;
   // everything the recording needs is allocated before it starts
   int st;
@@ -1490,6 +1492,7 @@ int mhd_adj_forward(mhd_adj* a, int nsteps, double dt0, double* J) {
 
 int mhd_adj_forward_group(int n, mhd_adj* const* as, const int* nsteps, const double* dt0,
                           double* J, double* ms) {
+  MHD_TRACE("mhd_adj_forward_group");
   int st = group_check(n, as);
   if (st) return st;
   if (!nsteps || !dt0) return MHD_ERR_WRONG_PARAMETER;
@@ -1564,6 +1567,7 @@ int mhd_adj_forward_group(int n, mhd_adj* const* as, const int* nsteps, const do
 }
 
 int mhd_adj_backward_group(int n, mhd_adj* const* as, double* ms) {
+  MHD_TRACE("mhd_adj_backward_group");
   int st = group_check(n, as);
   if (st) return st;
   for (int i = 0; i < n; i++)
@@ -1599,6 +1603,7 @@ int mhd_adj_backward_group(int n, mhd_adj* const* as, double* ms) {
 }
 
 int mhd_adj_replay(mhd_adj* a, const double* U0, double* J) {
+  MHD_TRACE("mhd_adj_replay");
   if (!a) return MHD_ERR_WRONG_PARAMETER;
   int st = check_replay(a);
   if (st) return st;
@@ -1656,6 +1661,7 @@ int mhd_adj_replay_problem(mhd_adj* a, int kind, const double* p, int np, double
 }
 
 int mhd_adj_backward(mhd_adj* a) {
+  MHD_TRACE("mhd_adj_backward");
   if (!a) return MHD_ERR_WRONG_PARAMETER;
   int st = check_ready(a);
   if (st) return st;

@@ -12,8 +12,9 @@
 #include <vector>
 
 #include "../../include/mhd2d_b200.h"
-#include "mhd_tma.cuh"
 #include "mhd_launch.h"
+#include "mhd_tma.cuh"
+#include "mhd_trace.h"
 
 using namespace mhd;
 
@@ -123,6 +124,7 @@ int check_bc_ready(mhd_ctx* c) {
 
 // Enqueue one spatial integration of state X into UL.
 void enqueue_integrate(mhd_ctx* c, double* X, bool chars) {
+  MHD_TRACE(X == c->U ? "L(U)" : (X == c->U1 ? "L(U1)" : "L(U2)"));
   const Grid& g = c->g;
   c->ks->bc(g, X, c->snap, c->ctl, c->stream);
   if (c->scheme == 3) c->ks->lf_alpha(g, X, c->aF, c->aG, c->ctl, c->stream);
@@ -198,6 +200,7 @@ int step_status(mhd_ctx* c) {
 
 // One full time step on the device state; dt in/out.
 int do_step(mhd_ctx* c, double* dt_inout) {
+  MHD_TRACE("step");
   int st = check_bc_ready(c);
   if (st) return st;
   const bool chars = (c->flags & MHD_FLAG_CHARACTERISTICS) != 0;
@@ -236,6 +239,7 @@ void divb_range(const mhd_ctx* c, int r[4]) {
 }
 
 int do_divb_calc(mhd_ctx* c, double* mx, double* tot) {
+  MHD_TRACE("divBCalculation");
   int r[4];
   divb_range(c, r);
   c->ks->divb(c->g, c->U, r, c->partial, c->npartial, c->ctl, c->stream);
@@ -251,6 +255,7 @@ int do_divb_calc(mhd_ctx* c, double* mx, double* tot) {
 }
 
 int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
+  MHD_TRACE("divBCorrectionSOR");
   touch_buf(c, 0);  // the B correction changes U's interior
   int r[4];
   divb_range(c, r);
@@ -510,6 +515,7 @@ int mhd_set_dirichlet(mhd_ctx* c, const double* left, const double* right, const
 }
 
 int mhd_integrate(mhd_ctx* c, double* dtIdeal) {
+  MHD_TRACE("mhd_integrate");
   if (!c) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   int st = check_bc_ready(c);
@@ -535,6 +541,7 @@ int mhd_integrate(mhd_ctx* c, double* dtIdeal) {
 }
 
 int mhd_integrate_host(mhd_ctx* c, double* U, double* UL, double* dtIdeal) {
+  MHD_TRACE("mhd_integrate_host");
   if (!c || !U) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   CK(h2d(c, c->U, U));
@@ -553,6 +560,7 @@ int mhd_step(mhd_ctx* c, double* dt_inout) {
 }
 
 int mhd_step_host(mhd_ctx* c, double* U, double* dt_inout) {
+  MHD_TRACE("mhd_step_host");
   if (!c || !U || !dt_inout) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   CK(h2d(c, c->U, U));
@@ -563,6 +571,7 @@ int mhd_step_host(mhd_ctx* c, double* U, double* dt_inout) {
 }
 
 int mhd_steps(mhd_ctx* c, int nsteps, double* dt_inout, double* dts) {
+  MHD_TRACE("mhd_steps");
   if (!c || !dt_inout || nsteps < 0) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   for (int n = 0; n < nsteps; n++) {
@@ -618,6 +627,7 @@ int mhd_nongrid_data(mhd_ctx* c, double out[7]) {
 
 int mhd_run(mhd_ctx* c, const mhd_run_params* p, mhd_nongrid_record* records, int max_records,
             mhd_run_result* res) {
+  MHD_TRACE("mhd_run");
   if (!c || !p || !res || (p->time_mode != 1 && p->time_mode != 2) ||
       (p->time_mode == 1 && p->steps < 1) || (p->nongrid_mode == 1 && p->nongrid_steps < 1) ||
       (p->nongrid_mode == 2 && !(p->nongrid_t > 0.0)) ||
@@ -698,6 +708,7 @@ int mhd_divb_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
 }
 
 int mhd_divb_clean(mhd_ctx* c, const mhd_sor_params* p, double* maxdivb, int* total_sweeps) {
+  MHD_TRACE("mhd_divb_clean");
   if (!c || !p) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
   double mx = -1.0, tot = 0.0;

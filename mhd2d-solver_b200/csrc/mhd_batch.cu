@@ -34,6 +34,7 @@
 #include "mhd_flux.cuh"
 #include "mhd_misc.cuh"
 #include "mhd_problems.cuh"
+#include "mhd_trace.h"
 
 namespace mhd {
 namespace MHD_KNS {
@@ -493,6 +494,7 @@ void enqueue_flux(mhd_batch* b, const TileShape& s) {
 
 // Enqueue one stage for every active run.
 void enqueue_stage(mhd_batch* b) {
+  MHD_TRACE("batch stage");
   const TileShape& s = tile_shape(b->tile);
   int* d = b->dints;
   kb_bc<<<dim3(16, b->n), 256, 0, b->stream>>>(b->dinst, b->dstate, d + W_NEXT_ROE);
@@ -732,6 +734,7 @@ int mhd_batch_init_problem(mhd_batch* b, int idx, int kind, const double* p, int
 }
 
 int mhd_batch_advance(mhd_batch* b, int stages, int check_every, int* n_active) {
+  MHD_TRACE("mhd_batch_advance");
   if (!b || stages < 0) return MHD_ERR_WRONG_PARAMETER;
   BK(cudaSetDevice(b->device));
   int st = refresh_tables(b);

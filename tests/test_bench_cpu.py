@@ -35,6 +35,67 @@ def _rank_main(rank, world, port, out):
     dist.destroy_process_group()
 
 
+def _shard_rank_main(rank, world, port, out):
+    """One rank of the sharded batched mix, run end to end on the CPU: the
+    rank takes its share of a small seeded mix (batch.shard_runs, no
+    exchange), advances each of its runs to its end time with the oracle
+    (the reference main loop), and joins the job's reductions: cell-updates
+    summed over ranks, time the slowest rank's."""
+    import time
+
+    import numpy as np
+    import torch.distributed as dist
+
+    sys.path.insert(0, os.path.join(ROOT, "mhd2d-solver_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from mhd2d_b200 import batch as B
+    from mhd2d_b200 import problems as P
+    from pyoracle import Oracle
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    bench = _load_bench()
+    mix = B.mixed_runs(12, seed=3, side_min=8, side_max=24)
+    costs = np.array([m.run.nx * m.run.ny for m in mix], dtype=np.float64)
+    mine = B.shard_runs(costs, world, rank)
+    t0 = time.perf_counter()
+    cell_updates = 0.0
+    for i in mine:
+        r = mix[i].run
+        p = P.explosion(r.nx, r.ny) if mix[i].kind == "explosion" else \
+            P.random_smooth(r.nx, r.ny, seed=i)
+        o = Oracle(r.nx, r.ny, p.dx, p.dy, r.gamma, r.bc, scheme=r.scheme, dt_min=r.dt_min,
+                   dt_max=r.dt_max, cfl=r.cfl)
+        U = p.U.copy()
+        res = o.run(U, r.dt0, t_max=0.02)
+        cell_updates += float(r.nx * r.ny * res["steps"])
+    ms = (time.perf_counter() - t0) * 1e3
+    out[rank] = (sorted(mine), cell_updates)
+    out[10 + rank] = bench.allreduce_sum(world, cell_updates)
+    out[20 + rank] = bench.allreduce_max(world, ms)
+    out[30 + rank] = ms
+    bench.barrier(world)
+    dist.destroy_process_group()
+
+
+def test_sharded_batched_mix_two_ranks_gloo():
+    """The instance-sharded batched path end to end on two gloo ranks: the
+    shares partition the runs, the summed cell-updates equal the sum of the
+    ranks' own counts, and the job time is the slower rank's."""
+    world, port = 2, 29533
+    with mp.Manager() as man:
+        out = man.dict()
+        mp.start_processes(_shard_rank_main, args=(world, port, out), nprocs=world, join=True,
+                           start_method="spawn")
+        shares = [out[r][0] for r in range(world)]
+        assert sorted(shares[0] + shares[1]) == list(range(12))
+        assert not set(shares[0]) & set(shares[1])
+        total = out[0][1] + out[1][1]
+        assert total > 0 and out[10] == total and out[11] == total
+        assert out[20] == out[21] == max(out[30], out[31])
+
+
 def test_batched_runs_shard_without_overlap_and_balanced():
     """Instance sharding of the batched runs (no exchange between GPUs): the
     shares of all ranks partition the runs, one rank takes all, and the
