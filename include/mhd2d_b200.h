@@ -325,9 +325,17 @@ int mhd_batch_set_tile( mhd_batch* b, int tile, int ctas_per_sm );
    kind MHD_PROBLEM_WAVE, p[0..15]: x0, y0, Lx, Ly, rho, u, v, w, Bx, By, Bz, p,
      epsilon, wave (0..6 = right eigenvector index), kx, ky  (readProblemWaveTest)
    kind MHD_PROBLEM_ORSZAG_TANG: no parameters (gamma from the run)
-   kind MHD_PROBLEM_PLASMA_SHEET, p[0..3+K]: x0, y0, delta, K, a_1..a_K */
+   kind MHD_PROBLEM_PLASMA_SHEET, p[0..3+K]: x0, y0, delta, K, a_1..a_K
+   kind MHD_PROBLEM_SHOCK_TUBE, p[0..18]: Lx, Ly, interface angle (degrees),
+     left state rho, u, v, w, Bx, By, Bz, p, right state (same order)
+     (readProblemShockTube, file_access.cpp:300-395; dx = Lx/nx, dy = Ly/ny)
+   kind MHD_PROBLEM_SHEET_LOBES, p[0..41]: Lx, Ly, start_x, start_y, sheet
+     start, sheet start foot, sheet thickness, profile (0 constant, 1 tanh),
+     transition (0 jump, 1 linear), transition points, then the left, right,
+     up and down states (rho, u, v, w, Bx, By, Bz, p each)
+     (readProblemPlasmaSheet, file_access.cpp:614-919; dx = Lx/nx, dy = Ly/ny) */
 enum { MHD_PROBLEM_EXPLOSION = 1, MHD_PROBLEM_WAVE = 2, MHD_PROBLEM_ORSZAG_TANG = 3,
-       MHD_PROBLEM_PLASMA_SHEET = 4 };
+       MHD_PROBLEM_PLASMA_SHEET = 4, MHD_PROBLEM_SHOCK_TUBE = 5, MHD_PROBLEM_SHEET_LOBES = 6 };
 int mhd_batch_init_problem( mhd_batch* b, int idx, int kind, const double* p, int np );
 
 int mhd_batch_stream( mhd_batch* b, void** stream );

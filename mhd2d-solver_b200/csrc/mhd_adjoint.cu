@@ -1424,13 +1424,14 @@ int mhd_adj_init_problem(mhd_adj* a, int kind, const double* p, int np) {
   ProblemArgs pa{};
   std::string err;
   cudaError_t ce = cudaSuccess;
-  const int st = problem_args(kind, p, np, a->g.gamma, a->stream, pa, err, ce);
+  const int st = problem_args(kind, p, np, a->g.gamma, a->stream, pa, err, ce, &a->g);
   if (ce != cudaSuccess) return afail(a, ce, "problem_args");
   if (st) return aset(a, st, true, err);
   AK(cudaMemsetAsync(a->U0, 0, a->blk * sizeof(double), a->stream));
   enqueue_problem(a->g, a->U0, pa, a->stream);
+  AK(release_problem(pa, a->stream));
   snapshot_into(a, a->U0, a->snap);
-  a->launches++;
+  a->launches += problem_launches(pa);
   AK(cudaStreamSynchronize(a->stream));
   AK(cudaGetLastError());
   a->recorded = false;
@@ -1644,12 +1645,13 @@ int mhd_adj_replay_problem(mhd_adj* a, int kind, const double* p, int np, double
   ProblemArgs pa{};
   std::string err;
   cudaError_t ce = cudaSuccess;
-  st = problem_args(kind, p, np, a->g.gamma, a->stream, pa, err, ce);
+  st = problem_args(kind, p, np, a->g.gamma, a->stream, pa, err, ce, &a->g);
   if (ce != cudaSuccess) return afail(a, ce, "problem_args");
   if (st) return aset(a, st, true, err);
   AK(cudaMemsetAsync(a->U, 0, a->blk * sizeof(double), a->stream));
   enqueue_problem(a->g, a->U, pa, a->stream);
-  a->launches++;
+  AK(release_problem(pa, a->stream));
+  a->launches += problem_launches(pa);
   snapshot_into(a, a->U, a->snapr);
   a->cur_snap = a->snapr;
   if ((st = reset_ctl(a))) return st;

@@ -723,13 +723,15 @@ int mhd_batch_init_problem(mhd_batch* b, int idx, int kind, const double* p, int
   ProblemArgs a{};
   std::string err;
   cudaError_t ce = cudaSuccess;
-  const int st = problem_args(kind, p, np, b->desc[idx].gamma, b->stream, a, err, ce);
+  const int st = problem_args(kind, p, np, b->desc[idx].gamma, b->stream, a, err, ce,
+                              &b->hinst[idx].g);
   if (ce != cudaSuccess) return bfail(b, ce, "problem_args");
   if (st) return bset(b, st, true, err);
   if (kind == MHD_PROBLEM_WAVE) b->launches += 1;
   enqueue_problem(b->hinst[idx].g, b->hinst[idx].U, a, b->stream);
-  b->launches += 1;
+  b->launches += problem_launches(a);
   BK(cudaGetLastError());
+  BK(release_problem(a, b->stream));
   return arm(b, idx);
 }
 

@@ -19,6 +19,7 @@ from . import (ENO_ROE, OK, RK3, STATUS_NAMES, BatchDesc, BatchState, MhdError, 
                library)
 
 PROBLEM_EXPLOSION, PROBLEM_WAVE, PROBLEM_ORSZAG_TANG, PROBLEM_PLASMA_SHEET = 1, 2, 3, 4
+PROBLEM_SHOCK_TUBE, PROBLEM_SHEET_LOBES = 5, 6
 TILE_7x32, TILE_3x32 = 0, 1
 WAVES = ("negative fast magnetosonic", "negative alfven", "negative slow magnetosonic",
          "entropy", "positive slow magnetosonic", "positive alfven",
@@ -133,6 +134,21 @@ class Batch:
     def init_plasma_sheet(self, i, amps, delta=0.1, x0=-2.0, y0=-1.0):
         a = list(amps)
         self.init_problem(i, PROBLEM_PLASMA_SHEET, [x0, y0, delta, float(len(a))] + a)
+
+    def init_shock_tube(self, i, lx, ly, angle, left, right):
+        """readProblemShockTube: left / right are natural states (rho, u, v,
+        w, Bx, By, Bz, p); the run's dx, dy must be lx / nx, ly / ny."""
+        self.init_problem(i, PROBLEM_SHOCK_TUBE, [lx, ly, angle] + list(left) + list(right))
+
+    def init_sheet_lobes(self, i, lx, ly, start_x, start_y, head, foot, thickness, tanh_profile,
+                         linear_transition, points, left, right, up, down):
+        """readProblemPlasmaSheet (the reference's lobe / sheet setup): the four
+        natural states (rho, u, v, w, Bx, By, Bz, p) of the left and right sheet
+        halves and the upper and lower lobes."""
+        p = [lx, ly, start_x, start_y, head, foot, thickness, float(bool(tanh_profile)),
+             float(bool(linear_transition)), float(points)]
+        self.init_problem(i, PROBLEM_SHEET_LOBES, p + list(left) + list(right) + list(up)
+                          + list(down))
 
     # -- stepping --------------------------------------------------------------------
     def advance(self, stages, check_every=0):
