@@ -485,9 +485,6 @@ def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1, store=-1):
     ctx.close()
     a = Adjoint(nx, ny, p.dx, p.dy, p.gamma, p.bc, checkpoint_every=K, device=dev, **kw)
     a.set_store(store)
-    # choice words of stored stages only: a replayed segment records its own
-    # again, and the memory goes to the stage store instead
-    a.set_masks(False)
     a.init_plasma_sheet(amps)
     J = a.forward(steps, dt0)
     a.backward()
@@ -498,7 +495,6 @@ def adjoint_measure(dev, steps, nx=1024, ny=512, K=64, seed=1, store=-1):
     # bound (perturbed frozen replays diverge), so it is checked where the
     # linearisation holds
     fd_steps = min(steps, 200)
-    a.set_masks(True)  # the frozen replays of the check need every stage's words
     J_short = a.forward(fd_steps, dt0)
     a.backward()
     g_short = a.sheet_gradient()
@@ -660,18 +656,16 @@ def batched_adjoint_measure(dev, n=64, steps=500, seed=2, K=16):
                     "compared with the sequential leg's bit for bit"}
 
 
-def fast_math_measure(dev, p, scheme, steps, n, base_flags):
-    """RK3 steps and the spatial operator of the FMA-contracted kernel set on
-    the bench's state, timed like the headline (CUDA events on the library
-    stream)."""
+def steps_measure(dev, p, scheme, steps, n, flags):
+    """RK3 steps and the spatial operator of one kernel set and scheme on the
+    bench's state, timed like the headline (CUDA events on the library
+    stream): value, ms per step, operator time and its FP64 fraction."""
     import torch
 
     import mhd2d_b200 as M
 
-    if base_flags & M.FLAG_FAST_MATH:
-        return None
     ctx = M.Context(n, n, p.dx, p.dy, p.gamma, p.bc, scheme=scheme, time_method=M.RK3,
-                    dt_min=1e-9, dt_max=0.03125, cfl=0.4, flags=M.FLAG_FAST_MATH, device=dev)
+                    dt_min=1e-9, dt_max=0.03125, cfl=0.4, flags=flags, device=dev)
     ctx.upload(p.U)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     dt = 0.03125
@@ -695,13 +689,24 @@ def fast_math_measure(dev, p, scheme, steps, n, base_flags):
     achieved = FLOPS_PER_CELL_INTEGRATE[scheme] * cells / (t_int * 1e-3) / 1e12
     return {"value": cells * steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / steps,
             "launch_ms": t_int, "achieved_tflops": achieved, "frac": achieved / peak,
-            "note": "FMA-contracted kernels with shared reciprocals and per-cell primitives; "
+            "flops_per_cell": FLOPS_PER_CELL_INTEGRATE[scheme]}
+
+
+def fast_math_measure(dev, p, scheme, steps, n, base_flags):
+    """The FMA-contracted kernel set on the bench's state (steps_measure)."""
+    import mhd2d_b200 as M
+
+    if base_flags & M.FLAG_FAST_MATH:
+        return None
+    out = steps_measure(dev, p, scheme, steps, n, M.FLAG_FAST_MATH)
+    out["note"] = ("FMA-contracted kernels with shared reciprocals and per-cell primitives; "
                     "not the headline: the reference decides the upwind side of a slow wave "
                     "whose speed u +- c_s rounds to zero (c_s from c2 - sqrt(c2^2 - a^2 c_a^2) "
                     "where B_x ~ 0) and breaks exact ENO ties of symmetric data by its own "
                     "rounding, so any other rounding changes single cell updates of the "
                     "Orszag-Tang vortex by O(1) relative; the contracted set agrees with the "
-                    "parity set to ~1e-14 per operator on states without such points"}
+                    "parity set to ~1e-14 per operator on states without such points")
+    return out
 
 
 def run_ours(args):
@@ -786,6 +791,10 @@ def run_ours(args):
     # the headline: it is not bit-identical and does not hold the reference
     # tolerance on this problem (see fast_math.note)
     fast = fast_math_measure(dev, p, scheme, args.steps, n, flags)
+    # the other ENO scheme of config 2 on the same state, parity build
+    other = M.ENO_LF if scheme == M.ENO_ROE else M.ENO_ROE
+    other_line = steps_measure(dev, p, other, args.steps, n, flags)
+    other_line["scheme"] = "eno-lf" if other == M.ENO_LF else "eno-roe"
 
     # SOR div-B cleaning, measured separately: a fixed number of red-black
     # sweeps on the evolved 4096^2 state (the convergence test never fires:
@@ -831,6 +840,7 @@ def run_ours(args):
                                         "MEASURED_PEAKS.json has no FP64 figure"},
             "clocks": clocks,
             "fast_math": fast,
+            "other_scheme": other_line,
             "sor": {"ms_per_sweep": sor_ms, "sweeps": done, "status": st_sor.status,
                     "gbs_min_traffic": sor_bytes / (sor_ms * 1e-3) / 1e9,
                     "note": "red-black sweep (2 colours + ghost refresh + convergence test), "

@@ -31,6 +31,21 @@ def _src(node):
     return ast.unparse(node)
 
 
+def acc(target, coef):
+    """The statement target += coef.  A coefficient that is a product P * Q
+    is accumulated with one fused multiply-add, target = fma(P, Q, target):
+    one rounding instead of two, and one FP64 instruction."""
+    try:
+        node = ast.parse(coef, mode="eval").body
+    except SyntaxError:
+        node = None
+    if isinstance(node, ast.BinOp) and isinstance(node.op, ast.Mult):
+        # ast.unparse writes a double negation as "--", a C decrement
+        left, right = (re.sub(r"-(?=-)", "- ", _src(x)) for x in (node.left, node.right))
+        return f"{target} = fma({left}, {right}, {target});"
+    return f"{target} += {coef};"
+
+
 class Rcp:
     """Reciprocals of the denominators met in one reverse sweep: each distinct
     denominator is divided once (rcpN = 1 / d) and the adjoints multiply."""
@@ -353,7 +368,7 @@ def emit_pairs():
                         continue
                     assert var in MID_FIELDS, var
                     field = "as" if var == "as_" else var
-                    lines.append(f"        mb.{field} += {c_expr(coef, MID_NAMES)};")
+                    lines.append("        " + acc(f"mb.{field}", c_expr(coef, MID_NAMES)))
                 if not lines:
                     continue
                 if seed.startswith("rs") or seed.startswith("rd"):
@@ -418,7 +433,7 @@ def emit_program(name, decl, stmts, inputs, prologue, seeds, epilogue, subst=Non
         for var, coef in reverse_of(expr, f"{t}_b", rcp):
             if var in CONSTS:
                 continue
-            lines.append(f"    {var}_b += {coef};")
+            lines.append("    " + acc(f"{var}_b", coef))
         if not lines:
             continue
         rev.append(f"  if (!{t}_fz && {t}_b != 0.0) {{" if len(st) > 2 else f"  if ({t}_b != 0.0) {{")
