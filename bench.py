@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--scheme", default="roe", choices=["roe", "lf"])
     ap.add_argument("--fast-math", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-baseline", type=int, default=1,
+                    help="time the reference on one host core beside the GPU work (0: skip)")
     ap.add_argument("--batch-runs", type=int, default=512,
                     help="runs of the batched-vs-sequential measurement (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=5)
@@ -776,7 +778,8 @@ def run_ours(args):
     state_bytes = 8 * (n + 4) * (n + 4) * 8
     # the reference on one host core, same grid, beside the GPU measurements
     # below (started after the e2e leg, whose host copies it would disturb)
-    base_proc = cpu_baseline_start(n, scheme) if rank == 0 and world == 1 else None
+    base_proc = (cpu_baseline_start(n, scheme)
+                 if rank == 0 and world == 1 and args.cpu_baseline else None)
 
     # roofline of the dominant kernel (the fused flux kernel; one spatial
     # operator = boundary fill + flux kernel, timed back to back on the
