@@ -120,9 +120,22 @@ int mhd_step( mhd_ctx* ctx, double* dt_inout );
 /* Host-buffer form: upload U, one step, download U. */
 int mhd_step_host( mhd_ctx* ctx, double* U, double* dt_inout );
 
-/* Several steps without host round trips in between (fixed count);
-   dts (optional, length nsteps) receives each step's dt. */
+/* Several steps in a row (the loop of TimeIntegrationRK3::step /
+   TimeIntegrationEuler::step calls, timeintegrationrk3.cpp:48-156);
+   dts (optional, length nsteps) receives each step's dt.  It stops at the
+   first failing step and returns its status (dt_inout then holds the last
+   completed step's dt).  By default the whole loop is one CUDA graph
+   launch: a while node over the steps with the RK3 retry loop as a nested
+   while node that the device-side controller drives, so the host waits once
+   per call instead of once per step; results are bit-identical to the
+   step-by-step loop.  The graph allows 4096 RK3 passes per step (a valid
+   run needs far fewer: every retry halves dt at least once); past that the
+   call returns MHD_ERR_NOT_CONVERGED. */
 int mhd_steps( mhd_ctx* ctx, int nsteps, double* dt_inout, double* dts );
+
+/* 1 (the default): mhd_steps runs as one CUDA graph launch; 0: one host
+   round trip per step (mhd_step in a loop).  Same results either way. */
+int mhd_set_step_graph( mhd_ctx* ctx, int enable );
 
 /* Replaces SpatialMethodEno::getCharacteristicsX/Y (spatialmethodeno.cpp:55-86)
    as called at timeintegrationrk3.cpp:151-152; requires

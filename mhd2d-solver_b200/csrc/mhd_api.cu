@@ -19,6 +19,46 @@
 using namespace mhd;
 
 namespace {
+// Counters of a graph step loop (mhd_ctx::gcnt).
+enum : int { G_STEPS = 0, G_RETRIES = 1, G_WANTED = 2, G_STEP_RETRIES = 3, G_NEG = 4, G_COUNT = 5 };
+// RK3 passes of one step the device loop allows: every retry restarts from
+// min(dt1, dt2, dt3), strictly below the dt it replaces, and the power-of-two
+// ladder of a double has fewer rungs than this, so a valid run never gets here
+constexpr long long kGraphRetryBound = 4096;
+
+// Before the retry loop and at the end of each retry pass: run another pass
+// while the controller asks for one.
+__global__ void k_graph_retry(const Ctl* c, long long* cnt, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const bool again = c->retry && !c->error && cnt[G_STEP_RETRIES] < kGraphRetryBound;
+  if (again) {
+    cnt[G_STEP_RETRIES] += 1;
+    cnt[G_RETRIES] += 1;
+  }
+  cudaGraphSetConditional(h, again ? 1u : 0u);
+}
+
+// End of one step of the device loop: count it, keep its dt, and go on while
+// steps are wanted and the step completed.
+__global__ void k_graph_step_end(const Ctl* c, long long* cnt, double* dts,
+                                 cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const bool done = !c->error && c->step_done;
+  cnt[G_NEG] += (long long)c->neg_count;
+  cnt[G_STEP_RETRIES] = 0;
+  if (done) {
+    dts[cnt[G_STEPS]] = c->dt;  // G_STEPS < G_WANTED <= capacity (the loop stops at G_WANTED)
+    cnt[G_STEPS] += 1;
+  }
+  cudaGraphSetConditional(h, (done && cnt[G_STEPS] < cnt[G_WANTED]) ? 1u : 0u);
+}
+
+__global__ void k_graph_arm(long long* cnt, long long wanted) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int q = 0; q < G_COUNT; q++) cnt[q] = 0;
+  cnt[G_WANTED] = wanted;
+}
+
 // FP64 FMA throughput probe: 8 independent chains per thread.
 __global__ void __launch_bounds__(256) k_fma_peak(double* out, int iters, double a, double b) {
   double x[8];
@@ -62,6 +102,17 @@ struct mhd_ctx {
   std::string msg;
   bool is_error = false;
   long long launches = 0, neg_pressure = 0;
+  // mhd_steps as one CUDA graph: a while node over steps, a nested while node
+  // over the RK3 retries (see build_step_graph)
+  int use_step_graph = 1;
+  cudaGraphExec_t step_graph = nullptr;
+  bool step_graph_chars = false;
+  int step_graph_tma = -1;
+  long long step_graph_launches[2] = {0, 0};  // kernels per step body / per retry pass
+  long long* gcnt = nullptr;   // device: G_* counters of a graph step loop
+  long long* hgcnt = nullptr;  // pinned mirror
+  double* gdts = nullptr;      // device: dt of every completed step
+  int gdts_cap = 0;
 };
 
 namespace {
@@ -228,6 +279,149 @@ int do_step(mhd_ctx* c, double* dt_inout) {
   if ((st = step_status(c))) return st;
   *dt_inout = c->hctl->dt;
   return set_status(c, MHD_OK, false, "");
+}
+
+void free_step_graph(mhd_ctx* c) {
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  c->step_graph = nullptr;
+}
+
+// Adds a while node to the graph being captured on c->stream, after what
+// was captured so far; returns its body graph.
+cudaError_t capture_while(mhd_ctx* c, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &cg, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, cg, deps, nd, &p)) != cudaSuccess) return e;
+  *body = p.conditional.phGraph_out[0];
+  return cudaStreamUpdateCaptureDependencies(c->stream, &node, 1,
+                                             cudaStreamSetCaptureDependencies);
+}
+
+// mhd_steps as one graph: while (steps wanted) { one step: the same launches
+// as do_step, with the RK3 retry loop as a nested while node whose condition
+// the controller's retry flag sets }.  Nothing is read on the host between
+// steps; the dt of every step lands in gdts.
+int build_step_graph(mhd_ctx* c, bool chars) {
+  free_step_graph(c);
+  const long long l0 = c->launches;
+  const bool rk3 = c->time_method != 1;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hs{}, hr{};
+  cudaGraph_t body = nullptr, rbody = nullptr;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&hs, g, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = hs;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+    if (e == cudaSuccess) body = p.conditional.phGraph_out[0];
+  }
+  if (e == cudaSuccess && rk3) e = cudaGraphConditionalHandleCreate(&hr, body, 0, 0);
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    enqueue_control(c, PH_RESET_CARRY);
+    enqueue_integrate(c, c->U, !rk3 && chars);
+    if (!rk3) {
+      enqueue_control(c, PH_EULER);
+      enqueue_combine(c, 0);
+      enqueue_control(c, PH_DONE);
+    } else {
+      enqueue_control(c, PH_RK_FIRST);
+      enqueue_rk3_tail(c, chars);
+      k_graph_retry<<<1, 32, 0, c->stream>>>(c->ctl, c->gcnt, hr);
+      e = capture_while(c, hr, &rbody);
+    }
+    k_graph_step_end<<<1, 32, 0, c->stream>>>(c->ctl, c->gcnt, c->gdts, hs);
+    cudaGraph_t out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(c->stream, &out);
+    if (e == cudaSuccess) e = e2;
+  }
+  c->step_graph_launches[0] = c->launches - l0 + (rk3 ? 2 : 1);
+  if (e == cudaSuccess && rk3) {
+    const long long l1 = c->launches;
+    e = cudaStreamBeginCaptureToGraph(c->stream, rbody, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      enqueue_control(c, PH_RK_RETRY);
+      enqueue_rk3_tail(c, chars);
+      k_graph_retry<<<1, 32, 0, c->stream>>>(c->ctl, c->gcnt, hr);
+      cudaGraph_t out = nullptr;
+      e = cudaStreamEndCapture(c->stream, &out);
+    }
+    c->step_graph_launches[1] = c->launches - l1 + 1;
+  }
+  c->launches = l0;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&c->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->step_graph = nullptr;
+    cudaGetLastError();
+    return cuda_fail(c, e, "build_step_graph");
+  }
+  c->step_graph_chars = chars;
+  c->step_graph_tma = tile_tma_enabled() ? 1 : 0;
+  return MHD_OK;
+}
+
+// nsteps steps through the step graph; the same results and statuses as
+// nsteps calls of do_step.
+int graph_steps(mhd_ctx* c, int nsteps, double* dt_inout, double* dts) {
+  int st = check_bc_ready(c);
+  if (st) return st;
+  const bool chars = (c->flags & MHD_FLAG_CHARACTERISTICS) != 0;
+  if (!c->gcnt) {
+    CK(cudaMalloc(&c->gcnt, G_COUNT * sizeof(long long)));
+    CK(cudaMallocHost(&c->hgcnt, G_COUNT * sizeof(long long)));
+  }
+  if (c->gdts_cap < nsteps) {  // the graph holds the buffer's address
+    free_step_graph(c);
+    if (c->gdts) CK(cudaFree(c->gdts));
+    c->gdts = nullptr;
+    CK(cudaMalloc(&c->gdts, size_t(nsteps) * sizeof(double)));
+    c->gdts_cap = nsteps;
+  }
+  if (!c->step_graph || c->step_graph_chars != chars ||
+      c->step_graph_tma != (tile_tma_enabled() ? 1 : 0))
+    if ((st = build_step_graph(c, chars))) return st;
+  k_graph_arm<<<1, 32, 0, c->stream>>>(c->gcnt, nsteps);
+  enqueue_control(c, PH_RESET_STEP, *dt_inout);  // the first step's dt_in
+  CK(cudaGraphLaunch(c->step_graph, c->stream));
+  CK(cudaMemcpyAsync(c->hgcnt, c->gcnt, G_COUNT * sizeof(long long), cudaMemcpyDeviceToHost,
+                     c->stream));
+  if ((st = read_ctl(c))) return st;
+  const long long done = c->hgcnt[G_STEPS];
+  c->launches += 1 + done * c->step_graph_launches[0] +
+                 c->hgcnt[G_RETRIES] * c->step_graph_launches[1] + (done < nsteps ? 1 : 0);
+  c->neg_pressure += c->hgcnt[G_NEG] - (long long)c->hctl->neg_count;  // step_status adds the last
+  if (done > 0) {
+    std::vector<double> h(done);
+    CK(cudaMemcpy(h.data(), c->gdts, done * sizeof(double), cudaMemcpyDeviceToHost));
+    if (dts) std::memcpy(dts, h.data(), done * sizeof(double));
+    *dt_inout = h[done - 1];
+  }
+  if (done == nsteps) {
+    c->neg_pressure += (long long)c->hctl->neg_count;
+    return set_status(c, MHD_OK, false, "");
+  }
+  if ((st = step_status(c))) return st;  // the failing step's status, as do_step reports it
+  return set_status(c, MHD_ERR_NOT_CONVERGED, true,
+                    "RK3 retry loop of the device step loop passed its bound\n! mhd_steps");
 }
 
 void divb_range(const mhd_ctx* c, int r[4]) {
@@ -431,6 +625,10 @@ int mhd_ctx_destroy(mhd_ctx* c) {
                     c->ratio, c->sor_xy};
   for (double* b : bufs)
     if (b) cudaFree(b);
+  free_step_graph(c);
+  if (c->gcnt) cudaFree(c->gcnt);
+  if (c->hgcnt) cudaFreeHost(c->hgcnt);
+  if (c->gdts) cudaFree(c->gdts);
   if (c->ctl) cudaFree(c->ctl);
   if (c->hctl) cudaFreeHost(c->hctl);
   if (c->hnan) cudaFreeHost(c->hnan);
@@ -451,7 +649,16 @@ int mhd_set_stepper(mhd_ctx* c, int time_method, double dt_min, double dt_max, d
   c->dt_min = dt_min;
   c->dt_max = dt_max;
   c->cfl = cfl;
+  free_step_graph(c);  // its controller launches carry the old limits
   return set_status(c, MHD_OK, false, "");
+}
+
+int mhd_set_step_graph(mhd_ctx* c, int enable) {
+  if (!c) return MHD_ERR_WRONG_PARAMETER;
+  CK(cudaSetDevice(c->device));
+  c->use_step_graph = enable ? 1 : 0;
+  if (!enable) free_step_graph(c);
+  return MHD_OK;
 }
 
 int mhd_last_error(const mhd_ctx* c, char* msg, size_t len, int* is_error) {
@@ -574,6 +781,7 @@ int mhd_steps(mhd_ctx* c, int nsteps, double* dt_inout, double* dts) {
   MHD_TRACE("mhd_steps");
   if (!c || !dt_inout || nsteps < 0) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
+  if (c->use_step_graph && nsteps > 0) return graph_steps(c, nsteps, dt_inout, dts);
   for (int n = 0; n < nsteps; n++) {
     int st = do_step(c, dt_inout);
     if (st) return st;

@@ -85,7 +85,8 @@ enum CtlPhase : int {
   PH_EULER = 5,        // after L(U): updateDt(dt)
   PH_IDEAL = 6,        // plain integrate: dtIdeal only
   PH_DONE = 7,         // mark the step complete
-  PH_RESET_INTEGRATE = 8
+  PH_RESET_INTEGRATE = 8,
+  PH_RESET_CARRY = 9   // as PH_RESET_STEP with dt_in = the previous step's dt (graph step loop)
 };
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {

@@ -204,6 +204,10 @@ __device__ __forceinline__ double min3(double a, double b, double c) {
 
 
 __device__ __forceinline__ void control_step(Ctl* c, const StepParams& p, int phase, double arg) {
+  if (phase == PH_RESET_CARRY) {  // the next step of a device-side step loop
+    arg = c->dt;
+    phase = PH_RESET_STEP;
+  }
   if (phase == PH_RESET_STEP || phase == PH_RESET_INTEGRATE) {
     c->skip = 0; c->retry = 0; c->error = 0; c->neg_last = 0; c->step_done = 0;
     c->maxX = 0ull; c->maxY = 0ull;

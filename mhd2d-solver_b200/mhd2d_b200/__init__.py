@@ -148,6 +148,7 @@ def library():
         "mhd_step": [vp, _dp],
         "mhd_step_host": [vp, _dp, _dp],
         "mhd_steps": [vp, C.c_int, _dp, _dp],
+        "mhd_set_step_graph": [vp, C.c_int],
         "mhd_get_characteristics": [vp, _dp, _dp, _dp, _dp],
         "mhd_divb_calc": [vp, _dp, _dp],
         "mhd_nongrid_data": [vp, _dp],
@@ -374,6 +375,10 @@ class Context:
         st = self._check(self.lib.mhd_divb_clean(self.h, C.byref(params), C.byref(m),
                                                  C.byref(sw)), "divb_clean")
         return self.last_status(st), m.value, sw.value
+
+    def set_step_graph(self, enable):
+        """steps() as one CUDA graph launch (default on) or one host round trip per step."""
+        self._check(self.lib.mhd_set_step_graph(self.h, int(bool(enable))), "set_step_graph")
 
     def set_sor_fused(self, enable):
         """Two-launch SOR sweeps where the grid allows them (default on)."""
