@@ -185,8 +185,8 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
   const int t = YDIR ? 2 + int(e / nf) : 2 + int(e % nt);
   const int ncell = YDIR ? g.ny : g.nx;
   const int lo_bc = YDIR ? BOTTOM : LEFT, hi_bc = YDIR ? TOP : RIGHT;
-  const int l1 = (g.bc[lo_bc] == OPEN && f < 2) ? 2 : 1;
-  const int l2 = (g.bc[hi_bc] == OPEN && f > ncell) ? 1 : 2;
+  const int l1 = (g.bc_of(lo_bc) == OPEN && f < 2) ? 2 : 1;
+  const int l2 = (g.bc_of(hi_bc) == OPEN && f > ncell) ? 1 : 2;
   // frame states of the stencil and their fluxes
   for (int p = 0; p < 4; p++) {
     double q[NF], F[NF], Gy[NF];
@@ -364,8 +364,8 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
 #pragma unroll
       for (int m = 0; m < NF; m++)
         if (m != 4) fb[m] += S[(7 * p + slot_of(m)) * NXY + off];
-      const int l1 = (g.bc[lo_bc] == OPEN && f < 2) ? 2 : 1;
-      const int l2 = (g.bc[hi_bc] == OPEN && f > ncell) ? 1 : 2;
+      const int l1 = (g.bc_of(lo_bc) == OPEN && f < 2) ? 2 : 1;
+      const int l2 = (g.bc_of(hi_bc) == OPEN && f > ncell) ? 1 : 2;
       if (p == l1) {
 #pragma unroll
         for (int k = 0; k < NF; k++) qb[k] += S[(28 + k) * NXY + off];
@@ -380,8 +380,14 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
 #pragma unroll
       for (int k = 0; k < NF; k++) q[k] = X[g.at(yd ? swap_xy(k) : k, i, j)];
       flux_x_adjoint(G.gm, q, fb, qb);
+      // constant indices on both branches (a runtime permutation would put part in local memory)
+      if (yd) {
 #pragma unroll
-      for (int k = 0; k < NF; k++) part[yd ? swap_xy(k) : k] = qb[k];
+        for (int k = 0; k < NF; k++) part[swap_xy(k)] = qb[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < NF; k++) part[k] = qb[k];
+      }
     }
   }
   // lu = (0 + x part) + y part on both lanes of the pair
@@ -409,64 +415,64 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
   }
 }
 
-// Transpose of the boundary fill (k_bc / bc_elem) for one side: adds the
-// adjoints of the side's two ghost layers (in T) to the interior cells of D
-// they were copied from.  pass 0: the copies (one thread per field and boundary cell,
-// both layers); Dirichlet ghosts hold the edge snapshot of the initial
-// state, so their adjoints go to lsnap (the side's [8][NY] or [8][NX]
-// array).  pass 1: the div B terms of Neumann Bx / By ghosts, gathered per
-// target cell so no two threads add to the same cell.
-__global__ void ka_adj_bc(Grid g, int side, int pass, const double* __restrict__ T,
-                          double* __restrict__ D, double* __restrict__ lsnap) {
+// Transpose of the boundary fill (k_bc / bc_elem), copy part, for field k
+// and boundary cell c of one side: adds the adjoints of the side's two ghost
+// layers (in T) to the interior cells of D they were copied from.
+// Dirichlet ghosts hold the edge snapshot of the initial state, so their
+// adjoints go to lsnap (the side's [8][NY] or [8][NX] array).  Every cell it
+// adds to lies in field k, row / column c.
+__device__ __forceinline__ void adj_bc_copy(const Grid& g, int side, int k, int c,
+                                            const double* __restrict__ T,
+                                            double* __restrict__ D,
+                                            double* __restrict__ lsnap) {
   const bool xs = side == LEFT || side == RIGHT;
-  const int nb = xs ? g.ny : g.nx;  // boundary cells along the side
-  const int b = g.bc[side];
-  const double rxy = g.dx / g.dy, ryx = g.dy / g.dx;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pass == 0) {
-    if (e >= NF * nb) return;
-    const int k = e / nb, c = 2 + e % nb;  // c: j (x sides) or i (y sides)
-    if (b == DIRICHLET) {
-      const int len = xs ? g.NY : g.NX;
-      double acc = 0.0;
-      for (int gl = 1; gl <= 2; gl++) {
-        if (side == LEFT) acc += T[g.at(k, 2 - gl, c)];
-        else if (side == RIGHT) acc += T[g.at(k, g.nx + 1 + gl, c)];
-        else if (side == BOTTOM) acc += T[g.at(k, c, 2 - gl)];
-        else acc += T[g.at(k, c, g.ny + 1 + gl)];
-      }
-      lsnap[k * len + c] += acc;
-      return;
-    }
+  const int b = g.bc_of(side);
+  if (b == DIRICHLET) {
+    const int len = xs ? g.NY : g.NX;
+    double acc = 0.0;
     for (int gl = 1; gl <= 2; gl++) {
-      int gi, gj, si, sj;  // ghost cell, its source
-      if (side == LEFT) {
-        gi = 2 - gl; gj = c; sj = c;
-        si = b == PERIODIC ? g.nx + 2 - gl : 2 + gl;
-        if (b == NEUMANN && k == 4 && c >= 3 && c < g.ny + 1) si = gi + 2;
-      } else if (side == RIGHT) {
-        gi = g.nx + 1 + gl; gj = c; sj = c;
-        si = b == PERIODIC ? 1 + gl : g.nx + 1 - gl;
-        if (b == NEUMANN && k == 4 && c >= 3 && c < g.ny + 1) si = gi - 2;
-      } else if (side == BOTTOM) {
-        gj = 2 - gl; gi = c; si = c;
-        sj = b == PERIODIC ? g.ny + 2 - gl : 2 + gl;
-        if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj + 2;
-      } else {
-        gj = g.ny + 1 + gl; gi = c; si = c;
-        sj = b == PERIODIC ? 1 + gl : g.ny + 1 - gl;
-        if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj - 2;
-      }
-      D[g.at(k, si, sj)] += T[g.at(k, gi, gj)];
+      if (side == LEFT) acc += T[g.at(k, 2 - gl, c)];
+      else if (side == RIGHT) acc += T[g.at(k, g.nx + 1 + gl, c)];
+      else if (side == BOTTOM) acc += T[g.at(k, c, 2 - gl)];
+      else acc += T[g.at(k, c, g.ny + 1 + gl)];
     }
+    lsnap[k * len + c] += acc;
     return;
   }
-  // pass 1: Neumann div B terms.  A left ghost Bx at row it, column c' reads
-  // By at row s5, columns c'-1 (coefficient -rxy) and c'+1 (+rxy); the
-  // target (By, s5, c) therefore collects -rxy * ghost(c+1) and
-  // +rxy * ghost(c-1).  The other sides mirror this.
-  if (b != NEUMANN || e >= nb) return;
-  const int c = 2 + e;
+  for (int gl = 1; gl <= 2; gl++) {
+    int gi, gj, si, sj;  // ghost cell, its source
+    if (side == LEFT) {
+      gi = 2 - gl; gj = c; sj = c;
+      si = b == PERIODIC ? g.nx + 2 - gl : 2 + gl;
+      if (b == NEUMANN && k == 4 && c >= 3 && c < g.ny + 1) si = gi + 2;
+    } else if (side == RIGHT) {
+      gi = g.nx + 1 + gl; gj = c; sj = c;
+      si = b == PERIODIC ? 1 + gl : g.nx + 1 - gl;
+      if (b == NEUMANN && k == 4 && c >= 3 && c < g.ny + 1) si = gi - 2;
+    } else if (side == BOTTOM) {
+      gj = 2 - gl; gi = c; si = c;
+      sj = b == PERIODIC ? g.ny + 2 - gl : 2 + gl;
+      if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj + 2;
+    } else {
+      gj = g.ny + 1 + gl; gi = c; si = c;
+      sj = b == PERIODIC ? 1 + gl : g.ny + 1 - gl;
+      if (b == NEUMANN && k == 5 && c >= 3 && c < g.nx + 1) sj = gj - 2;
+    }
+    D[g.at(k, si, sj)] += T[g.at(k, gi, gj)];
+  }
+}
+
+// Transpose of the boundary fill, div B part, for boundary cell c of a
+// Neumann side.  A left ghost Bx at row it, column c' reads By at row s5,
+// columns c'-1 (coefficient -rxy) and c'+1 (+rxy); the target (By, s5, c)
+// therefore collects -rxy * ghost(c+1) and +rxy * ghost(c-1).  The other
+// sides mirror this.  The cells it adds to lie in field 5 (x sides) or 4
+// (y sides), row / column c.
+__device__ __forceinline__ void adj_bc_divb(const Grid& g, int side, int c,
+                                            const double* __restrict__ T,
+                                            double* __restrict__ D) {
+  const bool xs = side == LEFT || side == RIGHT;
+  const double rxy = g.dx / g.dy, ryx = g.dy / g.dx;
   for (int layer = 0; layer < 2; layer++) {
     if (xs) {
       int gi, s5;
@@ -501,6 +507,28 @@ __global__ void ka_adj_bc(Grid g, int side, int pass, const double* __restrict__
       if (c - 1 >= 3 && c - 1 < g.nx + 1) acc += cp * T[g.at(5, c - 1, gj)];
       D[g.at(4, c, s4)] += acc;
     }
+  }
+}
+
+// Transpose of the boundary fill for the two sides of one direction (x:
+// left then right; y: bottom then top), one thread per field k and boundary
+// cell c.  Everything a thread adds lands in field k, row / column c (the
+// div B terms of a Neumann side are added by the thread of the field they
+// land in), so no two threads add to the same cell, and every cell takes its
+// terms in the order: low side copies, low side div B, high side copies,
+// high side div B.  The x launch runs before the y launch, which keeps the
+// order at the corners.
+__global__ void ka_adj_bc(Grid g, int ydir, const double* __restrict__ T, double* __restrict__ D,
+                          double* __restrict__ lsnap_lo, double* __restrict__ lsnap_hi) {
+  const int nb = ydir ? g.nx : g.ny;  // boundary cells along the sides
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= NF * nb) return;
+  const int k = e / nb, c = 2 + e % nb;
+  const int lo = ydir ? BOTTOM : LEFT, kdiv = ydir ? 4 : 5;
+  for (int h = 0; h < 2; h++) {
+    const int side = lo + h;
+    adj_bc_copy(g, side, k, c, T, D, h ? lsnap_hi : lsnap_lo);
+    if (k == kdiv && g.bc_of(side) == NEUMANN) adj_bc_divb(g, side, c, T, D);
   }
 }
 
@@ -943,13 +971,11 @@ void adjoint_stage(mhd_adj* a, int s, const StageRec& r, const double* X) {
       g, a->G, X, a->SX, a->SY, a->T, r.mode, r.in_buf, a->lU, a->lU1, a->lU2);
   a->launches += 3;
   double* dst = lb[r.in_buf];
-  for (int side = 0; side < 4; side++) {
-    const int nb = (side < 2) ? g.ny : g.nx;
-    ka_adj_bc<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, side, 0, a->T, dst,
-                                                              a->lsnap[side]);
-    a->launches++;
-    if (g.bc[side] != NEUMANN) continue;  // pass 1 is the Neumann div B term
-    ka_adj_bc<<<(nb + 127) / 128, 128, 0, a->stream>>>(g, side, 1, a->T, dst, a->lsnap[side]);
+  for (int ydir = 0; ydir < 2; ydir++) {
+    const int nb = ydir ? g.nx : g.ny;
+    ka_adj_bc<<<(NF * nb + 127) / 128, 128, 0, a->stream>>>(g, ydir, a->T, dst,
+                                                              a->lsnap[2 * ydir],
+                                                              a->lsnap[2 * ydir + 1]);
     a->launches++;
   }
 }

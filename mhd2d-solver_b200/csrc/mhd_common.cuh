@@ -27,6 +27,11 @@ struct Grid {
   long long fstride; // doubles per field plane (NX*pitch)
   double dx, dy, gamma;
   int bc[4];         // left, right, bottom, top
+  // bc[side] for a side known only at run time, by selects: indexing the
+  // kernel-parameter array with a run-time index copies the Grid to local memory
+  __host__ __device__ int bc_of(int side) const {
+    return side == 0 ? bc[0] : side == 1 ? bc[1] : side == 2 ? bc[2] : bc[3];
+  }
   __host__ __device__ long long at(int k, int i, int j) const {
     return (long long)k * fstride + (long long)i * pitch + off + j;
   }

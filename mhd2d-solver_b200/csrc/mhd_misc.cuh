@@ -43,7 +43,7 @@ __device__ __forceinline__ void bc_elem(const Grid& g, double* __restrict__ U, c
       const int k = int(q % NF); q /= NF;
       const int gl = 1 + int(q % 2);
       const int side = int(q / 2);  // 0 left, 1 right
-      const int b = g.bc[side];
+      const int b = g.bc_of(side);
       if (side == 0) {
         const int it = 2 - gl;
         double v;
@@ -77,7 +77,7 @@ __device__ __forceinline__ void bc_elem(const Grid& g, double* __restrict__ U, c
       const int i = 2 + int(q % nx); q /= nx;
       const int k = int(q % NF);
       const int side = int(q / NF);  // 0 bottom, 1 top
-      const int b = g.bc[2 + side];
+      const int b = g.bc_of(2 + side);
       if (side == 0) {
         const int jt = 2 - gl;
         double v;
