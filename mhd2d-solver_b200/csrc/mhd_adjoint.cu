@@ -54,7 +54,6 @@ namespace MHD_KNS {
 
 constexpr int ATI = 7, ATJ = 32, ANW = 8;  // flux tile of the forward runs
 using AGeom = TileGeom<ATI, ATJ>;
-constexpr int NSC = 44;  // scratch words per interface: 4 x 7 flux adjoints, 2 x 8 state adjoints
 
 struct StageRec {
   int in_buf;  // 0 U, 1 U1, 2 U2
@@ -154,35 +153,62 @@ __device__ __forceinline__ long long cell_at(const Grid& g, bool ydir, int k, in
 constexpr int AIB = 64;  // threads per block of ka_adj_iface (37 KB of shared memory)
 constexpr int AIB_MIN = 6;  // resident blocks per SM: 168 registers, 6 x 37 KB shared
 
-// Adjoint of the numerical flux of every interface of one direction.  One
-// thread per interface; the interface's frame is the x frame (y interfaces
-// work on x/y-swapped states, as the forward does).  Writes NSC scratch
-// words per interface: S[c][f][t] (x) or S[c][t][f] (y) with c = 7p +
-// slot(m) for the adjoint of the frame flux component m at stencil point p,
-// 28 + k for the adjoint of the frame state U1[k], 36 + k for U2[k].
+// Interface tiles of ka_adj_iface: each warp takes BF consecutive faces
+// along the direction times BT transverse cells (BF * BT = 32 threads) and
+// sums its faces' contributions per stencil cell before writing them.
+// The CL = BF + 3 cells a tile's stencils touch overlap the next tile's by
+// 3, so the scratch holds CL / BF cell records of 15 words per face instead
+// of the 44 words of every face.  x faces: 8 x 4 (consecutive lanes along
+// t, the contiguous j); y faces: 32 x 1 (lanes along f, j again).
+struct ITile {
+  int bf, bt, cl, ntile, nt;  // tile shape, tiles along the direction, transverse cells
+  long long plane;            // doubles per scratch word plane
+};
+constexpr int BF_X = 4, BF_Y = 32;
+// a cell is then touched by the stencils of at most two tiles (the gather reads two records)
+static_assert(BF_X >= 3 && BF_Y >= 3 && 32 % BF_X == 0 && 32 % BF_Y == 0, "interface tile shape");
+constexpr int NPW = 15;  // scratch words per cell record: 7 flux-adjoint slots, 8 state adjoints
+
+__host__ __device__ inline ITile itile(const Grid& g, bool ydir) {
+  ITile T;
+  T.bf = ydir ? BF_Y : BF_X;
+  T.bt = 32 / T.bf;
+  T.cl = T.bf + 3;
+  const int nf = ydir ? g.ny + 1 : g.nx + 1;  // faces 1..n+1 along the direction
+  T.nt = ydir ? g.nx : g.ny;                  // interior transverse cells 2..n+1
+  T.ntile = (nf + T.bf - 1) / T.bf;
+  T.plane = (long long)T.ntile * T.cl * T.nt;
+  return T;
+}
+
+// Scratch word w of the record of tile tau, touched cell c (cell tau*bf + c
+// along the direction) and transverse cell t: x records are ordered
+// [w][tau][c][t], y records [w][t][tau][c], so both run along j.
+__host__ __device__ inline long long rec_at(const ITile& T, bool ydir, int w, int tau, int c,
+                                            int t) {
+  const long long r = ydir ? (long long)(t - 2) * T.ntile * T.cl + (long long)tau * T.cl + c
+                           : ((long long)tau * T.cl + c) * T.nt + (t - 2);
+  return w * T.plane + r;
+}
+
+// Adjoint of the numerical flux of one interface f at transverse cell t
+// (the interface's frame is the x frame: y interfaces work on x/y-swapped
+// states, as the forward does).  Leaves in the thread's columns of sFb the
+// adjoints of the frame fluxes of the 4 stencil points (row 7p + slot(m))
+// and in sQ the adjoints of the frame states U1 (rows 0-7) and U2 (8-15).
 //
 // The characteristics are walked in pairs (0, 6), (2, 4), (1, 5), (3):
 // rows k and 6 - k share a symmetric part, so the adjoint of the pair's
 // eigenvector rows is one pass (pair_adjoint) over the summed and
 // differenced seeds.
 template <bool YDIR>
-__global__ void __launch_bounds__(AIB, AIB_MIN)
-    ka_adj_iface(Grid g, Gas G, const double* __restrict__ X, const unsigned* __restrict__ mask,
-                 const double* __restrict__ lB, double cL, double* __restrict__ S,
-                 double inv_d) {
-  __shared__ double sF[28][AIB];   // frame fluxes of the 4 stencil points
-  __shared__ double sFb[28][AIB];  // their adjoints
-  __shared__ double sQ[16][AIB];   // U1, U2 (frame)
-  const int tid = threadIdx.x;
-  const int nf = YDIR ? g.ny + 1 : g.nx + 1;  // faces 1..n+1 along the direction
-  const int nt = YDIR ? g.nx : g.ny;          // interior transverse cells 2..n+1
-  const long long n = (long long)nf * nt;
-  const long long NXY = (long long)g.NX * g.NY;
-  const long long e = blockIdx.x * (long long)blockDim.x + tid;
-  if (e >= n) return;
-  // consecutive threads walk the contiguous j direction
-  const int f = YDIR ? 1 + int(e % nf) : 1 + int(e / nt);
-  const int t = YDIR ? 2 + int(e / nf) : 2 + int(e % nt);
+__device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
+                                              const double* __restrict__ X,
+                                              const unsigned* __restrict__ mask,
+                                              const double* __restrict__ lB, double cL,
+                                              double inv_d, int f, int t, int tid,
+                                              double (*sF)[AIB], double (*sFb)[AIB],
+                                              double (*sQ)[AIB]) {
   const int ncell = YDIR ? g.ny : g.nx;
   const int lo_bc = YDIR ? BOTTOM : LEFT, hi_bc = YDIR ? TOP : RIGHT;
   const int l1 = (g.bc_of(lo_bc) == OPEN && f < 2) ? 2 : 1;
@@ -231,10 +257,10 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
     U1[k] = sQ[k][tid];
     U2[k] = sQ[8 + k][tid];
   }
-  double* out = YDIR ? S + (long long)t * g.NY + f : S + (long long)f * g.NY + t;
   Mid e0;
-  if (!midpoint(G, U1, U2, e0)) {
-    for (int c = 0; c < NSC; c++) out[c * NXY] = 0.0;
+  if (!midpoint(G, U1, U2, e0)) {  // sFb is still zero
+#pragma unroll
+    for (int k = 0; k < 16; k++) sQ[k][tid] = 0.0;
     return;
   }
   const unsigned mw = mask[YDIR ? (long long)t * g.NY + f : (long long)f * g.NY + t];
@@ -314,11 +340,85 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
 #pragma unroll
   for (int k = 0; k < NF; k++) { U1b[k] = 0.0; U2b[k] = 0.0; }
   midpoint_adjoint(G, e0, U1, U2, mb, U1b, U2b);
-  for (int c = 0; c < 28; c++) out[c * NXY] = sFb[c][tid];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    out[(28 + k) * NXY] = U1b[k];
-    out[(36 + k) * NXY] = U2b[k];
+    sQ[k][tid] = U1b[k];
+    sQ[8 + k][tid] = U2b[k];
+  }
+}
+
+// Adjoint of the numerical flux of every interface of one direction, one
+// thread per interface (iface_adjoint), one interface tile per warp
+// (ITile).  The warp then writes one record per touched cell: the sums of
+// its faces' flux adjoints (slot w < 7) and state adjoints (7 + k) at that
+// cell, added in the order of the stencil position p = 0..3 (faces
+// descending), the adjoint of U1 before that of U2 per face.
+template <bool YDIR>
+__global__ void __launch_bounds__(AIB, AIB_MIN)
+    ka_adj_iface(Grid g, Gas G, const double* __restrict__ X, const unsigned* __restrict__ mask,
+                 const double* __restrict__ lB, double cL, double* __restrict__ S,
+                 double inv_d) {
+  __shared__ double sF[28][AIB];   // frame fluxes of the 4 stencil points
+  __shared__ double sFb[28][AIB];  // their adjoints
+  __shared__ double sQ[16][AIB];   // U1, U2 (frame), then their adjoints
+  const int tid = threadIdx.x, lane = tid & 31, wbase = tid - lane;
+  const ITile T = itile(g, YDIR);
+  const int nf = YDIR ? g.ny + 1 : g.nx + 1, ncell = nf - 1;
+  const long long tile = (long long)blockIdx.x * (AIB / 32) + tid / 32;
+  const long long ntiles = (long long)T.ntile * ((T.nt + T.bt - 1) / T.bt);
+  const int tau = int(tile % T.ntile), tb = int(tile / T.ntile);
+  const int fl = YDIR ? lane % T.bf : lane / T.bt, tl = YDIR ? lane / T.bf : lane % T.bt;
+  const int f = 1 + tau * T.bf + fl, t = 2 + tb * T.bt + tl;
+  if (tile < ntiles && f <= nf && t <= T.nt + 1) {
+    iface_adjoint<YDIR>(g, G, X, mask, lB, cL, inv_d, f, t, tid, sF, sFb, sQ);
+  } else {
+#pragma unroll
+    for (int c = 0; c < 28; c++) sFb[c][tid] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) sQ[k][tid] = 0.0;
+  }
+  __syncwarp();
+  if (tile >= ntiles) return;
+  const int lo_bc = YDIR ? BOTTOM : LEFT, hi_bc = YDIR ? TOP : RIGHT;
+  const bool open_lo = g.bc_of(lo_bc) == OPEN, open_hi = g.bc_of(hi_bc) == OPEN;
+  for (int it = lane; it < T.cl * T.bt; it += 32) {
+    int c, tl2;
+    if (YDIR) {
+      c = it % T.cl; tl2 = it / T.cl;
+    } else {
+      tl2 = it % T.bt; c = it / T.bt;
+    }
+    const int t2 = 2 + tb * T.bt + tl2;
+    if (t2 > T.nt + 1) continue;
+    double fb[7], qb[NF];
+#pragma unroll
+    for (int w = 0; w < 7; w++) fb[w] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NF; k++) qb[k] = 0.0;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const int fl2 = c - p;
+      if (fl2 < 0 || fl2 >= T.bf) continue;
+      const int th = wbase + (YDIR ? tl2 * T.bf + fl2 : fl2 * T.bt + tl2);
+#pragma unroll
+      for (int w = 0; w < 7; w++) fb[w] += sFb[7 * p + w][th];
+      const int f2 = 1 + tau * T.bf + fl2;
+      const int l1 = (open_lo && f2 < 2) ? 2 : 1;
+      const int l2 = (open_hi && f2 > ncell) ? 1 : 2;
+      if (p == l1) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) qb[k] += sQ[k][th];
+      }
+      if (p == l2) {
+#pragma unroll
+        for (int k = 0; k < NF; k++) qb[k] += sQ[8 + k][th];
+      }
+    }
+    double* r = S + rec_at(T, YDIR, 0, tau, c, t2);
+#pragma unroll
+    for (int w = 0; w < 7; w++) r[w * T.plane] = fb[w];
+#pragma unroll
+    for (int k = 0; k < NF; k++) r[(7 + k) * T.plane] = qb[k];
   }
 }
 
@@ -348,34 +448,28 @@ __global__ void __launch_bounds__(128) ka_adj_gather(Grid g, Gas G, const double
   for (int k = 0; k < NF; k++) part[k] = 0.0;
   const int a = yd ? j : i;  // position along the direction
   const int t = yd ? i : j;  // transverse position
-  const int ncell = yd ? g.ny : g.nx, ntr = yd ? g.nx : g.ny;
+  const int ntr = yd ? g.nx : g.ny;
   if (valid && t >= 2 && t <= ntr + 1) {
     const double* S = yd ? SY : SX;
-    const int lo_bc = yd ? BOTTOM : LEFT, hi_bc = yd ? TOP : RIGHT;
+    const ITile TT = itile(g, yd);
     double fb[NF], qb[NF];
-    bool any = false;
 #pragma unroll
     for (int m = 0; m < NF; m++) { fb[m] = 0.0; qb[m] = 0.0; }
-    for (int p = 0; p < 4; p++) {
-      const int f = a + 1 - p;
-      if (f < 1 || f > ncell + 1) continue;
-      const long long off = yd ? (long long)t * g.NY + f : (long long)f * g.NY + t;
-      any = true;
+    // the records of the (one or two) tiles whose stencils touch the cell:
+    // the tile of the higher faces first, then the tile below it
+    const int tau1 = a / TT.bf, c1 = a % TT.bf;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int tau = tau1 - h, c = c1 + h * TT.bf;
+      if (tau < 0 || tau >= TT.ntile || c >= TT.cl) continue;
+      const double* r = S + rec_at(TT, yd, 0, tau, c, t);
 #pragma unroll
       for (int m = 0; m < NF; m++)
-        if (m != 4) fb[m] += S[(7 * p + slot_of(m)) * NXY + off];
-      const int l1 = (g.bc_of(lo_bc) == OPEN && f < 2) ? 2 : 1;
-      const int l2 = (g.bc_of(hi_bc) == OPEN && f > ncell) ? 1 : 2;
-      if (p == l1) {
+        if (m != 4) fb[m] += r[slot_of(m) * TT.plane];
 #pragma unroll
-        for (int k = 0; k < NF; k++) qb[k] += S[(28 + k) * NXY + off];
-      }
-      if (p == l2) {
-#pragma unroll
-        for (int k = 0; k < NF; k++) qb[k] += S[(36 + k) * NXY + off];
-      }
+      for (int k = 0; k < NF; k++) qb[k] += r[(7 + k) * TT.plane];
     }
-    if (any) {
+    {
       double q[NF];
 #pragma unroll
       for (int k = 0; k < NF; k++) q[k] = X[g.at(yd ? swap_xy(k) : k, i, j)];
@@ -955,15 +1049,16 @@ void adjoint_stage(mhd_adj* a, int s, const StageRec& r, const double* X) {
   double* lb[3] = {a->lU, a->lU1, a->lU2};
   const double* lB = lb[stage_out(r.mode)];
   const double cL = ul_coef(r.mode, r.dt);
-  const long long nx_faces = (long long)(g.nx + 1) * g.ny, ny_faces = (long long)(g.ny + 1) * g.nx;
+  const ITile tx = itile(g, false), ty = itile(g, true);
+  const int tpb = AIB / 32;  // interface tiles per block
+  const int nbx = int((tx.ntile * (long long)((tx.nt + tx.bt - 1) / tx.bt) + tpb - 1) / tpb);
+  const int nby = int((ty.ntile * (long long)((ty.nt + ty.bt - 1) / ty.bt) + tpb - 1) / tpb);
   // the two directions read the same inputs and write their own scratch
   // (SX, SY): the y faces run on the side stream, the gather waits for both
   cudaEventRecord(a->fork, a->stream);
   cudaStreamWaitEvent(a->side, a->fork, 0);
-  ka_adj_iface<false><<<int((nx_faces + AIB - 1) / AIB), AIB, 0, a->stream>>>(
-      g, a->G, X, mx, lB, cL, a->SX, 1.0 / g.dx);
-  ka_adj_iface<true><<<int((ny_faces + AIB - 1) / AIB), AIB, 0, a->side>>>(
-      g, a->G, X, my, lB, cL, a->SY, 1.0 / g.dy);
+  ka_adj_iface<false><<<nbx, AIB, 0, a->stream>>>(g, a->G, X, mx, lB, cL, a->SX, 1.0 / g.dx);
+  ka_adj_iface<true><<<nby, AIB, 0, a->side>>>(g, a->G, X, my, lB, cL, a->SY, 1.0 / g.dy);
   cudaEventRecord(a->join, a->side);
   cudaStreamWaitEvent(a->stream, a->join, 0);
   const long long ncell = (long long)g.NX * g.NY;
@@ -1369,11 +1464,11 @@ int mhd_adj_create(int nx, int ny, double dx, double dy, double gamma, const int
   }
   AK(cudaMalloc(&a->aF, sizeof(double) * NF * g.NY));
   AK(cudaMalloc(&a->aG, sizeof(double) * NF * g.NX));
-  const size_t sc = (size_t)NSC * g.NX * g.NY;
-  AK(cudaMalloc(&a->SX, sc * sizeof(double)));
-  AK(cudaMalloc(&a->SY, sc * sizeof(double)));
-  AK(cudaMemsetAsync(a->SX, 0, sc * sizeof(double), a->stream));
-  AK(cudaMemsetAsync(a->SY, 0, sc * sizeof(double), a->stream));
+  const size_t scx = (size_t)NPW * itile(g, false).plane, scy = (size_t)NPW * itile(g, true).plane;
+  AK(cudaMalloc(&a->SX, scx * sizeof(double)));
+  AK(cudaMalloc(&a->SY, scy * sizeof(double)));
+  AK(cudaMemsetAsync(a->SX, 0, scx * sizeof(double), a->stream));
+  AK(cudaMemsetAsync(a->SY, 0, scy * sizeof(double), a->stream));
   AK(cudaMalloc(&a->ctl, sizeof(Ctl)));
   AK(cudaMemsetAsync(a->ctl, 0, sizeof(Ctl), a->stream));
   AK(cudaMallocHost(&a->hctl, sizeof(Ctl)));
