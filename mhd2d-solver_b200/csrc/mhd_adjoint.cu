@@ -22,9 +22,11 @@
 //      eigen-system and the frozen ENO combination, and form the adjoints
 //      of the 4 stencil fluxes and of the two midpoint states
 //      (mhd_adjoint_gen.cuh, generated reverse-mode code); it reads the
-//      adjoint of UL as a multiple of the stage output's adjoint;
-//   2. ka_adj_gather: per cell, sum the contributions of every interface
-//      that used it and apply the transposed flux Jacobians; interior cells
+//      adjoint of UL as a multiple of the stage output's adjoint; each warp
+//      takes a tile of interfaces and writes one record per cell its
+//      stencils touch (the sums of its interfaces' contributions there);
+//   2. ka_adj_gather: per cell, add the one or two records of each
+//      direction and apply the transposed flux Jacobians; interior cells
 //      also apply the rest of the stage update's adjoint and add the result
 //      to the stage input's adjoint, ghost cells go to T;
 //   3. ka_adj_bc: transpose of the boundary fill (ghost adjoints in T ->
@@ -167,6 +169,10 @@ struct ITile {
 constexpr int BF_X = 4, BF_Y = 32;
 // a cell is then touched by the stencils of at most two tiles (the gather reads two records)
 static_assert(BF_X >= 3 && BF_Y >= 3 && 32 % BF_X == 0 && 32 % BF_Y == 0, "interface tile shape");
+// stencil cells of one warp's tile, and the row stride of the per-block cell arrays
+constexpr int NCW = (BF_X + 3) * (32 / BF_X) > (BF_Y + 3) * (32 / BF_Y) ? (BF_X + 3) * (32 / BF_X)
+                                                                      : (BF_Y + 3) * (32 / BF_Y);
+constexpr int CRS = (AIB / 32) * NCW;
 constexpr int NPW = 15;  // scratch words per cell record: 7 flux-adjoint slots, 8 state adjoints
 
 __host__ __device__ inline ITile itile(const Grid& g, bool ydir) {
@@ -193,9 +199,11 @@ __host__ __device__ inline long long rec_at(const ITile& T, bool ydir, int w, in
 
 // Adjoint of the numerical flux of one interface f at transverse cell t
 // (the interface's frame is the x frame: y interfaces work on x/y-swapped
-// states, as the forward does).  Leaves in the thread's columns of sFb the
-// adjoints of the frame fluxes of the 4 stencil points (row 7p + slot(m))
-// and in sQ the adjoints of the frame states U1 (rows 0-7) and U2 (8-15).
+// states, as the forward does).  The frame fluxes and states of its 4
+// stencil points come from the tile's cell arrays (point p: entry ci0 +
+// p * cstep of sC / sS).  Leaves in the thread's columns of sFb the adjoints
+// of the frame fluxes of the 4 stencil points (row 7p + slot(m)) and in sQ
+// the adjoints of the frame states U1 (rows 0-7) and U2 (8-15).
 //
 // The characteristics are walked in pairs (0, 6), (2, 4), (1, 5), (3):
 // rows k and 6 - k share a symmetric part, so the adjoint of the pair's
@@ -203,40 +211,18 @@ __host__ __device__ inline long long rec_at(const ITile& T, bool ydir, int w, in
 // differenced seeds.
 template <bool YDIR>
 __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
-                                              const double* __restrict__ X,
                                               const unsigned* __restrict__ mask,
                                               const double* __restrict__ lB, double cL,
                                               double inv_d, int f, int t, int tid,
-                                              double (*sF)[AIB], double (*sFb)[AIB],
-                                              double (*sQ)[AIB]) {
+                                              const double* __restrict__ sC,
+                                              const double* __restrict__ sS, int ci0, int cstep,
+                                              double (*sFb)[AIB], double (*sQ)[AIB]) {
   const int ncell = YDIR ? g.ny : g.nx;
   const int lo_bc = YDIR ? BOTTOM : LEFT, hi_bc = YDIR ? TOP : RIGHT;
   const int l1 = (g.bc_of(lo_bc) == OPEN && f < 2) ? 2 : 1;
   const int l2 = (g.bc_of(hi_bc) == OPEN && f > ncell) ? 1 : 2;
-  // frame states of the stencil and their fluxes
-  for (int p = 0; p < 4; p++) {
-    double q[NF], F[NF], Gy[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const int kk = YDIR ? swap_xy(k) : k;
-      q[k] = X[cell_at(g, YDIR, kk, f, t, p)];
-    }
-    phys_flux(G.gm, q, F, Gy);
-#pragma unroll
-    for (int m = 0; m < NF; m++) {
-      if (m == 4) continue;
-      sF[p * 7 + slot_of(m)][tid] = F[m];
-      sFb[p * 7 + slot_of(m)][tid] = 0.0;
-    }
-    if (p == l1) {
-#pragma unroll
-      for (int k = 0; k < NF; k++) sQ[k][tid] = q[k];
-    }
-    if (p == l2) {
-#pragma unroll
-      for (int k = 0; k < NF; k++) sQ[8 + k][tid] = q[k];
-    }
-  }
+  for (int c = 0; c < 28; c++) sFb[c][tid] = 0.0;
   // adjoint of the frame numerical flux: UL = -(F_f - F_{f-1}) / d - ...;
   // the adjoint of UL is cL times the adjoint lB of the stage update's output
   double lF[NF];
@@ -254,8 +240,8 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
   double U1[NF], U2[NF];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    U1[k] = sQ[k][tid];
-    U2[k] = sQ[8 + k][tid];
+    U1[k] = sS[k * CRS + ci0 + l1 * cstep];
+    U2[k] = sS[k * CRS + ci0 + l2 * cstep];
   }
   Mid e0;
   if (!midpoint(G, U1, U2, e0)) {  // sFb is still zero
@@ -298,7 +284,7 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
       for (int m = 0; m < NF; m++) {
         if (m == 4) { phi[m] = 0.0; continue; }
         const int s = slot_of(m);
-        phi[m] = ca * sF[7 * pa + s][tid] + cb * sF[7 * pa + 7 + s][tid];
+        phi[m] = ca * sC[s * CRS + ci0 + pa * cstep] + cb * sC[s * CRS + ci0 + (pa + 1) * cstep];
         fw += l[m] * phi[m];
       }
 #pragma unroll
@@ -329,11 +315,11 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
   }
   // U1, U2 again from shared memory (volatile: not kept live across the loop)
   {
-    const volatile double* vq = &sQ[0][0];
+    const volatile double* vq = sS;
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      U1[k] = vq[k * AIB + tid];
-      U2[k] = vq[(8 + k) * AIB + tid];
+      U1[k] = vq[k * CRS + ci0 + l1 * cstep];
+      U2[k] = vq[k * CRS + ci0 + l2 * cstep];
     }
   }
   double U1b[NF], U2b[NF];
@@ -358,19 +344,44 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
     ka_adj_iface(Grid g, Gas G, const double* __restrict__ X, const unsigned* __restrict__ mask,
                  const double* __restrict__ lB, double cL, double* __restrict__ S,
                  double inv_d) {
-  __shared__ double sF[28][AIB];   // frame fluxes of the 4 stencil points
-  __shared__ double sFb[28][AIB];  // their adjoints
-  __shared__ double sQ[16][AIB];   // U1, U2 (frame), then their adjoints
+  __shared__ double sC[7 * CRS];    // frame fluxes of the tiles' stencil cells
+  __shared__ double sS[NF * CRS];   // their frame states
+  __shared__ double sFb[28][AIB];  // per interface: adjoints of its 4 stencil points' fluxes
+  __shared__ double sQ[16][AIB];   // per interface: adjoints of U1, U2 (frame)
   const int tid = threadIdx.x, lane = tid & 31, wbase = tid - lane;
+  const int wc = (tid / 32) * NCW;  // the warp's cells in sC / sS
   const ITile T = itile(g, YDIR);
   const int nf = YDIR ? g.ny + 1 : g.nx + 1, ncell = nf - 1;
   const long long tile = (long long)blockIdx.x * (AIB / 32) + tid / 32;
   const long long ntiles = (long long)T.ntile * ((T.nt + T.bt - 1) / T.bt);
   const int tau = int(tile % T.ntile), tb = int(tile / T.ntile);
+  // the tile's stencil cells (c, tl2), cell tau*bf + c along the direction:
+  // states and fluxes once per cell (each is a stencil point of up to 4 faces)
+  if (tile < ntiles) {
+    for (int ci = lane; ci < T.cl * T.bt; ci += 32) {
+      const int c = YDIR ? ci % T.cl : ci / T.bt, tl2 = YDIR ? ci / T.cl : ci % T.bt;
+      const int a = tau * T.bf + c, t2 = 2 + tb * T.bt + tl2;
+      if (a > ncell + 3 || t2 > T.nt + 1) continue;  // read by no interface
+      double q[NF], F[NF], Gy[NF];
+#pragma unroll
+      for (int k = 0; k < NF; k++)
+        q[k] = X[YDIR ? g.at(swap_xy(k), t2, a) : g.at(k, a, t2)];
+      phys_flux(G.gm, q, F, Gy);
+#pragma unroll
+      for (int m = 0; m < NF; m++)
+        if (m != 4) sC[slot_of(m) * CRS + wc + ci] = F[m];
+#pragma unroll
+      for (int k = 0; k < NF; k++) sS[k * CRS + wc + ci] = q[k];
+    }
+  }
+  __syncwarp();
   const int fl = YDIR ? lane % T.bf : lane / T.bt, tl = YDIR ? lane / T.bf : lane % T.bt;
   const int f = 1 + tau * T.bf + fl, t = 2 + tb * T.bt + tl;
   if (tile < ntiles && f <= nf && t <= T.nt + 1) {
-    iface_adjoint<YDIR>(g, G, X, mask, lB, cL, inv_d, f, t, tid, sF, sFb, sQ);
+    // stencil point p of this face is cell (fl + p, tl)
+    const int ci0 = wc + (YDIR ? tl * T.cl + fl : fl * T.bt + tl);
+    const int cstep = YDIR ? 1 : T.bt;
+    iface_adjoint<YDIR>(g, G, mask, lB, cL, inv_d, f, t, tid, sC, sS, ci0, cstep, sFb, sQ);
   } else {
 #pragma unroll
     for (int c = 0; c < 28; c++) sFb[c][tid] = 0.0;
