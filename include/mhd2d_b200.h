@@ -404,6 +404,14 @@ int mhd_adj_set_store( mhd_adj* a, long long max_bytes );
    needs mask memory for its stored stages only.  Changing it discards the
    recording. */
 int mhd_adj_set_masks( mhd_adj* a, int keep_all );
+/* enable 1 (the default): the reverse sweep (interface adjoint, gather,
+   boundary transpose) is compiled with FMA contraction; the midpoint states
+   it recomputes keep the recording's rounding, so it differentiates the
+   recorded branches.  0: the parity build's rounding throughout, which is
+   the rounding of a plain FP64 tangent-linear model of the same map.  The
+   two gradients differ by rounding amplified by the eigen-system's
+   conditioning (1e-8 relative near B_perp = 0).  The recording is kept. */
+int mhd_adj_set_contract( mhd_adj* a, int enable );
 /* Initial state from the host (Dirichlet sides take their edges from it). */
 int mhd_adj_upload( mhd_adj* a, const double* U0 );
 /* Initial state generated on the device (kinds of mhd_batch_init_problem). */

@@ -55,40 +55,54 @@ __device__ __forceinline__ double flip(double x, unsigned m) {
   return __hiloint2double(__double2hiint(x) ^ (int)m, __double2loint(x));
 }
 
+// Products of midpoint().  A translation unit compiled with FMA contraction
+// that must still take the uncontracted builds' branches at the midpoint
+// (the discrete adjoint's reverse sweep recomputes the recording's midpoint)
+// defines MHD_MIDPOINT_UNFUSED: __dmul_rn is never fused into an FMA, so the
+// midpoint keeps the parity build's rounding there.  Elsewhere MP_MUL is the
+// plain product.
+#ifdef MHD_MIDPOINT_UNFUSED
+#define MP_MUL(a, b) __dmul_rn((a), (b))
+#else
+#define MP_MUL(a, b) ((a) * (b))
+#endif
+
 // Returns false on non-positive midpoint density (the reference's
 // ErrorNegativeDensity, spatialmethodeno.cpp:307-310).
 __device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const double* U2, Mid& e) {
   const double gm = G.gm;
-  const double r = 0.5 * (U1[0] + U2[0]);
-  e.u = 0.5 * (U1[1] / U1[0] + U2[1] / U2[0]);
-  e.v = 0.5 * (U1[2] / U1[0] + U2[2] / U2[0]);
-  e.w = 0.5 * (U1[3] / U1[0] + U2[3] / U2[0]);
-  const double bx = 0.5 * (U1[4] + U2[4]);
-  const double by = 0.5 * (U1[5] + U2[5]);
-  const double bz = 0.5 * (U1[6] + U2[6]);
+  const double r = MP_MUL(0.5, U1[0] + U2[0]);
+  e.u = MP_MUL(0.5, U1[1] / U1[0] + U2[1] / U2[0]);
+  e.v = MP_MUL(0.5, U1[2] / U1[0] + U2[2] / U2[0]);
+  e.w = MP_MUL(0.5, U1[3] / U1[0] + U2[3] / U2[0]);
+  const double bx = MP_MUL(0.5, U1[4] + U2[4]);
+  const double by = MP_MUL(0.5, U1[5] + U2[5]);
+  const double bz = MP_MUL(0.5, U1[6] + U2[6]);
   if (r <= 0.0) return false;
   const double u = e.u, v = e.v, w = e.w;
-  e.uu = u * u + v * v + w * w;
-  const double bb = bx * bx + by * by + bz * bz;
-  const double mml = U1[1] * U1[1] + U1[2] * U1[2] + U1[3] * U1[3];
-  const double bbl = U1[4] * U1[4] + U1[5] * U1[5] + U1[6] * U1[6];
-  const double mmr = U2[1] * U2[1] + U2[2] * U2[2] + U2[3] * U2[3];
-  const double bbr = U2[4] * U2[4] + U2[5] * U2[5] + U2[6] * U2[6];
-  const double ptl = (gm - 1.0) * (U1[7] - 0.5 * mml / U1[0] - 0.5 * bbl) + 0.5 * bbl;
-  const double ptr = (gm - 1.0) * (U2[7] - 0.5 * mmr / U2[0] - 0.5 * bbr) + 0.5 * bbr;
-  const double pt = 0.5 * (ptl + ptr);
-  double p = pt - 0.5 * bb;
+  e.uu = MP_MUL(u, u) + MP_MUL(v, v) + MP_MUL(w, w);
+  const double bb = MP_MUL(bx, bx) + MP_MUL(by, by) + MP_MUL(bz, bz);
+  const double mml = MP_MUL(U1[1], U1[1]) + MP_MUL(U1[2], U1[2]) + MP_MUL(U1[3], U1[3]);
+  const double bbl = MP_MUL(U1[4], U1[4]) + MP_MUL(U1[5], U1[5]) + MP_MUL(U1[6], U1[6]);
+  const double mmr = MP_MUL(U2[1], U2[1]) + MP_MUL(U2[2], U2[2]) + MP_MUL(U2[3], U2[3]);
+  const double bbr = MP_MUL(U2[4], U2[4]) + MP_MUL(U2[5], U2[5]) + MP_MUL(U2[6], U2[6]);
+  const double ptl =
+      MP_MUL(gm - 1.0, U1[7] - MP_MUL(0.5, mml) / U1[0] - MP_MUL(0.5, bbl)) + MP_MUL(0.5, bbl);
+  const double ptr =
+      MP_MUL(gm - 1.0, U2[7] - MP_MUL(0.5, mmr) / U2[0] - MP_MUL(0.5, bbr)) + MP_MUL(0.5, bbr);
+  const double pt = MP_MUL(0.5, ptl + ptr);
+  double p = pt - MP_MUL(0.5, bb);
   e.negp = 0;
   if (p < 0.0) { p = 0.0; e.negp = 1; }
 
-  double a2 = gm * p / r;
+  double a2 = MP_MUL(gm, p) / r;
   if (a2 < 0.0) a2 = 0.0;
   e.a2 = a2;
   e.a = sqrt(a2);
-  e.ca2 = bx * bx / r;
+  e.ca2 = MP_MUL(bx, bx) / r;
   e.ca = sqrt(e.ca2);
-  const double c2 = 0.5 * (bb / r + a2);
-  double ct = c2 * c2 - a2 * e.ca2;
+  const double c2 = MP_MUL(0.5, bb / r + a2);
+  double ct = MP_MUL(c2, c2) - MP_MUL(a2, e.ca2);
   if (ct < 0.0) ct = 0.0;
   const double sct = sqrt(ct);
   double cs2 = c2 - sct;
@@ -99,7 +113,7 @@ __device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const d
   e.cf2 = cf2; e.cf = sqrt(cf2);
 
   e.rr = sqrt(r);
-  const double bp2 = by * by + bz * bz;
+  const double bp2 = MP_MUL(by, by) + MP_MUL(bz, bz);
   e.sbxm = (bx < 0.0) ? 0x80000000u : 0u;
   const bool deg = (bp2 < SMALL) && (fabs(e.ca2 - a2) < SMALL);
   double af2 = deg ? 1.0 : (cf2 - e.ca2) / (cf2 - cs2);
@@ -117,9 +131,11 @@ __device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const d
     e.btz = G.rs2;
   }
   const double g21 = G.g21;
-  e.th1 = 1.0 / (af2 * a2 * (cf2 - g21 * a2) + as2 * cf2 * (cs2 - g21 * a2));
-  e.th2 = 1.0 / (flip(af2 * e.cf * e.a, e.sbxm) + flip(as2 * e.cs * e.ca, e.sbxm));
-  e.vb = e.bty * v + e.btz * w;
+  e.th1 = 1.0 / (MP_MUL(MP_MUL(af2, a2), cf2 - MP_MUL(g21, a2)) +
+                 MP_MUL(MP_MUL(as2, cf2), cs2 - MP_MUL(g21, a2)));
+  e.th2 = 1.0 / (flip(MP_MUL(MP_MUL(af2, e.cf), e.a), e.sbxm) +
+                 flip(MP_MUL(MP_MUL(as2, e.cs), e.ca), e.sbxm));
+  e.vb = MP_MUL(e.bty, v) + MP_MUL(e.btz, w);
 
   const bool sgnbt_pos = (by > 0.0) || (fabs(by) < SMALL && (bz > 0.0));
   const unsigned bt = sgnbt_pos ? 0u : 0x80000000u;

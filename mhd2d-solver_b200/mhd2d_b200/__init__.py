@@ -182,6 +182,7 @@ def library():
         "mhd_adj_destroy": [vp],
         "mhd_adj_set_store": [vp, C.c_longlong],
         "mhd_adj_set_masks": [vp, C.c_int],
+        "mhd_adj_set_contract": [vp, C.c_int],
         "mhd_adj_last_error": [vp, C.c_char_p, C.c_size_t, _ip],
         "mhd_adj_upload": [vp, _dp],
         "mhd_adj_init_problem": [vp, C.c_int, _dp, C.c_int],

@@ -62,6 +62,11 @@ class Adjoint:
         """Keep the ENO codes of every stage (True) or of stored stages only."""
         self._check(self.lib.mhd_adj_set_masks(self.h, 1 if keep_all else 0), "set_masks")
 
+    def set_contract(self, enable=True):
+        """Reverse sweep with FMA contraction (True, the default) or with the
+        parity build's rounding throughout (False).  The recording is kept."""
+        self._check(self.lib.mhd_adj_set_contract(self.h, 1 if enable else 0), "set_contract")
+
     # -- initial state ---------------------------------------------------------------
     def upload(self, U0):
         self._check(self.lib.mhd_adj_upload(self.h, _p(np.ascontiguousarray(U0))), "upload")
