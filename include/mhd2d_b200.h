@@ -201,6 +201,26 @@ typedef struct {
 int mhd_run( mhd_ctx* ctx, const mhd_run_params* p, mhd_nongrid_record* records,
              int max_records, mhd_run_result* result );
 
+/* The reference's binary grid dump of the context's current state, packed
+   on the device: the records outputGridDataBinary writes
+   (file_access.cpp:1193-1325) after toNaturalData (conversions.cpp:37-57),
+   with outputGridData's div B rules (file_access.cpp:1530-1677: Neumann and
+   open sides leave their edge cells at 0, periodic sides read periodic B
+   ghosts).  nx*ny records in i-major order of x, y, rho, [u, v, w, p if
+   natural], Bx, By, Bz, |div B|, [mx, my, mz, e if conservation], as
+   doubles or (single = 1) floats: the bytes the reference fwrites.  out:
+   host or device memory of out_bytes; *bytes (optional) gets the size, and
+   out = NULL only asks for it.  The state is not changed. */
+typedef struct {
+   int    natural;          /* [output] natural */
+   int    conservation;     /* [output] conservation */
+   int    single;           /* 1: binary floats, 0: binary doubles */
+   double start_x, start_y; /* grid origin (t_params start_x, start_y) */
+} mhd_grid_pack_params;
+
+int mhd_grid_pack( mhd_ctx* ctx, const mhd_grid_pack_params* p, void* out, size_t out_bytes,
+                   size_t* bytes );
+
 /* Counters of the last integrate / step: clamped midpoint pressures
    (the reference's "negative pressure" warning count) and kernel launches. */
 int mhd_get_counters( mhd_ctx* ctx, long long* neg_pressure, long long* launches );

@@ -13,6 +13,7 @@
 
 #include "../../include/mhd2d_b200.h"
 #include "mhd_launch.h"
+#include "mhd_output.h"
 #include "mhd_tma.cuh"
 #include "mhd_trace.h"
 
@@ -113,6 +114,8 @@ struct mhd_ctx {
   long long* hgcnt = nullptr;  // pinned mirror
   double* gdts = nullptr;      // device: dt of every completed step
   int gdts_cap = 0;
+  void* grid_buf = nullptr;    // device: packed grid-dump records (mhd_grid_pack)
+  size_t grid_buf_bytes = 0;
 };
 
 namespace {
@@ -632,6 +635,7 @@ int mhd_ctx_destroy(mhd_ctx* c) {
   if (c->ctl) cudaFree(c->ctl);
   if (c->hctl) cudaFreeHost(c->hctl);
   if (c->hnan) cudaFreeHost(c->hnan);
+  if (c->grid_buf) cudaFree(c->grid_buf);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return MHD_OK;
@@ -944,6 +948,36 @@ int mhd_get_counters(mhd_ctx* c, long long* neg_pressure, long long* launches) {
   if (neg_pressure) *neg_pressure = c->neg_pressure;
   if (launches) *launches = c->launches;
   return MHD_OK;
+}
+
+int mhd_grid_pack(mhd_ctx* c, const mhd_grid_pack_params* p, void* out, size_t out_bytes,
+                  size_t* bytes) {
+  MHD_TRACE("mhd_grid_pack");
+  if (!c || !p) return MHD_ERR_WRONG_PARAMETER;
+  const auto flag = [](int v) { return v == 0 || v == 1; };
+  if (!flag(p->natural) || !flag(p->conservation) || !flag(p->single))
+    return set_status(c, MHD_ERR_WRONG_PARAMETER, true, "mhd_grid_pack: flags must be 0 or 1");
+  const size_t need = size_t(output::grid_fields(p->natural, p->conservation)) * size_t(c->g.nx) *
+                      size_t(c->g.ny) * (p->single ? sizeof(float) : sizeof(double));
+  if (bytes) *bytes = need;
+  if (!out) return set_status(c, MHD_OK, false, "");  // size query
+  if (out_bytes < need)
+    return set_status(c, MHD_ERR_WRONG_PARAMETER, true, "mhd_grid_pack: output buffer too small");
+  CK(cudaSetDevice(c->device));
+  if (c->grid_buf_bytes < need) {
+    if (c->grid_buf) CK(cudaFree(c->grid_buf));
+    c->grid_buf = nullptr;
+    c->grid_buf_bytes = 0;
+    CK(cudaMalloc(&c->grid_buf, need));
+    c->grid_buf_bytes = need;
+  }
+  output::launch_grid_pack(c->g, c->U, p->natural != 0, p->conservation != 0, p->single != 0,
+                           p->start_x, p->start_y, c->grid_buf, c->stream);
+  CK(cudaPeekAtLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(out, c->grid_buf, need, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return set_status(c, MHD_OK, false, "");
 }
 
 int mhd_layout(const mhd_ctx* c, int* pitch, int* row_offset) {

@@ -99,6 +99,13 @@ class NongridRecord(C.Structure):
                 ("values", C.c_double * 7)]
 
 
+class GridPackParams(C.Structure):
+    """mhd_grid_pack_params."""
+
+    _fields_ = [("natural", C.c_int), ("conservation", C.c_int), ("single", C.c_int),
+                ("start_x", C.c_double), ("start_y", C.c_double)]
+
+
 class RunResult(C.Structure):
     """mhd_run_result."""
 
@@ -152,6 +159,8 @@ def library():
         "mhd_get_characteristics": [vp, _dp, _dp, _dp, _dp],
         "mhd_divb_calc": [vp, _dp, _dp],
         "mhd_nongrid_data": [vp, _dp],
+        "mhd_grid_pack": [vp, C.POINTER(GridPackParams), C.c_void_p, C.c_size_t,
+                          C.POINTER(C.c_size_t)],
         "mhd_set_tile_tma": [C.c_int, C.POINTER(C.c_longlong)],
         "mhd_set_sor_fused": [vp, C.c_int],
         "mhd_run": [vp, C.POINTER(RunParams), C.POINTER(NongridRecord), C.c_int,
@@ -347,6 +356,19 @@ class Context:
         out = np.zeros(7)
         self._check(self.lib.mhd_nongrid_data(self.h, _p(out)), "nongrid_data")
         return tuple(float(x) for x in out)
+
+    def grid_records(self, natural=True, conservation=True, single=False, start_x=0.0,
+                     start_y=0.0):
+        """The reference's binary grid dump of the state (mhd_grid_pack), as bytes."""
+        gp = GridPackParams(int(natural), int(conservation), int(single), start_x, start_y)
+        n = C.c_size_t(0)
+        self._check(self.lib.mhd_grid_pack(self.h, C.byref(gp), None, 0, C.byref(n)),
+                    "grid_pack")
+        buf = (C.c_char * n.value)()
+        st = self.lib.mhd_grid_pack(self.h, C.byref(gp), buf, n.value, None)
+        if st != OK:
+            raise MhdError(f"grid_pack: {self.last_status(st).message}")
+        return bytes(buf)
 
     def divb_sor(self, params):
         sw = C.c_int(0)

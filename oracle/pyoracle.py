@@ -27,6 +27,7 @@ ORACLE_SO = os.path.join(HERE, "_build", "libmhdoracle.so")
 TLM_SO = os.path.join(HERE, "_build", "libmhdtlm.so")
 REF_SO = os.path.join(HERE, "_ref", "libmhdref.so")
 REF_BENCH = os.path.join(HERE, "_ref", "ref_bench")
+REFIO_SO = os.path.join(HERE, "_ref", "libmhdrefio.so")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -121,6 +122,40 @@ def tlm_run(U0, dU0, nx, ny, dx, dy, gamma, bc, nsteps, dt0, time_method=2, dt_m
 
 def reference_available():
     return os.path.exists(REF_SO)
+
+
+def grid_writer_available():
+    return os.path.exists(REFIO_SO)
+
+
+_refio = None
+
+
+def ref_grid_records(U, dx, dy, gamma, bc, start_x=0.0, start_y=0.0, natural=True,
+                     conservation=True, binary_double=True):
+    """The bytes the reference's outputGridData writes for state U (its
+    binary grid dump, file_access.cpp:1193-1325), from oracle/_ref/libmhdrefio.so.
+    U is copied first: the writer overwrites B ghosts in place."""
+    global _refio
+    if _refio is None:
+        if not os.path.exists(REFIO_SO):
+            raise FileNotFoundError(f"{REFIO_SO} missing: run `make -C oracle ref`")
+        lib = C.CDLL(REFIO_SO)
+        lib.ref_grid_records.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_double, _ip, _dp, C.c_int, C.c_int,
+                                         C.c_int, C.c_void_p, C.c_longlong]
+        lib.ref_grid_records.restype = C.c_longlong
+        _refio = lib
+    W = np.ascontiguousarray(U, dtype=np.float64).copy()
+    _, NX, NY = W.shape
+    fields = 7 + (4 if natural else 0) + (4 if conservation else 0)
+    cap = fields * (NX - 4) * (NY - 4) * 8
+    buf = (C.c_char * cap)()
+    n = _refio.ref_grid_records(NX - 4, NY - 4, dx, dy, gamma, start_x, start_y, _bc(bc), _p(W),
+                                int(natural), int(conservation), int(binary_double), buf, cap)
+    if n < 0:
+        raise RuntimeError("ref_grid_records failed")
+    return bytes(buf[:n])
 
 
 def load_reference(fresh=False):
