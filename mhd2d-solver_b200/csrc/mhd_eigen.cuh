@@ -67,10 +67,23 @@ __device__ __forceinline__ double flip(double x, unsigned m) {
 #define MP_MUL(a, b) ((a) * (b))
 #endif
 
+// The midpoint state from the averaged density r, velocity (in e.u, e.v,
+// e.w), field (bx, by, bz) and total pressure pt.
+__device__ __forceinline__ bool midpoint_rest(const Gas& G, double r, double bx, double by,
+                                              double bz, double pt, Mid& e);
+
+// One side's total pressure as the midpoint forms it: (gamma - 1)(E -
+// |m|^2 / (2 rho) - |B|^2 / 2) + |B|^2 / 2.  The sums of squares are
+// frame-independent (the y frame swaps two of the terms of an addition).
+__device__ __forceinline__ double side_total_pressure(double gm, const double* q) {
+  const double mm = MP_MUL(q[1], q[1]) + MP_MUL(q[2], q[2]) + MP_MUL(q[3], q[3]);
+  const double bb = MP_MUL(q[4], q[4]) + MP_MUL(q[5], q[5]) + MP_MUL(q[6], q[6]);
+  return MP_MUL(gm - 1.0, q[7] - MP_MUL(0.5, mm) / q[0] - MP_MUL(0.5, bb)) + MP_MUL(0.5, bb);
+}
+
 // Returns false on non-positive midpoint density (the reference's
 // ErrorNegativeDensity, spatialmethodeno.cpp:307-310).
 __device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const double* U2, Mid& e) {
-  const double gm = G.gm;
   const double r = MP_MUL(0.5, U1[0] + U2[0]);
   e.u = MP_MUL(0.5, U1[1] / U1[0] + U2[1] / U2[0]);
   e.v = MP_MUL(0.5, U1[2] / U1[0] + U2[2] / U2[0]);
@@ -79,18 +92,42 @@ __device__ __forceinline__ bool midpoint(const Gas& G, const double* U1, const d
   const double by = MP_MUL(0.5, U1[5] + U2[5]);
   const double bz = MP_MUL(0.5, U1[6] + U2[6]);
   if (r <= 0.0) return false;
+  const double pt = MP_MUL(0.5, side_total_pressure(G.gm, U1) + side_total_pressure(G.gm, U2));
+  return midpoint_rest(G, r, bx, by, bz, pt, e);
+}
+
+// Per-cell part of the midpoint (the cell's velocity components and total
+// pressure, P = (u, v, w, pt) in x-frame order) for midpoint_p.
+__device__ __forceinline__ void cell_primitives(double gm, const double* q, double* P) {
+  P[0] = q[1] / q[0];
+  P[1] = q[2] / q[0];
+  P[2] = q[3] / q[0];
+  P[3] = side_total_pressure(gm, q);
+}
+
+// midpoint() from the two sides' cell_primitives (P1, P2 in the interface's
+// frame): the same values in the same operations, the per-side divisions
+// done once per cell.
+__device__ __forceinline__ bool midpoint_p(const Gas& G, const double* U1, const double* U2,
+                                           const double* P1, const double* P2, Mid& e) {
+  const double r = MP_MUL(0.5, U1[0] + U2[0]);
+  e.u = MP_MUL(0.5, P1[0] + P2[0]);
+  e.v = MP_MUL(0.5, P1[1] + P2[1]);
+  e.w = MP_MUL(0.5, P1[2] + P2[2]);
+  const double bx = MP_MUL(0.5, U1[4] + U2[4]);
+  const double by = MP_MUL(0.5, U1[5] + U2[5]);
+  const double bz = MP_MUL(0.5, U1[6] + U2[6]);
+  if (r <= 0.0) return false;
+  const double pt = MP_MUL(0.5, P1[3] + P2[3]);
+  return midpoint_rest(G, r, bx, by, bz, pt, e);
+}
+
+__device__ __forceinline__ bool midpoint_rest(const Gas& G, double r, double bx, double by,
+                                              double bz, double pt, Mid& e) {
+  const double gm = G.gm;
   const double u = e.u, v = e.v, w = e.w;
   e.uu = MP_MUL(u, u) + MP_MUL(v, v) + MP_MUL(w, w);
   const double bb = MP_MUL(bx, bx) + MP_MUL(by, by) + MP_MUL(bz, bz);
-  const double mml = MP_MUL(U1[1], U1[1]) + MP_MUL(U1[2], U1[2]) + MP_MUL(U1[3], U1[3]);
-  const double bbl = MP_MUL(U1[4], U1[4]) + MP_MUL(U1[5], U1[5]) + MP_MUL(U1[6], U1[6]);
-  const double mmr = MP_MUL(U2[1], U2[1]) + MP_MUL(U2[2], U2[2]) + MP_MUL(U2[3], U2[3]);
-  const double bbr = MP_MUL(U2[4], U2[4]) + MP_MUL(U2[5], U2[5]) + MP_MUL(U2[6], U2[6]);
-  const double ptl =
-      MP_MUL(gm - 1.0, U1[7] - MP_MUL(0.5, mml) / U1[0] - MP_MUL(0.5, bbl)) + MP_MUL(0.5, bbl);
-  const double ptr =
-      MP_MUL(gm - 1.0, U2[7] - MP_MUL(0.5, mmr) / U2[0] - MP_MUL(0.5, bbr)) + MP_MUL(0.5, bbr);
-  const double pt = MP_MUL(0.5, ptl + ptr);
   double p = pt - MP_MUL(0.5, bb);
   e.negp = 0;
   if (p < 0.0) { p = 0.0; e.negp = 1; }

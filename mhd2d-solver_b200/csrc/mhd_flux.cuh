@@ -24,6 +24,15 @@
 #include "mhd_eigen.cuh"
 #include "mhd_tma.cuh"
 
+// Per-cell primitives in the tile (sP: u, v, w and the midpoint formula's
+// total pressure), computed once per cell in phase 1 instead of once per
+// interface side.  The fast build forms them with one reciprocal of the
+// density; the parity build (MHD_PARITY_CELL_PRIM) with the reference's own
+// divisions and operation order, so the midpoint (midpoint_p) is bit-identical.
+#if defined(MHD_FAST) || defined(MHD_PARITY_CELL_PRIM)
+#define MHD_CELL_PRIM 1
+#endif
+
 #ifndef MHD_MINB
 #define MHD_MINB 2
 #endif
@@ -71,8 +80,8 @@ struct TileGeom {
   static constexpr int OFF_G = OFF_F + 7 * RU * TJ;        // sG[7][TI][CU], slots in y frame order
   static constexpr int OFF_FX = OFF_G + 7 * TI * CU;       // sFx[8][TI+1][TJ]
   static constexpr int OFF_GY = OFF_FX + 8 * (TI + 1) * TJ;  // sGy[8][TI][TJ+1], y frame order
-#ifdef MHD_FAST
-  // fast build: per-cell primitives sP[4][RU][CU] (u, v, w, total pressure)
+#ifdef MHD_CELL_PRIM
+  // per-cell primitives sP[4][RU][CU] (u, v, w, total pressure)
   static constexpr int OFF_P = OFF_GY + 8 * TI * (TJ + 1);
   static constexpr int TOTAL = OFF_P + 4 * RU * CU;
 #else
@@ -162,7 +171,7 @@ struct Lane {
   int qplane, qstep;
   bool swp;          // y interface: x/y roles swapped
   int l1, l2;        // stencil points of U1 / U2 (1 / 2, or open-boundary substitutes)
-#ifdef MHD_FAST
+#ifdef MHD_CELL_PRIM
   const double* p;   // primitives (u, v, w, pt) of point l at p[k*qplane + l*qstep]
   __device__ __forceinline__ double P(int k, int l) const {
     return p[(swp && k < 2 ? 1 - k : k) * qplane + l * qstep];
@@ -519,7 +528,7 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
     U2[k] = L.Q(k, L.l2);
   }
   Mid e;
-#ifdef MHD_FAST
+#ifdef MHD_CELL_PRIM
   if (!DENSE) {
     double P1[4], P2[4];
 #pragma unroll
@@ -527,7 +536,11 @@ __device__ __forceinline__ bool interface_flux(const Gas& G, const Lane& L, cons
       P1[k] = L.P(k, L.l1);
       P2[k] = L.P(k, L.l2);
     }
+#ifdef MHD_FAST
     if (!midpoint_fast(G, U1, U2, P1, P2, e)) return false;
+#else
+    if (!midpoint_p(G, U1, U2, P1, P2, e)) return false;
+#endif
   } else if (!midpoint(G, U1, U2, e)) {
     return false;
   }
