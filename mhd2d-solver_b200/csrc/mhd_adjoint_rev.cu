@@ -339,6 +339,12 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
   }
 }
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may be scheduled before the previous kernel
+// of its stream has finished; it waits here, before touching memory that
+// kernel writes or reads.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Per cell: sum the interface contributions of both directions and apply the
 // transposed flux Jacobians.  Two lanes per cell (an even / odd lane pair):
 // the even lane takes the x direction, the odd lane the y direction; the
@@ -531,6 +537,7 @@ __device__ __forceinline__ void adj_bc_divb(const Grid& g, int side, int c,
 // order at the corners.
 __global__ void ka_adj_bc(Grid g, int ydir, const double* __restrict__ T, double* __restrict__ D,
                           double* __restrict__ lsnap_lo, double* __restrict__ lsnap_hi) {
+  pdl_wait();
   const int nb = ydir ? g.nx : g.ny;  // boundary cells along the sides
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= NF * nb) return;
@@ -576,10 +583,23 @@ void launch_gather(const Grid& g, const GasConsts& gc, const double* X, const do
                                                                   in_buf, lU, lU1, lU2);
 }
 
+// The boundary transposes are a few thousand threads each: launched as
+// programmatic dependents of the kernel before them (ka_adj_bc waits in
+// pdl_wait), their launch latency overlaps that kernel's tail.
 void launch_bc(const Grid& g, int ydir, const double* T, double* D, double* lsnap_lo,
                double* lsnap_hi, cudaStream_t st) {
   const int nb = ydir ? g.nx : g.ny;
-  K::ka_adj_bc<<<(NF * nb + 127) / 128, 128, 0, st>>>(g, ydir, T, D, lsnap_lo, lsnap_hi);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((NF * nb + 127) / 128);
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, K::ka_adj_bc, g, ydir, T, D, lsnap_lo, lsnap_hi);
 }
 
 }  // namespace MHD_ADJREV
