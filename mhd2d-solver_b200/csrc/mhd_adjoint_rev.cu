@@ -58,8 +58,8 @@ __device__ __forceinline__ long long cell_at(const Grid& g, bool ydir, int k, in
   return ydir ? g.at(k, t, f - 1 + p) : g.at(k, f - 1 + p, t);
 }
 
-constexpr int AIB = 64;  // threads per block of ka_adj_iface (37 KB of shared memory)
-constexpr int AIB_MIN = 6;  // resident blocks per SM: 168 registers, 6 x 37 KB shared
+constexpr int AIB = 64;  // threads per block of ka_adj_iface (31 KB of shared memory)
+constexpr int AIB_MIN = 6;  // resident blocks per SM: 168 registers, 6 x 31 KB shared
 
 // Interface tiles of ka_adj_iface: each warp takes BF consecutive faces
 // along the direction times BT transverse cells (BF * BT = 32 threads) and
@@ -75,10 +75,14 @@ struct ITile {
 constexpr int BF_X = 4, BF_Y = 32;
 // a cell is then touched by the stencils of at most two tiles (the gather reads two records)
 static_assert(BF_X >= 3 && BF_Y >= 3 && 32 % BF_X == 0 && 32 % BF_Y == 0, "interface tile shape");
-// stencil cells of one warp's tile, and the row stride of the per-block cell arrays
+// Stencil cells of one warp's tile (NCW), and the warp's shared-memory
+// region: the cells' frame fluxes (7 x NCW), primitives (4 x NCW) and frame
+// states (8 x NCW).  Once the warp's interfaces are done with the fluxes and
+// primitives, their first 16 x 32 doubles hold the lanes' U1 / U2 adjoints.
 constexpr int NCW = (BF_X + 3) * (32 / BF_X) > (BF_Y + 3) * (32 / BF_Y) ? (BF_X + 3) * (32 / BF_X)
                                                                       : (BF_Y + 3) * (32 / BF_Y);
-constexpr int CRS = (AIB / 32) * NCW;
+constexpr int WOFF_P = 7 * NCW, WOFF_S = 11 * NCW, WREG = 19 * NCW;
+static_assert(16 * 32 <= WOFF_S, "U1 / U2 adjoints fit over the fluxes and primitives");
 constexpr int NPW = 15;  // scratch words per cell record: 7 flux-adjoint slots, 8 state adjoints
 
 __host__ __device__ inline ITile itile(const Grid& g, bool ydir) {
@@ -105,11 +109,12 @@ __host__ __device__ inline long long rec_at(const ITile& T, bool ydir, int w, in
 
 // Adjoint of the numerical flux of one interface f at transverse cell t
 // (the interface's frame is the x frame: y interfaces work on x/y-swapped
-// states, as the forward does).  The frame fluxes and states of its 4
-// stencil points come from the tile's cell arrays (point p: entry ci0 +
-// p * cstep of sC / sS).  Leaves in the thread's columns of sFb the adjoints
-// of the frame fluxes of the 4 stencil points (row 7p + slot(m)) and in sQ
-// the adjoints of the frame states U1 (rows 0-7) and U2 (8-15).
+// states, as the forward does).  The frame fluxes, primitives and states of
+// its 4 stencil points come from the warp's cell arrays at wr (point p: cell
+// ci0 + p * cstep); the midpoint is formed from the primitives (midpoint_p),
+// as the recording's flux kernel forms it.  Leaves in the thread's column of
+// sFb the adjoints of the frame fluxes of the 4 stencil points (row 7p +
+// slot(m)) and adds the adjoints of the frame states U1, U2 to U1b, U2b.
 //
 // The characteristics are walked in pairs (0, 6), (2, 4), (1, 5), (3):
 // rows k and 6 - k share a symmetric part, so the adjoint of the pair's
@@ -120,9 +125,12 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
                                               const unsigned* __restrict__ mask,
                                               const double* __restrict__ lB, double cL,
                                               double inv_d, int f, int t, int tid,
-                                              const double* __restrict__ sC,
-                                              const double* __restrict__ sS, int ci0, int cstep,
-                                              double (*sFb)[AIB], double (*sQ)[AIB]) {
+                                              const double* __restrict__ wr, int ci0,
+                                              int cstep, double (*sFb)[AIB], double* U1b,
+                                              double* U2b) {
+  const double* sC = wr;           // frame fluxes of the warp's cells
+  const double* sP = wr + WOFF_P;  // their primitives
+  const double* sS = wr + WOFF_S;  // their frame states
   const int ncell = YDIR ? g.ny : g.nx;
   const int lo_bc = YDIR ? BOTTOM : LEFT, hi_bc = YDIR ? TOP : RIGHT;
   const int l1 = (g.bc_of(lo_bc) == OPEN && f < 2) ? 2 : 1;
@@ -143,18 +151,19 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
       v += inv_d * (cL * lB[YDIR ? g.at(kk, t, cell_hi) : g.at(kk, cell_hi, t)]);
     lF[m] = v;
   }
-  double U1[NF], U2[NF];
+  double U1[NF], U2[NF], P1[4], P2[4];
 #pragma unroll
   for (int k = 0; k < NF; k++) {
-    U1[k] = sS[k * CRS + ci0 + l1 * cstep];
-    U2[k] = sS[k * CRS + ci0 + l2 * cstep];
+    U1[k] = sS[k * NCW + ci0 + l1 * cstep];
+    U2[k] = sS[k * NCW + ci0 + l2 * cstep];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    P1[k] = sP[k * NCW + ci0 + l1 * cstep];
+    P2[k] = sP[k * NCW + ci0 + l2 * cstep];
   }
   Mid e0;
-  if (!midpoint(G, U1, U2, e0)) {  // sFb is still zero
-#pragma unroll
-    for (int k = 0; k < 16; k++) sQ[k][tid] = 0.0;
-    return;
-  }
+  if (!midpoint_p(G, U1, U2, P1, P2, e0)) return;  // sFb, U1b, U2b stay zero
   const unsigned mw = mask[YDIR ? (long long)t * g.NY + f : (long long)f * g.NY + t];
   MidBar mb{};
 #pragma unroll 1
@@ -190,7 +199,7 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
       for (int m = 0; m < NF; m++) {
         if (m == 4) { phi[m] = 0.0; continue; }
         const int s = slot_of(m);
-        phi[m] = ca * sC[s * CRS + ci0 + pa * cstep] + cb * sC[s * CRS + ci0 + (pa + 1) * cstep];
+        phi[m] = ca * sC[s * NCW + ci0 + pa * cstep] + cb * sC[s * NCW + ci0 + (pa + 1) * cstep];
         fw += l[m] * phi[m];
       }
 #pragma unroll
@@ -224,19 +233,11 @@ __device__ __forceinline__ void iface_adjoint(const Grid& g, const Gas& G,
     const volatile double* vq = sS;
 #pragma unroll
     for (int k = 0; k < NF; k++) {
-      U1[k] = vq[k * CRS + ci0 + l1 * cstep];
-      U2[k] = vq[k * CRS + ci0 + l2 * cstep];
+      U1[k] = vq[k * NCW + ci0 + l1 * cstep];
+      U2[k] = vq[k * NCW + ci0 + l2 * cstep];
     }
   }
-  double U1b[NF], U2b[NF];
-#pragma unroll
-  for (int k = 0; k < NF; k++) { U1b[k] = 0.0; U2b[k] = 0.0; }
   midpoint_adjoint(G, e0, U1, U2, mb, U1b, U2b);
-#pragma unroll
-  for (int k = 0; k < NF; k++) {
-    sQ[k][tid] = U1b[k];
-    sQ[8 + k][tid] = U2b[k];
-  }
 }
 
 // Adjoint of the numerical flux of every interface of one direction, one
@@ -250,49 +251,59 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
     ka_adj_iface(Grid g, Gas G, const double* __restrict__ X, const unsigned* __restrict__ mask,
                  const double* __restrict__ lB, double cL, double* __restrict__ S,
                  double inv_d) {
-  __shared__ double sC[7 * CRS];    // frame fluxes of the tiles' stencil cells
-  __shared__ double sS[NF * CRS];   // their frame states
+  __shared__ double sW[(AIB / 32) * WREG];  // per warp: its cells' fluxes, primitives, states
   __shared__ double sFb[28][AIB];  // per interface: adjoints of its 4 stencil points' fluxes
-  __shared__ double sQ[16][AIB];   // per interface: adjoints of U1, U2 (frame)
-  const int tid = threadIdx.x, lane = tid & 31, wbase = tid - lane;
-  const int wc = (tid / 32) * NCW;  // the warp's cells in sC / sS
+  const int tid = threadIdx.x, lane = tid & 31;
+  double* wr = sW + (tid / 32) * WREG;
+  double* sQ = wr;  // [16][32]: the lanes' U1 / U2 adjoints, after the interfaces
   const ITile T = itile(g, YDIR);
   const int nf = YDIR ? g.ny + 1 : g.nx + 1, ncell = nf - 1;
   const long long tile = (long long)blockIdx.x * (AIB / 32) + tid / 32;
   const long long ntiles = (long long)T.ntile * ((T.nt + T.bt - 1) / T.bt);
   const int tau = int(tile % T.ntile), tb = int(tile / T.ntile);
   // the tile's stencil cells (c, tl2), cell tau*bf + c along the direction:
-  // states and fluxes once per cell (each is a stencil point of up to 4 faces)
+  // states, primitives and fluxes once per cell (each is a stencil point of
+  // up to 4 faces)
   if (tile < ntiles) {
     for (int ci = lane; ci < T.cl * T.bt; ci += 32) {
       const int c = YDIR ? ci % T.cl : ci / T.bt, tl2 = YDIR ? ci / T.cl : ci % T.bt;
       const int a = tau * T.bf + c, t2 = 2 + tb * T.bt + tl2;
       if (a > ncell + 3 || t2 > T.nt + 1) continue;  // read by no interface
-      double q[NF], F[NF], Gy[NF];
+      double q[NF], F[NF], Gy[NF], P[4];
 #pragma unroll
       for (int k = 0; k < NF; k++)
         q[k] = X[YDIR ? g.at(swap_xy(k), t2, a) : g.at(k, a, t2)];
       phys_flux(G.gm, q, F, Gy);
+      cell_primitives(G.gm, q, P);
 #pragma unroll
       for (int m = 0; m < NF; m++)
-        if (m != 4) sC[slot_of(m) * CRS + wc + ci] = F[m];
+        if (m != 4) wr[slot_of(m) * NCW + ci] = F[m];
 #pragma unroll
-      for (int k = 0; k < NF; k++) sS[k * CRS + wc + ci] = q[k];
+      for (int k = 0; k < 4; k++) wr[WOFF_P + k * NCW + ci] = P[k];
+#pragma unroll
+      for (int k = 0; k < NF; k++) wr[WOFF_S + k * NCW + ci] = q[k];
     }
   }
   __syncwarp();
   const int fl = YDIR ? lane % T.bf : lane / T.bt, tl = YDIR ? lane / T.bf : lane % T.bt;
   const int f = 1 + tau * T.bf + fl, t = 2 + tb * T.bt + tl;
+  double U1b[NF], U2b[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) { U1b[k] = 0.0; U2b[k] = 0.0; }
   if (tile < ntiles && f <= nf && t <= T.nt + 1) {
     // stencil point p of this face is cell (fl + p, tl)
-    const int ci0 = wc + (YDIR ? tl * T.cl + fl : fl * T.bt + tl);
+    const int ci0 = YDIR ? tl * T.cl + fl : fl * T.bt + tl;
     const int cstep = YDIR ? 1 : T.bt;
-    iface_adjoint<YDIR>(g, G, mask, lB, cL, inv_d, f, t, tid, sC, sS, ci0, cstep, sFb, sQ);
+    iface_adjoint<YDIR>(g, G, mask, lB, cL, inv_d, f, t, tid, wr, ci0, cstep, sFb, U1b, U2b);
   } else {
 #pragma unroll
     for (int c = 0; c < 28; c++) sFb[c][tid] = 0.0;
+  }
+  __syncwarp();  // every lane is done with the fluxes and primitives sQ overwrites
 #pragma unroll
-    for (int k = 0; k < 16; k++) sQ[k][tid] = 0.0;
+  for (int k = 0; k < NF; k++) {
+    sQ[k * 32 + lane] = U1b[k];
+    sQ[(8 + k) * 32 + lane] = U2b[k];
   }
   __syncwarp();
   if (tile >= ntiles) return;
@@ -316,7 +327,8 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
     for (int p = 0; p < 4; p++) {
       const int fl2 = c - p;
       if (fl2 < 0 || fl2 >= T.bf) continue;
-      const int th = wbase + (YDIR ? tl2 * T.bf + fl2 : fl2 * T.bt + tl2);
+      const int tw = YDIR ? tl2 * T.bf + fl2 : fl2 * T.bt + tl2;  // the face's lane
+      const int th = (tid - lane) + tw;
 #pragma unroll
       for (int w = 0; w < 7; w++) fb[w] += sFb[7 * p + w][th];
       const int f2 = 1 + tau * T.bf + fl2;
@@ -324,11 +336,11 @@ __global__ void __launch_bounds__(AIB, AIB_MIN)
       const int l2 = (open_hi && f2 > ncell) ? 1 : 2;
       if (p == l1) {
 #pragma unroll
-        for (int k = 0; k < NF; k++) qb[k] += sQ[k][th];
+        for (int k = 0; k < NF; k++) qb[k] += sQ[k * 32 + tw];
       }
       if (p == l2) {
 #pragma unroll
-        for (int k = 0; k < NF; k++) qb[k] += sQ[8 + k][th];
+        for (int k = 0; k < NF; k++) qb[k] += sQ[(8 + k) * 32 + tw];
       }
     }
     double* r = S + rec_at(T, YDIR, 0, tau, c, t2);
