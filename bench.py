@@ -66,6 +66,10 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-complete-stride", type=int, default=8,
                     help="runs to completion: every k-th run of the mix (1: all 512; 0: skip)")
+    ap.add_argument("--cleaning-steps", type=int, default=3,
+                    help="config 2's div-B cleaning at 512^2: steps timed (0: off)")
+    ap.add_argument("--cleaning-full", type=int, default=1,
+                    help="also one step with cleaning at the headline size (to the sweep cap)")
     ap.add_argument("--adjoint-steps", type=int, default=2000,
                     help="steps of the plasma-sheet adjoint measurement (0: skip it)")
     ap.add_argument("--adjoint-grid", default="1024x512")
@@ -555,6 +559,38 @@ def central_fd_measure(dev, n):
             "note": "3 state passes of 64 B per cell each; HBM-bound"}
 
 
+def cleaning_measure(dev, n, steps, rsteps=100000):
+    """Config 2's div-B cleaning: Orszag-Tang n^2, RK3 ENO-Roe steps, each
+    followed by one red-black SOR solve (omega 1.7 static, stop at
+    r_max/phi_max <= 1e-10, at most rsteps sweeps; main.cpp:207-242 with one
+    solve per step).  Per step: the step's and the solve's wall time (each
+    call returns to the host), the sweeps and the status of the solve, and
+    max|div B| after it."""
+    import mhd2d_b200 as M
+    from mhd2d_b200 import problems as P
+
+    p = P.ot_vortex(n)
+    ctx = M.Context(p.nx, p.ny, p.dx, p.dy, p.gamma, p.bc, scheme=M.ENO_ROE, time_method=M.RK3,
+                    device=dev, dt_min=1e-6, dt_max=0.03125, cfl=0.4)
+    ctx.upload(p.U)
+    sp = M.sor_params(1, 1, rsteps, 1e-10, 0.0, True, 1.7)
+    dt = 0.03125
+    rows = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        st, dt = ctx.step(dt)
+        t1 = time.perf_counter()
+        cst, divb, sweeps = ctx.divb_clean(sp)
+        t2 = time.perf_counter()
+        rows.append({"step_ms": (t1 - t0) * 1e3, "clean_ms": (t2 - t1) * 1e3, "sweeps": sweeps,
+                     "status": cst.status, "max_divb": divb})
+    ctx.close()
+    return {"workload": f"orszag-tang {n}x{n}, eno-roe, rk3, red-black SOR every step "
+                        f"(omega 1.7, r_max/phi_max <= 1e-10, at most {rsteps} sweeps)",
+            "steps": rows,
+            "ms_per_sweep": sum(r["clean_ms"] for r in rows) / max(1, sum(r["sweeps"] for r in rows))}
+
+
 def adjoint_wave_plan(specs, steps, K, budget):
     """Instances packed into waves whose recordings fit in `budget` bytes of
     device memory together, with every stage input kept (no segment replays):
@@ -855,6 +891,14 @@ def run_ours(args):
     cfd = central_fd_measure(dev, n)
     if rank == 0:
         line["central_fd"] = cfd
+    if args.cleaning_steps > 0:
+        # config 2 with its cleaning at 512^2, where the solve converges, and one
+        # step of it at the headline size, where it runs to the sweep cap
+        cl = {"converging": cleaning_measure(dev, 512, args.cleaning_steps)}
+        if args.cleaning_full:
+            cl["full_size"] = cleaning_measure(dev, n, 1)
+        if rank == 0:
+            line["cleaning"] = cl
     if args.batch_runs > 0:
         bm = batched_measure(dev, args.batch_runs, args.batch_steps, world=world, rank=rank)
         if args.batch_complete_stride > 0:

@@ -160,6 +160,12 @@ int mhd_nongrid_data( mhd_ctx* ctx, double out[7] );
    potential, followed by the B correction.  *sweeps gets the sweep count. */
 int mhd_divb_sor( mhd_ctx* ctx, const mhd_sor_params* p, int* sweeps );
 
+/* enable 1 (the default): the sweep loop of an SOR solve runs as one CUDA
+   graph launch (a device-side while loop over passes of 16 sweeps, ended by
+   the solve's own stop rule); 0: passes issued from the host, which reads the
+   stop flag after each.  The same sweeps and values either way. */
+int mhd_set_sor_graph( mhd_ctx* ctx, int enable );
+
 /* The cleaning loop of main.cpp:207-242 (up to sor_steps solves until
    max|div B| < sor_divbmax), final max|div B| in *maxdivb. */
 int mhd_divb_clean( mhd_ctx* ctx, const mhd_sor_params* p, double* maxdivb, int* total_sweeps );

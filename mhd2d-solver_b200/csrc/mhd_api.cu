@@ -23,9 +23,24 @@ namespace {
 // Counters of a graph step loop (mhd_ctx::gcnt).
 enum : int { G_STEPS = 0, G_RETRIES = 1, G_WANTED = 2, G_STEP_RETRIES = 3, G_NEG = 4, G_COUNT = 5 };
 // RK3 passes of one step the device loop allows: every retry restarts from
-// min(dt1, dt2, dt3), strictly below the dt it replaces, and the power-of-two
-// ladder of a double has fewer rungs than this, so a valid run never gets here
+// min(dt1, dt2, dt3), strictly below the dt it replaces, and a step retries a
+// few times in practice; a step that has not settled after this many passes
+// ends the loop with MHD_ERR_NOT_CONVERGED (the host loop has no bound)
 constexpr long long kGraphRetryBound = 4096;
+
+// SOR sweeps per pass of the device solve loop (mhd_set_sor_graph).
+constexpr int kSorChunk = 16;
+
+// After each pass of the SOR graph: go on while the solve has not met its
+// stop rule (the sweeps turn into no-ops once it has: r_max/phi_max <= rmax
+// or the sweep cap), at most `bound` passes.
+__global__ void k_sor_again(const Ctl* c, long long* cnt, long long bound,
+                            cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const long long n = *cnt + 1;
+  *cnt = n;
+  cudaGraphSetConditional(h, (!c->sor_done && n < bound) ? 1u : 0u);
+}
 
 // Before the retry loop and at the end of each retry pass: run another pass
 // while the controller asks for one.
@@ -116,6 +131,13 @@ struct mhd_ctx {
   int gdts_cap = 0;
   void* grid_buf = nullptr;    // device: packed grid-dump records (mhd_grid_pack)
   size_t grid_buf_bytes = 0;
+  // an SOR solve's sweep loop as one CUDA graph (a while node over passes of
+  // kSorChunk sweeps); rebuilt when the solve parameters it bakes in change
+  int use_sor_graph = 1;
+  cudaGraphExec_t sor_graph = nullptr;
+  double sor_graph_key[4] = {0.0, 0.0, 0.0, 0.0};  // rmax, sweep cap, omega, fused
+  long long* sor_cnt = nullptr;  // device: passes the SOR graph ran
+  long long sor_graph_launches = 0;  // kernels per pass
 };
 
 namespace {
@@ -451,6 +473,69 @@ int do_divb_calc(mhd_ctx* c, double* mx, double* tot) {
   return MHD_OK;
 }
 
+// The sweep loop of one SOR solve on the device: a graph with a while node
+// whose body is kSorChunk sweeps and k_sor_again.  It replaces the host loop's
+// passes of kSorChunk sweeps and its read of the stop flag after each; the
+// sweeps, their order and their values are the same.
+int sor_graph_solve(mhd_ctx* c, const int r[4], const double coef[6], double rmax,
+                    double max_sweeps, int fused) {
+  const double key[4] = {rmax, max_sweeps, coef[5], double(fused)};
+  if (c->sor_graph && std::memcmp(key, c->sor_graph_key, sizeof key) != 0) {
+    cudaGraphExecDestroy(c->sor_graph);
+    c->sor_graph = nullptr;
+  }
+  if (!c->sor_cnt) CK(cudaMalloc(&c->sor_cnt, sizeof(long long)));
+  if (!c->sor_graph) {
+    const double passes = std::ceil(max_sweeps / kSorChunk) + 1.0;
+    const long long bound = passes < 9.0e18 ? (long long)passes : (long long)9.0e18;
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h{};
+    cudaGraph_t body = nullptr;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      cudaGraphNodeParams np{};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+      if (e == cudaSuccess) body = np.conditional.phGraph_out[0];
+    }
+    const long long l0 = c->launches;
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      for (int s = 0; s < kSorChunk; s++)
+        c->ks->sor_sweep(c->g, c->phi, c->sor_xy, r, coef, rmax, max_sweeps, c->ratio, c->ctl,
+                         fused, c->stream);
+      k_sor_again<<<1, 32, 0, c->stream>>>(c->ctl, c->sor_cnt, bound, h);
+      cudaGraph_t out = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(c->stream, &out);
+      if (e == cudaSuccess) e = e2;
+    }
+    c->sor_graph_launches = (long long)kSorChunk * (fused ? 2 : 5) + 1;
+    c->launches = l0;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&c->sor_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      c->sor_graph = nullptr;
+      cudaGetLastError();
+      return cuda_fail(c, e, "sor_graph_solve");
+    }
+    std::memcpy(c->sor_graph_key, key, sizeof key);
+  }
+  CK(cudaMemsetAsync(c->sor_cnt, 0, sizeof(long long), c->stream));
+  CK(cudaGraphLaunch(c->sor_graph, c->stream));
+  long long passes = 0;
+  CK(cudaMemcpyAsync(&passes, c->sor_cnt, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  const int st = read_ctl(c);  // synchronizes the stream
+  c->launches += 1 + passes * c->sor_graph_launches;
+  return st;
+}
+
 int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
   MHD_TRACE("divBCorrectionSOR");
   touch_buf(c, 0);  // the B correction changes U's interior
@@ -480,7 +565,7 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
   CK(cudaMemsetAsync(&c->ctl->sor_done, 0, 3 * sizeof(int), c->stream));  // + sor_ticket
   CK(cudaMemcpyAsync(c->ratio, &nan_ratio, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   long long issued = 0;
-  const int chunk = 16;
+  const int chunk = kSorChunk;
   // fused sweeps: 2 launches per sweep instead of 5 (same arithmetic, same
   // values; see sor_fused_ok), with the ghosts refreshed around the solve
   const int fused = sor_fused_ok(g) && c->sor_fused ? 1 : 0;
@@ -489,16 +574,21 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
       c->ks->phi_bc(g, c->phi, c->ctl, c->stream);
       c->launches += 1;
     }
-    for (;;) {
-      for (int s = 0; s < chunk; s++) {
-        c->ks->sor_sweep(g, c->phi, c->sor_xy, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio,
-                         c->ctl, fused, c->stream);
-        c->launches += fused ? 2 : 5;
-      }
-      issued += chunk;
-      int st = read_ctl(c);
+    if (c->use_sor_graph) {
+      const int st = sor_graph_solve(c, r, coef, p->sor_rmax, p->sor_rsteps, fused);
       if (st) return st;
-      if (c->hctl->sor_done) break;
+    } else {
+      for (;;) {
+        for (int s = 0; s < chunk; s++) {
+          c->ks->sor_sweep(g, c->phi, c->sor_xy, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio,
+                           c->ctl, fused, c->stream);
+          c->launches += fused ? 2 : 5;
+        }
+        issued += chunk;
+        int st = read_ctl(c);
+        if (st) return st;
+        if (c->hctl->sor_done) break;
+      }
     }
     if (fused) {
       c->ks->phi_bc(g, c->phi, c->ctl, c->stream);
@@ -636,6 +726,8 @@ int mhd_ctx_destroy(mhd_ctx* c) {
   if (c->hctl) cudaFreeHost(c->hctl);
   if (c->hnan) cudaFreeHost(c->hnan);
   if (c->grid_buf) cudaFree(c->grid_buf);
+  if (c->sor_graph) cudaGraphExecDestroy(c->sor_graph);
+  if (c->sor_cnt) cudaFree(c->sor_cnt);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return MHD_OK;
@@ -948,6 +1040,12 @@ int mhd_get_counters(mhd_ctx* c, long long* neg_pressure, long long* launches) {
   if (neg_pressure) *neg_pressure = c->neg_pressure;
   if (launches) *launches = c->launches;
   return MHD_OK;
+}
+
+int mhd_set_sor_graph(mhd_ctx* c, int enable) {
+  if (!c || (enable != 0 && enable != 1)) return MHD_ERR_WRONG_PARAMETER;
+  c->use_sor_graph = enable;
+  return set_status(c, MHD_OK, false, "");
 }
 
 int mhd_grid_pack(mhd_ctx* c, const mhd_grid_pack_params* p, void* out, size_t out_bytes,

@@ -227,6 +227,31 @@ def test_sor_fused_sweeps_match_unfused_and_oracle(shape, bc, fusable):
 
 @pytest.mark.parametrize("shape,bc", [((200, 136), (1, 1, 1, 1)), ((150, 97), (3, 4, 2, 3)),
                                       ((64, 256), (4, 4, 1, 1))])
+@pytest.mark.parametrize("rsteps", [7, 16, 33, 20000])
+def test_sor_graph_matches_host_loop(shape, bc, rsteps):
+    """The sweep loop as one graph launch (the default) against passes issued
+    from the host: the same status, sweep count and corrected field over two
+    warm-started solves, with sweep caps below, at and past one pass of 16
+    sweeps and a solve left to converge; a second context changes the sweep
+    cap between solves (the graph is rebuilt)."""
+    p = P.random_smooth(*shape, seed=shape[1] + rsteps, bc=bc)
+    sp = M.sor_params(1, 3, rsteps, 1e-10, 1e-10, True, 1.7)
+    ctxs = [make_ctx(p, flags=0), make_ctx(p, flags=0)]
+    ctxs[1].set_sor_graph(False)
+    for _ in range(2):
+        res = [ctx.divb_sor(sp) for ctx in ctxs]
+        assert (res[0][0].status, res[0][1]) == (res[1][0].status, res[1][1])
+        assert same(ctxs[0].download(), ctxs[1].download())
+    sp2 = M.sor_params(1, 3, rsteps + 5, 1e-10, 1e-10, True, 1.6)
+    res = [ctx.divb_sor(sp2) for ctx in ctxs]
+    assert (res[0][0].status, res[0][1]) == (res[1][0].status, res[1][1])
+    assert same(ctxs[0].download(), ctxs[1].download())
+    for ctx in ctxs:
+        ctx.close()
+
+
+@pytest.mark.parametrize("shape,bc", [((200, 136), (1, 1, 1, 1)), ((150, 97), (3, 4, 2, 3)),
+                                      ((64, 256), (4, 4, 1, 1))])
 @pytest.mark.parametrize("rsteps", [7, 8, 20000])
 def test_sor_sweep_forms_on_larger_grids(shape, bc, rsteps):
     """The default sweeps (two launches where every periodic extent is a
