@@ -155,24 +155,28 @@ void l_sor_sweep(const Grid& g, double* phi, const double* xy, const int range[4
                  Ctl* ctl, int fused, cudaStream_t s) {
   DivRange R{range[0], range[1], range[2], range[3]};
   SorCoef c{coef[0], coef[1], coef[2], coef[3], coef[4], coef[5]};
-  dim3 grid((sor_pairs(R) + SOR_THREADS - 1) / SOR_THREADS,
-            (R.x1 - R.x0 + SOR_ROWS - 1) / SOR_ROWS);
+  // rows per block: SOR_ROWS, halved while the grid would have fewer than 4
+  // blocks per SM of a B200 (148 SMs)
+  const int bx = (sor_pairs(R) + SOR_THREADS - 1) / SOR_THREADS, rows = R.x1 - R.x0;
+  int rpb = SOR_ROWS;
+  while (rpb > 1 && (long long)bx * ((rows + rpb - 1) / rpb) < 4LL * 148) rpb /= 2;
+  dim3 grid(bx, (rows + rpb - 1) / rpb);
   const int m = g.nx > g.ny ? g.nx : g.ny;
   const double4* f = reinterpret_cast<const double4*>(xy);
   if (fused) {
     k_sor_half<true><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, rtol, max_sweeps,
-                                                  last_ratio);
+                                                  last_ratio, rpb);
     k_sor_half<true><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, rtol, max_sweeps,
-                                                  last_ratio);
+                                                  last_ratio, rpb);
     return;
   }
   // ghosts are refreshed after each colour: with periodic sides they mirror
   // points of the other colour (see k_sor_half)
   k_sor_half<false><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 0, ctl, rtol, max_sweeps,
-                                                 last_ratio);
+                                                 last_ratio, rpb);
   k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 0);
   k_sor_half<false><<<grid, SOR_THREADS, 0, s>>>(g, phi, f, R, c, 1, ctl, rtol, max_sweeps,
-                                                 last_ratio);
+                                                 last_ratio, rpb);
   k_phi_bc<<<grid1d(2LL * m, 256), 256, 0, s>>>(g, phi, ctl, 0);
   k_sor_check<<<1, 32, 0, s>>>(ctl, rtol, max_sweeps, last_ratio);
 }

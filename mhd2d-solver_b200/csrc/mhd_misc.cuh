@@ -405,8 +405,9 @@ struct SorCoef {
   double pxf, pyf, bxf, byf, coef, omega;
 };
 
-// Rows per block of k_sor_half: each block reduces its update / potential
-// maxima over SOR_ROWS rows before its two atomics.
+// Rows per block of k_sor_half (at most): each block reduces its update /
+// potential maxima over its rows before its two atomics.  Small grids take
+// fewer rows per block so that the half sweep still spreads over the SMs.
 constexpr int SOR_ROWS = 8;
 constexpr int SOR_THREADS = 128;
 
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
                                                           const double4* __restrict__ xy,
                                                           DivRange R, SorCoef s, int color,
                                                           Ctl* c, double rtol, double max_sweeps,
-                                                          double* last_ratio) {
+                                                          double* last_ratio, int rpb) {
   if (c->sor_done) return;
   __shared__ double red[2][SOR_THREADS / 32];
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -478,8 +479,8 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
   const long long P = g.pitch;
   double rmax = 0.0, pmax = 0.0;
   if (q < Q) {
-    for (int rr = 0; rr < SOR_ROWS; rr++) {
-      const int ir = blockIdx.y * SOR_ROWS + rr;
+    for (int rr = 0; rr < rpb; rr++) {
+      const int ir = blockIdx.y * rpb + rr;
       const int i = R.x0 + ir;
       if (i >= R.x1) break;
       const int jb = 2 * (2 * q + ((color + (i >> 1)) & 1));
