@@ -160,6 +160,12 @@ int mhd_nongrid_data( mhd_ctx* ctx, double out[7] );
    potential, followed by the B correction.  *sweeps gets the sweep count. */
 int mhd_divb_sor( mhd_ctx* ctx, const mhd_sor_params* p, int* sweeps );
 
+/* enable 1 (the default): mhd_step_host copies the host state in row bands
+   on a second stream, and the first spatial operator (ENO-Roe, grids of at
+   least 32 tile rows) starts on the bands already copied; 0: one copy, then
+   the step.  Bit-identical either way. */
+int mhd_set_step_host_banded( mhd_ctx* ctx, int enable );
+
 /* enable 1 (the default): the sweep loop of an SOR solve runs as one CUDA
    graph launch (a device-side while loop over passes of 16 sweeps, ended by
    the solve's own stop rule); 0: passes issued from the host, which reads the

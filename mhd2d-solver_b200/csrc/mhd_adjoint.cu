@@ -372,7 +372,7 @@ void launch_flux(mhd_adj* a, const double* X, unsigned* slot) {
   tile_tma_launches() += use_tma;
   kern<<<grid, ANW * 32, AGeom::TMA_BYTES, a->stream>>>(g, X, a->UL, a->aF, a->aG, 1.0 / g.dx,
                                                      1.0 / g.dy, a->G, a->ctl, co, slot,
-                                                     slot + (size_t)g.NX * g.NY, tm, use_tma);
+                                                     slot + (size_t)g.NX * g.NY, tm, use_tma, 0);
   a->launches++;
 }
 

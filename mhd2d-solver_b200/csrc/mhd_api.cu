@@ -138,6 +138,10 @@ struct mhd_ctx {
   double sor_graph_key[4] = {0.0, 0.0, 0.0, 0.0};  // rmax, sweep cap, omega, fused
   long long* sor_cnt = nullptr;  // device: passes the SOR graph ran
   long long sor_graph_launches = 0;  // kernels per pass
+  // mhd_step_host: the host state is copied in row bands on copy_stream
+  int use_banded_h2d = 1;  // mhd_set_step_host_banded
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t band_ev[9] = {};  // [0]: the main stream's work before the copy; [1..8]: bands
 };
 
 namespace {
@@ -209,6 +213,81 @@ void enqueue_integrate(mhd_ctx* c, double* X, bool chars) {
   c->chars_buf = X == c->U ? 0 : (X == c->U1 ? 1 : (X == c->U2 ? 2 : -1));
 }
 
+// Row bands of mhd_step_host's copy of the host state.
+constexpr int kStepHostBands = 8;
+
+// The first spatial operator of a step whose state arrives from host memory:
+// the state is copied in kStepHostBands row bands on copy_stream, and on the
+// main stream each band is followed by the bottom / top ghost fill of the
+// rows it completes and the flux tile rows whose cells (ghosts included)
+// are then all in place.  After the last band: the left / right ghost fill
+// and the remaining tile rows (the first, which reads the left ghost rows,
+// and the last ones).  Every tile and every ghost value is computed as in
+// enqueue_integrate (the same kernels on the same inputs), so the results are
+// bit-identical; the copy of the later bands overlaps the earlier tiles.
+// ENO-Roe only: ENO-LF needs its dissipation coefficients from the whole grid
+// first.
+int enqueue_integrate_from_host(mhd_ctx* c, const double* Uh, bool chars) {
+  MHD_TRACE("L(U) from host");
+  const Grid& g = c->g;
+  if (!c->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : c->band_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  if (c->chars_buf == 0) c->chars_buf = -1;  // new interior for U
+  // the copy overwrites U: after the main stream's work on it so far
+  CK(cudaEventRecord(c->band_ev[0], c->stream));
+  CK(cudaStreamWaitEvent(c->copy_stream, c->band_ev[0], 0));
+  const int tr = c->ks->flux_tile_rows(c->scheme);
+  const int nti = (g.nx + tr - 1) / tr;
+  double* const* ch = chars ? c->ch : nullptr;
+  int ydone = 2;  // bottom / top ghosts filled for rows [2, ydone)
+  int tdone = 1;  // tile rows [1, tdone) launched
+  for (int b = 0; b < kStepHostBands; b++) {
+    const int r0 = int((long long)b * g.NX / kStepHostBands);
+    const int r1 = int((long long)(b + 1) * g.NX / kStepHostBands);
+    for (int k = 0; k < NF; k++)
+      CK(cudaMemcpy2DAsync(c->U + k * g.fstride + (long long)r0 * g.pitch + g.off,
+                           g.pitch * sizeof(double), Uh + ((long long)k * g.NX + r0) * g.NY,
+                           g.NY * sizeof(double), g.NY * sizeof(double), size_t(r1 - r0),
+                           cudaMemcpyHostToDevice, c->copy_stream));
+    CK(cudaEventRecord(c->band_ev[1 + b], c->copy_stream));
+    CK(cudaStreamWaitEvent(c->stream, c->band_ev[1 + b], 0));
+    // rows [0, r1) are on the device; a row's bottom / top ghosts read its
+    // neighbour rows too (Neumann div B terms)
+    const int yhi = std::min(r1 - 1, g.nx + 2);
+    if (yhi > ydone) {
+      c->ks->bc_part(g, c->U, c->snap, c->ctl, 2, ydone, yhi, c->stream);
+      c->launches += 1;
+      ydone = yhi;
+    }
+    // tile row t reads cell rows [t*tr, t*tr + tr + 4): all filled, none a right ghost row
+    const int ready = std::min(ydone, g.nx + 2);
+    const int thi = ready >= tr + 4 ? (ready - tr - 4) / tr + 1 : 0;
+    if (thi > tdone) {
+      c->ks->flux_rows(c->scheme, g, c->U, c->UL, c->aF, c->aG, c->ctl, ch, tdone, thi,
+                       c->stream);
+      c->launches += 1;
+      tdone = thi;
+    }
+  }
+  c->ks->bc_part(g, c->U, c->snap, c->ctl, 1, 0, 0, c->stream);
+  c->launches += 1;
+  if (ydone < g.nx + 2) {
+    c->ks->bc_part(g, c->U, c->snap, c->ctl, 2, ydone, g.nx + 2, c->stream);
+    c->launches += 1;
+  }
+  c->ks->flux_rows(c->scheme, g, c->U, c->UL, c->aF, c->aG, c->ctl, ch, 0, 1, c->stream);
+  c->launches += 1;
+  if (tdone < nti) {
+    c->ks->flux_rows(c->scheme, g, c->U, c->UL, c->aF, c->aG, c->ctl, ch, tdone, nti,
+                     c->stream);
+    c->launches += 1;
+  }
+  c->chars_buf = 0;
+  return MHD_OK;
+}
+
 // The interior of buffer b (0 U, 1 U1, 2 U2) is about to change.
 void touch_buf(mhd_ctx* c, int b) {
   if (c->chars_buf == b) c->chars_buf = -1;
@@ -275,13 +354,20 @@ int step_status(mhd_ctx* c) {
 }
 
 // One full time step on the device state; dt in/out.
-int do_step(mhd_ctx* c, double* dt_inout) {
+// One time step.  Uh (optional): the state comes from host memory, copied
+// in row bands that the first spatial operator follows
+// (enqueue_integrate_from_host).
+int do_step(mhd_ctx* c, double* dt_inout, const double* Uh = nullptr) {
   MHD_TRACE("step");
   int st = check_bc_ready(c);
   if (st) return st;
   const bool chars = (c->flags & MHD_FLAG_CHARACTERISTICS) != 0;
   enqueue_control(c, PH_RESET_STEP, *dt_inout);
-  enqueue_integrate(c, c->U, c->time_method == 1 && chars);
+  if (Uh) {
+    if ((st = enqueue_integrate_from_host(c, Uh, c->time_method == 1 && chars))) return st;
+  } else {
+    enqueue_integrate(c, c->U, c->time_method == 1 && chars);
+  }
   if (c->time_method == 1) {
     enqueue_control(c, PH_EULER);
     enqueue_combine(c, 0);
@@ -728,6 +814,9 @@ int mhd_ctx_destroy(mhd_ctx* c) {
   if (c->grid_buf) cudaFree(c->grid_buf);
   if (c->sor_graph) cudaGraphExecDestroy(c->sor_graph);
   if (c->sor_cnt) cudaFree(c->sor_cnt);
+  for (cudaEvent_t& e : c->band_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return MHD_OK;
@@ -866,8 +955,16 @@ int mhd_step_host(mhd_ctx* c, double* U, double* dt_inout) {
   MHD_TRACE("mhd_step_host");
   if (!c || !U || !dt_inout) return MHD_ERR_WRONG_PARAMETER;
   CK(cudaSetDevice(c->device));
-  CK(h2d(c, c->U, U));
-  int st = do_step(c, dt_inout);
+  int st;
+  // ENO-Roe on grids of many tile rows: the copy of the state overlaps the
+  // first spatial operator (bit-identical; see enqueue_integrate_from_host)
+  const int tr = c->ks->flux_tile_rows(c->scheme);
+  if (c->scheme == 2 && c->use_banded_h2d && c->g.nx >= 4 * kStepHostBands * tr) {
+    st = do_step(c, dt_inout, U);
+  } else {
+    CK(h2d(c, c->U, U));
+    st = do_step(c, dt_inout);
+  }
   CK(d2h(c, U, c->U));
   CK(cudaStreamSynchronize(c->stream));
   return st;
@@ -1040,6 +1137,12 @@ int mhd_get_counters(mhd_ctx* c, long long* neg_pressure, long long* launches) {
   if (neg_pressure) *neg_pressure = c->neg_pressure;
   if (launches) *launches = c->launches;
   return MHD_OK;
+}
+
+int mhd_set_step_host_banded(mhd_ctx* c, int enable) {
+  if (!c || (enable != 0 && enable != 1)) return MHD_ERR_WRONG_PARAMETER;
+  c->use_banded_h2d = enable;
+  return set_status(c, MHD_OK, false, "");
 }
 
 int mhd_set_sor_graph(mhd_ctx* c, int enable) {

@@ -726,9 +726,9 @@ __global__ void __launch_bounds__(NW * 32, NW * 32 > 256 ? 1 : MHD_MINB)
 k_flux(Grid g, const double* __restrict__ U, double* __restrict__ UL,
        const double* __restrict__ alphaF, const double* __restrict__ alphaG,
        double inv_dx, double inv_dy, Gas G, Ctl* ctl, CharOut co, unsigned* maskX,
-       unsigned* maskY, const __grid_constant__ CUtensorMap tmU, int use_tma) {
+       unsigned* maskY, const __grid_constant__ CUtensorMap tmU, int use_tma, int ti0) {
   if (ctl->skip) return;
-  const int tj = blockIdx.x, ti = blockIdx.y;
+  const int tj = blockIdx.x, ti = ti0 + blockIdx.y;  // ti0: first tile row of this launch
 #define MHD_TILE_TMA 1
 #include "mhd_flux_tile.inc"
 #undef MHD_TILE_TMA

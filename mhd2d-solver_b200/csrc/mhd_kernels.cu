@@ -72,9 +72,10 @@ void l_lf_alpha(const Grid& g, const double* U, double* aF, double* aG, Ctl* ctl
   k_lf_alpha<<<grid, 256, 0, s>>>(g, U, aF, aG, ctl);
 }
 
+// Tile rows [ti0, ti1) of the spatial operator (ti1 < 0: to the last).
 template <int SCHEME, bool CHARS>
 void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const double* aG,
-            Ctl* ctl, double* const ch[4], cudaStream_t s) {
+            Ctl* ctl, double* const ch[4], cudaStream_t s, int ti0 = 0, int ti1 = -1) {
   constexpr int ti = FluxShape<SCHEME>::TI, nw = FluxShape<SCHEME>::NW;
   using Gm = TileGeom<ti, TJ>;
   auto kern = k_flux<SCHEME, CHARS, ti, TJ, nw>;
@@ -83,7 +84,10 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Gm::TMA_BYTES));
     attr = true;
   }
-  dim3 grid((g.ny + TJ - 1) / TJ, (g.nx + ti - 1) / ti);
+  const int nti = (g.nx + ti - 1) / ti;
+  if (ti1 < 0 || ti1 > nti) ti1 = nti;
+  if (ti1 <= ti0) return;
+  dim3 grid((g.ny + TJ - 1) / TJ, ti1 - ti0);
   CharOut co{ch ? ch[0] : nullptr, ch ? ch[1] : nullptr, ch ? ch[2] : nullptr,
              ch ? ch[3] : nullptr};
 #ifdef MHD_FAST
@@ -96,7 +100,7 @@ void flux_t(const Grid& g, const double* U, double* UL, const double* aF, const 
   const int use_tma = tile_tma_enabled() && make_box_map(g, U, Gm::CU, Gm::RU, &tm) ? 1 : 0;
   tile_tma_launches() += use_tma;
   kern<<<grid, nw * 32, Gm::TMA_BYTES, s>>>(g, U, UL, aF, aG, 1.0 / g.dx, 1.0 / g.dy, G, ctl, co,
-                                          nullptr, nullptr, tm, use_tma);
+                                          nullptr, nullptr, tm, use_tma, ti0);
 }
 
 void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
@@ -115,6 +119,33 @@ void l_flux(int scheme, const Grid& g, const double* U, double* UL, const double
     if (chars) flux_t<2, true>(g, U, UL, aF, aG, ctl, ch, s);
     else flux_t<2, false>(g, U, UL, aF, aG, ctl, ch, s);
   }
+}
+
+// Tile rows [ti0, ti1) of the ENO spatial operator (schemes 2 and 3; the
+// ENO-LF coefficients must be complete).
+void l_flux_rows(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
+                 const double* aG, Ctl* ctl, double* const ch[4], int ti0, int ti1,
+                 cudaStream_t s) {
+  const bool chars = ch && ch[0];
+  if (scheme == 3) {
+    if (chars) flux_t<3, true>(g, U, UL, aF, aG, ctl, ch, s, ti0, ti1);
+    else flux_t<3, false>(g, U, UL, aF, aG, ctl, ch, s, ti0, ti1);
+  } else {
+    if (chars) flux_t<2, true>(g, U, UL, aF, aG, ctl, ch, s, ti0, ti1);
+    else flux_t<2, false>(g, U, UL, aF, aG, ctl, ch, s, ti0, ti1);
+  }
+}
+
+int l_flux_tile_rows(int scheme) {
+  return scheme == 3 ? FluxShape<3>::TI : FluxShape<2>::TI;
+}
+
+void l_bc_part(const Grid& g, double* U, const double* const snap[4], const Ctl* ctl, int part,
+               int i0, int i1, cudaStream_t s) {
+  const Snap d{snap[0], snap[1], snap[2], snap[3]};
+  const long long n = part == 1 ? 2LL * 2 * NF * g.ny : 2LL * NF * (i1 - i0) * 2;
+  if (n <= 0) return;
+  k_bc_part<<<grid1d(n, 256), 256, 0, s>>>(g, U, d, ctl, part, i0, i1);
 }
 
 void l_combine(const Grid& g, int mode, double* U, double* U1, double* U2, const double* UL,
@@ -208,6 +239,7 @@ int l_launches(int scheme) { return scheme == 2 ? 2 : 3; }  // bc, [alpha], flux
 using namespace MHD_KNS;
 extern const KernelSet MHD_KSET = {MHD_KSET_NAME, l_bc, l_snapshot, l_lf_alpha, l_flux,
                                    l_combine, l_control, l_divb, l_sor_rhs, l_sor_sweep,
-                                   l_phi_bc, l_sor_correct, l_totals, l_smem, l_launches};
+                                   l_phi_bc, l_sor_correct, l_totals, l_smem, l_launches,
+                                   l_bc_part, l_flux_rows, l_flux_tile_rows};
 
 }  // namespace mhd

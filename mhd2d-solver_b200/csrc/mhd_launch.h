@@ -56,6 +56,16 @@ struct KernelSet {
   int (*totals)(const Grid& g, const double* U, double* partial, int max_blocks, cudaStream_t s);
   int (*flux_smem_bytes)();
   int (*launches_per_integrate)(int scheme);
+  // the boundary fill in parts (the same values as bc): part 1 the left /
+  // right sides, part 2 the bottom / top sides of rows [i0, i1) (2 <= i0,
+  // i1 <= nx + 2)
+  void (*bc_part)(const Grid& g, double* U, const double* const snap[4], const Ctl* ctl,
+                  int part, int i0, int i1, cudaStream_t s);
+  // tile rows [ti0, ti1) of the ENO spatial operator (flux_tile_rows cell rows each)
+  void (*flux_rows)(int scheme, const Grid& g, const double* U, double* UL, const double* aF,
+                    const double* aG, Ctl* ctl, double* const chars[4], int ti0, int ti1,
+                    cudaStream_t s);
+  int (*flux_tile_rows)(int scheme);
 };
 
 extern const KernelSet kExact;

@@ -117,6 +117,33 @@ __global__ void k_bc(Grid g, double* __restrict__ U, Snap d, const Ctl* ctl) {
     bc_elem(g, U, d, e);
 }
 
+// Part of the boundary fill, the same elements as k_bc: part 1 the left /
+// right sides (every field, row and layer); part 2 the bottom / top sides of
+// rows [i0, i1) only.  The two sides' values depend on interior cells only
+// (never on another side's ghosts), so the parts of a fill can run in any
+// order and at different times.
+__global__ void k_bc_part(Grid g, double* __restrict__ U, Snap d, const Ctl* ctl, int part,
+                          int i0, int i1) {
+  if (ctl->skip) return;
+  const long long nlr = 2LL * 2 * NF * g.ny;  // left / right elements come first
+  const long long n = part == 1 ? nlr : 2LL * NF * (i1 - i0) * 2;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    if (part == 1) {
+      bc_elem(g, U, d, q);
+      continue;
+    }
+    // q -> (side, field, row i, layer) with i in [i0, i1), layer fastest
+    long long r = q;
+    const int gl = int(r % 2); r /= 2;
+    const int ii = int(r % (i1 - i0)); r /= (i1 - i0);
+    const int k = int(r % NF);
+    const int side = int(r / NF);
+    const long long e = nlr + (((long long)side * NF + k) * g.nx + (i0 + ii - 2)) * 2 + gl;
+    bc_elem(g, U, d, e);
+  }
+}
+
 // Dirichlet edge snapshot (spatialintegrationmethod.cpp:39-59).
 __global__ void k_snapshot(Grid g, const double* __restrict__ U, double* l, double* r, double* b,
                            double* t) {

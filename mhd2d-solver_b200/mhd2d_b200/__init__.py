@@ -164,6 +164,7 @@ def library():
         "mhd_set_tile_tma": [C.c_int, C.POINTER(C.c_longlong)],
         "mhd_set_sor_fused": [vp, C.c_int],
         "mhd_set_sor_graph": [vp, C.c_int],
+        "mhd_set_step_host_banded": [vp, C.c_int],
         "mhd_run": [vp, C.POINTER(RunParams), C.POINTER(NongridRecord), C.c_int,
                     C.POINTER(RunResult)],
         "mhd_divb_sor": [vp, C.POINTER(SorParams), _ip],
@@ -403,6 +404,11 @@ class Context:
     def set_step_graph(self, enable):
         """steps() as one CUDA graph launch (default on) or one host round trip per step."""
         self._check(self.lib.mhd_set_step_graph(self.h, int(bool(enable))), "set_step_graph")
+
+    def set_step_host_banded(self, enable):
+        """step_host: banded host copy overlapping the first operator (default on) or one copy."""
+        self._check(self.lib.mhd_set_step_host_banded(self.h, int(bool(enable))),
+                    "set_step_host_banded")
 
     def set_sor_graph(self, enable):
         """SOR sweep loop as one CUDA graph launch (default on) or host-issued passes."""

@@ -1,0 +1,76 @@
+"""mhd_step_host, the step through host memory (the end-to-end call of the
+bench): with the banded copy (the first spatial operator follows the copied
+row bands) and with one copy, against device-resident steps, bit for bit,
+including the characteristics of an Euler step and the step's dt."""
+import numpy as np
+import pytest
+
+import mhd2d_b200 as M
+from mhd2d_b200 import problems as P
+from gpu_helpers import make_ctx, same
+
+pytestmark = pytest.mark.gpu
+
+BCS = [
+    (M.PERIODIC,) * 4,
+    (M.NEUMANN, M.OPEN, M.DIRICHLET, M.PERIODIC),
+    (M.OPEN, M.NEUMANN, M.NEUMANN, M.OPEN),
+    (M.DIRICHLET,) * 4,
+]
+
+
+def _host_steps(p, banded, nsteps, **kw):
+    ctx = make_ctx(p, **kw)
+    ctx.set_step_host_banded(banded)
+    U = np.ascontiguousarray(p.U.copy())
+    dt, dts = 1e-3, []
+    for _ in range(nsteps):
+        st, dt = ctx.step_host(U, dt)
+        assert not st.isError
+        dts.append(dt)
+    chars = ctx.characteristics() if kw.get("flags", 0) & M.FLAG_CHARACTERISTICS else None
+    ctx.close()
+    return U, dts, chars
+
+
+def _device_steps(p, nsteps, **kw):
+    ctx = make_ctx(p, **kw)
+    dt, dts = 1e-3, []
+    for _ in range(nsteps):
+        st, dt = ctx.step(dt)
+        assert not st.isError
+        dts.append(dt)
+    U = ctx.download()
+    chars = ctx.characteristics() if kw.get("flags", 0) & M.FLAG_CHARACTERISTICS else None
+    ctx.close()
+    return U, dts, chars
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("shape", [(320, 96), (231, 130)])
+def test_step_host_banded_matches_device_steps(bc, shape):
+    """ENO-Roe RK3 on grids of 33 to 46 tile rows: the banded copy, one copy
+    and device-resident steps give the same states and dts."""
+    p = P.random_smooth(*shape, seed=sum(bc) + shape[0], bc=bc)
+    kw = dict(scheme=M.ENO_ROE, dt_max=0.01, flags=0)
+    Ub, db, _ = _host_steps(p, True, 4, **kw)
+    Uo, do, _ = _host_steps(p, False, 4, **kw)
+    Ud, dd, _ = _device_steps(p, 4, **kw)
+    assert db == do == dd
+    assert same(Ub[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
+    assert same(Uo[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
+
+
+def test_step_host_banded_euler_characteristics_and_blocky_state():
+    """Euler with the characteristics flag (the first operator keeps them) on a
+    shocked state; the banded copy keeps them bit for bit."""
+    bc = (M.NEUMANN, M.NEUMANN, M.PERIODIC, M.PERIODIC)
+    p = P.random_blocky(300, 128, seed=3, bc=bc)
+    kw = dict(scheme=M.ENO_ROE, time_method=M.EULER, dt_max=0.002,
+              flags=M.FLAG_CHARACTERISTICS)
+    Ub, db, cb = _host_steps(p, True, 3, **kw)
+    Ud, dd, cd = _device_steps(p, 3, **kw)
+    assert db == dd
+    assert same(Ub[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
+    for a, b in zip(cb, cd):
+        assert same(a, b)
