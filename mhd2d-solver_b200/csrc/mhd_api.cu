@@ -246,13 +246,18 @@ int enqueue_integrate_from_host(mhd_ctx* c, const double* Uh, bool chars) {
   for (int b = 0; b < kStepHostBands; b++) {
     const int r0 = int((long long)b * g.NX / kStepHostBands);
     const int r1 = int((long long)(b + 1) * g.NX / kStepHostBands);
-    for (int k = 0; k < NF; k++)
-      CK(cudaMemcpy2DAsync(c->U + k * g.fstride + (long long)r0 * g.pitch + g.off,
-                           g.pitch * sizeof(double), Uh + ((long long)k * g.NX + r0) * g.NY,
-                           g.NY * sizeof(double), g.NY * sizeof(double), size_t(r1 - r0),
-                           cudaMemcpyHostToDevice, c->copy_stream));
-    CK(cudaEventRecord(c->band_ev[1 + b], c->copy_stream));
-    CK(cudaStreamWaitEvent(c->stream, c->band_ev[1 + b], 0));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < NF && e == cudaSuccess; k++)
+      e = cudaMemcpy2DAsync(c->U + k * g.fstride + (long long)r0 * g.pitch + g.off,
+                            g.pitch * sizeof(double), Uh + ((long long)k * g.NX + r0) * g.NY,
+                            g.NY * sizeof(double), g.NY * sizeof(double), size_t(r1 - r0),
+                            cudaMemcpyHostToDevice, c->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->band_ev[1 + b], c->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->band_ev[1 + b], 0);
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(c->copy_stream);  // no copy into U outlives the call
+      return cuda_fail(c, e, "mhd_step_host: banded copy");
+    }
     // rows [0, r1) are on the device; a row's bottom / top ghosts read its
     // neighbour rows too (Neumann div B terms)
     const int yhi = std::min(r1 - 1, g.nx + 2);

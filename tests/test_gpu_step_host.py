@@ -61,6 +61,19 @@ def test_step_host_banded_matches_device_steps(bc, shape):
     assert same(Uo[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
 
 
+def test_step_host_lf_and_central_fd_keep_one_copy():
+    """Schemes without the banded first operator (ENO-LF needs its whole-grid
+    coefficients first; central FD) take the one-copy path: the same states."""
+    bc = (M.PERIODIC, M.PERIODIC, M.NEUMANN, M.OPEN)
+    p = P.random_smooth(300, 64, seed=11, bc=bc)
+    for scheme in (M.ENO_LF, M.CENTRAL_FD):
+        kw = dict(scheme=scheme, dt_max=0.01, flags=0)
+        Ub, db, _ = _host_steps(p, True, 3, **kw)
+        Ud, dd, _ = _device_steps(p, 3, **kw)
+        assert db == dd
+        assert same(Ub[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
+
+
 def test_step_host_banded_euler_characteristics_and_blocky_state():
     """Euler with the characteristics flag (the first operator keeps them) on a
     shocked state; the banded copy keeps them bit for bit."""
