@@ -61,17 +61,16 @@ def test_step_host_banded_matches_device_steps(bc, shape):
     assert same(Uo[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
 
 
-def test_step_host_lf_and_central_fd_keep_one_copy():
-    """Schemes without the banded first operator (ENO-LF needs its whole-grid
-    coefficients first; central FD) take the one-copy path: the same states."""
+def test_step_host_lf_keeps_one_copy():
+    """ENO-LF (its dissipation coefficients come from the whole grid before
+    the first flux) takes the one-copy path: the same states and dts."""
     bc = (M.PERIODIC, M.PERIODIC, M.NEUMANN, M.OPEN)
     p = P.random_smooth(300, 64, seed=11, bc=bc)
-    for scheme in (M.ENO_LF, M.CENTRAL_FD):
-        kw = dict(scheme=scheme, dt_max=0.01, flags=0)
-        Ub, db, _ = _host_steps(p, True, 3, **kw)
-        Ud, dd, _ = _device_steps(p, 3, **kw)
-        assert db == dd
-        assert same(Ub[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
+    kw = dict(scheme=M.ENO_LF, dt_max=0.01, flags=0)
+    Ub, db, _ = _host_steps(p, True, 3, **kw)
+    Ud, dd, _ = _device_steps(p, 3, **kw)
+    assert db == dd
+    assert same(Ub[:, 2:-2, 2:-2], Ud[:, 2:-2, 2:-2])
 
 
 def test_step_host_banded_euler_characteristics_and_blocky_state():
