@@ -799,6 +799,11 @@ def run_ours(args):
     host = torch.empty((8, n + 4, n + 4), dtype=torch.float64, pin_memory=True).numpy()
     host[...] = ctx.download()
     e2e_steps = max(1, args.e2e_steps)
+    # one untimed call first: its first launches of the banded copy kernels
+    # and the copy stream's creation are set-up, not per-step cost
+    st, dt = ctx.step_host(host, dt)
+    if st.isError:
+        raise RuntimeError(st.message)
     barrier(world)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)

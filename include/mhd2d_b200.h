@@ -160,10 +160,13 @@ int mhd_nongrid_data( mhd_ctx* ctx, double out[7] );
    potential, followed by the B correction.  *sweeps gets the sweep count. */
 int mhd_divb_sor( mhd_ctx* ctx, const mhd_sor_params* p, int* sweeps );
 
-/* enable 1 (the default): mhd_step_host copies the host state in row bands
-   on a second stream, and the first spatial operator (ENO-Roe, grids of at
-   least 32 tile rows) starts on the bands already copied; 0: one copy, then
-   the step.  Bit-identical either way. */
+/* enable 1 (the default), on grids of at least 32 tile rows: mhd_step_host
+   copies the host state in row bands on a second stream and the first
+   spatial operator (ENO-Roe) starts on the bands already copied; with RK3
+   (ENO-Roe, ENO-LF) the last spatial operator runs in row bands whose
+   results are copied back while the next bands run (copied again after an
+   RK3 retry).  0: one copy in, the step, one copy out.  Bit-identical
+   either way. */
 int mhd_set_step_host_banded( mhd_ctx* ctx, int enable );
 
 /* enable 1 (the default): the sweep loop of an SOR solve runs as one CUDA

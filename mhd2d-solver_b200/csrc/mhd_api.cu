@@ -321,6 +321,67 @@ void enqueue_rk3_tail(mhd_ctx* c, bool chars) {
   enqueue_control(c, PH_DONE);
 }
 
+// The RK3 stages after the first operator for a step whose result goes to
+// host memory (mhd_step_host): the first two stage updates and L(U1) as in
+// enqueue_rk3_tail, then L(U2) in kStepHostBands bands of flux tile rows.
+// After each band, its rows' last stage update goes to U1
+// (combine_final_rows: the values the in-place update gives U, with U's
+// ghost cells beside them) and copy_stream copies those rows to Uh while the
+// next bands are computed.  The last stage's retry decision needs every
+// band's wave-speed maxima, so it follows the last band: do_step keeps the
+// copied rows only when no retry and no error followed (and then copies U1
+// to U on the device), otherwise it waits for the copies, runs the step as
+// enqueue_rk3_tail would and the caller copies U again.  The tiles, stage
+// updates and maxima are the same kernels on the same inputs: bit-identical.
+int enqueue_rk3_tail_to_host(mhd_ctx* c, bool chars, double* Uh) {
+  MHD_TRACE("RK3 tail to host");
+  const Grid& g = c->g;
+  if (!c->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : c->band_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  enqueue_combine(c, 1);
+  enqueue_integrate(c, c->U1, false);
+  enqueue_control(c, PH_RK_SECOND);
+  enqueue_combine(c, 2);
+  MHD_TRACE("L(U2) in bands");
+  c->ks->bc(g, c->U2, c->snap, c->ctl, c->stream);
+  if (c->scheme == 3) c->ks->lf_alpha(g, c->U2, c->aF, c->aG, c->ctl, c->stream);
+  c->launches += c->scheme == 3 ? 2 : 1;
+  const int tr = c->ks->flux_tile_rows(c->scheme);
+  const int nti = (g.nx + tr - 1) / tr;
+  double* const* ch = chars ? c->ch : nullptr;
+  for (int b = 0; b < kStepHostBands; b++) {
+    const int t0 = int((long long)b * nti / kStepHostBands);
+    const int t1 = int((long long)(b + 1) * nti / kStepHostBands);
+    // tile row t updates cell rows [2 + t*tr, 2 + (t+1)*tr); the first band
+    // also takes ghost rows 0, 1 and the last one the rows from its tiles to NX
+    const int r0 = b == 0 ? 0 : 2 + t0 * tr;
+    const int r1 = b == kStepHostBands - 1 ? g.NX : 2 + t1 * tr;
+    if (t1 > t0) {
+      c->ks->flux_rows(c->scheme, g, c->U2, c->UL, c->aF, c->aG, c->ctl, ch, t0, t1, c->stream);
+      c->launches += 1;
+    }
+    c->ks->combine_final_rows(g, r0, r1, c->U, c->U1, c->U2, c->UL, c->ctl, c->stream);
+    c->launches += 1;
+    cudaError_t e = cudaEventRecord(c->band_ev[1 + b], c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_stream, c->band_ev[1 + b], 0);
+    for (int k = 0; k < NF && e == cudaSuccess && r1 > r0; k++)
+      e = cudaMemcpy2DAsync(Uh + ((long long)k * g.NX + r0) * g.NY, g.NY * sizeof(double),
+                            c->U1 + k * g.fstride + (long long)r0 * g.pitch + g.off,
+                            g.pitch * sizeof(double), g.NY * sizeof(double), size_t(r1 - r0),
+                            cudaMemcpyDeviceToHost, c->copy_stream);
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(c->copy_stream);  // no copy into Uh outlives the call
+      return cuda_fail(c, e, "mhd_step_host: banded copy back");
+    }
+  }
+  c->chars_buf = 2;
+  enqueue_control(c, PH_RK_FINAL);
+  enqueue_control(c, PH_DONE);
+  return MHD_OK;
+}
+
 // Fatal statuses of the central-FD integration, with the reference's
 // message (spatialmethodcentralfd2.cpp:71-77, 151-156) and a caller suffix.
 int cfd_status(mhd_ctx* c, const char* where) {
@@ -358,11 +419,14 @@ int step_status(mhd_ctx* c) {
   return MHD_OK;
 }
 
-// One full time step on the device state; dt in/out.
-// One time step.  Uh (optional): the state comes from host memory, copied
-// in row bands that the first spatial operator follows
-// (enqueue_integrate_from_host).
-int do_step(mhd_ctx* c, double* dt_inout, const double* Uh = nullptr) {
+// One time step on the device state; dt in/out.  Uh (optional): the state
+// comes from host memory, copied in row bands that the first spatial
+// operator follows (enqueue_integrate_from_host).  Uo (optional, RK3): the
+// result goes to host memory in row bands that follow the last spatial
+// operator (enqueue_rk3_tail_to_host); *copied tells whether Uo got it.
+int do_step(mhd_ctx* c, double* dt_inout, const double* Uh = nullptr, double* Uo = nullptr,
+            bool* copied = nullptr) {
+  if (copied) *copied = false;
   MHD_TRACE("step");
   int st = check_bc_ready(c);
   if (st) return st;
@@ -380,8 +444,25 @@ int do_step(mhd_ctx* c, double* dt_inout, const double* Uh = nullptr) {
     if ((st = read_ctl(c))) return st;
   } else {
     enqueue_control(c, PH_RK_FIRST);
-    enqueue_rk3_tail(c, chars);
-    if ((st = read_ctl(c))) return st;
+    if (Uo) {
+      if ((st = enqueue_rk3_tail_to_host(c, chars, Uo))) return st;
+      st = read_ctl(c);
+      const bool keep = !st && !c->hctl->retry && !c->hctl->error;
+      cudaError_t e = cudaSuccess;
+      // the step's result, now in U1, becomes the device state (overlapping
+      // the copies still in flight, which read U1)
+      if (keep)
+        e = cudaMemcpyAsync(c->U, c->U1, size_t(NF) * c->g.fstride * sizeof(double),
+                            cudaMemcpyDeviceToDevice, c->stream);
+      const cudaError_t e2 = cudaStreamSynchronize(c->copy_stream);
+      if (st) return st;
+      if (e == cudaSuccess) e = e2;
+      if (e != cudaSuccess) return cuda_fail(c, e, "mhd_step_host: copy back");
+      if (copied) *copied = keep;
+    } else {
+      enqueue_rk3_tail(c, chars);
+      if ((st = read_ctl(c))) return st;
+    }
     // Like TimeIntegrationRK3::step (timeintegrationrk3.cpp:81-148) the
     // retries have no cap: each one restarts from min(dt1, dt2, dt3), which
     // is strictly below the dt it replaces, so the ladder runs out in
@@ -964,13 +1045,18 @@ int mhd_step_host(mhd_ctx* c, double* U, double* dt_inout) {
   // ENO-Roe on grids of many tile rows: the copy of the state overlaps the
   // first spatial operator (bit-identical; see enqueue_integrate_from_host)
   const int tr = c->ks->flux_tile_rows(c->scheme);
-  if (c->scheme == 2 && c->use_banded_h2d && c->g.nx >= 4 * kStepHostBands * tr) {
-    st = do_step(c, dt_inout, U);
+  const bool bands = c->use_banded_h2d && c->g.nx >= 4 * kStepHostBands * tr;
+  // RK3 with an ENO scheme: the copy back follows the last spatial
+  // operator's row bands (see enqueue_rk3_tail_to_host)
+  double* Uo = bands && c->time_method != 1 && (c->scheme == 2 || c->scheme == 3) ? U : nullptr;
+  bool copied = false;
+  if (c->scheme == 2 && bands) {
+    st = do_step(c, dt_inout, U, Uo, &copied);
   } else {
     CK(h2d(c, c->U, U));
-    st = do_step(c, dt_inout);
+    st = do_step(c, dt_inout, nullptr, Uo, &copied);
   }
-  CK(d2h(c, U, c->U));
+  if (!copied) CK(d2h(c, U, c->U));
   CK(cudaStreamSynchronize(c->stream));
   return st;
 }

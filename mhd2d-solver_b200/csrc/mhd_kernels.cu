@@ -154,6 +154,13 @@ void l_combine(const Grid& g, int mode, double* U, double* U1, double* U2, const
   k_combine<<<grid, 256, 0, s>>>(g, mode, U, U1, U2, UL, ctl);
 }
 
+void l_combine_final_rows(const Grid& g, int i0, int i1, double* U, double* U1, double* U2,
+                          const double* UL, const Ctl* ctl, cudaStream_t s) {
+  if (i1 <= i0) return;
+  dim3 grid((g.NY + 255) / 256, i1 - i0, NF);
+  k_combine_final_rows<<<grid, 256, 0, s>>>(g, i0, i1, U, U1, U2, UL, ctl);
+}
+
 void l_control(Ctl* ctl, double dx, double dy, double dt_min, double dt_max, double cfl,
                int phase, double arg, cudaStream_t s) {
   StepParams p{dx, dy, dt_min, dt_max, cfl};
@@ -240,6 +247,7 @@ using namespace MHD_KNS;
 extern const KernelSet MHD_KSET = {MHD_KSET_NAME, l_bc, l_snapshot, l_lf_alpha, l_flux,
                                    l_combine, l_control, l_divb, l_sor_rhs, l_sor_sweep,
                                    l_phi_bc, l_sor_correct, l_totals, l_smem, l_launches,
-                                   l_bc_part, l_flux_rows, l_flux_tile_rows};
+                                   l_bc_part, l_flux_rows, l_flux_tile_rows,
+                                   l_combine_final_rows};
 
 }  // namespace mhd

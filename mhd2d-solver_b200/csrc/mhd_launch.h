@@ -66,6 +66,10 @@ struct KernelSet {
                     const double* aG, Ctl* ctl, double* const chars[4], int ti0, int ti1,
                     cudaStream_t s);
   int (*flux_tile_rows)(int scheme);
+  // the last RK3 stage update of rows [i0, i1) (0 <= i0, i1 <= NX) into U1,
+  // U's ghost cells copied beside it (mhd_step_host's copy-back overlap)
+  void (*combine_final_rows)(const Grid& g, int i0, int i1, double* U, double* U1, double* U2,
+                             const double* UL, const Ctl* ctl, cudaStream_t s);
 };
 
 extern const KernelSet kExact;

@@ -177,6 +177,7 @@ __device__ __forceinline__ void combine_at(int mode, double dt, long long a,
     case 0: U[a] = U[a] + dt * UL[a]; break;
     case 1: U1[a] = U[a] + dt * UL[a]; break;
     case 2: U2[a] = (3.0 / 4.0) * U[a] + (1.0 / 4.0) * U1[a] + (1.0 / 4.0) * dt * UL[a]; break;
+    case 4: U1[a] = (1.0 / 3.0) * U[a] + (2.0 / 3.0) * U2[a] + (2.0 / 3.0) * dt * UL[a]; break;
     default: U[a] = (1.0 / 3.0) * U[a] + (2.0 / 3.0) * U2[a] + (2.0 / 3.0) * dt * UL[a]; break;
   }
 }
@@ -190,6 +191,25 @@ __global__ void k_combine(Grid g, int mode, double* __restrict__ U, double* __re
   const int k = blockIdx.z;
   if (j >= g.ny + 2) return;
   combine_at(mode, dt, g.at(k, i, j), U, U1, U2, UL);
+}
+
+// The last RK3 stage update of rows [i0, i1) (ghost rows included) written
+// to U1 instead of U: the interior gets the same update as mode 3 (mode 4 of
+// combine_at), the ghost cells a copy of U's.  The rows of U1 then hold what
+// U holds after the in-place update, while U keeps the step's start state
+// for a retry.
+__global__ void k_combine_final_rows(Grid g, int i0, int i1, double* __restrict__ U,
+                                     double* __restrict__ U1, double* __restrict__ U2,
+                                     const double* __restrict__ UL, const Ctl* ctl) {
+  if (ctl->skip) return;
+  const double dt = ctl->dt;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = i0 + blockIdx.y;
+  const int k = blockIdx.z;
+  if (j >= g.NY || i >= i1) return;
+  const long long a = g.at(k, i, j);
+  if (i >= 2 && i < g.nx + 2 && j >= 2 && j < g.ny + 2) combine_at(4, dt, a, U, U1, U2, UL);
+  else U1[a] = U[a];
 }
 
 // ---------------------------------------------------------------------------
@@ -441,6 +461,7 @@ constexpr int SOR_THREADS = 128;
 // Same-colour column pairs per row: thread q of a row owns columns
 // jb = 2*(2q + b), jb + 1 with b = (colour + (i>>1)) & 1.
 __host__ __device__ __forceinline__ int sor_pairs(const DivRange& R) { return (R.y1 + 3) / 4 + 1; }
+
 
 // The divergence source terms of the SOR update are fixed during a solve:
 // X = bxf*(Bx[i+1][j] - Bx[i-1][j]), Y = byf*(By[i][j+1] - By[i][j-1]), the
