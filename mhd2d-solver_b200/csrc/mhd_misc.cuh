@@ -527,12 +527,28 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
   const long long P = g.pitch;
   double rmax = 0.0, pmax = 0.0;
   if (q < Q) {
-    for (int rr = 0; rr < rpb; rr++) {
+    // The block's rows are walked two apart (offsets 0, 2, 4, ..., then 1,
+    // 3, 5, ...).  Row i + 2's pair sits two columns from row i's, so the
+    // pair row i reads above it is the one row i + 2 reads at its left or
+    // right, and the one row i reads at its right or left is the one row
+    // i + 2 reads below it.  All four are points of the other colour, which a
+    // half sweep does not change: a load whose address equals one of the
+    // previous row's takes that value.  Every point reads the same values.
+    const double* c_up = nullptr;
+    const double* c_lf = nullptr;
+    const double* c_rt = nullptr;
+    double2 v_up = make_double2(0.0, 0.0), v_lf = v_up, v_rt = v_up;
+    const int half = (rpb + 1) / 2;
+    for (int k = 0; k < rpb; k++) {
+      const int rr = k < half ? 2 * k : 2 * (k - half) + 1;
+      if (k == half) c_up = c_lf = c_rt = nullptr;  // the second chain starts
       const int ir = blockIdx.y * rpb + rr;
       const int i = R.x0 + ir;
-      if (i >= R.x1) break;
       const int jb = 2 * (2 * q + ((color + (i >> 1)) & 1));
-      if (jb + 1 < R.y0 || jb >= R.y1) continue;
+      if (i >= R.x1 || jb + 1 < R.y0 || jb >= R.y1) {
+        c_up = c_lf = c_rt = nullptr;
+        continue;
+      }
       double* prow = phi + (long long)i * P + g.off;
       const double4 f = xy[((long long)color * H + ir) * Q + q];
       const double* urow = prow + 2 * P;
@@ -544,11 +560,19 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
         if (g.bc[BOTTOM] == PERIODIC && jl < 2) jl += g.ny;
         if (g.bc[TOP] == PERIODIC && jr >= g.ny + 2) jr -= g.ny;
       }
-      const double2 up = *reinterpret_cast<const double2*>(urow + jb);
-      const double2 dn = *reinterpret_cast<const double2*>(drow + jb);
-      const double2 lf = *reinterpret_cast<const double2*>(prow + jl);
-      const double2 rt = *reinterpret_cast<const double2*>(prow + jr);
+      const double* pu = urow + jb;
+      const double* pd = drow + jb;
+      const double* pl = prow + jl;
+      const double* pr = prow + jr;
+      const double2 up = *reinterpret_cast<const double2*>(pu);
+      const double2 dn = pd == c_lf ? v_lf
+                         : (pd == c_rt ? v_rt : *reinterpret_cast<const double2*>(pd));
+      const double2 lf = pl == c_up ? v_up : *reinterpret_cast<const double2*>(pl);
+      const double2 rt = pr == c_up ? v_up : *reinterpret_cast<const double2*>(pr);
       double2 me = *reinterpret_cast<const double2*>(prow + jb);
+      c_up = pu; v_up = up;
+      c_lf = pl; v_lf = lf;
+      c_rt = pr; v_rt = rt;
       const double ax[2] = {up.x, up.y}, bx[2] = {dn.x, dn.y};
       const double ay[2] = {rt.x, rt.y}, by[2] = {lf.x, lf.y};
       const double X[2] = {f.x, f.y}, Y[2] = {f.z, f.w};
