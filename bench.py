@@ -70,6 +70,9 @@ def parse():
                     help="config 2's div-B cleaning at 512^2: steps timed (0: off)")
     ap.add_argument("--cleaning-full", type=int, default=1,
                     help="also one step with cleaning at the headline size (to the sweep cap)")
+    ap.add_argument("--sor-graph", type=int, default=1,
+                    help="0: the timed SOR sweeps are issued from the host instead of one graph "
+                         "launch (same sweeps; lets a profiler see each sweep kernel)")
     ap.add_argument("--adjoint-steps", type=int, default=2000,
                     help="steps of the plasma-sheet adjoint measurement (0: skip it)")
     ap.add_argument("--adjoint-grid", default="1024x512")
@@ -845,6 +848,7 @@ def run_ours(args):
     # sweeps on the evolved 4096^2 state (the convergence test never fires:
     # rmax 0), timed with CUDA events on the library stream.
     sor_sweeps = 200
+    ctx.set_sor_graph(bool(args.sor_graph))
     ctx.divb_sor(M.sor_params(1, 1, 2, 0.0, 0.0, True, 1.7))  # warm-up (first-call allocation)
     torch.cuda.synchronize()
     s0 = torch.cuda.Event(enable_timing=True)
