@@ -259,6 +259,13 @@ int mhd_set_tile_tma( int enable, long long* tma_launches );
    tests in a launch of its own (five launches).  Results are identical. */
 int mhd_set_sor_fused( mhd_ctx* ctx, int enable );
 
+/* How a thread of an SOR half sweep (div_b_fix.cpp:262-280, red-black)
+   walks its rows: 0 (the default) by grid size; 1 one row at a time,
+   reusing the loads its previous row made (faster on grids below ~2 M
+   cells); 2 two rows' loads in flight at a time (faster above).  A half
+   sweep's rows are independent, so the results are identical. */
+int mhd_set_sor_rows( mhd_ctx* ctx, int mode );
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record
    events or order their own work against the context's kernels. */
 int mhd_stream( const mhd_ctx* ctx, void** stream );

@@ -111,6 +111,7 @@ struct mhd_ctx {
   double *phi = nullptr, *partial = nullptr, *ratio = nullptr;
   double* sor_xy = nullptr;  // source terms of the current SOR solve (allocated on first use)
   int sor_fused = 1;         // fused SOR sweeps where the grid allows them (mhd_set_sor_fused)
+  int sor_rows = 0;          // rows per SOR thread step (mhd_set_sor_rows; 0: by grid size)
   int npartial = 0;
   Ctl* ctl = nullptr;
   Ctl* hctl = nullptr;  // pinned mirror
@@ -135,7 +136,7 @@ struct mhd_ctx {
   // kSorChunk sweeps); rebuilt when the solve parameters it bakes in change
   int use_sor_graph = 1;
   cudaGraphExec_t sor_graph = nullptr;
-  double sor_graph_key[4] = {0.0, 0.0, 0.0, 0.0};  // rmax, sweep cap, omega, fused
+  double sor_graph_key[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // rmax, sweep cap, omega, fused, rows
   long long* sor_cnt = nullptr;  // device: passes the SOR graph ran
   long long sor_graph_launches = 0;  // kernels per pass
   // mhd_step_host: the host state is copied in row bands on copy_stream
@@ -651,7 +652,7 @@ int do_divb_calc(mhd_ctx* c, double* mx, double* tot) {
 // sweeps, their order and their values are the same.
 int sor_graph_solve(mhd_ctx* c, const int r[4], const double coef[6], double rmax,
                     double max_sweeps, int fused) {
-  const double key[4] = {rmax, max_sweeps, coef[5], double(fused)};
+  const double key[5] = {rmax, max_sweeps, coef[5], double(fused), double(c->sor_rows)};
   if (c->sor_graph && std::memcmp(key, c->sor_graph_key, sizeof key) != 0) {
     cudaGraphExecDestroy(c->sor_graph);
     c->sor_graph = nullptr;
@@ -682,7 +683,7 @@ int sor_graph_solve(mhd_ctx* c, const int r[4], const double coef[6], double rma
     if (e == cudaSuccess) {
       for (int s = 0; s < kSorChunk; s++)
         c->ks->sor_sweep(c->g, c->phi, c->sor_xy, r, coef, rmax, max_sweeps, c->ratio, c->ctl,
-                         fused, c->stream);
+                         fused, c->sor_rows, c->stream);
       k_sor_again<<<1, 32, 0, c->stream>>>(c->ctl, c->sor_cnt, bound, h);
       cudaGraph_t out = nullptr;
       const cudaError_t e2 = cudaStreamEndCapture(c->stream, &out);
@@ -753,7 +754,7 @@ int do_sor(mhd_ctx* c, const mhd_sor_params* p, int* sweeps) {
       for (;;) {
         for (int s = 0; s < chunk; s++) {
           c->ks->sor_sweep(g, c->phi, c->sor_xy, r, coef, p->sor_rmax, p->sor_rsteps, c->ratio,
-                           c->ctl, fused, c->stream);
+                           c->ctl, fused, c->sor_rows, c->stream);
           c->launches += fused ? 2 : 5;
         }
         issued += chunk;
@@ -1310,6 +1311,12 @@ int mhd_set_tile_tma(int enable, long long* tma_launches) {
   if (enable != 0 && enable != 1 && enable != -1) return MHD_ERR_WRONG_PARAMETER;
   if (enable >= 0) tile_tma_flag() = enable != 0;
   if (tma_launches) *tma_launches = tile_tma_launches();
+  return MHD_OK;
+}
+
+int mhd_set_sor_rows(mhd_ctx* c, int mode) {
+  if (!c || mode < 0 || mode > 2) return MHD_ERR_WRONG_PARAMETER;
+  c->sor_rows = mode;
   return MHD_OK;
 }
 

@@ -43,10 +43,11 @@ struct KernelSet {
   // fused = 1: two launches that read periodic ghosts at their source and
   // run the convergence check in the second one (sor_fused_ok must hold;
   // the caller refreshes the ghosts with phi_bc before the first and after
-  // the last sweep of the solve)
+  // the last sweep of the solve).  rows_mode: 0 by grid size, 1 one row at a
+  // time with reused loads, 2 two rows in flight per thread (same values)
   void (*sor_sweep)(const Grid& g, double* phi, const double* xy, const int range[4],
                     const double coef[6], double rtol, double max_sweeps, double* last_ratio,
-                    Ctl* ctl, int fused, cudaStream_t s);
+                    Ctl* ctl, int fused, int rows_mode, cudaStream_t s);
   // potential ghosts (div_b_fix.cpp:282-364), regardless of the stop flag
   void (*phi_bc)(const Grid& g, double* phi, const Ctl* ctl, cudaStream_t s);
   void (*sor_correct)(const Grid& g, double* U, const double* phi, const int range[4],

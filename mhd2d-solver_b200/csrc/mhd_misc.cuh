@@ -510,11 +510,106 @@ __device__ __forceinline__ void sor_check(Ctl* c, double rtol, double max_sweeps
   if (ratio <= rtol || c->sor_sweeps >= max_sweeps) c->sor_done = 1;
 }
 
+// One row of a half sweep in registers (k_sor_half): the thread's pair of
+// the row, its four neighbour pairs and its source terms.
+struct SorRow {
+  double2 up, dn, lf, rt, me;
+  double4 f;
+  double* pme;
+  int jb;
+  bool ok;
+};
+
+// The previous row of a chain (k_sor_half): addresses and values of its
+// other-colour loads.
+struct SorChain {
+  const double* up = nullptr;
+  const double* lf = nullptr;
+  const double* rt = nullptr;
+  double2 vup, vlf, vrt;
+};
+
+// Loads row offset ir of a half sweep (when it is in the range and holds
+// points of the thread's pair); REUSE: takes the values the chain's
+// previous row loaded from the same addresses.
+template <bool FUSED, bool REUSE>
+__device__ __forceinline__ void sor_row_load(const Grid& g, const double* __restrict__ phi,
+                                             const double4* __restrict__ xy, const DivRange& R,
+                                             int color, int q, int Q, int H, long long P, int ir,
+                                             SorChain& c, SorRow& o) {
+  const int i = R.x0 + ir;
+  const int jb = 2 * (2 * q + ((color + (i >> 1)) & 1));
+  o.ok = i < R.x1 && !(jb + 1 < R.y0 || jb >= R.y1);
+  if (!o.ok) {
+    c.up = c.lf = c.rt = nullptr;
+    return;
+  }
+  const double* prow = phi + (long long)i * P + g.off;
+  const double* urow = prow + 2 * P;
+  const double* drow = prow - 2 * P;
+  int jl = jb - 2, jr = jb + 2;
+  if (FUSED) {
+    urow = phi + (long long)sor_src_row(g, i + 2) * P + g.off;
+    drow = phi + (long long)sor_src_row(g, i - 2) * P + g.off;
+    if (g.bc[BOTTOM] == PERIODIC && jl < 2) jl += g.ny;
+    if (g.bc[TOP] == PERIODIC && jr >= g.ny + 2) jr -= g.ny;
+  }
+  const double* pu = urow + jb;
+  const double* pd = drow + jb;
+  const double* pl = prow + jl;
+  const double* pr = prow + jr;
+  o.f = xy[((long long)color * H + ir) * Q + q];
+  o.up = *reinterpret_cast<const double2*>(pu);
+  if (REUSE) {
+    o.dn = pd == c.lf ? c.vlf : (pd == c.rt ? c.vrt : *reinterpret_cast<const double2*>(pd));
+    o.lf = pl == c.up ? c.vup : *reinterpret_cast<const double2*>(pl);
+    o.rt = pr == c.up ? c.vup : *reinterpret_cast<const double2*>(pr);
+    c.up = pu; c.vup = o.up;
+    c.lf = pl; c.vlf = o.lf;
+    c.rt = pr; c.vrt = o.rt;
+  } else {
+    o.dn = *reinterpret_cast<const double2*>(pd);
+    o.lf = *reinterpret_cast<const double2*>(pl);
+    o.rt = *reinterpret_cast<const double2*>(pr);
+  }
+  o.me = *reinterpret_cast<const double2*>(prow + jb);
+  o.pme = const_cast<double*>(prow) + jb;
+  o.jb = jb;
+}
+
+// The reference's per-point update (div_b_fix.cpp:262-280) of a loaded row's
+// pair, its maxima, and the store of the pair.
+__device__ __forceinline__ void sor_row_update(const SorCoef& s, const DivRange& R,
+                                               const SorRow& o, double& rmax, double& pmax) {
+  const double ax[2] = {o.up.x, o.up.y}, bx[2] = {o.dn.x, o.dn.y};
+  const double ay[2] = {o.rt.x, o.rt.y}, by[2] = {o.lf.x, o.lf.y};
+  const double X[2] = {o.f.x, o.f.y}, Y[2] = {o.f.z, o.f.w};
+  double out[2] = {o.me.x, o.me.y};
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int j = o.jb + t;
+    if (j >= R.y0 && j < R.y1) {
+      double r = s.pxf * (ax[t] + bx[t]);
+      r += s.pyf * (ay[t] + by[t]);
+      r += X[t];
+      r += Y[t];
+      r *= s.coef;
+      r -= out[t];
+      out[t] += s.omega * r;
+      rmax = take_max(rmax, fabs(r));
+      pmax = take_max(pmax, fabs(out[t]));
+    }
+  }
+  *reinterpret_cast<double2*>(o.pme) = make_double2(out[0], out[1]);
+}
+
 // One colour of a red-black sweep.  The potential pairs are read and written
 // as 16-byte items (jb is even, the padded row offset is even).  FUSED:
 // periodic ghosts are read at their source points, and the last block of the
-// colour-1 launch runs the convergence test.
-template <bool FUSED>
+// colour-1 launch runs the convergence test.  PAIRS: two rows' loads in
+// flight per thread (large grids); otherwise one row at a time, with the
+// loads its chain's previous row made reused (sor_pairs_ok picks).
+template <bool FUSED, bool PAIRS>
 __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __restrict__ phi,
                                                           const double4* __restrict__ xy,
                                                           DivRange R, SorCoef s, int color,
@@ -527,74 +622,42 @@ __global__ void __launch_bounds__(SOR_THREADS) k_sor_half(Grid g, double* __rest
   const long long P = g.pitch;
   double rmax = 0.0, pmax = 0.0;
   if (q < Q) {
-    // The block's rows are walked two apart (offsets 0, 2, 4, ..., then 1,
-    // 3, 5, ...).  Row i + 2's pair sits two columns from row i's, so the
-    // pair row i reads above it is the one row i + 2 reads at its left or
-    // right, and the one row i reads at its right or left is the one row
-    // i + 2 reads below it.  All four are points of the other colour, which a
-    // half sweep does not change: a load whose address equals one of the
-    // previous row's takes that value.  Every point reads the same values.
-    const double* c_up = nullptr;
-    const double* c_lf = nullptr;
-    const double* c_rt = nullptr;
-    double2 v_up = make_double2(0.0, 0.0), v_lf = v_up, v_rt = v_up;
+    // The block's rows form two chains, offsets 0, 2, 4, ... and 1, 3, 5, ...
+    // Rows are independent within a half sweep: a row writes only its own
+    // pair, and its neighbour pairs are points of the other colour, which the
+    // half sweep does not change.  So any order reads the same values.
     const int half = (rpb + 1) / 2;
-    for (int k = 0; k < rpb; k++) {
-      const int rr = k < half ? 2 * k : 2 * (k - half) + 1;
-      if (k == half) c_up = c_lf = c_rt = nullptr;  // the second chain starts
-      const int ir = blockIdx.y * rpb + rr;
-      const int i = R.x0 + ir;
-      const int jb = 2 * (2 * q + ((color + (i >> 1)) & 1));
-      if (i >= R.x1 || jb + 1 < R.y0 || jb >= R.y1) {
-        c_up = c_lf = c_rt = nullptr;
-        continue;
+    if (PAIRS) {
+      // one row of each chain per iteration, both rows' loads issued before
+      // either row is updated: twice as many loads in flight
+      SorChain none;
+      for (int k = 0; k < half; k++) {
+        SorRow a, b;
+        sor_row_load<FUSED, false>(g, phi, xy, R, color, q, Q, H, P, blockIdx.y * rpb + 2 * k,
+                                   none, a);
+        if (2 * k + 1 < rpb)
+          sor_row_load<FUSED, false>(g, phi, xy, R, color, q, Q, H, P,
+                                     blockIdx.y * rpb + 2 * k + 1, none, b);
+        else
+          b.ok = false;
+        if (a.ok) sor_row_update(s, R, a, rmax, pmax);
+        if (b.ok) sor_row_update(s, R, b, rmax, pmax);
       }
-      double* prow = phi + (long long)i * P + g.off;
-      const double4 f = xy[((long long)color * H + ir) * Q + q];
-      const double* urow = prow + 2 * P;
-      const double* drow = prow - 2 * P;
-      int jl = jb - 2, jr = jb + 2;
-      if (FUSED) {
-        urow = phi + (long long)sor_src_row(g, i + 2) * P + g.off;
-        drow = phi + (long long)sor_src_row(g, i - 2) * P + g.off;
-        if (g.bc[BOTTOM] == PERIODIC && jl < 2) jl += g.ny;
-        if (g.bc[TOP] == PERIODIC && jr >= g.ny + 2) jr -= g.ny;
+    } else {
+      // one chain after the other.  Row i + 2's pair sits two columns from
+      // row i's: the pair row i reads above it is the one row i + 2 reads at
+      // its left or right, and the one row i reads at its right or left is
+      // the one row i + 2 reads below it.  A load whose address equals one
+      // of the chain's previous row's takes that value (3 loads of the
+      // potential per row instead of 5).
+      SorChain c;
+      for (int k = 0; k < rpb; k++) {
+        const int rr = k < half ? 2 * k : 2 * (k - half) + 1;
+        if (k == half) c = SorChain();  // the second chain starts
+        SorRow a;
+        sor_row_load<FUSED, true>(g, phi, xy, R, color, q, Q, H, P, blockIdx.y * rpb + rr, c, a);
+        if (a.ok) sor_row_update(s, R, a, rmax, pmax);
       }
-      const double* pu = urow + jb;
-      const double* pd = drow + jb;
-      const double* pl = prow + jl;
-      const double* pr = prow + jr;
-      const double2 up = *reinterpret_cast<const double2*>(pu);
-      const double2 dn = pd == c_lf ? v_lf
-                         : (pd == c_rt ? v_rt : *reinterpret_cast<const double2*>(pd));
-      const double2 lf = pl == c_up ? v_up : *reinterpret_cast<const double2*>(pl);
-      const double2 rt = pr == c_up ? v_up : *reinterpret_cast<const double2*>(pr);
-      double2 me = *reinterpret_cast<const double2*>(prow + jb);
-      c_up = pu; v_up = up;
-      c_lf = pl; v_lf = lf;
-      c_rt = pr; v_rt = rt;
-      const double ax[2] = {up.x, up.y}, bx[2] = {dn.x, dn.y};
-      const double ay[2] = {rt.x, rt.y}, by[2] = {lf.x, lf.y};
-      const double X[2] = {f.x, f.y}, Y[2] = {f.z, f.w};
-      double out[2] = {me.x, me.y};
-#pragma unroll
-      for (int t = 0; t < 2; t++) {
-        const int j = jb + t;
-        if (j >= R.y0 && j < R.y1) {
-          double r = s.pxf * (ax[t] + bx[t]);
-          r += s.pyf * (ay[t] + by[t]);
-          r += X[t];
-          r += Y[t];
-          r *= s.coef;
-          r -= out[t];
-          out[t] += s.omega * r;
-          rmax = take_max(rmax, fabs(r));
-          pmax = take_max(pmax, fabs(out[t]));
-        }
-      }
-      me.x = out[0];
-      me.y = out[1];
-      *reinterpret_cast<double2*>(prow + jb) = me;
     }
   }
   rmax = warp_max(rmax);

@@ -163,6 +163,7 @@ def library():
                           C.POINTER(C.c_size_t)],
         "mhd_set_tile_tma": [C.c_int, C.POINTER(C.c_longlong)],
         "mhd_set_sor_fused": [vp, C.c_int],
+        "mhd_set_sor_rows": [vp, C.c_int],
         "mhd_set_sor_graph": [vp, C.c_int],
         "mhd_set_step_host_banded": [vp, C.c_int],
         "mhd_run": [vp, C.POINTER(RunParams), C.POINTER(NongridRecord), C.c_int,
@@ -417,6 +418,10 @@ class Context:
     def set_sor_fused(self, enable):
         """Two-launch SOR sweeps where the grid allows them (default on)."""
         self._check(self.lib.mhd_set_sor_fused(self.h, int(bool(enable))), "set_sor_fused")
+
+    def set_sor_rows(self, mode):
+        """SOR rows per thread step: 0 by grid size, 1 one row (reused loads), 2 two rows."""
+        self._check(self.lib.mhd_set_sor_rows(self.h, int(mode)), "set_sor_rows")
 
     def stream(self):
         """The context's cudaStream_t as an integer handle."""

@@ -225,6 +225,51 @@ def test_sor_fused_sweeps_match_unfused_and_oracle(shape, bc, fusable):
     assert (launches[0] < launches[1]) == fusable
 
 
+@pytest.mark.parametrize("shape,bc", [
+    ((40, 36), (1, 1, 1, 1)), ((44, 40), (1, 3, 4, 1)), ((48, 40), (3, 1, 2, 2)),
+    ((41, 37), (4, 4, 4, 4)), ((42, 36), (1, 1, 1, 1)), ((48, 38), (4, 1, 3, 1))])
+def test_sor_row_walks_match_oracle(shape, bc):
+    """A half sweep's thread walks its rows one at a time reusing its previous
+    row's loads (mode 1) or with two rows' loads in flight (mode 2): both give
+    the oracle's red-black solve bit for bit (status, sweeps, corrected field)
+    over two warm-started solves, in the two- and five-launch sweeps."""
+    p = P.random_smooth(*shape, seed=5 * shape[0] + sum(bc), bc=bc)
+    sp = M.sor_params(1, 5, 20000, 1e-10, 1e-10, True, 1.7)
+    osp = SorParams(1, 5, 20000.0, 1e-10, 1e-10, 1, 1.7)
+    o = Oracle(p.nx, p.ny, p.dx, p.dy, p.gamma, bc)
+    Uo = p.U.copy()
+    ctxs = [make_ctx(p, flags=0) for _ in range(2)]
+    ctxs[0].set_sor_rows(1)
+    ctxs[1].set_sor_rows(2)
+    for _ in range(2):
+        so, eo, swo = o.divb_sor(Uo, osp, red_black=1)
+        for ctx in ctxs:
+            st, sweeps = ctx.divb_sor(sp)
+            assert (st.status, int(st.isError), sweeps) == (so, eo, swo)
+            assert same(ctx.download(), Uo)
+    for ctx in ctxs:
+        ctx.close()
+
+
+@pytest.mark.parametrize("shape,bc", [((1600, 1400), (1, 1, 1, 1)), ((1430, 1466), (4, 1, 3, 2))])
+def test_sor_row_walks_agree_on_large_grids(shape, bc):
+    """Grids above the size where the default switches to two rows in flight:
+    the default, mode 1 and mode 2 give the same status, sweep count and
+    corrected field (bit for bit) over two warm-started solves of 300 sweeps."""
+    p = P.random_smooth(*shape, seed=shape[1], bc=bc)
+    sp = M.sor_params(1, 5, 300, 1e-10, 1e-10, True, 1.7)
+    out = []
+    for mode in (0, 1, 2):
+        ctx = make_ctx(p, flags=0)
+        ctx.set_sor_rows(mode)
+        res = [ctx.divb_sor(sp) for _ in range(2)]
+        out.append(([(r[0].status, int(r[0].isError), r[1]) for r in res], ctx.download()))
+        ctx.close()
+    for r, U in out[1:]:
+        assert r == out[0][0]
+        assert same(U, out[0][1])
+
+
 @pytest.mark.parametrize("shape,bc", [((200, 136), (1, 1, 1, 1)), ((150, 97), (3, 4, 2, 3)),
                                       ((64, 256), (4, 4, 1, 1))])
 @pytest.mark.parametrize("rsteps", [7, 16, 33, 20000])
